@@ -1,0 +1,130 @@
+/*
+ * sadmrg.h -- C ABI of the B200 two-site DMRG hot path.
+ *
+ * Plain C: pointers, sizes and ints; no C++ or torch types.  Every function
+ * returns 0 on success or a positive status (SADMRG_ERR_*) and never exits the
+ * process.  sadmrg_last_error() gives the message of the last failure.
+ *
+ * One handle = one CUDA device + one stream; calls on a handle are stream
+ * ordered and must come from one host thread at a time.
+ *
+ * Scalars: real data is double; complex data is interleaved (re, im) double,
+ * the layout of std::complex<double>.  Dense blocks are column-major with
+ * bond 0 fastest, exactly as the reference's Dense<Scalar>.
+ *
+ * Reference interfaces replaced (lingwangqs/symmetry-adapted-DMRG-library):
+ *   sadmrg_heff_*         DMRG::hamiltonian_vector_multiplication_idmrg   src/dmrg_inst.cpp:283-371
+ *                         BlockTensor::hamiltonian_vector_multiplication   src/block_tensor_inst.cpp:2170-2318
+ *   sadmrg_heff_lanczos   Lanczos::initialize_lanczos + lanczos1         src/dmrg_inst.cpp:1201-1348
+ *   sadmrg_chain_env_update
+ *                         DMRG::prepare_site_operator_from_left/right      src/dmrg_inst.cpp:440-695
+ *                         (BlockTensor::operator_initial / operator_transformation / operator_pairup /
+ *                          overlap_transformation, src/block_tensor_inst.cpp:1283-2167)
+ *   sadmrg_svd_truncate   BlockTensor::svd                                 src/block_tensor_inst.cpp:501-637
+ *   sadmrg_chain_*        DMRG<Scalar,Sym>::DMRG / do_idmrg / prepare_sweep / sweep / get_enr
+ *                                                                           dmrg.hpp:98-131, src/dmrg_inst.cpp:63-943
+ */
+#ifndef SADMRG_H
+#define SADMRG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sadmrg_handle sadmrg_handle;
+
+enum {
+  SADMRG_OK = 0,
+  SADMRG_ERR_ARG = 1,
+  SADMRG_ERR_CUDA = 2,
+  SADMRG_ERR_NOMEM = 3,
+  SADMRG_ERR_STATE = 4,
+  SADMRG_ERR_NUMERIC = 5,
+  SADMRG_ERR_LIMIT = 6,
+  SADMRG_ERR_DEVICE_FLAG = 7
+};
+
+enum { SADMRG_SYM_U1 = 0, SADMRG_SYM_SU2 = 1 };
+enum { SADMRG_PREC_FP64 = 0, SADMRG_PREC_TF32X3 = 1 };
+
+/* A block-sparse tensor (the reference's BlockTensor): bonds with sector
+ * labels (U1 charge or SU2 2J) and reduced dimensions, the present blocks by
+ * their block index (mixed radix over sector indices, bond 0 fastest), and the
+ * present blocks' data concatenated in ascending block-index order. */
+typedef struct {
+  int nbond;
+  int locspin;
+  const int* dir;              /* [nbond] */
+  const int* nmom;             /* [nbond] sectors per bond */
+  const int* q;                /* [sum nmom] sector labels, bond after bond */
+  const int* d;                /* [sum nmom] sector dimensions */
+  int nblocks;
+  const long long* block_index;/* [nblocks], ascending */
+  const void* data;            /* all present blocks */
+} sadmrg_tensor_desc;
+
+int sadmrg_version(void);
+int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out);
+int sadmrg_destroy(sadmrg_handle* h);
+const char* sadmrg_last_error(const sadmrg_handle* h);
+
+/* ---- frozen two-site problem: H_eff * psi ---------------------------------
+ * ops[] holds every block operator once; term i pairs ops[op1[i]] (left block,
+ * legs (a, channel, a')) with ops[op2[i]] (right block, legs (b, channel, b')),
+ * the right operators already summed with their couplings as the reference
+ * does before calling BlockTensor::hamiltonian_vector_multiplication.
+ * hh_left / hh_right may be NULL (null block Hamiltonian).  psi fixes the
+ * block structure of every vector passed to apply / lanczos. */
+int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadmrg_tensor_desc* hh_left,
+                     const sadmrg_tensor_desc* hh_right, int nops, const sadmrg_tensor_desc* ops, int nterms,
+                     const int* op1, const int* op2);
+/* psi elements, algorithmic flops and bytes of one matvec, number of sector products */
+int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks);
+/* out = H_eff psi with host buffers (copies in and out on the handle's stream) */
+int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision);
+/* out = H_eff psi with device pointers (no copies) */
+int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision);
+/* Lanczos ground state (lanczos1) from psi; psi is overwritten by the Ritz vector.
+ * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
+ * FP64 restart from its result. */
+int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energy, int* matvecs);
+
+/* ---- block SVD truncation ---------------------------------------------------
+ * psi: 2-leg two-site vector.  tu / tv: the current site tensors (only their
+ * bonds 0 and 1 are read).  p1 / p2: powers of the singular values absorbed
+ * into U / V.  The new site tensors are staged and read with sadmrg_staged_*
+ * (which = 0 for U, 1 for V). */
+int sadmrg_svd_truncate(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadmrg_tensor_desc* tu,
+                        const sadmrg_tensor_desc* tv, double p1, double p2, int max_dcut, int* kept,
+                        double* discarded_weight);
+
+/* ---- chain driver (DMRG<Scalar,Sym>) ---------------------------------------
+ * lx, ly: lattice as the reference's DMRG(xx, yy, ...) constructor (a chain of
+ * L sites is lx = 1, ly = L); open = 1 drops the periodic wrap; J2 adds
+ * next-nearest-neighbour couplings along the site order. */
+int sadmrg_chain_create(sadmrg_handle* h, int lx, int ly, int bondd, int physpn, int totspin, int open, double J2);
+int sadmrg_chain_set_precision(sadmrg_handle* h, int precision);
+int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy);
+int sadmrg_chain_prepare_sweep(sadmrg_handle* h);
+int sadmrg_chain_sweep(sadmrg_handle* h, double* energy);
+/* sectors of bond 2 of site tensor uu[site]: labels and dimensions */
+int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d);
+/* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded] */
+int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
+/* kind: 0 = uu[site], 1 = hh[site], 2 = opr[site][k] */
+int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t);
+int sadmrg_chain_stage_tensor(sadmrg_handle* h, int kind, int site, int k);
+/* prepare_site_operator_from_left (dir = 0) / from_right (dir = 1);
+ * real_env = 1: with uu[site] itself; 0: in the fused (block x site) basis */
+int sadmrg_chain_env_update(sadmrg_handle* h, int site, int dir, int real_env);
+
+/* ---- staged tensors (results) ----------------------------------------------- */
+int sadmrg_staged_info(sadmrg_handle* h, int which, int* nbond, int* locspin, int* nsectors, int* nblocks,
+                       long long* nelem);
+int sadmrg_staged_read(sadmrg_handle* h, int which, int* dir, int* nmom, int* q, int* d, long long* block_index,
+                       void* data);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SADMRG_H */

@@ -1,0 +1,398 @@
+// capi.cpp -- extern "C" boundary (include/sadmrg.h).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/sadmrg.h"
+#include "dmrg.hpp"
+
+using namespace sadmrg;
+
+template <class S>
+struct State {
+  std::unique_ptr<HeffPlan<S>> heff;
+  std::unique_ptr<Chain<S>> chain;
+  BTensor<S> staged[2];
+  DevBuf io;   // psi in / out for host-buffer calls
+};
+
+struct sadmrg_handle {
+  Ctx ctx;
+  int device = 0;
+  std::string err;
+  State<double> sd;
+  State<dcmplex> sz;
+};
+
+static int fail(sadmrg_handle* h, int code, const std::string& m) {
+  if (h) h->err = m;
+  return code;
+}
+
+template <class F>
+static int guard(sadmrg_handle* h, F&& f) {
+  if (!h) return SADMRG_ERR_ARG;
+  try {
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return fail(h, SADMRG_ERR_CUDA, cudaGetErrorString(e));
+    f();
+    return SADMRG_OK;
+  } catch (const Error& e) {
+    return fail(h, e.code, e.what());
+  } catch (const std::exception& e) {
+    return fail(h, SADMRG_ERR_ARG, e.what());
+  }
+}
+
+template <class S>
+static BTensor<S> from_desc(Ctx& c, const sadmrg_tensor_desc* t) {
+  SADMRG_REQUIRE(t && t->nbond >= 1 && t->nbond <= 4, SADMRG_ERR_ARG, "tensor desc: bad nbond");
+  std::vector<Bond> bonds;
+  int o = 0;
+  for (int b = 0; b < t->nbond; ++b) {
+    std::vector<int> q(t->q + o, t->q + o + t->nmom[b]), d(t->d + o, t->d + o + t->nmom[b]);
+    o += t->nmom[b];
+    Bond bd;
+    bd.dir = t->dir[b];
+    bd.q = q;   // the caller gives the sectors in the reference's (sorted) order
+    bd.d = d;
+    for (size_t k = 1; k < q.size(); ++k)
+      SADMRG_REQUIRE(q[k] > q[k - 1], SADMRG_ERR_ARG, "tensor desc: sector labels must ascend");
+    bonds.push_back(bd);
+  }
+  Struct st(c.sym, t->locspin, bonds);
+  std::vector<char> pres(st.nten(), 0);
+  for (int i = 0; i < t->nblocks; ++i) {
+    const long long bi = t->block_index[i];
+    SADMRG_REQUIRE(bi >= 0 && bi < st.nten(), SADMRG_ERR_ARG, "tensor desc: block index out of range");
+    SADMRG_REQUIRE(i == 0 || bi > t->block_index[i - 1], SADMRG_ERR_ARG, "tensor desc: block indices must ascend");
+    int q[8], d[8];
+    SADMRG_REQUIRE(st.block(bi, q, d), SADMRG_ERR_ARG, "tensor desc: block not allowed by symmetry");
+    pres[bi] = 1;
+  }
+  BTensor<S> r = ops::from_host<S>(c, st, pres, static_cast<const S*>(t->data));
+  // small operators keep a host copy (site operators are read on the host)
+  if (r.nelem <= 64 && t->data) r.host.assign(static_cast<const S*>(t->data), static_cast<const S*>(t->data) + r.nelem);
+  return r;
+}
+
+template <class S>
+static State<S>& st_of(sadmrg_handle* h);
+template <> State<double>& st_of<double>(sadmrg_handle* h) { return h->sd; }
+template <> State<dcmplex>& st_of<dcmplex>(sadmrg_handle* h) { return h->sz; }
+
+template <class F>
+static int dispatch(sadmrg_handle* h, F&& f) {
+  return guard(h, [&]() {
+    if (h->ctx.cplx) f((dcmplex*)nullptr);
+    else f((double*)nullptr);
+  });
+}
+
+extern "C" {
+
+int sadmrg_version(void) { return 10000; }
+
+int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out) {
+  if (!out || (sym != 0 && sym != 1)) return SADMRG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return SADMRG_ERR_CUDA;
+  if (device < 0 || device >= ndev) return SADMRG_ERR_ARG;
+  auto* h = new (std::nothrow) sadmrg_handle();
+  if (!h) return SADMRG_ERR_NOMEM;
+  h->device = device;
+  h->ctx.sym = sym ? Sym::SU2 : Sym::U1;
+  h->ctx.cplx = cplx != 0;
+  const int rc = guard(h, [&]() {
+    SADMRG_CUDA(cudaStreamCreateWithFlags(&h->ctx.stream, cudaStreamNonBlocking));
+    SADMRG_CUDA(cudaMalloc(&h->ctx.d_scalars, 64 * sizeof(double)));
+    SADMRG_CUDA(cudaMalloc(&h->ctx.d_partial, sizeof(double) * 2 * 512 * (size_t)h->ctx.npart));
+    if (h->ctx.sym == Sym::SU2) h->ctx.cgc = std::make_unique<CGCFactors>(1);
+  });
+  if (rc != SADMRG_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SADMRG_OK;
+}
+
+int sadmrg_destroy(sadmrg_handle* h) {
+  if (!h) return SADMRG_OK;
+  cudaSetDevice(h->device);
+  if (h->ctx.stream) cudaStreamSynchronize(h->ctx.stream);
+  h->sd = State<double>();
+  h->sz = State<dcmplex>();
+  if (h->ctx.stream) {
+    cudaStreamSynchronize(h->ctx.stream);
+    cudaStreamDestroy(h->ctx.stream);
+  }
+  delete h;
+  return SADMRG_OK;
+}
+
+const char* sadmrg_last_error(const sadmrg_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadmrg_tensor_desc* hhl,
+                     const sadmrg_tensor_desc* hhr, int nops, const sadmrg_tensor_desc* opsd, int nterms,
+                     const int* op1, const int* op2) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(psi && nops >= 0 && nterms >= 0, SADMRG_ERR_ARG, "heff_plan: bad arguments");
+    BTensor<S> p = from_desc<S>(c, psi);
+    BTensor<S> hl, hr;
+    if (hhl) hl = from_desc<S>(c, hhl);
+    if (hhr) hr = from_desc<S>(c, hhr);
+    std::vector<BTensor<S>> ov(nops);
+    std::vector<const BTensor<S>*> opl(nops);
+    for (int i = 0; i < nops; ++i) { ov[i] = from_desc<S>(c, &opsd[i]); opl[i] = &ov[i]; }
+    std::vector<PairTerm> terms(nterms);
+    for (int i = 0; i < nterms; ++i) {
+      SADMRG_REQUIRE(op1[i] >= 0 && op1[i] < nops && op2[i] >= 0 && op2[i] < nops, SADMRG_ERR_ARG,
+                     "heff_plan: operator index out of range");
+      terms[i].op1 = op1[i];
+      terms[i].op2 = op2[i];
+    }
+    auto& S_ = st_of<S>(h);
+    S_.heff = std::make_unique<HeffPlan<S>>(build_heff<S>(c, p, hhl ? &hl : nullptr, hhr ? &hr : nullptr, opl, terms));
+    S_.io.alloc(sizeof(S) * 2 * std::max<long long>(S_.heff->n, 1), c.stream);
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_info: no plan");
+    if (n) *n = S_.heff->n;
+    if (flops) *flops = (double)S_.heff->flops;
+    if (bytes) *bytes = (double)S_.heff->bytes;
+    if (ntasks) *ntasks = S_.heff->ntasks;
+  });
+}
+
+int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply: no plan");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_apply: precision");
+    const long long n = S_.heff->n;
+    S* din = S_.io.template as<S>();
+    S* dout = din + n;
+    SADMRG_CUDA(cudaMemcpyAsync(din, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
+    S_.heff->apply(c, din, dout, precision);
+    SADMRG_CUDA(cudaMemcpyAsync(out_host, dout, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply_device: no plan");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_apply: precision");
+    S_.heff->apply(h->ctx, static_cast<const S*>(psi_dev), static_cast<S*>(out_dev), precision);
+  });
+}
+
+int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energy, int* matvecs) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_lanczos: no plan");
+    SADMRG_REQUIRE(mlanc >= 2, SADMRG_ERR_ARG, "heff_lanczos: mlanc < 2");
+    const long long n = S_.heff->n;
+    S* dv = S_.io.template as<S>();
+    SADMRG_CUDA(cudaMemcpyAsync(dv, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
+    LanczosStats st = lanczos_solve<S>(c, *S_.heff, dv, mlanc, precision);
+    SADMRG_CUDA(cudaMemcpyAsync(psi_host, dv, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    if (energy) *energy = st.energy;
+    if (matvecs) *matvecs = st.matvecs;
+  });
+}
+
+int sadmrg_svd_truncate(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadmrg_tensor_desc* tu,
+                        const sadmrg_tensor_desc* tv, double p1, double p2, int max_dcut, int* kept,
+                        double* discarded_weight) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(max_dcut > 0, SADMRG_ERR_ARG, "svd_truncate: max_dcut must be positive");
+    BTensor<S> p = from_desc<S>(c, psi), u = from_desc<S>(c, tu), v = from_desc<S>(c, tv);
+    SvdStats s = block_svd<S>(c, p, u, p1, v, p2, max_dcut, nullptr);
+    auto& S_ = st_of<S>(h);
+    S_.staged[0] = std::move(u);
+    S_.staged[1] = std::move(v);
+    if (kept) *kept = s.kept;
+    if (discarded_weight) *discarded_weight = s.discarded_weight;
+  });
+}
+
+int sadmrg_chain_create(sadmrg_handle* h, int lx, int ly, int bondd, int physpn, int totspin, int open, double J2) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    SADMRG_REQUIRE(lx >= 1 && ly >= 1 && bondd >= 1, SADMRG_ERR_ARG, "chain_create: bad size");
+    st_of<S>(h).chain = std::make_unique<Chain<S>>(h->ctx, lx, ly, bondd, physpn, totspin, open, J2);
+  });
+}
+
+int sadmrg_chain_set_precision(sadmrg_handle* h, int precision) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "precision");
+    S_.chain->prec = precision;
+  });
+}
+
+int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    S_.chain->do_idmrg();
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+    if (energy) *energy = S_.chain->energy();
+  });
+}
+
+int sadmrg_chain_prepare_sweep(sadmrg_handle* h) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    S_.chain->prepare_sweep();
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+  });
+}
+
+int sadmrg_chain_sweep(sadmrg_handle* h, double* energy) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    S_.chain->sweep();
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+    if (energy) *energy = S_.chain->energy();
+  });
+}
+
+int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(site >= 0 && site < S_.chain->ns, SADMRG_ERR_ARG, "chain_bond: site");
+    const auto& u = S_.chain->uu[site];
+    if (u.st.nbond() < 3) { *nsec = 0; return; }
+    const Bond& b = u.st.bonds[2];
+    *nsec = b.nmom();
+    SADMRG_REQUIRE(b.nmom() <= cap, SADMRG_ERR_LIMIT, "chain_bond: capacity");
+    for (int k = 0; k < b.nmom(); ++k) { q[k] = b.q[k]; d[k] = b.d[k]; }
+  });
+}
+
+int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    const Timers& t = S_.chain->timers;
+    const double v[9] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
+                         (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded};
+    for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
+  });
+}
+
+int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    auto& ch = *S_.chain;
+    SADMRG_REQUIRE(site >= 0 && site < ch.ns && k >= 0 && k < ch.ns, SADMRG_ERR_ARG, "set_tensor: index");
+    BTensor<S> v = t ? from_desc<S>(h->ctx, t) : BTensor<S>();
+    if (kind == 0) ch.uu[site] = std::move(v);
+    else if (kind == 1) ch.hh[site] = std::move(v);
+    else if (kind == 2) ch.opr[site][k] = std::move(v);
+    else throw Error(SADMRG_ERR_ARG, "set_tensor: kind");
+  });
+}
+
+int sadmrg_chain_stage_tensor(sadmrg_handle* h, int kind, int site, int k) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    auto& ch = *S_.chain;
+    SADMRG_REQUIRE(site >= 0 && site < ch.ns && k >= 0 && k < ch.ns, SADMRG_ERR_ARG, "stage_tensor: index");
+    const BTensor<S>* src = nullptr;
+    if (kind == 0) src = &ch.uu[site];
+    else if (kind == 1) src = &ch.hh[site];
+    else if (kind == 2) src = &ch.opr[site][k];
+    else throw Error(SADMRG_ERR_ARG, "stage_tensor: kind");
+    S_.staged[0] = src->null() ? BTensor<S>() : clone(h->ctx, *src);
+  });
+}
+
+int sadmrg_chain_env_update(sadmrg_handle* h, int site, int dir, int real_env) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    auto& ch = *S_.chain;
+    SADMRG_REQUIRE(site >= 0 && site < ch.ns, SADMRG_ERR_ARG, "env_update: site");
+    if (dir == 0) ch.prepare_site_operator_from_left(site, real_env != 0);
+    else ch.prepare_site_operator_from_right(site, real_env != 0);
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+  });
+}
+
+int sadmrg_staged_info(sadmrg_handle* h, int which, int* nbond, int* locspin, int* nsectors, int* nblocks,
+                       long long* nelem) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    SADMRG_REQUIRE(which == 0 || which == 1, SADMRG_ERR_ARG, "staged: which");
+    const BTensor<S>& t = st_of<S>(h).staged[which];
+    *nbond = t.st.nbond();
+    *locspin = t.st.locspin;
+    int ns = 0, nb = 0;
+    for (auto& b : t.st.bonds) ns += b.nmom();
+    for (long i = 0; i < t.nten(); ++i) nb += t.present(i) ? 1 : 0;
+    *nsectors = ns;
+    *nblocks = nb;
+    *nelem = t.nelem;
+  });
+}
+
+int sadmrg_staged_read(sadmrg_handle* h, int which, int* dir, int* nmom, int* q, int* d, long long* block_index,
+                       void* data) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    SADMRG_REQUIRE(which == 0 || which == 1, SADMRG_ERR_ARG, "staged: which");
+    const BTensor<S>& t = st_of<S>(h).staged[which];
+    int o = 0;
+    for (int b = 0; b < t.st.nbond(); ++b) {
+      dir[b] = t.st.bonds[b].dir;
+      nmom[b] = t.st.bonds[b].nmom();
+      for (int k = 0; k < nmom[b]; ++k) { q[o] = t.st.bonds[b].q[k]; d[o] = t.st.bonds[b].d[k]; ++o; }
+    }
+    int nb = 0;
+    for (long i = 0; i < t.nten(); ++i)
+      if (t.present(i)) block_index[nb++] = i;
+    if (t.nelem > 0)
+      SADMRG_CUDA(cudaMemcpyAsync(data, t.data(), sizeof(S) * t.nelem, cudaMemcpyDeviceToHost, h->ctx.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+  });
+}
+
+}  // extern "C"

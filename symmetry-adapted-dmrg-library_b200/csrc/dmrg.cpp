@@ -1,0 +1,936 @@
+// dmrg.cpp -- H_eff plans, Lanczos, block SVD truncation and the sweep driver.
+#include "dmrg.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace sadmrg {
+
+template <class S> static constexpr bool kCx = ScalarInfo<S>::cplx;
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------------------
+// H_eff * psi plan (DMRG::hamiltonian_vector_multiplication_idmrg, src/dmrg_inst.cpp:283-371,
+// and BlockTensor::hamiltonian_vector_multiplication, src/block_tensor_inst.cpp:2170-2318)
+template <class S>
+HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, const BTensor<S>* hhR,
+                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms) {
+  HeffPlan<S> H;
+  H.psi_st = psi.st;
+  H.psi_off = psi.off;
+  H.n = psi.nelem;
+  // pack every operator the plan reads into one buffer (base id 2)
+  std::vector<long long> base(opl.size(), -1);
+  long long tot = 0, hl = -1, hr = -1;
+  if (hhL && !hhL->null()) { hl = tot; tot += hhL->nelem; }
+  if (hhR && !hhR->null()) { hr = tot; tot += hhR->nelem; }
+  for (size_t i = 0; i < opl.size(); ++i)
+    if (opl[i] && !opl[i]->null()) { base[i] = tot; tot += opl[i]->nelem; }
+  H.opsbuf = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(tot, 1), c.stream);
+  auto cp = [&](const BTensor<S>* t, long long at) {
+    if (t->nelem > 0)
+      SADMRG_CUDA(cudaMemcpyAsync(H.opsbuf->template as<S>() + at, t->data(), sizeof(S) * t->nelem, cudaMemcpyDeviceToDevice,
+                                  c.stream));
+  };
+  if (hl >= 0) cp(hhL, hl);
+  if (hr >= 0) cp(hhR, hr);
+  for (size_t i = 0; i < opl.size(); ++i)
+    if (base[i] >= 0) cp(opl[i], base[i]);
+
+  GemmPlan& p = H.plan;
+  const std::vector<Blk> P = blocks_of(psi);
+  std::vector<int> job_of(psi.nten(), -1);
+  for (auto& b : P) job_of[b.idx] = p.add_job(1, 1, b.off, b.d[0], b.d[1], b.d[0], 0);
+  const Struct& ps = psi.st;
+  int q[8], d[8];
+  // diagonal terms: hh_L^T psi  (contract(hh[il], 0, vec1, 0))
+  if (hl >= 0) {
+    const Bond& cb = hhL->st.bonds[0];
+    for (auto& o : P) {
+      for (int j = 0; j < cb.nmom(); ++j) {
+        int qa[2] = {cb.q[j], o.q[0]};   // hh block (j, x)
+        int qb[2] = {cb.q[j], o.q[1]};   // psi block (j, b)
+        if (!hhL->st.allowed_labels(qa) || !ps.allowed_labels(qb)) continue;
+        const long ka = hhL->st.index(qa), kb = ps.index(qb);
+        if (ka < 0 || kb < 0 || !hhL->present(ka) || !psi.present(kb)) continue;
+        p.add_term(job_of[o.idx], 2, hl + hhL->off[ka], cb.d[j], 0, psi.off[kb], cb.d[j], cb.d[j], TF_TA, 1.0, 0.0);
+      }
+    }
+  }
+  // diagonal terms: psi hh_R  (contract(vec1, 1, hh[ir], 0))
+  if (hr >= 0) {
+    const Bond& cb = hhR->st.bonds[0];
+    for (auto& o : P) {
+      for (int j = 0; j < cb.nmom(); ++j) {
+        int qa[2] = {o.q[0], cb.q[j]};   // psi block (a, j)
+        int qb[2] = {cb.q[j], o.q[1]};   // hh block (j, y)
+        if (!ps.allowed_labels(qa) || !hhR->st.allowed_labels(qb)) continue;
+        const long ka = ps.index(qa), kb = hhR->st.index(qb);
+        if (ka < 0 || kb < 0 || !psi.present(ka) || !hhR->present(kb)) continue;
+        p.add_term(job_of[o.idx], 0, psi.off[ka], o.d[0], 2, hr + hhR->off[kb], cb.d[j], cb.d[j], 0, 1.0, 0.0);
+      }
+    }
+  }
+  // pair terms: out(a',b') += fac * op1^T psi op2
+  for (auto& t : terms) {
+    const BTensor<S>& o1 = *opl[t.op1];
+    const BTensor<S>& o2 = *opl[t.op2];
+    if (o1.null() || o2.null()) continue;
+    SADMRG_REQUIRE(o1.st.bonds[2].q == ps.bonds[0].q && o2.st.bonds[2].q == ps.bonds[1].q, SADMRG_ERR_ARG,
+                   "heff: operator bonds do not match psi");
+    const auto O1 = blocks_of(o1);
+    std::vector<std::array<int, 3>> o2q;
+    std::vector<long long> o2off;
+    std::vector<int> o2d0;
+    for (long l = 0; l < o2.nten(); ++l)
+      if (o2.st.block(l, q, d) && o2.present(l)) {
+        o2q.push_back({q[0], q[1], q[2]});
+        o2off.push_back(base[t.op2] + o2.off[l]);
+        o2d0.push_back(d[0] * d[1]);
+      }
+    for (auto& pk : P)
+      for (auto& a : O1) {
+        if (a.q[0] != pk.q[0]) continue;
+        SADMRG_REQUIRE(a.d[1] == 1, SADMRG_ERR_ARG, "heff: channel leg dim != 1");
+        int x = -1;
+        long long xo = 0;
+        for (size_t l = 0; l < o2q.size(); ++l) {
+          if (o2q[l][0] != pk.q[1] || a.q[1] != o2q[l][1]) continue;
+          int lab[2] = {a.q[2], o2q[l][2]};
+          if (!ps.allowed_labels(lab)) continue;
+          const long m = ps.index(lab);
+          if (m < 0 || !psi.present(m)) continue;
+          double fac = 1.0;
+          if (c.sym == Sym::SU2) {
+            fac = c.cgc->hamilt_vec(a.q[0], a.q[1], a.q[2]);
+            if (std::fabs(fac) < 1e-12) continue;
+          }
+          if (x < 0) {
+            xo = p.alloc_scratch((long long)a.d[2] * pk.d[1]);
+            x = p.add_job(0, 3, xo, a.d[2], pk.d[1], a.d[2], 0);
+            p.add_term(x, 2, base[t.op1] + a.off, a.d[0], 0, pk.off, pk.d[0], pk.d[0], TF_TA, 1.0, 0.0);
+          }
+          p.add_term(job_of[m], 3, xo, a.d[2], 2, o2off[l], o2d0[l], pk.d[1], 0, fac, 0.0);
+        }
+      }
+  }
+  p.finalize(c, kCx<S>);
+  H.scratch = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(p.scratch_elems, 1), c.stream);
+  H.flops = p.flops;
+  H.bytes = (2 * H.n + tot) * (long long)sizeof(S);
+  H.ntasks = (int)p.flat_terms.size();
+  return H;
+}
+
+template <class S>
+void HeffPlan<S>::apply(Ctx& c, const S* psi, S* out, int prec) const {
+  Bases b{};
+  b.p[0] = const_cast<S*>(psi);
+  b.p[1] = out;
+  b.p[2] = opsbuf->get();
+  b.p[3] = scratch->get();
+  plan.run(c, kCx<S>, prec, b);
+}
+
+// ---------------------------------------------------------------------------
+// symmetric tridiagonal eigenproblem (replaces LAPACK dstev, src/dmrg_inst.cpp:1216-1231):
+// implicit QL with Wilkinson-type shifts (the tql2 algorithm of Bowdler, Martin,
+// Reinsch and Wilkinson, 1968).  d: diagonal, e[i]: coupling of i and i+1.
+// On return d is ascending and z (column-major n x n) holds the eigenvectors.
+static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
+  z.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) z[i + (size_t)i * n] = 1.0;
+  e.resize(n, 0.0);
+  if (n > 0) e[n - 1] = 0.0;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0, m;
+    do {
+      for (m = l; m < n - 1; ++m) {
+        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
+      }
+      if (m != l) {
+        if (iter++ == 100) throw Error(SADMRG_ERR_NUMERIC, "tridiagonal QL did not converge");
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = std::hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? std::fabs(r) : -std::fabs(r)));
+        double s = 1.0, cc = 1.0, pp = 0.0;
+        int i;
+        bool deflated = false;
+        for (i = m - 1; i >= l; --i) {
+          double f = s * e[i], b = cc * e[i];
+          e[i + 1] = (r = std::hypot(f, g));
+          if (r == 0.0) { d[i + 1] -= pp; e[m] = 0.0; deflated = true; break; }
+          s = f / r;
+          cc = g / r;
+          g = d[i + 1] - pp;
+          r = (d[i] - g) * s + 2.0 * cc * b;
+          d[i + 1] = g + (pp = s * r);
+          g = cc * r - b;
+          for (int k = 0; k < n; ++k) {
+            f = z[k + (size_t)(i + 1) * n];
+            z[k + (size_t)(i + 1) * n] = s * z[k + (size_t)i * n] + cc * f;
+            z[k + (size_t)i * n] = cc * z[k + (size_t)i * n] - s * f;
+          }
+        }
+        if (deflated) continue;
+        d[l] -= pp;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+    } while (m != l);
+  }
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return d[a] < d[b]; });
+  std::vector<double> d2(n), z2((size_t)n * n);
+  for (int k = 0; k < n; ++k) {
+    d2[k] = d[ord[k]];
+    std::memcpy(&z2[(size_t)k * n], &z[(size_t)ord[k] * n], sizeof(double) * n);
+  }
+  d.swap(d2);
+  z.swap(z2);
+}
+
+// ---------------------------------------------------------------------------
+// Lanczos
+template <class S>
+struct Krylov {
+  Ctx& c;
+  long long n;
+  int mlanc;
+  DevBuf ff, vh, coef, dots, beta, cdev;
+  Krylov(Ctx& cc, long long nn, int ml) : c(cc), n(nn), mlanc(ml) {
+    ff.alloc(sizeof(S) * n * (mlanc + 1), c.stream);
+    vh.alloc(sizeof(S) * n * 2, c.stream);
+    coef.alloc(sizeof(S) * (mlanc + 4), c.stream);
+    dots.alloc(sizeof(S) * (mlanc + 4), c.stream);
+    beta.alloc(sizeof(double) * (mlanc + 4), c.stream);
+    cdev.alloc(sizeof(double) * (mlanc + 4), c.stream);
+    SADMRG_CUDA(cudaMemsetAsync(beta.get(), 0, sizeof(double) * (mlanc + 4), c.stream));
+  }
+  S* F(int i) { return ff.as<S>() + (size_t)i * n; }
+  void mdot(const S* V, int nv, const S* x, void* out) {
+    launch_multi_dot(kCx<S>, V, n, nv, x, n, c.d_partial, c.npart, out, c.stream);
+    c.launches += 2;
+  }
+  S dot_host(const S* a, const S* b) {  // <a|b>
+    mdot(a, 1, b, dots.get());
+    S r;
+    SADMRG_CUDA(cudaMemcpyAsync(&r, dots.get(), sizeof(S), cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    return r;
+  }
+  void scale_host(S* x, double s) {
+    launch_scale(kCx<S>, x, s, 0.0, n, c.stream);
+    ++c.launches;
+  }
+  // vout = sum_j coef[j] F(j)
+  void ritz(S* vout, const std::vector<double>& z, int m) {
+    SADMRG_CUDA(cudaMemcpyAsync(cdev.get(), z.data(), sizeof(double) * m, cudaMemcpyHostToDevice, c.stream));
+    launch_lincomb(kCx<S>, vout, F(0), n, m, cdev.as<double>(), n, c.stream);
+    ++c.launches;
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
+};
+
+template <class S>
+LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
+  LanczosStats st;
+  const long long n = H.n;
+  Krylov<S> K(c, n, mlanc);
+  std::vector<double> aal(mlanc, 0.0), nnl(mlanc + 1, 0.0), eig, z;
+  const double tol = 1.e-6;
+  auto matvec = [&](const S* in, S* out) {
+    H.apply(c, in, out, prec);
+    ++st.matvecs;
+    if (prec == PREC_FP64) ++st.matvecs_fp64;
+  };
+  auto diatridiag = [&](int m) {
+    eig.assign(aal.begin(), aal.begin() + m);
+    std::vector<double> e(m, 0.0);
+    for (int i = 0; i + 1 < m; ++i) e[i] = nnl[i + 1];
+    tridiag_eig(m, eig, e, z);
+  };
+  auto ritz_vec = [&](int m) {
+    std::vector<double> col(z.begin(), z.begin() + m);  // eigenvector of the lowest Ritz value
+    K.ritz(v, col, m);
+  };
+  // Lanczos::check_eigenvector (src/dmrg_inst.cpp:1241-1254)
+  auto check = [&](double& ee, double& ov) {
+    S* vv = K.vh.template as<S>();
+    S* hv = vv + n;
+    const double nor = std::sqrt(std::fabs(real_of(K.dot_host(v, v))));
+    K.scale_host(v, 1.0 / nor);
+    SADMRG_CUDA(cudaMemcpyAsync(vv, v, sizeof(S) * n, cudaMemcpyDeviceToDevice, c.stream));
+    matvec(vv, hv);
+    K.mdot(vv, 2, hv, K.dots.get());  // <v|h>, <h|h>
+    S r[2];
+    SADMRG_CUDA(cudaMemcpyAsync(r, K.dots.get(), sizeof(S) * 2, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    const double prod = std::sqrt(std::fabs(real_of(r[1])));
+    ee = prod;
+    ov = std::abs(r[0]) / prod;
+    st.overlap = ov;
+  };
+  // ff[0] = normalised v (Lanczos::initialize_lanczos, src/dmrg_inst.cpp:1201-1213)
+  SADMRG_CUDA(cudaMemcpyAsync(K.F(0), v, sizeof(S) * n, cudaMemcpyDeviceToDevice, c.stream));
+  {
+    const double nor = std::sqrt(std::fabs(real_of(K.dot_host(K.F(0), K.F(0)))));
+    if (nor > 1e-12) K.scale_host(K.F(0), 1.0 / nor);
+  }
+  // one Lanczos step: F(m) = H F(m-1) - a F(m-1) - b F(m-2), reorthogonalised, normalised
+  auto step = [&](int m, bool reorth) {
+    matvec(K.F(m - 1), K.F(m));
+    K.mdot(K.F(m - 1), 1, K.F(m), K.dots.get());
+    launch_lanczos_scalar(kCx<S>, 0, K.dots.get(), K.beta.template as<double>() + (m - 1), K.coef.get(), c.stream);
+    ++c.launches;
+    if (m >= 2)
+      launch_multi_axpy(kCx<S>, K.F(m), K.F(m - 2), n, 2, K.coef.get(), n, c.stream);
+    else
+      launch_multi_axpy(kCx<S>, K.F(m), K.F(m - 1), n, 1, K.coef.template as<S>() + 1, n, c.stream);
+    ++c.launches;
+    if (reorth) {
+      K.mdot(K.F(0), m, K.F(m), K.dots.get());
+      launch_multi_axpy(kCx<S>, K.F(m), K.F(0), n, m, K.dots.get(), n, c.stream);
+      ++c.launches;
+    }
+    K.mdot(K.F(m), 1, K.F(m), K.dots.get());
+    launch_lanczos_scalar(kCx<S>, 1, K.dots.get(), nullptr, K.beta.template as<double>() + m, c.stream);
+    launch_scale_inv(kCx<S>, K.F(m), K.beta.template as<double>() + m, n, c.stream);
+    c.launches += 2;
+    S co[2];
+    double bm;
+    SADMRG_CUDA(cudaMemcpyAsync(co, K.coef.get(), sizeof(S) * 2, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaMemcpyAsync(&bm, K.beta.template as<double>() + m, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    aal[m - 1] = real_of(co[1]);
+    nnl[m] = bm;
+    st.iters = m;
+  };
+  double ee = 0.0, ov = 0.0;
+  step(1, false);
+  if (mlanc == 2) {
+    if (nnl[1] < tol) {
+      diatridiag(1);
+      ritz_vec(1);
+      st.energy = eig[0];
+      return st;
+    }
+    matvec(K.F(1), K.F(2));
+    const S a1 = K.dot_host(K.F(1), K.F(2));
+    aal[1] = real_of(a1);
+    diatridiag(2);
+    ritz_vec(2);
+    st.energy = eig[0];
+    return st;
+  }
+  for (int m = 2; m < mlanc; ++m) {
+    step(m, true);
+    diatridiag(m);
+    if (nnl[m] < tol) {
+      ritz_vec(m);
+      check(ee, ov);
+      st.energy = eig[0];
+      return st;
+    }
+    if (m % 4 == 0) {
+      ritz_vec(m);
+      check(ee, ov);
+      if (std::fabs(ov - 1.0) < 1e-8) { st.energy = eig[0]; return st; }
+    }
+  }
+  matvec(K.F(mlanc - 1), K.F(mlanc));
+  aal[mlanc - 1] = real_of(K.dot_host(K.F(mlanc - 1), K.F(mlanc)));
+  diatridiag(mlanc);
+  ritz_vec(mlanc);
+  check(ee, ov);
+  st.energy = eig[0];
+  return st;
+}
+
+template <class S>
+LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
+  if (prec == PREC_FP64) return lanczos1<S>(c, H, v, mlanc, PREC_FP64);
+  LanczosStats a = lanczos1<S>(c, H, v, mlanc, prec);
+  LanczosStats b = lanczos1<S>(c, H, v, mlanc, PREC_FP64);  // FP64 defect-correction restart
+  b.matvecs += a.matvecs;
+  b.iters += a.iters;
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// block SVD and truncation (BlockTensor::svd, src/block_tensor_inst.cpp:501-637)
+template <class S>
+SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
+                   int max_dcut, std::vector<double>* wout) {
+  SvdStats out;
+  const Bond bb20 = tu.st.bonds[0], bb21 = tu.st.bonds[1], bb22 = tv.st.bonds[0], bb23 = tv.st.bonds[1];
+  const Bond bb0 = Bond::fuse(c.sym, bb20, bb21), bb1 = Bond::fuse(c.sym, bb22, bb23);
+  const int nm1 = bb0.nmom(), nm2 = bb1.nmom();
+  SADMRG_REQUIRE(psi.st.nbond() == 2 && psi.st.bonds[0].q == bb0.q && psi.st.bonds[1].q == bb1.q &&
+                     psi.st.bonds[0].d == bb0.d && psi.st.bonds[1].d == bb1.d,
+                 SADMRG_ERR_ARG, "svd: psi does not match the fused bonds of the site tensors");
+  std::vector<SvdJob> jobs;
+  std::vector<int> job_of(nm1, -1), sec_j(nm1, -1);
+  long long wtot = 0, stot = 0;
+  for (int i = 0; i < nm1; ++i)
+    for (int j = 0; j < nm2; ++j) {
+      if (bb0.q[i] != bb1.q[j] || !psi.present(i + (long)j * nm1)) continue;
+      SvdJob J{};
+      J.m = bb0.d[i];
+      J.n = bb1.d[j];
+      J.trans = J.m < J.n ? 1 : 0;
+      const long long R = std::max(J.m, J.n), C = std::min(J.m, J.n);
+      J.aoff = psi.off[i + (long)j * nm1];
+      J.woff = wtot;
+      wtot += R * C;
+      J.voff = wtot;
+      wtot += C * C;
+      J.soff = stot;
+      stot += C;
+      job_of[i] = (int)jobs.size();
+      sec_j[i] = j;
+      jobs.push_back(J);
+    }
+  DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
+  const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream);
+  c.launches += 1;
+  SADMRG_REQUIRE(sweeps > 0 || jobs.empty(), SADMRG_ERR_NUMERIC, "svd: Jacobi sweeps did not converge");
+  out.sweeps_max = sweeps;
+  std::vector<double> hs(stot);
+  if (stot > 0) SADMRG_CUDA(cudaMemcpyAsync(hs.data(), sv.get(), sizeof(double) * stot, cudaMemcpyDeviceToHost, c.stream));
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  // per sector: descending order, relative cut-off 1e-10, cap max_dcut (Dense::svd, src/dense_inst.cpp:497-506)
+  std::vector<std::vector<int>> order(jobs.size());
+  std::vector<std::vector<double>> ssort(jobs.size());
+  std::vector<int> dc(nm1, 0);
+  std::vector<double> wsort;
+  std::vector<int> isort;
+  double wtotal = 0.0;
+  for (int i = 0; i < nm1; ++i) {
+    if (job_of[i] < 0) continue;
+    const SvdJob& J = jobs[job_of[i]];
+    const int C = std::min(J.m, J.n);
+    auto& o = order[job_of[i]];
+    o.resize(C);
+    std::iota(o.begin(), o.end(), 0);
+    std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return hs[J.soff + a] > hs[J.soff + b]; });
+    auto& s = ssort[job_of[i]];
+    s.resize(C);
+    for (int k = 0; k < C; ++k) { s[k] = hs[J.soff + o[k]]; wtotal += s[k] * s[k]; }
+    const double smax = (C > 0 && s[0] > 1e-16) ? s[0] : 1.0;
+    int kept = 0;
+    for (int k = 0; k < C; ++k)
+      if (s[k] / smax > 1e-10) ++kept;
+    if (kept == 0) kept = 1;
+    if (max_dcut > 0 && kept > max_dcut) kept = max_dcut;
+    dc[i] = kept;
+    for (int k = 0; k < kept; ++k) { wsort.push_back(s[k]); isort.push_back(i); }
+  }
+  // global descending sort without tie-break (sort2, src/block_tensor_inst.cpp:38-50)
+  {
+    std::vector<std::pair<double, int>> tmp(wsort.size());
+    for (size_t k = 0; k < wsort.size(); ++k) tmp[k] = {wsort[k], isort[k]};
+    std::sort(tmp.begin(), tmp.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    for (size_t k = 0; k < wsort.size(); ++k) { wsort[k] = tmp[k].first; isort[k] = tmp[k].second; }
+  }
+  const int ntot = (int)wsort.size();
+  const int dcut = ntot > max_dcut ? max_dcut : ntot;
+  std::vector<int> dim(nm1, 0);
+  for (int k = 0; k < dcut; ++k) dim[isort[k]]++;
+  std::vector<int> amom, bdim;
+  double kept_w = 0.0;
+  if (wout) wout->clear();
+  for (int i = 0; i < nm1; ++i)
+    if (dim[i] > 0) {
+      amom.push_back(bb0.q[i]);
+      bdim.push_back(dim[i]);
+      for (int k = 0; k < dim[i]; ++k) {
+        kept_w += ssort[job_of[i]][k] * ssort[job_of[i]][k];
+        if (wout) wout->push_back(ssort[job_of[i]][k]);
+      }
+    }
+  out.kept = dcut;
+  out.discarded_weight = wtotal > 0 ? std::max(0.0, 1.0 - kept_w / wtotal) : 0.0;
+  Bond nb(bb0.dir, amom, bdim);
+  Bond nbv = nb;
+  if (c.sym == Sym::U1) nbv.invert();
+  Struct su(c.sym, 0, {bb20, bb21, nb}), svs(c.sym, 0, {bb22, bb23, nbv});
+  // positions of (x, y) pairs inside each fused sector (BlockTensor::fuse ordering)
+  auto fuse_pos = [&](const Bond& a, const Bond& b, const Bond& f) {
+    Struct fs(c.sym, 0, {a, b, f});
+    std::vector<long long> pos(fs.nten(), -1);
+    std::vector<int> acc(f.nmom(), 0);
+    int q[8], d[8];
+    for (long i = 0; i < fs.nten(); ++i) {
+      if (!fs.block(i, q, d)) continue;
+      const int k = f.index_of(q[2]);
+      pos[i] = acc[k];
+      acc[k] += d[0] * d[1];
+    }
+    return std::make_pair(fs, pos);
+  };
+  auto fu = fuse_pos(bb20, bb21, bb0), fv = fuse_pos(bb22, bb23, bb1);
+  // permutation and sorted singular values for the gathers
+  std::vector<int> perm;
+  std::vector<double> wsorted;
+  std::vector<long long> poff(jobs.size(), 0);
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    poff[j] = (long long)perm.size();
+    perm.insert(perm.end(), order[j].begin(), order[j].end());
+    wsorted.insert(wsorted.end(), ssort[j].begin(), ssort[j].end());
+  }
+  DevBuf dperm(sizeof(int) * std::max<size_t>(perm.size(), 1), c.stream),
+      dw(sizeof(double) * std::max<size_t>(wsorted.size(), 1), c.stream);
+  if (!perm.empty()) {
+    SADMRG_CUDA(cudaMemcpyAsync(dperm.get(), perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice, c.stream));
+    SADMRG_CUDA(cudaMemcpyAsync(dw.get(), wsorted.data(), sizeof(double) * wsorted.size(), cudaMemcpyHostToDevice, c.stream));
+  }
+  auto build = [&](const Struct& st, const std::pair<Struct, std::vector<long long>>& fz, const Bond& fb,
+                   bool left) -> BTensor<S> {
+    int q[8], d[8];
+    std::vector<char> pres(st.nten(), 0);
+    std::vector<Gather> gs;
+    for (long m = 0; m < st.nten(); ++m) {
+      if (!st.block(m, q, d)) continue;
+      const int i = bb0.index_of(q[2]);
+      if (i < 0 || dim[i] == 0) continue;
+      int fq[3] = {q[0], q[1], q[2]};
+      if (!fz.first.allowed_labels(fq)) continue;
+      const long fi = fz.first.index(fq);
+      if (fi < 0 || fz.second[fi] < 0) continue;
+      (void)fb;
+      pres[m] = 1;
+    }
+    BTensor<S> t = alloc_tensor<S>(c, st, pres);
+    for (long m = 0; m < st.nten(); ++m) {
+      if (!pres[m]) continue;
+      st.block(m, q, d);
+      const int i = bb0.index_of(q[2]);
+      const int jb = job_of[i];
+      const SvdJob& J = jobs[jb];
+      int fq[3] = {q[0], q[1], q[2]};
+      const long long pos = fz.second[fz.first.index(fq)];
+      Gather g{};
+      g.doff = t.off[m];
+      g.rows = d[0] * d[1];
+      g.kept = dim[i];
+      g.woff = poff[jb];
+      g.poff = poff[jb];
+      if (left) {  // U columns scaled by s^p1
+        g.conj = 0;
+        if (!J.trans) { g.soff = J.woff + pos; g.lds = J.m; g.p = p1 - 1.0; }
+        else          { g.soff = J.voff + pos; g.lds = J.m; g.p = p1; }
+      } else {     // conj(V) columns scaled by s^p2
+        g.conj = 1;
+        if (!J.trans) { g.soff = J.voff + pos; g.lds = J.n; g.p = p2; }
+        else          { g.soff = J.woff + pos; g.lds = J.n; g.p = p2 - 1.0; }
+      }
+      gs.push_back(g);
+    }
+    if (!gs.empty()) {
+      DevBuf dg(sizeof(Gather) * gs.size(), c.stream);
+      SADMRG_CUDA(cudaMemcpyAsync(dg.get(), gs.data(), sizeof(Gather) * gs.size(), cudaMemcpyHostToDevice, c.stream));
+      launch_gather(kCx<S>, t.data(), wv.get(), dw.as<double>(), dperm.as<int>(), dg.as<Gather>(), (int)gs.size(),
+                    c.stream);
+      ++c.launches;
+      SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    return t;
+  };
+  BTensor<S> nu = build(su, fu, bb0, true);
+  BTensor<S> nv = build(svs, fv, bb1, false);
+  tu = std::move(nu);
+  tv = std::move(nv);
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// chain
+template <class S>
+Chain<S>::Chain(Ctx& cc, int lx_, int ly_, int bondd_, int physpn_, int totspin_, int open, double J2)
+    : c(cc), lx(lx_), ly(ly_), ns(lx_ * ly_), bondd(bondd_), physpn(physpn_), totspin(totspin_), max_dcut(bondd_) {
+  SADMRG_REQUIRE(ns >= 6 && ns % 2 == 0, SADMRG_ERR_ARG, "chain: need an even number of sites >= 6");
+  SADMRG_REQUIRE(physpn == 1, SADMRG_ERR_ARG, "chain: spin-1/2 sites only");
+  uu.resize(ns);
+  hh.resize(ns);
+  opr.assign(ns, std::vector<BTensor<S>>(ns));
+  hmap.assign(ns, std::vector<int>(ns, 0));
+  fll.assign(ns, std::vector<int>(ns, 0));
+  frr.assign(ns, std::vector<int>(ns, 0));
+  coup.assign(ns + 1, 0.0);
+  // snake-ordered lattice bonds (src/dmrg_inst.cpp:121-144); open = no wrap-around
+  auto site = [&](int x, int y) { return (x % 2 == 0) ? x * ly + y : x * ly + (ly - 1 - y); };
+  for (int i = 0; i < ns; ++i) {
+    const int x1 = i / ly, y1 = (x1 % 2 == 0) ? i % ly : ly - 1 - (i % ly);
+    for (int k = 0; k < 2; ++k) {
+      int x2 = x1, y2 = y1;
+      if (k == 0) { x2 = x1 + 1; if (x2 >= lx) { if (open) continue; x2 %= lx; } }
+      else        { y2 = y1 + 1; if (y2 >= ly) { if (open) continue; y2 %= ly; } }
+      const int j = site(x2, y2);
+      if (i != j) { hmap[i][j] = 1; hmap[j][i] = 1; }
+    }
+  }
+  coup[1] = 1.0;
+  if (J2 != 0.0) {
+    for (int i = 0; i + 2 < ns; ++i) { hmap[i][i + 2] = 2; hmap[i + 2][i] = 2; }
+    coup[2] = J2;
+  }
+  for (int i = 0; i < ns; ++i) {
+    for (int j = 0; j < i; ++j)
+      for (int k = i + 1; k < ns; ++k)
+        if (hmap[j][k] != 0) fll[i][j] = 1;
+    for (int j = i + 1; j < ns; ++j)
+      for (int k = 0; k < i; ++k)
+        if (hmap[j][k] != 0) frr[i][j] = 1;
+  }
+  if (c.sym == Sym::SU2 && !c.cgc) c.cgc = std::make_unique<CGCFactors>(physpn);
+  init_local_operators();
+}
+
+// DMRG::initialize_local_operators (src/dmrg_inst.cpp:222-260) with
+// BlockTensor::make_spinor_start (src/block_tensor_inst.cpp:1145-1217)
+template <class S>
+void Chain<S>::init_local_operators() {
+  const int p = physpn;
+  if (c.sym == Sym::SU2) {
+    Struct st(Sym::SU2, 0, {Bond(-1, {p}, {1}), Bond(-1, {2}, {1}), Bond(1, {p}, {1})});
+    const double r = std::sqrt(3.0) / 2.0;
+    for (int k = 0; k < 2; ++k) {
+      S val = S(k == 0 ? r : -r);
+      sigma[k] = ops::from_host<S>(c, st, {1}, &val);
+      sigma[k].host = {val};
+    }
+    return;
+  }
+  std::vector<int> qs, ones;
+  for (int i = 0; i <= p; ++i) { qs.push_back(-p + 2 * i); ones.push_back(1); }
+  Bond bp(-1, qs, ones), bk(1, qs, ones);
+  Struct s0(Sym::U1, 0, {bp, Bond(-1, {-2, 0, 2}, {1, 1, 1}), bk});
+  Struct s1(Sym::U1, 0, {bp, Bond(1, {-2, 0, 2}, {1, 1, 1}), bk});
+  for (int k = 0; k < 2; ++k) {
+    const Struct& st = k == 0 ? s0 : s1;
+    std::vector<char> pres(st.nten(), 0);
+    std::vector<S> vals;
+    int q[8], d[8];
+    for (long i = 0; i < st.nten(); ++i) {
+      if (!st.block(i, q, d)) continue;
+      // sigma[1] carries the channel charge reversed (contract with fuse_to_singlet + shift)
+      const int qc = (k == 0) ? q[1] : -q[1];
+      double v;
+      if (q[0] == q[2] && qc == 0) v = q[0] / 2.0;
+      else if (q[0] != q[2]) v = 1.0 / std::sqrt(2.0);
+      else continue;
+      pres[i] = 1;
+      vals.push_back(S(v));
+    }
+    sigma[k] = ops::from_host<S>(c, st, pres, vals.data());
+    sigma[k].host = vals;
+  }
+}
+
+template <class S>
+void Chain<S>::random_init(BTensor<S>& t) {
+  std::vector<S> h(t.nelem);
+  for (long long i = 0; i < t.nelem; ++i) {
+    if constexpr (kCx<S>) h[i] = S(dist(rng), dist(rng));
+    else h[i] = dist(rng);
+  }
+  if (t.nelem > 0)
+    SADMRG_CUDA(cudaMemcpyAsync(t.data(), h.data(), sizeof(S) * t.nelem, cudaMemcpyHostToDevice, c.stream));
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// DMRG::prepare_site_operator_from_left (src/dmrg_inst.cpp:440-511 and 587-639)
+template <class S>
+void Chain<S>::prepare_site_operator_from_left(int i, bool real_env) {
+  const double t0 = now_s();
+  BTensor<S> u1;
+  if (!real_env) u1 = ops::fuse<S>(c, uu[i].st.bonds[0], uu[i].st.bonds[1]);
+  const BTensor<S>& U = real_env ? uu[i] : u1;
+  if (real_env && i == 0) {
+    opr[0][0] = ops::operator_initial<S>(c, U, U, sigma[0], 0);
+    hh[0] = BTensor<S>();
+    timers.env += now_s() - t0;
+    return;
+  }
+  BTensor<S> hnew;
+  if (!hh[i - 1].null()) hnew = ops::overlap_transformation<S>(c, U, U, hh[i - 1], 0);
+  std::vector<BTensor<S>> newopr(i);
+  for (int k = 0; k < i; ++k)
+    if (fll[i][k] == 1) newopr[k] = ops::operator_transformation<S>(c, U, U, opr[i - 1][k], 0);
+  BTensor<S> op;
+  for (int m = 0; m < i; ++m)
+    if (hmap[i][m] > 0) ops::add_into<S>(c, op, opr[i - 1][m], S(coup[hmap[i][m]]));
+  if (!op.null()) {
+    BTensor<S> ht = ops::operator_pairup<S>(c, U, U, op, sigma[1], 0);
+    ops::add_into<S>(c, hnew, ht, S(1.0));
+  }
+  for (int k = 0; k < i; ++k)
+    if (fll[i][k] == 1) opr[i][k] = std::move(newopr[k]);
+  opr[i][i] = ops::operator_initial<S>(c, U, U, sigma[0], 0);
+  hh[i] = std::move(hnew);
+  timers.env += now_s() - t0;
+}
+
+// DMRG::prepare_site_operator_from_right (src/dmrg_inst.cpp:515-583 and 643-695)
+template <class S>
+void Chain<S>::prepare_site_operator_from_right(int i, bool real_env) {
+  const double t0 = now_s();
+  BTensor<S> u1;
+  if (!real_env) u1 = ops::fuse<S>(c, uu[i].st.bonds[0], uu[i].st.bonds[1]);
+  const BTensor<S>& U = real_env ? uu[i] : u1;
+  if (real_env && i == ns - 1) {
+    opr[i][i] = ops::operator_initial<S>(c, U, U, sigma[1], 1);
+    hh[i] = BTensor<S>();
+    timers.env += now_s() - t0;
+    return;
+  }
+  BTensor<S> hnew;
+  if (!hh[i + 1].null()) hnew = ops::overlap_transformation<S>(c, U, U, hh[i + 1], 1);
+  std::vector<BTensor<S>> newopr(ns);
+  for (int m = 0; m < ns - 1 - i; ++m) {
+    const int k = i + 1 + m;
+    if (frr[i][k] == 1) newopr[k] = ops::operator_transformation<S>(c, U, U, opr[i + 1][k], 1);
+  }
+  BTensor<S> op;
+  for (int m = 0; m < ns - 1 - i; ++m) {
+    const int k = i + 1 + m;
+    if (hmap[i][k] > 0) ops::add_into<S>(c, op, opr[i + 1][k], S(coup[hmap[i][k]]));
+  }
+  if (!op.null()) {
+    BTensor<S> ht = ops::operator_pairup<S>(c, U, U, op, sigma[0], 1);
+    ops::add_into<S>(c, hnew, ht, S(1.0));
+  }
+  for (int m = 0; m < ns - 1 - i; ++m) {
+    const int k = i + 1 + m;
+    if (frr[i][k] == 1) opr[i][k] = std::move(newopr[k]);
+  }
+  opr[i][i] = ops::operator_initial<S>(c, U, U, sigma[1], 1);
+  hh[i] = std::move(hnew);
+  timers.env += now_s() - t0;
+}
+
+// DMRG::prepare_input_vector (src/dmrg_inst.cpp:412-437)
+template <class S>
+void Chain<S>::prepare_input_vector(int il, int ir, BTensor<S>& vec) {
+  const double t0 = now_s();
+  BTensor<S> t1 = ops::fuse<S>(c, uu[il].st.bonds[0], uu[il].st.bonds[1]);
+  BTensor<S> t2 = ops::fuse<S>(c, uu[ir].st.bonds[0], uu[ir].st.bonds[1]);
+  BTensor<S> left = ops::overlap_initial<S>(c, uu[il], t1, 0);
+  BTensor<S> rght = ops::overlap_initial<S>(c, uu[ir], t2, 1);
+  if (c.sym == Sym::SU2) ops::take_conjugate(left, 0);
+  vec = ops::contract<S>(c, left, 0, rght, 0);
+  ops::makeup_input_vector<S>(c, vec);
+  timers.prep += now_s() - t0;
+}
+
+// DMRG::prepare_input_vector_initial (src/dmrg_inst.cpp:375-410)
+template <class S>
+void Chain<S>::prepare_input_vector_initial(int il, int ir, BTensor<S>& vec) {
+  const double t0 = now_s();
+  BTensor<S> t1 = ops::fuse<S>(c, uu[il].st.bonds[0], uu[il].st.bonds[1]);
+  BTensor<S> t2 = ops::fuse<S>(c, uu[ir].st.bonds[0], uu[ir].st.bonds[1]);
+  BTensor<S> left = ops::overlap_initial<S>(c, uu[il], t1, 0);
+  BTensor<S> rght = ops::overlap_initial<S>(c, uu[ir], t2, 1);
+  Bond b0 = left.st.bonds[0], b1 = rght.st.bonds[0];
+  b0.invert();
+  b1.invert();
+  BTensor<S> tmp = ops::fuse_to_singlet<S>(c, b0, b1);
+  BTensor<S> tmp3 = ops::contract<S>(c, left, 0, tmp, 0);
+  vec = ops::contract<S>(c, tmp3, 1, rght, 0);
+  ops::makeup_input_vector<S>(c, vec);
+  timers.prep += now_s() - t0;
+}
+
+// operator set of DMRG::hamiltonian_vector_multiplication_idmrg (src/dmrg_inst.cpp:309-351)
+template <class S>
+HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec) {
+  std::vector<const BTensor<S>*> opl;
+  std::vector<BTensor<S>> sums;
+  sums.reserve(ns);
+  std::vector<PairTerm> terms;
+  int m1, m4;
+  if (il < ns / 2) { m1 = il + 1; m4 = ns - ir; }
+  else { m1 = ns - ir; m4 = il + 1; }
+  for (int m0 = 0; m0 < m1; ++m0) {
+    int j = 0, k = 0;
+    if (il < ns / 2) j = m0;
+    else k = ir + m0;
+    BTensor<S> op;
+    for (int m = 0; m < m4; ++m) {
+      if (il < ns / 2) k = ir + m;
+      else j = m;
+      if (hmap[j][k] > 0) ops::add_into<S>(c, op, il < ns / 2 ? opr[ir][k] : opr[il][j], S(coup[hmap[j][k]]));
+    }
+    if (op.null()) continue;
+    sums.push_back(std::move(op));
+    const BTensor<S>* fixed = (il < ns / 2) ? &opr[il][j] : &opr[ir][k];
+    if (fixed->null()) continue;
+    PairTerm t;
+    opl.push_back(fixed);
+    const int fi = (int)opl.size() - 1;
+    opl.push_back(&sums.back());
+    const int si = (int)opl.size() - 1;
+    if (il < ns / 2) { t.op1 = fi; t.op2 = si; }
+    else { t.op1 = si; t.op2 = fi; }
+    terms.push_back(t);
+  }
+  return build_heff<S>(c, vec, hh[il].null() ? nullptr : &hh[il], hh[ir].null() ? nullptr : &hh[ir], opl, terms);
+}
+
+// DMRG::lanczos_solve_eigenvector_idmrg (src/dmrg_inst.cpp:264-279)
+template <class S>
+void Chain<S>::lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec) {
+  const double t0 = now_s();
+  int mlanc = mlanc_max;
+  long long ndata = 0;
+  {
+    int q[8], d[8];
+    for (long i = 0; i < vec.nten(); ++i)
+      if (vec.st.block(i, q, d)) ndata += vec.st.block_elems(i);
+  }
+  if (mlanc > ndata) mlanc = (int)ndata + 1;
+  if (mlanc < 2) mlanc = 2;
+  HeffPlan<S> H = heff_plan(il, ir, vec);
+  LanczosStats st = lanczos_solve<S>(c, H, vec.data(), mlanc, prec);
+  gs_enr = st.energy;
+  timers.matvecs += st.matvecs;
+  timers.heff_flops += (double)H.flops * st.matvecs;
+  timers.lanczos += now_s() - t0;
+}
+
+template <class S>
+void Chain<S>::wavefunc_transformation(int i, int dir) {
+  const double t0 = now_s();
+  if (dir == 0) ops::right2left_vectran<S>(c, uu[i]);
+  else ops::left2right_vectran<S>(c, uu[i]);
+  timers.prep += now_s() - t0;
+}
+
+template <class S>
+void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
+  const double t0 = now_s();
+  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &ww);
+  last_discarded = s.discarded_weight;
+  timers.svd += now_s() - t0;
+}
+
+// boundary tensors (src/dmrg_inst.cpp:710-740 and 812-840)
+template <class S>
+static void edge_tensors(Chain<S>& ch, Bond& bphys_l, Bond& bphys_r) {
+  Ctx& c = ch.c;
+  Bond b0, b3;
+  if (c.sym == Sym::SU2) {
+    b0 = Bond(1, {0}, {1});
+    bphys_l = Bond(1, {ch.physpn}, {1});
+    bphys_r = Bond(1, {ch.physpn}, {1});
+    b3 = Bond(1, {ch.totspin}, {1});
+  } else {
+    b0 = Bond(1, {0}, {1});
+    bphys_l = Bond(1, {-1, 1}, {1, 1});
+    bphys_r = Bond(1, {-1, 1}, {1, 1});
+    b3 = Bond(-1, {ch.totspin}, {1});
+  }
+  ch.uu[0] = ops::fuse<S>(c, b0, bphys_l);
+  ch.uu[ch.ns - 1] = ops::fuse<S>(c, bphys_r, b3);
+}
+
+// DMRG::do_idmrg (src/dmrg_inst.cpp:699-804)
+template <class S>
+void Chain<S>::do_idmrg() {
+  Bond bl, br;
+  edge_tensors(*this, bl, br);
+  BTensor<S> vec;
+  for (int i = 0; i <= ns / 2 - 2; ++i) {
+    prepare_site_operator_from_left(i, true);
+    prepare_site_operator_from_right(ns - 1 - i, true);
+    Bond b0 = uu[i].st.bonds[2], b1 = uu[ns - 1 - i].st.bonds[2];
+    b0.invert();
+    b1.invert();
+    uu[i + 1] = ops::fuse<S>(c, b0, bl);
+    uu[ns - 2 - i] = ops::fuse<S>(c, br, b1);
+    if (((i + 2) * 2 * physpn >= totspin && i >= 1) || i == ns / 2 - 2) {
+      prepare_input_vector_initial(i + 1, ns - 2 - i, vec);
+      prepare_site_operator_from_left(i + 1, false);
+      prepare_site_operator_from_right(ns - 2 - i, false);
+      random_init(vec);
+      lanczos_solve_eigenvector(i + 1, ns - 2 - i, vec);
+      if (i == ns / 2 - 2) svd_step(vec, i + 1, ns - 2 - i, 1.0, 0.0);
+      else svd_step(vec, i + 1, ns - 2 - i, 0.0, 0.0);
+    }
+  }
+}
+
+// DMRG::prepare_sweep (src/dmrg_inst.cpp:808-854)
+template <class S>
+void Chain<S>::prepare_sweep() {
+  Bond bl, br;
+  edge_tensors(*this, bl, br);
+  for (int i = 0; i < ns / 2 - 1; ++i) {
+    prepare_site_operator_from_left(i, true);
+    prepare_site_operator_from_right(ns - 1 - i, true);
+  }
+}
+
+// DMRG::sweep (src/dmrg_inst.cpp:874-943)
+template <class S>
+void Chain<S>::sweep() {
+  BTensor<S> vec;
+  for (int i = ns / 2; i >= nfree + 2; --i) {
+    wavefunc_transformation(i - 1, 1);
+    prepare_site_operator_from_right(i, true);
+    prepare_input_vector(i - 2, i - 1, vec);
+    prepare_site_operator_from_left(i - 2, false);
+    prepare_site_operator_from_right(i - 1, false);
+    lanczos_solve_eigenvector(i - 2, i - 1, vec);
+    if (i > nfree + 2) svd_step(vec, i - 2, i - 1, 1.0, 0.0);
+    else svd_step(vec, i - 2, i - 1, 0.0, 1.0);
+  }
+  for (int i = nfree; i < ns - nfree - 2; ++i) {
+    wavefunc_transformation(i + 1, 0);
+    prepare_site_operator_from_left(i, true);
+    prepare_input_vector(i + 1, i + 2, vec);
+    prepare_site_operator_from_left(i + 1, false);
+    prepare_site_operator_from_right(i + 2, false);
+    lanczos_solve_eigenvector(i + 1, i + 2, vec);
+    if (i < ns - nfree - 3) svd_step(vec, i + 1, i + 2, 0.0, 1.0);
+    else svd_step(vec, i + 1, i + 2, 1.0, 0.0);
+  }
+  for (int i = ns - nfree - 1; i >= ns / 2 + 1; --i) {
+    wavefunc_transformation(i - 1, 1);
+    prepare_site_operator_from_right(i, true);
+    prepare_input_vector(i - 2, i - 1, vec);
+    prepare_site_operator_from_left(i - 2, false);
+    prepare_site_operator_from_right(i - 1, false);
+    lanczos_solve_eigenvector(i - 2, i - 1, vec);
+    svd_step(vec, i - 2, i - 1, 1.0, 0.0);
+  }
+}
+
+template struct HeffPlan<double>;
+template struct HeffPlan<dcmplex>;
+template HeffPlan<double> build_heff<double>(Ctx&, const BTensor<double>&, const BTensor<double>*,
+                                             const BTensor<double>*, const std::vector<const BTensor<double>*>&,
+                                             const std::vector<PairTerm>&);
+template HeffPlan<dcmplex> build_heff<dcmplex>(Ctx&, const BTensor<dcmplex>&, const BTensor<dcmplex>*,
+                                               const BTensor<dcmplex>*, const std::vector<const BTensor<dcmplex>*>&,
+                                               const std::vector<PairTerm>&);
+template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
+template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
+template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
+template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
+template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,
+                                    int, std::vector<double>*);
+template SvdStats block_svd<dcmplex>(Ctx&, const BTensor<dcmplex>&, BTensor<dcmplex>&, double, BTensor<dcmplex>&,
+                                     double, int, std::vector<double>*);
+template class Chain<double>;
+template class Chain<dcmplex>;
+
+}  // namespace sadmrg

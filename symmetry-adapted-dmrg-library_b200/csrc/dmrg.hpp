@@ -1,0 +1,119 @@
+// dmrg.hpp -- two-site DMRG driver on device-resident block tensors.
+//
+// Mirrors the reference's DMRG<Scalar,Sym> / Lanczos<Scalar,Sym> control flow
+// (dmrg.hpp, src/dmrg_inst.cpp) step for step: iDMRG warm-up, prepare_sweep,
+// sweep (left, right, return passes), with every data-bearing operation run on
+// the GPU and only sector bookkeeping on the host.
+#pragma once
+#include <array>
+#include <chrono>
+#include <random>
+#include <string>
+
+#include "ops.hpp"
+
+namespace sadmrg {
+
+// H_eff * psi for a fixed two-site problem: all sector products of one matvec
+// in two grouped launches (stage 0: X = op1^T psi; stage 1: out = sum f X op2
+// + diagonal terms), built once per bond and replayed for every Lanczos step.
+template <class S>
+struct HeffPlan {
+  GemmPlan plan;
+  std::shared_ptr<DevBuf> opsbuf;    // packed operator data
+  std::shared_ptr<DevBuf> scratch;
+  Struct psi_st;
+  std::vector<long long> psi_off;
+  long long n = 0;                   // psi elements
+  long long flops = 0;               // algorithmic flops per matvec
+  long long bytes = 0;               // psi in + out + operators, once
+  int ntasks = 0;
+  void apply(Ctx& c, const S* psi, S* out, int prec) const;
+};
+
+struct PairTerm {
+  int op1 = -1, op2 = -1;            // indices into the operator list
+};
+
+template <class S>
+HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, const BTensor<S>* hhR,
+                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms);
+
+struct LanczosStats {
+  int matvecs = 0;
+  int matvecs_fp64 = 0;
+  int iters = 0;
+  double energy = 0.0;
+  double overlap = 0.0;
+};
+
+// Lanczos::lanczos1 (src/dmrg_inst.cpp:1286-1348) on device vectors.
+// v (length n) holds the start vector on entry and the Ritz vector on exit.
+template <class S>
+LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec);
+// Mixed precision: lanczos1 with 3xTF32 matvecs, then an FP64 restart from
+// its Ritz vector (defect correction) so the energy is an FP64 Lanczos result.
+template <class S>
+LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec);
+
+struct SvdStats {
+  int kept = 0;
+  double discarded_weight = 0.0;
+  int sweeps_max = 0;
+};
+
+// BlockTensor::svd (src/block_tensor_inst.cpp:501-637)
+template <class S>
+SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
+                   int max_dcut, std::vector<double>* wout);
+
+struct Timers {
+  double lanczos = 0, env = 0, svd = 0, prep = 0;
+  long long matvecs = 0;
+  double heff_flops = 0;
+};
+
+template <class S>
+class Chain {
+ public:
+  Chain(Ctx& c, int lx, int ly, int bondd, int physpn, int totspin, int open, double J2);
+  void do_idmrg();
+  void prepare_sweep();
+  void sweep();
+  double energy() const { return gs_enr; }
+
+  // building blocks (public for the frozen-problem API and tests)
+  void prepare_site_operator_from_left(int i, bool real_env);
+  void prepare_site_operator_from_right(int i, bool real_env);
+  void prepare_input_vector(int il, int ir, BTensor<S>& vec);
+  void prepare_input_vector_initial(int il, int ir, BTensor<S>& vec);
+  HeffPlan<S> heff_plan(int il, int ir, const BTensor<S>& vec);
+  void lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec);
+  void wavefunc_transformation(int i, int dir);
+
+  Ctx& c;
+  int lx, ly, ns, bondd, physpn, totspin, nfree = 2;
+  int max_dcut;
+  std::vector<std::vector<int>> hmap, fll, frr;
+  std::vector<double> coup;
+  std::vector<BTensor<S>> uu, hh;
+  std::vector<std::vector<BTensor<S>>> opr;
+  std::array<BTensor<S>, 2> sigma;
+  double gs_enr = 0.0;
+  std::vector<double> ww;
+  double last_discarded = 0.0;
+  // Lanczos settings (reference constants at src/dmrg_inst.cpp:267,1289,1338)
+  int mlanc_max = 40;
+  int prec = PREC_FP64;
+  Timers timers;
+  std::mt19937_64 rng{42};  // the reference's generator (src/dense_inst.cpp:23-24)
+  std::uniform_real_distribution<double> dist{-1.0, 1.0};
+  std::vector<std::string> log;
+
+ private:
+  void random_init(BTensor<S>& t);
+  void init_local_operators();
+  void svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2);
+};
+
+}  // namespace sadmrg

@@ -1,0 +1,516 @@
+// kernels.cu -- sm_100a kernels for the two-site DMRG hot path.
+//
+//  * grouped_gemm_f64 / grouped_gemm_z64: one launch runs every sector GEMM of
+//    a task list (H_eff*psi, environment updates, projector products).  FP64
+//    products run on the double-precision tensor path (mma.sync m8n8k4 .f64);
+//    tcgen05 has no f64 kind on sm_100a.
+//  * block utilities (segment axpy, block transpose, fuse fill, SVD gather);
+//  * Krylov vector kernels with deterministic two-pass reductions;
+//  * one-sided (Hestenes) block Jacobi SVD, column blocks staged in shared
+//    memory, rotations accumulated into a small matrix applied to V at the end.
+#include <cuda_runtime.h>
+#include <cstdio>
+
+#include "kernels.cuh"
+
+namespace sadmrg {
+
+// --------------------------------------------------------------------------
+// FP64 tensor-core MMA: D(8x8) += A(8x4, row) * B(4x8, col)
+// A frag: a = A[lane>>2][lane&3];  B frag: b = B[lane&3][lane>>2]
+// C frag: c0,c1 = C[lane>>2][2*(lane&3) + {0,1}]
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kGemmThreads = 128;
+
+template <int BM, int BN, int BK>
+__global__ void __launch_bounds__(kGemmThreads) grouped_gemm_f64(const GemmTerm* __restrict__ terms,
+                                                                 const GemmJob* __restrict__ jobs,
+                                                                 const GemmTile* __restrict__ tiles, Bases bases) {
+  constexpr int PAD = 4;
+  __shared__ double As[BK][BM + PAD];
+  __shared__ double Bs[BK][BN + PAD];
+  const GemmTile t = tiles[blockIdx.x];
+  const GemmJob J = jobs[t.job];
+  const int row0 = t.tm * BM, col0 = t.tn * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
+  double acc[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  for (int ti = 0; ti < J.nt; ++ti) {
+    const GemmTerm T = terms[J.t0 + ti];
+    const double* __restrict__ A = static_cast<const double*>(bases.p[T.abuf]) + T.aoff;
+    const double* __restrict__ B = static_cast<const double*>(bases.p[T.bbuf]) + T.boff;
+    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
+    const double alpha = T.ar;
+    for (int k0 = 0; k0 < T.k; k0 += BK) {
+#pragma unroll 4
+      for (int e = tid; e < BM * BK; e += kGemmThreads) {
+        int i, kk;
+        if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
+        const int gi = row0 + i, gk = k0 + kk;
+        double v = 0.0;
+        if (gi < J.m && gk < T.k) v = ta ? A[gk + (long long)gi * T.lda] : A[gi + (long long)gk * T.lda];
+        As[kk][i] = v * alpha;
+      }
+#pragma unroll 4
+      for (int e = tid; e < BK * BN; e += kGemmThreads) {
+        int j, kk;
+        if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+        const int gj = col0 + j, gk = k0 + kk;
+        double v = 0.0;
+        if (gj < J.n && gk < T.k) v = tb ? B[gj + (long long)gk * T.ldb] : B[gk + (long long)gj * T.ldb];
+        Bs[kk][j] = v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k4 = 0; k4 < BK; k4 += 4) {
+        double af[MT], bf[NT];
+#pragma unroll
+        for (int mi = 0; mi < MT; ++mi) af[mi] = As[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni) bf[ni] = Bs[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
+#pragma unroll
+        for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
+      }
+      __syncthreads();
+    }
+  }
+  double* __restrict__ C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
+  const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = row0 + wm * WM + mi * 8 + (lane >> 2);
+        const int c = col0 + wn * WN + ni * 8 + 2 * (lane & 3) + e;
+        if (r < J.m && c < J.n) {
+          const long long idx = r + (long long)c * J.ldc;
+          C[idx] = accum ? C[idx] + acc[mi][ni][e] : acc[mi][ni][e];
+        }
+      }
+}
+
+// complex (interleaved re,im): products split into real DMMAs,
+// rr = Re*Re, ii = Im*Im, im = Re*Im + Im*Re;  C = (rr - ii) + i*im
+template <int BM, int BN, int BK>
+__global__ void __launch_bounds__(kGemmThreads) grouped_gemm_z64(const GemmTerm* __restrict__ terms,
+                                                                 const GemmJob* __restrict__ jobs,
+                                                                 const GemmTile* __restrict__ tiles, Bases bases) {
+  constexpr int PAD = 4;
+  __shared__ double Ar[BK][BM + PAD], Ai[BK][BM + PAD];
+  __shared__ double Br[BK][BN + PAD], Bi[BK][BN + PAD];
+  const GemmTile t = tiles[blockIdx.x];
+  const GemmJob J = jobs[t.job];
+  const int row0 = t.tm * BM, col0 = t.tn * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
+  double rr[MT][NT][2], ii[MT][NT][2], im[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) rr[i][j][e] = ii[i][j][e] = im[i][j][e] = 0.0;
+
+  for (int ti = 0; ti < J.nt; ++ti) {
+    const GemmTerm T = terms[J.t0 + ti];
+    const double2* __restrict__ A = static_cast<const double2*>(bases.p[T.abuf]) + T.aoff;
+    const double2* __restrict__ B = static_cast<const double2*>(bases.p[T.bbuf]) + T.boff;
+    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
+    const double ca = (T.flags & TF_CA) ? -1.0 : 1.0, cb = (T.flags & TF_CB) ? -1.0 : 1.0;
+    for (int k0 = 0; k0 < T.k; k0 += BK) {
+      for (int e = tid; e < BM * BK; e += kGemmThreads) {
+        int i, kk;
+        if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
+        const int gi = row0 + i, gk = k0 + kk;
+        double2 v = make_double2(0.0, 0.0);
+        if (gi < J.m && gk < T.k) v = ta ? A[gk + (long long)gi * T.lda] : A[gi + (long long)gk * T.lda];
+        v.y *= ca;
+        Ar[kk][i] = v.x * T.ar - v.y * T.ai;
+        Ai[kk][i] = v.x * T.ai + v.y * T.ar;
+      }
+      for (int e = tid; e < BK * BN; e += kGemmThreads) {
+        int j, kk;
+        if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+        const int gj = col0 + j, gk = k0 + kk;
+        double2 v = make_double2(0.0, 0.0);
+        if (gj < J.n && gk < T.k) v = tb ? B[gj + (long long)gk * T.ldb] : B[gk + (long long)gj * T.ldb];
+        Br[kk][j] = v.x;
+        Bi[kk][j] = v.y * cb;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k4 = 0; k4 < BK; k4 += 4) {
+        double ar[MT], ai[MT], br[NT], bi[NT];
+#pragma unroll
+        for (int mi = 0; mi < MT; ++mi) {
+          ar[mi] = Ar[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
+          ai[mi] = Ai[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
+        }
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni) {
+          br[ni] = Br[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
+          bi[ni] = Bi[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
+        }
+#pragma unroll
+        for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < NT; ++ni) {
+            dmma884(rr[mi][ni][0], rr[mi][ni][1], ar[mi], br[ni]);
+            dmma884(ii[mi][ni][0], ii[mi][ni][1], ai[mi], bi[ni]);
+            dmma884(im[mi][ni][0], im[mi][ni][1], ar[mi], bi[ni]);
+            dmma884(im[mi][ni][0], im[mi][ni][1], ai[mi], br[ni]);
+          }
+      }
+      __syncthreads();
+    }
+  }
+  double2* __restrict__ C = static_cast<double2*>(bases.p[J.cbuf]) + J.coff;
+  const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = row0 + wm * WM + mi * 8 + (lane >> 2);
+        const int c = col0 + wn * WN + ni * 8 + 2 * (lane & 3) + e;
+        if (r < J.m && c < J.n) {
+          const long long idx = r + (long long)c * J.ldc;
+          double2 v = make_double2(rr[mi][ni][e] - ii[mi][ni][e], im[mi][ni][e]);
+          if (accum) { double2 o = C[idx]; v.x += o.x; v.y += o.y; }
+          C[idx] = v;
+        }
+      }
+}
+
+constexpr int kRealBM = 64, kRealBN = 64, kRealBK = 16;
+constexpr int kCplxBM = 32, kCplxBN = 32, kCplxBK = 16;
+
+int gemm_tile_m(bool cplx, int /*prec*/) { return cplx ? kCplxBM : kRealBM; }
+int gemm_tile_n(bool cplx, int /*prec*/) { return cplx ? kCplxBN : kRealBN; }
+
+void launch_grouped_gemm_tf32x3(bool cplx, const GemmTerm* terms, const GemmJob* jobs, const GemmTile* tiles,
+                                int ntiles, const Bases& b, cudaStream_t s);
+
+void launch_grouped_gemm(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const GemmTile* tiles,
+                         int ntiles, const Bases& b, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  if (prec == PREC_TF32X3) { launch_grouped_gemm_tf32x3(cplx, terms, jobs, tiles, ntiles, b, s); return; }
+  if (cplx)
+    grouped_gemm_z64<kCplxBM, kCplxBN, kCplxBK><<<ntiles, kGemmThreads, 0, s>>>(terms, jobs, tiles, b);
+  else
+    grouped_gemm_f64<kRealBM, kRealBN, kRealBK><<<ntiles, kGemmThreads, 0, s>>>(terms, jobs, tiles, b);
+}
+
+// --------------------------------------------------------------------------
+// block utilities
+template <bool CPLX>
+__global__ void seg_axpy_kernel(void* y, const void* x, const Seg* segs) {
+  const Seg sg = segs[blockIdx.x];
+  const long long stride = (long long)blockDim.x * gridDim.y;
+  for (long long i = (long long)blockIdx.y * blockDim.x + threadIdx.x; i < sg.n; i += stride) {
+    if (CPLX) {
+      const double2 v = static_cast<const double2*>(x)[sg.soff + i];
+      double2& o = static_cast<double2*>(y)[sg.doff + i];
+      o.x += v.x * sg.ar - v.y * sg.ai;
+      o.y += v.x * sg.ai + v.y * sg.ar;
+    } else {
+      static_cast<double*>(y)[sg.doff + i] += sg.ar * static_cast<const double*>(x)[sg.soff + i];
+    }
+  }
+}
+
+void launch_seg_axpy(bool cplx, void* y, const void* x, const Seg* segs, int nseg, cudaStream_t s) {
+  if (nseg <= 0) return;
+  dim3 grid(nseg, 16);
+  if (cplx) seg_axpy_kernel<true><<<grid, 256, 0, s>>>(y, x, segs);
+  else seg_axpy_kernel<false><<<grid, 256, 0, s>>>(y, x, segs);
+}
+
+template <class T>
+__global__ void block_transpose_kernel(T* dst, const T* src, const Transp* jobs) {
+  __shared__ T tile[32][33];
+  const Transp tj = jobs[blockIdx.x];
+  const int tr = (tj.rows + 31) / 32, tc = (tj.cols + 31) / 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int tIdx = blockIdx.y; tIdx < tr * tc; tIdx += gridDim.y) {
+    const int bi = (tIdx % tr) * 32, bj = (tIdx / tr) * 32;
+    for (int k = ty; k < 32; k += 8) {
+      const int r = bi + tx, c = bj + k;
+      if (r < tj.rows && c < tj.cols) tile[k][tx] = src[tj.soff + r + (long long)c * tj.rows];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+      const int r = bj + tx, c = bi + k;  // dst is cols x rows
+      if (r < tj.cols && c < tj.rows) dst[tj.doff + r + (long long)c * tj.cols] = tile[tx][k];
+    }
+    __syncthreads();
+  }
+}
+
+void launch_block_transpose(bool cplx, void* dst, const void* src, const Transp* t, int nt, cudaStream_t s) {
+  if (nt <= 0) return;
+  dim3 grid(nt, 32);
+  if (cplx) block_transpose_kernel<double2><<<grid, 256, 0, s>>>((double2*)dst, (const double2*)src, t);
+  else block_transpose_kernel<double><<<grid, 256, 0, s>>>((double*)dst, (const double*)src, t);
+}
+
+template <bool CPLX>
+__global__ void fuse_fill_kernel(void* data, const FuseFill* f) {
+  const FuseFill ff = f[blockIdx.x];
+  const long long plane = (long long)ff.d0 * ff.d1;
+  for (long long e = threadIdx.x; e < plane; e += blockDim.x) {
+    const int a = (int)(e % ff.d0), b = (int)(e / ff.d0);
+    const long long idx = ff.off + a + (long long)b * ff.d0 + (long long)(ff.pos + b * ff.d0 + a) * plane;
+    if (CPLX) static_cast<double2*>(data)[idx] = make_double2(1.0, 0.0);
+    else static_cast<double*>(data)[idx] = 1.0;
+  }
+}
+
+void launch_fuse_fill(bool cplx, void* data, const FuseFill* f, int nf, cudaStream_t s) {
+  if (nf <= 0) return;
+  if (cplx) fuse_fill_kernel<true><<<nf, 256, 0, s>>>(data, f);
+  else fuse_fill_kernel<false><<<nf, 256, 0, s>>>(data, f);
+}
+
+template <bool CPLX>
+__global__ void gather_kernel(void* dst, const void* src, const double* w, const int* perm, const Gather* g) {
+  const Gather G = g[blockIdx.x];
+  const long long total = (long long)G.rows * G.kept;
+  for (long long e = (long long)blockIdx.y * blockDim.x + threadIdx.x; e < total; e += (long long)blockDim.x * gridDim.y) {
+    const int r = (int)(e % G.rows), c = (int)(e / G.rows);
+    const double wv = w[G.woff + c];
+    double sc = 1.0;
+    if (G.p != 0.0) sc = (wv > 0.0) ? pow(wv, G.p) : 0.0;
+    const long long si = G.soff + r + (long long)perm[G.poff + c] * G.lds;
+    if (CPLX) {
+      double2 v = static_cast<const double2*>(src)[si];
+      if (G.conj) v.y = -v.y;
+      v.x *= sc; v.y *= sc;
+      static_cast<double2*>(dst)[G.doff + e] = v;
+    } else {
+      static_cast<double*>(dst)[G.doff + e] = static_cast<const double*>(src)[si] * sc;
+    }
+  }
+}
+
+void launch_gather(bool cplx, void* dst, const void* src, const double* w, const int* perm, const Gather* g, int ng,
+                   cudaStream_t s) {
+  if (ng <= 0) return;
+  dim3 grid(ng, 8);
+  if (cplx) gather_kernel<true><<<grid, 256, 0, s>>>(dst, src, w, perm, g);
+  else gather_kernel<false><<<grid, 256, 0, s>>>(dst, src, w, perm, g);
+}
+
+template <bool CPLX>
+__global__ void scale_kernel(void* x, double ar, double ai, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {
+    if (CPLX) {
+      const double2 v = static_cast<double2*>(x)[i];
+      static_cast<double2*>(x)[i] = make_double2(v.x * ar - v.y * ai, v.x * ai + v.y * ar);
+    } else {
+      static_cast<double*>(x)[i] *= ar;
+    }
+  }
+}
+
+void launch_scale(bool cplx, void* x, double ar, double ai, long long n, cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)min((n + 255) / 256, 148LL * 8);
+  if (cplx) scale_kernel<true><<<blocks, 256, 0, s>>>(x, ar, ai, n);
+  else scale_kernel<false><<<blocks, 256, 0, s>>>(x, ar, ai, n);
+}
+
+template <bool CPLX>
+__global__ void fill_kernel(void* x, double vr, double vi, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {
+    if (CPLX) static_cast<double2*>(x)[i] = make_double2(vr, vi);
+    else static_cast<double*>(x)[i] = vr;
+  }
+}
+
+void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)min((n + 255) / 256, 148LL * 8);
+  if (cplx) fill_kernel<true><<<blocks, 256, 0, s>>>(x, vr, vi, n);
+  else fill_kernel<false><<<blocks, 256, 0, s>>>(x, vr, vi, n);
+}
+
+template <bool CPLX>
+__global__ void lanczos_scalar_kernel(int op, const void* dot, const double* beta_prev, void* out) {
+  const double re = CPLX ? static_cast<const double2*>(dot)[0].x : static_cast<const double*>(dot)[0];
+  if (op == 0) {
+    if (CPLX) {
+      static_cast<double2*>(out)[0] = make_double2(beta_prev[0], 0.0);
+      static_cast<double2*>(out)[1] = make_double2(re, 0.0);
+    } else {
+      static_cast<double*>(out)[0] = beta_prev[0];
+      static_cast<double*>(out)[1] = re;
+    }
+  } else {
+    static_cast<double*>(out)[0] = sqrt(fabs(re));
+  }
+}
+
+void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s) {
+  if (cplx) lanczos_scalar_kernel<true><<<1, 1, 0, s>>>(op, dot, beta_prev, out);
+  else lanczos_scalar_kernel<false><<<1, 1, 0, s>>>(op, dot, beta_prev, out);
+}
+
+// --------------------------------------------------------------------------
+// Krylov vector kernels
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool CPLX>
+__global__ void multi_dot_partial(const void* V, long long ldv, int nv, const void* x, long long n, double* partial) {
+  __shared__ double red[2][32];
+  const long long per = (n + gridDim.x - 1) / gridDim.x;
+  const long long lo = per * blockIdx.x, hi = min(n, lo + per);
+  for (int j = 0; j < nv; ++j) {
+    double sr = 0.0, si = 0.0;
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      if (CPLX) {
+        const double2 a = static_cast<const double2*>(V)[j * ldv + i];
+        const double2 b = static_cast<const double2*>(x)[i];
+        sr += a.x * b.x + a.y * b.y;  // conj(a) * b
+        si += a.x * b.y - a.y * b.x;
+      } else {
+        sr += static_cast<const double*>(V)[j * ldv + i] * static_cast<const double*>(x)[i];
+      }
+    }
+    sr = warp_sum(sr);
+    if (CPLX) si = warp_sum(si);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int nw = blockDim.x >> 5;
+      double a = (l < nw) ? red[0][l] : 0.0, b = (l < nw) ? red[1][l] : 0.0;
+      a = warp_sum(a);
+      if (CPLX) b = warp_sum(b);
+      if (l == 0) {
+        partial[(blockIdx.x * (long long)nv + j) * 2 + 0] = a;
+        partial[(blockIdx.x * (long long)nv + j) * 2 + 1] = b;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <bool CPLX>
+__global__ void multi_dot_final(const double* partial, int npart, int nv, void* out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nv) return;
+  double a = 0.0, b = 0.0;
+  for (int p = 0; p < npart; ++p) {
+    a += partial[(p * (long long)nv + j) * 2 + 0];
+    b += partial[(p * (long long)nv + j) * 2 + 1];
+  }
+  if (CPLX) static_cast<double2*>(out)[j] = make_double2(a, b);
+  else static_cast<double*>(out)[j] = a;
+}
+
+void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n, double* partial,
+                      int npart, void* out, cudaStream_t s) {
+  if (nv <= 0) return;
+  if (cplx) {
+    multi_dot_partial<true><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
+    multi_dot_final<true><<<(nv + 127) / 128, 128, 0, s>>>(partial, npart, nv, out);
+  } else {
+    multi_dot_partial<false><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
+    multi_dot_final<false><<<(nv + 127) / 128, 128, 0, s>>>(partial, npart, nv, out);
+  }
+}
+
+template <bool CPLX>
+__global__ void multi_axpy_kernel(void* x, const void* V, long long ldv, int nv, const void* c, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {
+    if (CPLX) {
+      double2 acc = static_cast<double2*>(x)[i];
+      for (int j = 0; j < nv; ++j) {
+        const double2 cj = static_cast<const double2*>(c)[j];
+        const double2 v = static_cast<const double2*>(V)[j * ldv + i];
+        acc.x -= cj.x * v.x - cj.y * v.y;
+        acc.y -= cj.x * v.y + cj.y * v.x;
+      }
+      static_cast<double2*>(x)[i] = acc;
+    } else {
+      double acc = static_cast<double*>(x)[i];
+      for (int j = 0; j < nv; ++j) acc -= static_cast<const double*>(c)[j] * static_cast<const double*>(V)[j * ldv + i];
+      static_cast<double*>(x)[i] = acc;
+    }
+  }
+}
+
+void launch_multi_axpy(bool cplx, void* x, const void* V, long long ldv, int nv, const void* c, long long n,
+                       cudaStream_t s) {
+  if (nv <= 0 || n <= 0) return;
+  const int blocks = (int)min((n + 255) / 256, 148LL * 8);
+  if (cplx) multi_axpy_kernel<true><<<blocks, 256, 0, s>>>(x, V, ldv, nv, c, n);
+  else multi_axpy_kernel<false><<<blocks, 256, 0, s>>>(x, V, ldv, nv, c, n);
+}
+
+template <bool CPLX>
+__global__ void scale_inv_kernel(void* x, const double* scal, long long n) {
+  const double inv = 1.0 / scal[0];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {
+    if (CPLX) { double2 v = static_cast<double2*>(x)[i]; v.x *= inv; v.y *= inv; static_cast<double2*>(x)[i] = v; }
+    else static_cast<double*>(x)[i] *= inv;
+  }
+}
+
+void launch_scale_inv(bool cplx, void* x, const double* scal, long long n, cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)min((n + 255) / 256, 148LL * 8);
+  if (cplx) scale_inv_kernel<true><<<blocks, 256, 0, s>>>(x, scal, n);
+  else scale_inv_kernel<false><<<blocks, 256, 0, s>>>(x, scal, n);
+}
+
+template <bool CPLX>
+__global__ void lincomb_kernel(void* y, const void* V, long long ldv, int nv, const double* c, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {
+    if (CPLX) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int j = 0; j < nv; ++j) {
+        const double2 v = static_cast<const double2*>(V)[j * ldv + i];
+        acc.x += c[j] * v.x;
+        acc.y += c[j] * v.y;
+      }
+      static_cast<double2*>(y)[i] = acc;
+    } else {
+      double acc = 0.0;
+      for (int j = 0; j < nv; ++j) acc += c[j] * static_cast<const double*>(V)[j * ldv + i];
+      static_cast<double*>(y)[i] = acc;
+    }
+  }
+}
+
+void launch_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, const double* c_dev, long long n,
+                    cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)min((n + 255) / 256, 148LL * 8);
+  if (cplx) lincomb_kernel<true><<<blocks, 256, 0, s>>>(y, V, ldv, nv, c_dev, n);
+  else lincomb_kernel<false><<<blocks, 256, 0, s>>>(y, V, ldv, nv, c_dev, n);
+}
+
+}  // namespace sadmrg

@@ -1,0 +1,109 @@
+// kernels.cuh -- device task formats and launchers.
+//
+// Every contraction on the hot path (H_eff*psi, environment updates, the
+// projector products after the SVD) is lowered on the host to a list of dense
+// sector GEMMs; one launch executes a whole list.  Operands are addressed as
+// (base buffer id, element offset) so a plan built once per bond can be run on
+// any psi / output vector by swapping base pointers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+namespace sadmrg {
+
+enum TermFlags : int { TF_TA = 1, TF_CA = 2, TF_TB = 4, TF_CB = 8 };
+enum JobFlags : int { JF_ACCUM = 1 };   // C += sum(terms); otherwise C = sum(terms)
+enum Precision : int { PREC_FP64 = 0, PREC_TF32X3 = 1 };
+constexpr int kMaxBases = 8;
+
+struct GemmTerm {             // alpha * op(A) * op(B), A: m x k, B: k x n after op
+  long long aoff, boff;       // element offsets (elements of the scalar type)
+  int abuf, bbuf;             // base buffer ids
+  int lda, ldb, k, flags;
+  double ar, ai;              // alpha (imaginary part ignored for real data)
+};
+struct GemmJob {              // C (m x n, column-major, ldc) receives its terms
+  long long coff;
+  int cbuf, m, n, ldc;
+  int t0, nt, flags;
+};
+struct GemmTile {
+  int job, tm, tn;
+};
+struct Bases {
+  void* p[kMaxBases];
+};
+
+// Grouped GEMM over a tile table (one CTA per output tile, terms accumulated in
+// registers, no atomics: each output element is written by exactly one CTA).
+void launch_grouped_gemm(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs,
+                         const GemmTile* tiles, int ntiles, const Bases& b, cudaStream_t s);
+int gemm_tile_m(bool cplx, int prec);
+int gemm_tile_n(bool cplx, int prec);
+
+// ---- block utilities -------------------------------------------------------
+struct Seg {                  // y[doff + i] (+)= alpha * x[soff + i], i < n
+  long long doff, soff;
+  long long n;
+  double ar, ai;
+};
+void launch_seg_axpy(bool cplx, void* y, const void* x, const Seg* segs, int nseg, cudaStream_t s);
+
+struct Transp {               // dst (cols x rows) = src (rows x cols)^T
+  long long soff, doff;
+  int rows, cols;
+};
+void launch_block_transpose(bool cplx, void* dst, const void* src, const Transp* t, int nt, cudaStream_t s);
+
+struct FuseFill {             // identity embedding of a fuse block (d0,d1,d2): 1 at (a,b,pos+b*d0+a)
+  long long off;
+  int d0, d1, d2, pos;
+};
+void launch_fuse_fill(bool cplx, void* data, const FuseFill* f, int nf, cudaStream_t s);
+
+struct Gather {               // dst (rows x kept) = src[rows, perm[c]] * w[c]^p  (optionally conjugated)
+  long long soff, doff;       // soff: first row of the source column block (column 0)
+  int lds, rows, kept, conj;
+  long long woff;             // sorted singular values (double) offset
+  long long poff;             // offset into the column permutation
+  double p;                   // exponent applied to singular values (0 => none)
+};
+void launch_gather(bool cplx, void* dst, const void* src, const double* w, const int* perm, const Gather* g, int ng,
+                   cudaStream_t s);
+// x *= alpha (host scalar)
+void launch_scale(bool cplx, void* x, double ar, double ai, long long n, cudaStream_t s);
+// fill with a constant
+void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStream_t s);
+// tiny scalar helpers for the Krylov recurrence (single thread)
+//   op 0: coef[0] = beta_prev[0]; coef[1] = Re(dot[0])     (three-term recurrence)
+//   op 1: out[0] = sqrt(|Re(dot[0])|)                       (norm)
+void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s);
+
+// ---- Krylov vector operations ---------------------------------------------
+// out[j] = <V_j | x> (conjugated first argument), j < nv, deterministic
+void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n,
+                      double* partial, int npart, void* out, cudaStream_t s);
+// x -= sum_j c[j] V_j   (c read from device memory)
+void launch_multi_axpy(bool cplx, void* x, const void* V, long long ldv, int nv, const void* c, long long n,
+                       cudaStream_t s);
+// x *= 1 / scal[0].  scal is a device double.
+void launch_scale_inv(bool cplx, void* x, const double* scal, long long n, cudaStream_t s);
+// y = sum_j c[j] V_j (host coefficients, real)
+void launch_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, const double* c_dev, long long n,
+                    cudaStream_t s);
+
+// ---- one-sided Jacobi SVD of sector blocks --------------------------------
+struct SvdJob {
+  long long aoff;             // input block (m x n, lda = m) in the input buffer
+  long long woff;             // work: max(m,n) x min(m,n) columns being orthogonalised
+  long long voff;             // accumulated rotations: min(m,n) x min(m,n)
+  long long soff;             // singular values (double), min(m,n)
+  int m, n, trans;            // trans = 1 when m < n (work on A^H)
+};
+// Host driver: one launch per round of block pairs, one sync per sweep to test
+// convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
+int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
+                   int max_sweeps, cudaStream_t s);
+
+}  // namespace sadmrg

@@ -1,0 +1,741 @@
+// ops.cpp -- block-sparse operations of the reference, lowered to device task lists.
+#include "ops.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace sadmrg {
+
+Ctx::~Ctx() {
+  if (d_scalars) cudaFree(d_scalars);
+  if (d_partial) cudaFree(d_partial);
+}
+
+// ---------------------------------------------------------------------------
+// tensors
+template <class S>
+std::vector<Blk> blocks_of(const BTensor<S>& t) {
+  std::vector<Blk> v;
+  const int nb = t.st.nbond();
+  for (long i = 0; i < t.nten(); ++i) {
+    if (t.off[i] < 0) continue;
+    Blk b{};
+    b.idx = i;
+    int q[8], d[8];
+    t.st.block(i, q, d);
+    for (int k = 0; k < 4; ++k) { b.q[k] = k < nb ? q[k] : 0; b.d[k] = k < nb ? d[k] : 1; }
+    b.off = t.off[i];
+    v.push_back(b);
+  }
+  return v;
+}
+
+template <class S>
+BTensor<S> alloc_tensor(Ctx& c, const Struct& st, const std::vector<char>& present) {
+  BTensor<S> t;
+  t.st = st;
+  const long nt = st.nten();
+  t.off.assign(nt, -1);
+  long long n = 0;
+  for (long i = 0; i < nt; ++i)
+    if (present[i]) { t.off[i] = n; n += st.block_elems(i); }
+  t.nelem = n;
+  t.buf = std::make_shared<DevBuf>();
+  if (n > 0) {
+    t.buf->alloc(sizeof(S) * n, c.stream);
+    SADMRG_CUDA(cudaMemsetAsync(t.buf->get(), 0, sizeof(S) * n, c.stream));
+  }
+  return t;
+}
+
+template <class S>
+BTensor<S> clone(Ctx& c, const BTensor<S>& t) {
+  BTensor<S> r;
+  r.st = t.st;
+  r.off = t.off;
+  r.nelem = t.nelem;
+  r.host = t.host;
+  r.buf = std::make_shared<DevBuf>();
+  if (t.nelem > 0) {
+    r.buf->alloc(sizeof(S) * t.nelem, c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(r.buf->get(), t.buf->get(), sizeof(S) * t.nelem, cudaMemcpyDeviceToDevice, c.stream));
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+int GemmPlan::add_job(int stage, int cbuf, long long coff, int m, int n, int ldc, int flags) {
+  GemmJob j{};
+  j.coff = coff; j.cbuf = cbuf; j.m = m; j.n = n; j.ldc = ldc; j.flags = flags;
+  jobs.push_back(j);
+  job_terms.emplace_back();
+  job_stage.push_back(stage);
+  return (int)jobs.size() - 1;
+}
+
+void GemmPlan::add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
+                        double ar, double ai) {
+  GemmTerm t{};
+  t.aoff = aoff; t.boff = boff; t.abuf = abuf; t.bbuf = bbuf;
+  t.lda = std::max(lda, 1); t.ldb = std::max(ldb, 1); t.k = k; t.flags = flags; t.ar = ar; t.ai = ai;
+  job_terms[job].push_back(t);
+}
+
+void GemmPlan::finalize(Ctx& c, bool cplx) {
+  flat_terms.clear();
+  flops = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    jobs[j].t0 = (int)flat_terms.size();
+    jobs[j].nt = (int)job_terms[j].size();
+    for (auto& t : job_terms[j]) {
+      flat_terms.push_back(t);
+      flops += (cplx ? 8LL : 2LL) * jobs[j].m * (long long)jobs[j].n * t.k;
+    }
+  }
+  const int BM = gemm_tile_m(cplx, 0), BN = gemm_tile_n(cplx, 0);
+  std::vector<std::vector<std::pair<long long, GemmTile>>> per(nstage);
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    long long cost = 1;
+    for (auto& t : job_terms[j]) cost += t.k;
+    const int tm = (jobs[j].m + BM - 1) / BM, tn = (jobs[j].n + BN - 1) / BN;
+    for (int a = 0; a < tm; ++a)
+      for (int b = 0; b < tn; ++b) per[job_stage[j]].push_back({cost, GemmTile{(int)j, a, b}});
+  }
+  tiles.clear();
+  stage_tiles.assign(nstage + 1, 0);
+  for (int s = 0; s < nstage; ++s) {
+    stage_tiles[s] = (int)tiles.size();
+    // longest work first, so the long accumulation lists start early
+    std::stable_sort(per[s].begin(), per[s].end(),
+                     [](const std::pair<long long, GemmTile>& a, const std::pair<long long, GemmTile>& b) {
+                       return a.first > b.first;
+                     });
+    for (auto& p : per[s]) tiles.push_back(p.second);
+  }
+  stage_tiles[nstage] = (int)tiles.size();
+  const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size(),
+               bl = sizeof(GemmTile) * tiles.size();
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t total = al(bt) + al(bj) + al(bl) + 256;
+  std::vector<unsigned char> h(total, 0);
+  if (bt) std::memcpy(h.data(), flat_terms.data(), bt);
+  if (bj) std::memcpy(h.data() + al(bt), jobs.data(), bj);
+  if (bl) std::memcpy(h.data() + al(bt) + al(bj), tiles.data(), bl);
+  dev = std::make_shared<DevBuf>(total, c.stream);
+  SADMRG_CUDA(cudaMemcpyAsync(dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
+  unsigned char* base = dev->as<unsigned char>();
+  d_terms = reinterpret_cast<GemmTerm*>(base);
+  d_jobs = reinterpret_cast<GemmJob*>(base + al(bt));
+  d_tiles = reinterpret_cast<GemmTile*>(base + al(bt) + al(bj));
+  // the host copy must stay alive until the async copy completes
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi) const {
+  if (stage_hi < 0) stage_hi = nstage;
+  for (int s = stage_lo; s < stage_hi; ++s) {
+    const int nt = stage_tiles[s + 1] - stage_tiles[s];
+    if (nt <= 0) continue;
+    launch_grouped_gemm(cplx, prec, d_terms, d_jobs, d_tiles + stage_tiles[s], nt, b, c.stream);
+    ++c.launches;
+  }
+  SADMRG_CUDA(cudaGetLastError());
+  c.gemm_flops += flops;
+}
+
+namespace ops {
+
+template <class S> static constexpr bool kC = ScalarInfo<S>::cplx;
+template <class S> static double re_of(S x) { return real_of(x); }
+static double im_of(double) { return 0.0; }
+static double im_of(dcmplex x) { return x.imag(); }
+
+static Struct mk(Sym s, int ls, std::vector<Bond> b) { return Struct(s, ls, std::move(b)); }
+
+// Run a two-stage plan whose scratch products go to base 'sbuf'.
+template <class S>
+static void exec(Ctx& c, GemmPlan& p, Bases b, int sbuf) {
+  if (p.empty()) return;
+  p.finalize(c, kC<S>);
+  DevBuf scratch;
+  if (p.scratch_elems > 0) scratch.alloc(sizeof(S) * p.scratch_elems, c.stream);
+  b.p[sbuf] = scratch.get();
+  p.run(c, kC<S>, PREC_FP64, b);
+}
+
+// fuse(b1, b2): 3-leg identity embedding (src/block_tensor_inst.cpp:708-748)
+template <class S>
+BTensor<S> fuse(Ctx& c, const Bond& b1, const Bond& b2) {
+  Bond f = Bond::fuse(c.sym, b1, b2);
+  Struct st = mk(c.sym, 0, {b1, b2, f});
+  const long nt = st.nten();
+  std::vector<char> pres(nt, 0);
+  int q[8], d[8];
+  for (long i = 0; i < nt; ++i) pres[i] = st.block(i, q, d) ? 1 : 0;
+  BTensor<S> t = alloc_tensor<S>(c, st, pres);
+  std::vector<int> pos(f.nmom(), 0);
+  std::vector<FuseFill> ff;
+  for (long i = 0; i < nt; ++i) {
+    if (!pres[i]) continue;
+    st.block(i, q, d);
+    const int k = f.index_of(q[2]);
+    SADMRG_REQUIRE(pos[k] + d[0] * d[1] <= d[2], SADMRG_ERR_ARG, "fuse: fused dimension overflow");
+    ff.push_back(FuseFill{t.off[i], d[0], d[1], d[2], pos[k]});
+    pos[k] += d[0] * d[1];
+  }
+  if (!ff.empty()) {
+    DevBuf dff(sizeof(FuseFill) * ff.size(), c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(dff.get(), ff.data(), sizeof(FuseFill) * ff.size(), cudaMemcpyHostToDevice, c.stream));
+    launch_fuse_fill(kC<S>, t.data(), dff.as<FuseFill>(), (int)ff.size(), c.stream);
+    ++c.launches;
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return t;
+}
+
+// fuse_to_singlet: all-ones 2-leg blocks (src/block_tensor_inst.cpp:785-816)
+template <class S>
+BTensor<S> fuse_to_singlet(Ctx& c, const Bond& b1, const Bond& b2) {
+  Struct st = mk(c.sym, 0, {b1, b2});
+  const int n1 = b1.nmom(), n2 = b2.nmom();
+  std::vector<char> pres(st.nten(), 0);
+  for (int j = 0; j < n2; ++j)
+    for (int i = 0; i < n1; ++i) {
+      const bool ok = (c.sym == Sym::SU2) ? (b1.q[i] == b2.q[j]) : (b1.q[i] * b1.dir + b2.q[j] * b2.dir == 0);
+      if (ok) pres[i + j * n1] = 1;
+    }
+  BTensor<S> t = alloc_tensor<S>(c, st, pres);
+  launch_fill(kC<S>, t.data(), 1.0, 0.0, t.nelem, c.stream);
+  ++c.launches;
+  return t;
+}
+
+// overlap_initial (src/block_tensor_inst.cpp:1662-1788): out(a',b') = sum U^T conj(V)
+template <class S>
+BTensor<S> overlap_initial(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, int flag) {
+  SADMRG_REQUIRE(uu.st.bonds[flag] == vv.st.bonds[flag] && uu.st.bonds[1 - flag] == vv.st.bonds[1 - flag],
+                 SADMRG_ERR_ARG, "overlap_initial: inconsistent bonds");
+  Bond b1 = vv.st.bonds[2];
+  b1.invert();
+  Struct st = mk(c.sym, 0, {uu.st.bonds[2], b1});
+  auto U = blocks_of(uu), V = blocks_of(vv);
+  std::vector<std::vector<std::pair<int, int>>> contrib(st.nten());
+  for (size_t j = 0; j < U.size(); ++j)
+    for (size_t k = 0; k < V.size(); ++k) {
+      if (U[j].q[0] != V[k].q[0] || U[j].q[1] != V[k].q[1]) continue;
+      int lab[2] = {U[j].q[2], V[k].q[2]};
+      const long m = st.index(lab);
+      SADMRG_REQUIRE(m >= 0, SADMRG_ERR_ARG, "overlap_initial: output sector missing");
+      contrib[m].push_back({(int)j, (int)k});
+    }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  GemmPlan p;
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    const Blk& u0 = U[contrib[m][0].first];
+    const Blk& v0 = V[contrib[m][0].second];
+    const int job = p.add_job(1, 2, out.off[m], u0.d[2], v0.d[2], u0.d[2], 0);
+    for (auto& jk : contrib[m]) {
+      const Blk& u = U[jk.first];
+      const Blk& v = V[jk.second];
+      const int k = u.d[0] * u.d[1];
+      p.add_term(job, 0, u.off, k, 1, v.off, k, k, TF_TA | TF_CB, 1.0, 0.0);
+    }
+  }
+  Bases b{};
+  b.p[0] = uu.data(); b.p[1] = vv.data(); b.p[2] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+// overlap_transformation (src/block_tensor_inst.cpp:1791-1951): out = U^T op conj(V)
+template <class S>
+BTensor<S> overlap_transformation(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, const BTensor<S>& op, int flag) {
+  {
+    Bond a = op.st.bonds[0];
+    a.invert();
+    SADMRG_REQUIRE(uu.st.bonds[flag] == a && vv.st.bonds[flag] == op.st.bonds[1], SADMRG_ERR_ARG,
+                   "overlap_transformation: inconsistent bonds");
+  }
+  Bond b1 = vv.st.bonds[2];
+  b1.invert();
+  Struct st = mk(c.sym, 0, {uu.st.bonds[2], b1});
+  auto O = blocks_of(op), U = blocks_of(uu), V = blocks_of(vv);
+  struct Item { int x; long long voff; int vrows; };
+  std::vector<std::vector<Item>> contrib(st.nten());
+  GemmPlan p;
+  // stage 0: X = U^T op, once per (op block, uu block) pair that feeds an output
+  for (size_t k = 0; k < U.size(); ++k)
+    for (size_t j = 0; j < O.size(); ++j) {
+      const Blk& o = O[j];
+      const Blk& u = U[k];
+      if (o.q[0] != u.q[flag]) continue;
+      SADMRG_REQUIRE(u.d[1 - flag] == 1, SADMRG_ERR_ARG, "overlap_transformation: physical leg dim != 1");
+      int x = -1;
+      for (size_t l = 0; l < V.size(); ++l) {
+        const Blk& v = V[l];
+        if (o.q[1] != v.q[flag]) continue;
+        if (u.q[1 - flag] != v.q[1 - flag]) continue;
+        int lab[2] = {u.q[2], v.q[2]};
+        if (!st.allowed_labels(lab)) continue;
+        const long m = st.index(lab);
+        if (x < 0) {
+          const long long xo = p.alloc_scratch((long long)u.d[2] * o.d[1]);
+          x = p.add_job(0, 3, xo, u.d[2], o.d[1], u.d[2], 0);
+          p.add_term(x, 0, u.off, u.d[flag], 2, o.off, o.d[0], u.d[flag], TF_TA, 1.0, 0.0);
+        }
+        contrib[m].push_back(Item{x, v.off, v.d[flag]});
+      }
+    }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    int lab[8], dd[8];
+    st.block(m, lab, dd);
+    const int job = p.add_job(1, 4, out.off[m], dd[0], dd[1], dd[0], 0);
+    for (auto& it : contrib[m]) {
+      const GemmJob& x = p.jobs[it.x];
+      p.add_term(job, 3, x.coff, x.m, 1, it.voff, it.vrows, x.n, TF_CB, 1.0, 0.0);
+    }
+  }
+  Bases b{};
+  b.p[0] = uu.data(); b.p[1] = vv.data(); b.p[2] = op.data(); b.p[4] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+// operator_transformation (src/block_tensor_inst.cpp:1472-1658): out(a',c,b') = fac U^T op conj(V)
+template <class S>
+BTensor<S> operator_transformation(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, const BTensor<S>& op, int flag) {
+  {
+    Bond a = op.st.bonds[0];
+    a.invert();
+    SADMRG_REQUIRE(uu.st.bonds[flag] == a && vv.st.bonds[flag] == op.st.bonds[2], SADMRG_ERR_ARG,
+                   "operator_transformation: inconsistent bonds");
+  }
+  Bond b2 = vv.st.bonds[2];
+  b2.invert();
+  Struct st = mk(c.sym, 0, {uu.st.bonds[2], op.st.bonds[1], b2});
+  auto O = blocks_of(op), U = blocks_of(uu), V = blocks_of(vv);
+  struct Item { int x; long long voff; int vrows; double fac; };
+  std::vector<std::vector<Item>> contrib(st.nten());
+  GemmPlan p;
+  for (size_t k = 0; k < U.size(); ++k)
+    for (size_t j = 0; j < O.size(); ++j) {
+      const Blk& o = O[j];
+      const Blk& u = U[k];
+      if (o.q[0] != u.q[flag]) continue;
+      SADMRG_REQUIRE(u.d[1 - flag] == 1 && o.d[1] == 1, SADMRG_ERR_ARG,
+                     "operator_transformation: physical / channel leg dim != 1");
+      int x = -1;
+      for (size_t l = 0; l < V.size(); ++l) {
+        const Blk& v = V[l];
+        if (o.q[2] != v.q[flag]) continue;
+        if (u.q[1 - flag] != v.q[1 - flag]) continue;
+        int lab[3] = {u.q[2], o.q[1], v.q[2]};
+        if (!st.allowed_labels(lab)) continue;
+        const long m = st.index(lab);
+        double fac = 1.0;
+        if (c.sym == Sym::SU2) {
+          fac = c.cgc->transformation(flag, u.q[2], o.q[1], v.q[2], u.q[flag], v.q[flag], u.q[1 - flag]);
+          if (std::fabs(fac) < 1e-8) continue;
+        }
+        if (x < 0) {
+          const long long xo = p.alloc_scratch((long long)u.d[2] * o.d[2]);
+          x = p.add_job(0, 3, xo, u.d[2], o.d[2], u.d[2], 0);
+          p.add_term(x, 0, u.off, u.d[flag], 2, o.off, o.d[0], u.d[flag], TF_TA, 1.0, 0.0);
+        }
+        contrib[m].push_back(Item{x, v.off, v.d[flag], fac});
+      }
+    }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    int lab[8], dd[8];
+    st.block(m, lab, dd);
+    const int job = p.add_job(1, 4, out.off[m], dd[0], dd[2], dd[0] * dd[1], 0);
+    for (auto& it : contrib[m]) {
+      const GemmJob& x = p.jobs[it.x];
+      p.add_term(job, 3, x.coff, x.m, 1, it.voff, it.vrows, x.n, TF_CB, it.fac, 0.0);
+    }
+  }
+  Bases b{};
+  b.p[0] = uu.data(); b.p[1] = vv.data(); b.p[2] = op.data(); b.p[4] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+// operator_pairup (src/block_tensor_inst.cpp:1954-2167): out(a',b') = fac op2 U^T op1 conj(V)
+template <class S>
+BTensor<S> operator_pairup(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, const BTensor<S>& op1,
+                           const BTensor<S>& op2, int flag) {
+  {
+    Bond a = op1.st.bonds[0];
+    a.invert();
+    Bond ch = op2.st.bonds[1];
+    if (c.sym == Sym::U1) ch.invert();
+    SADMRG_REQUIRE(uu.st.bonds[flag] == a && vv.st.bonds[flag] == op1.st.bonds[2] && op1.st.bonds[1] == ch,
+                   SADMRG_ERR_ARG, "operator_pairup: inconsistent bonds");
+    SADMRG_REQUIRE(!op2.host.empty(), SADMRG_ERR_STATE, "operator_pairup: site operator has no host copy");
+  }
+  Bond b1 = vv.st.bonds[2];
+  b1.invert();
+  Struct st = mk(c.sym, 0, {uu.st.bonds[2], b1});
+  auto O = blocks_of(op1), U = blocks_of(uu), V = blocks_of(vv);
+  // site operator blocks, including null ones (presence checked after matching)
+  struct SBlk { int q[3]; long long off; };
+  std::vector<SBlk> P;
+  {
+    int q[8], d[8];
+    for (long n = 0; n < op2.nten(); ++n)
+      if (op2.st.block(n, q, d)) P.push_back(SBlk{{q[0], q[1], q[2]}, op2.off[n]});
+  }
+  struct Item { int x; long long voff; int vrows; S alpha; };
+  std::vector<std::vector<Item>> contrib(st.nten());
+  GemmPlan p;
+  for (size_t k = 0; k < U.size(); ++k)
+    for (size_t j = 0; j < O.size(); ++j) {
+      const Blk& o = O[j];
+      const Blk& u = U[k];
+      if (o.q[0] != u.q[flag]) continue;
+      SADMRG_REQUIRE(u.d[1 - flag] == 1 && o.d[1] == 1, SADMRG_ERR_ARG, "operator_pairup: leg dim != 1");
+      int x = -1;
+      for (size_t l = 0; l < V.size(); ++l) {
+        const Blk& v = V[l];
+        if (o.q[2] != v.q[flag]) continue;
+        for (auto& s2 : P) {
+          if (s2.q[0] != u.q[1 - flag] || s2.q[2] != v.q[1 - flag] || s2.q[1] != o.q[1]) continue;
+          int lab[2] = {u.q[2], v.q[2]};
+          if (!st.allowed_labels(lab)) continue;
+          const long m = st.index(lab);
+          if (s2.off < 0) continue;
+          double fac = 1.0;
+          if (c.sym == Sym::SU2) {
+            fac = c.cgc->pairup(flag, u.q[2], u.q[flag], v.q[flag], o.q[1], s2.q[0], s2.q[2]);
+            if (std::fabs(fac) < 1e-8) continue;
+          }
+          if (x < 0) {
+            const long long xo = p.alloc_scratch((long long)u.d[2] * o.d[2]);
+            x = p.add_job(0, 3, xo, u.d[2], o.d[2], u.d[2], 0);
+            p.add_term(x, 0, u.off, u.d[flag], 2, o.off, o.d[0], u.d[flag], TF_TA, 1.0, 0.0);
+          }
+          const S alpha = S(fac) * op2.host[s2.off];
+          contrib[m].push_back(Item{x, v.off, v.d[flag], alpha});
+        }
+      }
+    }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    int lab[8], dd[8];
+    st.block(m, lab, dd);
+    const int job = p.add_job(1, 4, out.off[m], dd[0], dd[1], dd[0], 0);
+    for (auto& it : contrib[m]) {
+      const GemmJob& x = p.jobs[it.x];
+      p.add_term(job, 3, x.coff, x.m, 1, it.voff, it.vrows, x.n, TF_CB, re_of(it.alpha), im_of(it.alpha));
+    }
+  }
+  Bases b{};
+  b.p[0] = uu.data(); b.p[1] = vv.data(); b.p[2] = op1.data(); b.p[4] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+// operator_initial (src/block_tensor_inst.cpp:1283-1469): out(a',c,b') = fac op U^T conj(V)
+template <class S>
+BTensor<S> operator_initial(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, const BTensor<S>& op, int flag) {
+  {
+    Bond a = op.st.bonds[0];
+    a.invert();
+    SADMRG_REQUIRE(uu.st.bonds[1 - flag] == a && vv.st.bonds[1 - flag] == op.st.bonds[2], SADMRG_ERR_ARG,
+                   "operator_initial: inconsistent bonds");
+    SADMRG_REQUIRE(!op.host.empty(), SADMRG_ERR_STATE, "operator_initial: site operator has no host copy");
+  }
+  Bond b2 = vv.st.bonds[2];
+  b2.invert();
+  Struct st = mk(c.sym, 0, {uu.st.bonds[2], op.st.bonds[1], b2});
+  auto O = blocks_of(op), U = blocks_of(uu), V = blocks_of(vv);
+  struct Item { long long uoff, voff; int k; S alpha; };
+  std::vector<std::vector<Item>> contrib(st.nten());
+  for (size_t k = 0; k < U.size(); ++k)
+    for (size_t j = 0; j < O.size(); ++j) {
+      const Blk& o = O[j];
+      const Blk& u = U[k];
+      if (o.q[0] != u.q[1 - flag]) continue;
+      SADMRG_REQUIRE(o.d[0] * o.d[1] * o.d[2] == 1, SADMRG_ERR_ARG, "operator_initial: site operator block not 1x1x1");
+      for (size_t l = 0; l < V.size(); ++l) {
+        const Blk& v = V[l];
+        if (o.q[2] != v.q[1 - flag]) continue;
+        if (u.q[flag] != v.q[flag]) continue;
+        int lab[3] = {u.q[2], o.q[1], v.q[2]};
+        if (!st.allowed_labels(lab)) continue;
+        const long m = st.index(lab);
+        double fac = 1.0;
+        if (c.sym == Sym::SU2) {
+          fac = c.cgc->onsite(flag, u.q[2], o.q[1], v.q[2], u.q[flag], o.q[0], o.q[2]);
+          if (std::fabs(fac) < 1e-8) continue;
+        }
+        contrib[m].push_back(Item{u.off, v.off, u.d[0] * u.d[1], S(fac) * op.host[o.off]});
+      }
+    }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  GemmPlan p;
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    int lab[8], dd[8];
+    st.block(m, lab, dd);
+    const int job = p.add_job(1, 2, out.off[m], dd[0], dd[2], dd[0] * dd[1], 0);
+    for (auto& it : contrib[m])
+      p.add_term(job, 0, it.uoff, it.k, 1, it.voff, it.k, it.k, TF_TA | TF_CB, re_of(it.alpha), im_of(it.alpha));
+  }
+  Bases b{};
+  b.p[0] = uu.data(); b.p[1] = vv.data(); b.p[2] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+// generic contraction (src/block_tensor_inst.cpp:1046-1126) for a contracted
+// bond that is the first or the last of each operand (the shapes the sweep uses).
+template <class S>
+BTensor<S> contract(Ctx& c, const BTensor<S>& t1, int i1, const BTensor<S>& t2, int i2) {
+  const int n1 = t1.st.nbond(), n2 = t2.st.nbond();
+  SADMRG_REQUIRE((i1 == 0 || i1 == n1 - 1) && (i2 == 0 || i2 == n2 - 1), SADMRG_ERR_ARG,
+                 "contract: contracted bond must be first or last");
+  {
+    Bond b = t2.st.bonds[i2];
+    b.invert();
+    SADMRG_REQUIRE(t1.st.bonds[i1] == b, SADMRG_ERR_ARG, "contract: bonds cannot be contracted");
+  }
+  std::vector<Bond> bb;
+  for (int i = 0; i < n1 - 1; ++i) bb.push_back(t1.st.bonds[(i1 + 1 + i) % n1]);
+  for (int i = 0; i < n2 - 1; ++i) bb.push_back(t2.st.bonds[(i2 + 1 + i) % n2]);
+  Struct st = mk(c.sym, t1.st.locspin + t2.st.locspin, bb);
+  const Bond& cb = t1.st.bonds[i1];
+  struct Item { long long aoff, boff; int k; };
+  std::vector<std::vector<Item>> contrib(st.nten());
+  std::vector<int> rowsA(st.nten(), 0), colsB(st.nten(), 0);
+  int q[8], d[8], qa[8], qb[8];
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!st.block(m, q, d)) continue;
+    for (int k = 0; k < n1 - 1; ++k) qa[(i1 + 1 + k) % n1] = q[k];
+    for (int k = 0; k < n2 - 1; ++k) qb[(i2 + 1 + k) % n2] = q[k + n1 - 1];
+    for (int j = 0; j < cb.nmom(); ++j) {
+      qa[i1] = cb.q[j];
+      qb[i2] = cb.q[j];
+      if (!t1.st.allowed_labels(qa) || !t2.st.allowed_labels(qb)) continue;
+      const long ka = t1.st.index(qa), kb = t2.st.index(qb);
+      if (ka < 0 || kb < 0 || !t1.present(ka) || !t2.present(kb)) continue;
+      contrib[m].push_back(Item{t1.off[ka], t2.off[kb], cb.d[j]});
+    }
+  }
+  std::vector<char> pres(st.nten(), 0);
+  for (long m = 0; m < st.nten(); ++m) pres[m] = !contrib[m].empty();
+  BTensor<S> out = alloc_tensor<S>(c, st, pres);
+  GemmPlan p;
+  for (long m = 0; m < st.nten(); ++m) {
+    if (!pres[m]) continue;
+    st.block(m, q, d);
+    long long rows = 1, cols = 1;
+    for (int k = 0; k < n1 - 1; ++k) rows *= d[k];
+    for (int k = 0; k < n2 - 1; ++k) cols *= d[n1 - 1 + k];
+    const int job = p.add_job(1, 2, out.off[m], (int)rows, (int)cols, (int)rows, 0);
+    for (auto& it : contrib[m]) {
+      // A' = t1 with the contracted bond last (rows x k): transposed view when it is first
+      const int fa = (i1 == 0) ? TF_TA : 0;
+      const int lda = (i1 == 0) ? it.k : (int)rows;
+      const int fb = (i2 == 0) ? 0 : TF_TB;
+      const int ldb = (i2 == 0) ? it.k : (int)cols;
+      p.add_term(job, 0, it.aoff, lda, 1, it.boff, ldb, it.k, fa | fb, 1.0, 0.0);
+    }
+  }
+  Bases b{};
+  b.p[0] = t1.data(); b.p[1] = t2.data(); b.p[2] = out.data();
+  exec<S>(c, p, b, 3);
+  return out;
+}
+
+template <class S>
+void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha) {
+  if (src.null()) return;
+  if (dst.null()) {
+    dst = clone(c, src);
+    if (alpha != S(1)) scale(c, dst, alpha);
+    return;
+  }
+  SADMRG_REQUIRE(dst.st == src.st, SADMRG_ERR_ARG, "add_into: different structures");
+  bool same = true;
+  for (long i = 0; i < dst.nten(); ++i)
+    if (src.present(i) && !dst.present(i)) { same = false; break; }
+  BTensor<S> target;
+  std::vector<Seg> sd, ss;
+  if (!same) {
+    std::vector<char> pres(dst.nten(), 0);
+    for (long i = 0; i < dst.nten(); ++i) pres[i] = dst.present(i) || src.present(i);
+    target = alloc_tensor<S>(c, dst.st, pres);
+    for (long i = 0; i < dst.nten(); ++i)
+      if (dst.present(i)) sd.push_back(Seg{target.off[i], dst.off[i], dst.st.block_elems(i), 1.0, 0.0});
+  }
+  BTensor<S>& T = same ? dst : target;
+  for (long i = 0; i < src.nten(); ++i)
+    if (src.present(i)) ss.push_back(Seg{T.off[i], src.off[i], src.st.block_elems(i), re_of(alpha), im_of(alpha)});
+  DevBuf dsegs(sizeof(Seg) * (sd.size() + ss.size()) + 16, c.stream);
+  std::vector<Seg> all = sd;
+  all.insert(all.end(), ss.begin(), ss.end());
+  SADMRG_CUDA(cudaMemcpyAsync(dsegs.get(), all.data(), sizeof(Seg) * all.size(), cudaMemcpyHostToDevice, c.stream));
+  if (!sd.empty()) { launch_seg_axpy(kC<S>, T.data(), dst.data(), dsegs.as<Seg>(), (int)sd.size(), c.stream); ++c.launches; }
+  if (!ss.empty()) {
+    launch_seg_axpy(kC<S>, T.data(), src.data(), dsegs.as<Seg>() + sd.size(), (int)ss.size(), c.stream);
+    ++c.launches;
+  }
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  if (!same) dst = std::move(target);
+}
+
+template <class S>
+void scale(Ctx& c, BTensor<S>& t, S alpha) {
+  launch_scale(kC<S>, t.data(), re_of(alpha), im_of(alpha), t.nelem, c.stream);
+  ++c.launches;
+  if (!t.host.empty())
+    for (auto& x : t.host) x *= alpha;
+}
+
+template <class S>
+void take_conjugate(BTensor<S>& t, int bond) {
+  t.st.bonds[bond].invert();
+}
+
+// makeup_input_vector (src/block_tensor_inst.cpp:1231-1257)
+template <class S>
+void makeup_input_vector(Ctx& c, BTensor<S>& t) {
+  SADMRG_REQUIRE(t.st.nbond() == 2, SADMRG_ERR_ARG, "makeup_input_vector: not a 2-leg tensor");
+  const Bond &b0 = t.st.bonds[0], &b1 = t.st.bonds[1];
+  std::vector<char> pres(t.nten(), 0);
+  bool changed = false;
+  for (long i = 0; i < t.nten(); ++i) pres[i] = t.present(i);
+  for (int i = 0; i < b0.nmom(); ++i)
+    for (int j = 0; j < b1.nmom(); ++j)
+      if (b0.q[i] == b1.q[j] && !pres[i + (long)j * b0.nmom()]) { pres[i + (long)j * b0.nmom()] = 1; changed = true; }
+  if (!changed) return;
+  BTensor<S> n = alloc_tensor<S>(c, t.st, pres);
+  std::vector<Seg> sg;
+  for (long i = 0; i < t.nten(); ++i)
+    if (t.present(i)) sg.push_back(Seg{n.off[i], t.off[i], t.st.block_elems(i), 1.0, 0.0});
+  if (!sg.empty()) {
+    DevBuf d(sizeof(Seg) * sg.size(), c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(d.get(), sg.data(), sizeof(Seg) * sg.size(), cudaMemcpyHostToDevice, c.stream));
+    launch_seg_axpy(kC<S>, n.data(), t.data(), d.as<Seg>(), (int)sg.size(), c.stream);
+    ++c.launches;
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  t = std::move(n);
+}
+
+// left2right_vectran / right2left_vectran (src/block_tensor_inst.cpp:429-497)
+template <class S>
+static void vectran(Ctx& c, BTensor<S>& t, int ishift, int s0, int s1) {
+  SADMRG_REQUIRE(t.st.nbond() == 3, SADMRG_ERR_ARG, "vectran: not a 3-leg tensor");
+  Struct st1 = t.st.shifted(s0, s1);
+  std::vector<char> pres(st1.nten(), 0);
+  std::vector<std::pair<long, long>> map;
+  int q[8], d[8], q1[8];
+  for (long i = 0; i < t.nten(); ++i) {
+    if (!t.st.block(i, q, d) || !t.present(i)) continue;
+    for (int k = 0; k < 3; ++k) q1[(k + ishift) % 3] = q[k];
+    const long j = st1.index(q1);
+    if (j < 0) continue;
+    pres[j] = 1;
+    map.push_back({i, j});
+  }
+  if (c.sym == Sym::SU2) {
+    st1.bonds[0].dir = 1;
+    st1.bonds[1].dir = 1;
+    st1.bonds[2].dir = -1;
+  }
+  BTensor<S> n = alloc_tensor<S>(c, st1, pres);
+  std::vector<Transp> tr;
+  for (auto& ij : map) {
+    t.st.block(ij.first, q, d);
+    // Dense::shift(s0, s1): transpose of (B x A) with B = product of the first p = 3 - ishift dims
+    const int p = 3 - ishift;
+    long long B = 1, A = 1;
+    for (int k = 0; k < p; ++k) B *= d[k];
+    for (int k = p; k < 3; ++k) A *= d[k];
+    tr.push_back(Transp{t.off[ij.first], n.off[ij.second], (int)B, (int)A});
+  }
+  if (!tr.empty()) {
+    DevBuf dt(sizeof(Transp) * tr.size(), c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(dt.get(), tr.data(), sizeof(Transp) * tr.size(), cudaMemcpyHostToDevice, c.stream));
+    launch_block_transpose(kC<S>, n.data(), t.data(), dt.as<Transp>(), (int)tr.size(), c.stream);
+    ++c.launches;
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  t = std::move(n);
+}
+
+template <class S> void left2right_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 2, 1, 0); }
+template <class S> void right2left_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 1, 2, 0); }
+
+template <class S>
+BTensor<S> from_host(Ctx& c, const Struct& st, const std::vector<char>& present, const S* data) {
+  BTensor<S> t = alloc_tensor<S>(c, st, present);
+  if (t.nelem > 0 && data)
+    SADMRG_CUDA(cudaMemcpyAsync(t.data(), data, sizeof(S) * t.nelem, cudaMemcpyHostToDevice, c.stream));
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  return t;
+}
+
+template <class S>
+std::vector<S> to_host(Ctx& c, const BTensor<S>& t) {
+  std::vector<S> h(t.nelem);
+  if (t.nelem > 0)
+    SADMRG_CUDA(cudaMemcpyAsync(h.data(), t.data(), sizeof(S) * t.nelem, cudaMemcpyDeviceToHost, c.stream));
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  return h;
+}
+
+#define SADMRG_INST(S)                                                                                           \
+  template BTensor<S> fuse<S>(Ctx&, const Bond&, const Bond&);                                                   \
+  template BTensor<S> fuse_to_singlet<S>(Ctx&, const Bond&, const Bond&);                                        \
+  template BTensor<S> overlap_initial<S>(Ctx&, const BTensor<S>&, const BTensor<S>&, int);                       \
+  template BTensor<S> overlap_transformation<S>(Ctx&, const BTensor<S>&, const BTensor<S>&, const BTensor<S>&,   \
+                                                int);                                                            \
+  template BTensor<S> operator_initial<S>(Ctx&, const BTensor<S>&, const BTensor<S>&, const BTensor<S>&, int);   \
+  template BTensor<S> operator_transformation<S>(Ctx&, const BTensor<S>&, const BTensor<S>&, const BTensor<S>&,  \
+                                                 int);                                                           \
+  template BTensor<S> operator_pairup<S>(Ctx&, const BTensor<S>&, const BTensor<S>&, const BTensor<S>&,          \
+                                         const BTensor<S>&, int);                                                \
+  template BTensor<S> contract<S>(Ctx&, const BTensor<S>&, int, const BTensor<S>&, int);                         \
+  template void add_into<S>(Ctx&, BTensor<S>&, const BTensor<S>&, S);                                            \
+  template void scale<S>(Ctx&, BTensor<S>&, S);                                                                  \
+  template void take_conjugate<S>(BTensor<S>&, int);                                                             \
+  template void makeup_input_vector<S>(Ctx&, BTensor<S>&);                                                       \
+  template void left2right_vectran<S>(Ctx&, BTensor<S>&);                                                        \
+  template void right2left_vectran<S>(Ctx&, BTensor<S>&);                                                        \
+  template BTensor<S> from_host<S>(Ctx&, const Struct&, const std::vector<char>&, const S*);                     \
+  template std::vector<S> to_host<S>(Ctx&, const BTensor<S>&);
+
+SADMRG_INST(double)
+SADMRG_INST(dcmplex)
+
+}  // namespace ops
+
+template std::vector<Blk> blocks_of<double>(const BTensor<double>&);
+template std::vector<Blk> blocks_of<dcmplex>(const BTensor<dcmplex>&);
+template BTensor<double> alloc_tensor<double>(Ctx&, const Struct&, const std::vector<char>&);
+template BTensor<dcmplex> alloc_tensor<dcmplex>(Ctx&, const Struct&, const std::vector<char>&);
+template BTensor<double> clone<double>(Ctx&, const BTensor<double>&);
+template BTensor<dcmplex> clone<dcmplex>(Ctx&, const BTensor<dcmplex>&);
+
+}  // namespace sadmrg

@@ -1,0 +1,92 @@
+// tensor.hpp -- device-resident block-sparse tensors and the task-plan builder.
+//
+// A BTensor keeps the reference's block structure (Struct = bonds, directions,
+// locspin; a block is present or null) on the host and all present blocks in
+// one contiguous device buffer, in block-index order, each block column-major
+// with bond 0 fastest (the reference's Dense layout, src/dense_inst.cpp:28-45).
+// For SU(2) the blocks hold reduced matrix elements; the CGC blocks of the
+// reference are never materialised, because every CGC the hot path needs is a
+// standard one (make_cgc / identity / singlet) and its effect is a scalar
+// factor folded into the task (src/block_tensor_inst.cpp:1433-1441, 2268-2272).
+#pragma once
+#include <cuda_runtime.h>
+#include <memory>
+#include <vector>
+
+#include "cgc.hpp"
+#include "common.hpp"
+#include "kernels.cuh"
+#include "symmetry.hpp"
+
+namespace sadmrg {
+
+struct Ctx {
+  cudaStream_t stream = nullptr;
+  Sym sym = Sym::U1;
+  bool cplx = false;
+  int physpn = 1;
+  std::unique_ptr<CGCFactors> cgc;
+  double* d_scalars = nullptr;   // small device scratch for reductions
+  double* d_partial = nullptr;
+  int npart = 296;
+  long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
+  long long launches = 0;        // kernels launched by this context
+  ~Ctx();
+};
+
+template <class S>
+struct BTensor {
+  Struct st;
+  std::vector<long long> off;  // element offset of each block, -1 if null
+  long long nelem = 0;
+  std::shared_ptr<DevBuf> buf;
+  std::vector<S> host;         // host mirror, only kept for tiny local operators
+
+  bool null() const { return st.nbond() == 0; }
+  S* data() const { return buf ? buf->as<S>() : nullptr; }
+  bool present(long b) const { return b >= 0 && b < (long)off.size() && off[b] >= 0; }
+  long nten() const { return (long)off.size(); }
+};
+
+struct Blk {
+  long idx;
+  int q[4];
+  int d[4];
+  long long off;
+  long long rows() const { return (long long)d[0] * (d[1] > 0 ? d[1] : 1); }  // for 3-leg (d0*d1) x d2
+};
+
+// allowed and present blocks in block-index order
+template <class S> std::vector<Blk> blocks_of(const BTensor<S>& t);
+
+// allocate a tensor whose present blocks are flagged; zero-filled
+template <class S> BTensor<S> alloc_tensor(Ctx& c, const Struct& st, const std::vector<char>& present);
+template <class S> BTensor<S> clone(Ctx& c, const BTensor<S>& t);
+
+// A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.
+struct GemmPlan {
+  std::vector<std::vector<GemmTerm>> job_terms;
+  std::vector<GemmJob> jobs;
+  std::vector<int> job_stage;
+  long long scratch_elems = 0;
+  int nstage = 2;
+  // device copy
+  std::vector<GemmTile> tiles;
+  std::vector<int> stage_tiles;   // tile offsets per stage (size nstage+1)
+  std::vector<GemmTerm> flat_terms;
+  std::shared_ptr<DevBuf> dev;
+  GemmTerm* d_terms = nullptr;
+  GemmJob* d_jobs = nullptr;
+  GemmTile* d_tiles = nullptr;
+  long long flops = 0;            // algorithmic flops of one execution (real multiply-adds * 2)
+
+  int add_job(int stage, int cbuf, long long coff, int m, int n, int ldc, int flags);
+  void add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
+                double ar, double ai);
+  long long alloc_scratch(long long elems) { long long o = scratch_elems; scratch_elems += elems; return o; }
+  void finalize(Ctx& c, bool cplx);
+  void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1) const;
+  bool empty() const { return jobs.empty(); }
+};
+
+}  // namespace sadmrg

@@ -1,0 +1,306 @@
+"""sadmrg -- Python binding of the B200 two-site DMRG library (ctypes over the C ABI).
+
+The shared library ``libsadmrg_b200.so`` next to this file holds the sm_100a
+kernels and the host bookkeeping; this module only marshals numpy arrays across
+the ``extern "C"`` boundary declared in ``include/sadmrg.h``.  There is no
+fallback: if the library or a CUDA device is missing, calls raise.
+
+Block-sparse tensors cross the boundary as :class:`BlockTensorData` (the
+reference's BlockTensor: bonds with sector labels / dimensions, the present
+blocks by block index, and their column-major data concatenated in block order).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsadmrg_b200.so")
+
+SYM_U1, SYM_SU2 = 0, 1
+PREC_FP64, PREC_TF32X3 = 0, 1
+
+EXPORTED = [
+    "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
+    "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device",
+    "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
+    "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
+    "sadmrg_chain_sweep", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
+    "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
+]
+
+
+class TensorDesc(C.Structure):
+    _fields_ = [
+        ("nbond", C.c_int), ("locspin", C.c_int),
+        ("dir", C.POINTER(C.c_int)), ("nmom", C.POINTER(C.c_int)),
+        ("q", C.POINTER(C.c_int)), ("d", C.POINTER(C.c_int)),
+        ("nblocks", C.c_int), ("block_index", C.POINTER(C.c_longlong)),
+        ("data", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (once) and declare the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libsadmrg_b200.so not built at {path}; run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    vp, ip, dp, lp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_longlong)
+    td = C.POINTER(TensorDesc)
+    sig = {
+        "sadmrg_version": ([], C.c_int),
+        "sadmrg_create": ([C.c_int, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+        "sadmrg_destroy": ([vp], C.c_int),
+        "sadmrg_last_error": ([vp], C.c_char_p),
+        "sadmrg_heff_plan": ([vp, td, td, td, C.c_int, td, C.c_int, ip, ip], C.c_int),
+        "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
+        "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
+        "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
+        "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
+        "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
+        "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
+        "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
+        "sadmrg_chain_idmrg": ([vp, dp], C.c_int),
+        "sadmrg_chain_prepare_sweep": ([vp], C.c_int),
+        "sadmrg_chain_sweep": ([vp, dp], C.c_int),
+        "sadmrg_chain_bond": ([vp, C.c_int, C.c_int, ip, ip, ip], C.c_int),
+        "sadmrg_chain_stats": ([vp, dp, C.c_int], C.c_int),
+        "sadmrg_chain_set_tensor": ([vp, C.c_int, C.c_int, C.c_int, td], C.c_int),
+        "sadmrg_chain_stage_tensor": ([vp, C.c_int, C.c_int, C.c_int], C.c_int),
+        "sadmrg_chain_env_update": ([vp, C.c_int, C.c_int, C.c_int], C.c_int),
+        "sadmrg_staged_info": ([vp, C.c_int, ip, ip, ip, ip, lp], C.c_int),
+        "sadmrg_staged_read": ([vp, C.c_int, ip, ip, ip, ip, lp, vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+class SadmrgError(RuntimeError):
+    pass
+
+
+@dataclass
+class BlockTensorData:
+    """Host image of a BlockTensor: bonds, present blocks, concatenated data."""
+    dirs: List[int]
+    qs: List[List[int]]
+    ds: List[List[int]]
+    locspin: int
+    blocks: np.ndarray            # int64 block indices, ascending
+    data: np.ndarray              # float64 or complex128, all present blocks
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def nbond(self) -> int:
+        return len(self.dirs)
+
+    def block_labels(self, idx: int):
+        out = []
+        for b in range(self.nbond):
+            n = len(self.qs[b])
+            out.append(idx % n)
+            idx //= n
+        return out
+
+    def block_dims(self, idx: int):
+        sec = self.block_labels(idx)
+        return [self.ds[b][s] for b, s in enumerate(sec)]
+
+    def block_views(self):
+        """(block index, labels, column-major ndarray view) for every present block."""
+        off = 0
+        res = []
+        for bi in self.blocks:
+            sec = self.block_labels(int(bi))
+            dims = [self.ds[b][s] for b, s in enumerate(sec)]
+            n = int(np.prod(dims))
+            arr = self.data[off:off + n].reshape(dims[::-1]).transpose()
+            res.append((int(bi), [self.qs[b][s] for b, s in enumerate(sec)], arr))
+            off += n
+        return res
+
+    def desc(self) -> TensorDesc:
+        dirs = np.ascontiguousarray(self.dirs, dtype=np.int32)
+        nmom = np.ascontiguousarray([len(q) for q in self.qs], dtype=np.int32)
+        q = np.ascontiguousarray([x for qq in self.qs for x in qq], dtype=np.int32)
+        d = np.ascontiguousarray([x for dd in self.ds for x in dd], dtype=np.int32)
+        blocks = np.ascontiguousarray(self.blocks, dtype=np.int64)
+        data = np.ascontiguousarray(self.data)
+        self._keep = [dirs, nmom, q, d, blocks, data]
+        ip = C.POINTER(C.c_int)
+        return TensorDesc(self.nbond, int(self.locspin), dirs.ctypes.data_as(ip), nmom.ctypes.data_as(ip),
+                          q.ctypes.data_as(ip), d.ctypes.data_as(ip), len(blocks),
+                          blocks.ctypes.data_as(C.POINTER(C.c_longlong)), data.ctypes.data)
+
+
+class Handle:
+    """One device + one stream (sadmrg_create)."""
+
+    def __init__(self, sym: int = SYM_U1, cplx: bool = False, device: int = 0):
+        self.lib = load()
+        self.cplx = bool(cplx)
+        self.dtype = np.complex128 if cplx else np.float64
+        h = C.c_void_p()
+        rc = self.lib.sadmrg_create(int(sym), int(bool(cplx)), int(device), C.byref(h))
+        if rc != 0:
+            raise SadmrgError(f"sadmrg_create failed with status {rc}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sadmrg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.sadmrg_last_error(self.h)
+            raise SadmrgError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
+
+    # -- frozen two-site problem -------------------------------------------
+    def heff_plan(self, psi: BlockTensorData, hh_left: Optional[BlockTensorData],
+                  hh_right: Optional[BlockTensorData], ops: Sequence[BlockTensorData],
+                  terms: Sequence[tuple]):
+        self._psi_template = psi
+        d_psi = psi.desc()
+        d_hl = C.pointer(hh_left.desc()) if hh_left is not None else None
+        d_hr = C.pointer(hh_right.desc()) if hh_right is not None else None
+        arr = (TensorDesc * max(len(ops), 1))()
+        for i, o in enumerate(ops):
+            arr[i] = o.desc()
+        op1 = np.ascontiguousarray([t[0] for t in terms], dtype=np.int32)
+        op2 = np.ascontiguousarray([t[1] for t in terms], dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        rc = self.lib.sadmrg_heff_plan(self.h, C.byref(d_psi), d_hl, d_hr, len(ops), arr, len(terms),
+                                       op1.ctypes.data_as(ip), op2.ctypes.data_as(ip))
+        self._check(rc, "heff_plan")
+
+    def heff_info(self):
+        n = C.c_longlong()
+        fl, by = C.c_double(), C.c_double()
+        nt = C.c_int()
+        self._check(self.lib.sadmrg_heff_info(self.h, C.byref(n), C.byref(fl), C.byref(by), C.byref(nt)), "heff_info")
+        return {"n": n.value, "flops": fl.value, "bytes": by.value, "ntasks": nt.value}
+
+    def heff_apply(self, psi: np.ndarray, precision: int = PREC_FP64) -> np.ndarray:
+        x = np.ascontiguousarray(psi, dtype=self.dtype)
+        out = np.empty_like(x)
+        self._check(self.lib.sadmrg_heff_apply(self.h, x.ctypes.data, out.ctypes.data, int(precision)), "heff_apply")
+        return out
+
+    def heff_apply_device(self, psi_ptr: int, out_ptr: int, precision: int = PREC_FP64):
+        self._check(self.lib.sadmrg_heff_apply_device(self.h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
+                                                      int(precision)), "heff_apply_device")
+
+    def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
+        x = np.array(psi, dtype=self.dtype, copy=True)
+        e = C.c_double()
+        mv = C.c_int()
+        self._check(self.lib.sadmrg_heff_lanczos(self.h, x.ctypes.data, int(mlanc), int(precision), C.byref(e),
+                                                 C.byref(mv)), "heff_lanczos")
+        return e.value, x, mv.value
+
+    # -- SVD -------------------------------------------------------------------
+    def svd_truncate(self, psi: BlockTensorData, tu: BlockTensorData, tv: BlockTensorData, p1: float, p2: float,
+                     max_dcut: int):
+        kept = C.c_int()
+        dw = C.c_double()
+        a, b, c = psi.desc(), tu.desc(), tv.desc()
+        self._check(self.lib.sadmrg_svd_truncate(self.h, C.byref(a), C.byref(b), C.byref(c), float(p1), float(p2),
+                                                 int(max_dcut), C.byref(kept), C.byref(dw)), "svd_truncate")
+        return self.staged(0), self.staged(1), kept.value, dw.value
+
+    def staged(self, which: int) -> Optional[BlockTensorData]:
+        nb, ls, ns, nbl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ne = C.c_longlong()
+        self._check(self.lib.sadmrg_staged_info(self.h, int(which), C.byref(nb), C.byref(ls), C.byref(ns),
+                                                C.byref(nbl), C.byref(ne)), "staged_info")
+        if nb.value == 0:
+            return None
+        dirs = np.zeros(nb.value, np.int32)
+        nmom = np.zeros(nb.value, np.int32)
+        q = np.zeros(ns.value, np.int32)
+        d = np.zeros(ns.value, np.int32)
+        blocks = np.zeros(nbl.value, np.int64)
+        data = np.zeros(ne.value, self.dtype)
+        ip = C.POINTER(C.c_int)
+        self._check(self.lib.sadmrg_staged_read(self.h, int(which), dirs.ctypes.data_as(ip), nmom.ctypes.data_as(ip),
+                                                q.ctypes.data_as(ip), d.ctypes.data_as(ip),
+                                                blocks.ctypes.data_as(C.POINTER(C.c_longlong)), data.ctypes.data),
+                    "staged_read")
+        qs, ds, o = [], [], 0
+        for n in nmom:
+            qs.append([int(x) for x in q[o:o + n]])
+            ds.append([int(x) for x in d[o:o + n]])
+            o += n
+        return BlockTensorData([int(x) for x in dirs], qs, ds, ls.value, blocks, data)
+
+    # -- chain -----------------------------------------------------------------
+    def chain_create(self, lx: int, ly: int, bondd: int, physpn: int = 1, totspin: int = 0, open_bc: bool = True,
+                     J2: float = 0.0):
+        self._check(self.lib.sadmrg_chain_create(self.h, lx, ly, bondd, physpn, totspin, int(bool(open_bc)),
+                                                 float(J2)), "chain_create")
+
+    def chain_set_precision(self, prec: int):
+        self._check(self.lib.sadmrg_chain_set_precision(self.h, int(prec)), "chain_set_precision")
+
+    def chain_idmrg(self) -> float:
+        e = C.c_double()
+        self._check(self.lib.sadmrg_chain_idmrg(self.h, C.byref(e)), "chain_idmrg")
+        return e.value
+
+    def chain_prepare_sweep(self):
+        self._check(self.lib.sadmrg_chain_prepare_sweep(self.h), "chain_prepare_sweep")
+
+    def chain_sweep(self) -> float:
+        e = C.c_double()
+        self._check(self.lib.sadmrg_chain_sweep(self.h, C.byref(e)), "chain_sweep")
+        return e.value
+
+    def chain_bond(self, site: int):
+        cap = 4096
+        n = C.c_int()
+        q = np.zeros(cap, np.int32)
+        d = np.zeros(cap, np.int32)
+        ip = C.POINTER(C.c_int)
+        self._check(self.lib.sadmrg_chain_bond(self.h, int(site), cap, C.byref(n), q.ctypes.data_as(ip),
+                                               d.ctypes.data_as(ip)), "chain_bond")
+        return [(int(q[i]), int(d[i])) for i in range(n.value)]
+
+    def chain_stats(self):
+        out = np.zeros(9)
+        self._check(self.lib.sadmrg_chain_stats(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), 9), "chain_stats")
+        keys = ["lanczos_s", "env_s", "svd_s", "prep_s", "matvecs", "heff_flops", "gemm_flops", "launches",
+                "discarded"]
+        return dict(zip(keys, out.tolist()))
+
+    def chain_set_tensor(self, kind: int, site: int, k: int, t: Optional[BlockTensorData]):
+        d = C.byref(t.desc()) if t is not None else None
+        self._check(self.lib.sadmrg_chain_set_tensor(self.h, int(kind), int(site), int(k), d), "chain_set_tensor")
+
+    def chain_get_tensor(self, kind: int, site: int, k: int = 0) -> Optional[BlockTensorData]:
+        self._check(self.lib.sadmrg_chain_stage_tensor(self.h, int(kind), int(site), int(k)), "chain_stage_tensor")
+        return self.staged(0)
+
+    def chain_env_update(self, site: int, direction: int, real_env: bool):
+        self._check(self.lib.sadmrg_chain_env_update(self.h, int(site), int(direction), int(bool(real_env))),
+                    "chain_env_update")

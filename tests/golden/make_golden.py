@@ -1,0 +1,135 @@
+"""Generate the golden fixtures from the reference CPU build (oracle/_ref/ref_harness).
+
+Run in a container that has the reference sources (the harness is built by
+``make -C oracle``).  Writes small ``.npz`` files next to this script:
+
+* ``centre_<case>.npz``   -- the operands and results of one two-site step at
+  the chain centre, exactly as the reference computes them: environments before
+  and after ``prepare_site_operator_from_right``, psi, H_eff*psi, the Lanczos
+  energy and the SVD factors / singular values that follow.
+* ``sweeps_<case>.npz``   -- energies after iDMRG and after every sweep, and the
+  sector dimensions of every bond after every sweep.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+# name -> harness arguments
+CENTRE_CASES = {
+    "u1_real": ["-sym", "u1", "-cplx", "0", "-L", "12", "-d", "16", "-sweeps", "2"],
+    "su2_real": ["-sym", "su2", "-cplx", "0", "-L", "12", "-d", "16", "-sweeps", "2"],
+    "u1_cplx": ["-sym", "u1", "-cplx", "1", "-L", "12", "-d", "16", "-sweeps", "2"],
+    "su2_cplx": ["-sym", "su2", "-cplx", "1", "-L", "12", "-d", "16", "-sweeps", "2"],
+    "u1_j2": ["-sym", "u1", "-cplx", "0", "-L", "12", "-d", "16", "-sweeps", "2", "-J2", "0.5"],
+    "su2_ladder": ["-sym", "su2", "-cplx", "0", "-lx", "6", "-ly", "2", "-d", "16", "-sweeps", "2"],
+}
+SWEEP_CASES = {
+    "u1_L16_D32": ["-sym", "u1", "-L", "16", "-d", "32", "-sweeps", "3"],
+    "su2_L16_D32": ["-sym", "su2", "-L", "16", "-d", "32", "-sweeps", "3"],
+    "u1c_L12_D24": ["-sym", "u1", "-cplx", "1", "-L", "12", "-d", "24", "-sweeps", "2"],
+    "su2c_L12_D24": ["-sym", "su2", "-cplx", "1", "-L", "12", "-d", "24", "-sweeps", "2"],
+    "u1_j2_L16_D32": ["-sym", "u1", "-L", "16", "-d", "32", "-sweeps", "3", "-J2", "0.5"],
+    "su2_ladder_2x8_D32": ["-sym", "su2", "-lx", "8", "-ly", "2", "-d", "32", "-sweeps", "3"],
+    "u1_L8_periodic": ["-sym", "u1", "-L", "8", "-d", "32", "-sweeps", "2", "-open", "0"],
+    "su2_L12_periodic": ["-sym", "su2", "-L", "12", "-d", "64", "-sweeps", "2", "-open", "0"],
+    "u1_L32_D64": ["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "2"],
+}
+
+
+def read_tensor(dirpath: str, name: str, cplx: bool) -> dict:
+    meta = {}
+    blocks = []
+    bonds = []
+    with open(os.path.join(dirpath, name + ".txt")) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "nbond":
+                meta["nbond"], meta["locspin"], meta["nten"] = int(t[1]), int(t[3]), int(t[5])
+            elif t[0] == "bond":
+                qi, di = t.index("q"), t.index("d")
+                bonds.append((int(t[3]), [int(x) for x in t[qi + 1:di]], [int(x) for x in t[di + 1:]]))
+            elif t[0] == "block":
+                blocks.append(int(t[1]))
+    raw = np.fromfile(os.path.join(dirpath, name + ".bin"), dtype=np.complex128 if cplx else np.float64)
+    return {
+        "dirs": np.array([b[0] for b in bonds], np.int32),
+        "nmom": np.array([len(b[1]) for b in bonds], np.int32),
+        "q": np.array([x for b in bonds for x in b[1]], np.int32),
+        "d": np.array([x for b in bonds for x in b[2]], np.int32),
+        "locspin": np.int32(meta.get("locspin", 0)),
+        "blocks": np.array(blocks, np.int64),
+        "data": raw,
+    }
+
+
+def run(args, workdir):
+    out = subprocess.run([HARNESS] + args, cwd=workdir, capture_output=True, text=True, check=True)
+    return out.stdout
+
+
+def parse_sweeps(stdout: str):
+    e_idmrg = None
+    energies, bonds = [], {}
+    for line in stdout.splitlines():
+        t = line.split()
+        if not t:
+            continue
+        if t[0] == "IDMRG":
+            e_idmrg = float(t[2])
+        elif t[0] == "SWEEP":
+            energies.append(float(t[3]))
+        elif t[0] == "BONDS":
+            s, site = int(t[1]), int(t[3])
+            bonds.setdefault(s, {})[site] = [tuple(int(v) for v in x.split(":")) for x in t[4:]]
+    return e_idmrg, energies, bonds
+
+
+def main():
+    if not os.path.exists(HARNESS):
+        sys.exit("build the reference harness first: make -C oracle")
+    for name, args in CENTRE_CASES.items():
+        cplx = args[args.index("-cplx") + 1] == "1"
+        with tempfile.TemporaryDirectory() as wd:
+            dd = os.path.join(wd, "dump")
+            stdout = run(args + ["-dump", dd], wd)
+            e_idmrg, energies, _ = parse_sweeps(stdout)
+            meta = open(os.path.join(dd, "meta.txt")).read()
+            arrays = {}
+            for fn in sorted(os.listdir(dd)):
+                if fn.endswith(".txt") and fn != "meta.txt":
+                    tn = fn[:-4]
+                    for k, v in read_tensor(dd, tn, cplx).items():
+                        arrays[f"{tn}__{k}"] = v
+            arrays["meta"] = np.array(meta)
+            arrays["sweep_energies"] = np.array(energies)
+            np.savez_compressed(os.path.join(HERE, f"centre_{name}.npz"), **arrays)
+            print("wrote", name, len(arrays))
+    for name, args in SWEEP_CASES.items():
+        with tempfile.TemporaryDirectory() as wd:
+            stdout = run(args, wd)
+        e_idmrg, energies, bonds = parse_sweeps(stdout)
+        last = bonds[max(bonds)] if bonds else {}
+        sites = sorted(last)
+        flat = [f"{s}:" + ",".join(f"{q}x{d}" for q, d in last[s]) for s in sites]
+        np.savez_compressed(os.path.join(HERE, f"sweeps_{name}.npz"), args=np.array(" ".join(args)),
+                            e_idmrg=np.float64(e_idmrg), energies=np.array(energies), bonds=np.array(flat))
+        print("wrote", name, e_idmrg, energies)
+
+
+if __name__ == "__main__":
+    main()
