@@ -107,9 +107,21 @@ int sadmrg_chain_set_precision(sadmrg_handle* h, int precision);
 int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy);
 int sadmrg_chain_prepare_sweep(sadmrg_handle* h);
 int sadmrg_chain_sweep(sadmrg_handle* h, double* energy);
+/* DMRG::read_mps(bond_read) / save_mps2 checkpoint files (src/dmrg_inst.cpp:947-1079):
+ * uu-<ns>-<D>-<2S>-0-<site>.dat (bond structure, text) and .bin (block data, then
+ * SU(2) CGC blocks) in directory dir.  read_mps is followed by prepare_sweep. */
+int sadmrg_chain_read_mps(sadmrg_handle* h, const char* dir, int bond_read);
+int sadmrg_chain_save_mps(sadmrg_handle* h, const char* dir);
+/* Freeze the two-site problem at bond (il, il+1): psi = the current site tensors'
+ * product (DMRG::prepare_input_vector), the fused environments and the H_eff plan
+ * become the handle's heff plan (sadmrg_heff_*), psi is staged (which = 0).  If
+ * export_dir is not NULL or empty the problem is also written there, one
+ * <name>.txt (bonds and present blocks) + <name>.bin (data) pair per tensor. */
+int sadmrg_chain_freeze(sadmrg_handle* h, int il, const char* export_dir);
 /* sectors of bond 2 of site tensor uu[site]: labels and dimensions */
 int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d);
-/* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded] */
+/* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded,
+ *          near_ties (truncations whose cut split a pair of singular values equal to 1e-8)] */
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
 /* kind: 0 = uu[site], 1 = hh[site], 2 = opr[site][k] */
 int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t);

@@ -53,6 +53,8 @@ struct Opts {
   int D = 32, sec = 0, sweeps = 2, threads = 1, maxangm = 0, open = 1;
   double J2 = 0.0;
   std::string dump;  // directory: dump the centre two-site problem there
+  std::string save;  // directory: save_mps2 after iDMRG (checkpoint files)
+  std::string read;  // directory: read_mps + prepare_sweep instead of iDMRG
   int bench_heff = 0;  // time this many H*v calls on the centre problem
   int quiet = 1;
 };
@@ -159,16 +161,38 @@ static int run(const Opts& o) {
   chain.ww[0] = new double[wlen]();
 
   auto t0 = std::chrono::steady_clock::now();
-  mute();
-  chain.do_idmrg();
-  unmute();
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd))) cwd[0] = 0;
+  if (!o.read.empty()) {
+    // DMRG::read_mps + prepare_sweep (src/dmrg_inst.cpp:1031-1079, 808-854)
+    if (chdir(o.read.c_str()) != 0) { std::cerr << "cannot enter " << o.read << "\n"; return 3; }
+    mute();
+    bool ok = chain.read_mps(o.D);
+    if (ok) chain.prepare_sweep();
+    unmute();
+    if (chdir(cwd) != 0) return 3;
+    if (!ok) { std::cerr << "read_mps failed in " << o.read << "\n"; return 3; }
+  } else {
+    mute();
+    chain.do_idmrg();
+    unmute();
+  }
+  if (!o.save.empty()) {
+    mkdir(o.save.c_str(), 0755);
+    if (chdir(o.save.c_str()) != 0) return 3;
+    chain.save_mps2(0);
+    if (chdir(cwd) != 0) return 3;
+  }
   auto t1 = std::chrono::steady_clock::now();
   std::cout << std::setprecision(16) << "IDMRG E " << chain.get_enr() << " seconds "
             << std::chrono::duration<double>(t1 - t0).count() << "\n";
+  print_bonds(chain, "BONDS -1");
   for (int s = 0; s < o.sweeps; ++s) {
     auto a = std::chrono::steady_clock::now();
     mute();
+    if (chdir("/tmp") != 0) return 3;  // sweep() writes its checkpoint files to the working directory
     chain.sweep();
+    if (chdir(cwd) != 0) return 3;
     unmute();
     auto b = std::chrono::steady_clock::now();
     std::cout << std::setprecision(16) << "SWEEP " << s << " E " << chain.get_enr() << " seconds "
@@ -285,6 +309,8 @@ int main(int argc, char** argv) {
     else if (a == "-open") o.open = std::stoi(nxt());
     else if (a == "-J2") o.J2 = std::stod(nxt());
     else if (a == "-dump") o.dump = nxt();
+    else if (a == "-save") o.save = nxt();
+    else if (a == "-read") o.read = nxt();
     else if (a == "-bench_heff") o.bench_heff = std::stoi(nxt());
     else if (a == "-verbose") o.quiet = 0;
     else { std::cerr << "unknown option " << a << "\n"; return 2; }

@@ -286,6 +286,41 @@ int sadmrg_chain_sweep(sadmrg_handle* h, double* energy) {
   });
 }
 
+int sadmrg_chain_read_mps(sadmrg_handle* h, const char* dir, int bond_read) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(dir, SADMRG_ERR_ARG, "read_mps: null path");
+    SADMRG_REQUIRE(S_.chain->read_mps(dir, bond_read), SADMRG_ERR_ARG, "read_mps: checkpoint files missing");
+  });
+}
+
+int sadmrg_chain_save_mps(sadmrg_handle* h, const char* dir) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(dir, SADMRG_ERR_ARG, "save_mps: null path");
+    S_.chain->save_mps(dir);
+  });
+}
+
+int sadmrg_chain_freeze(sadmrg_handle* h, int il, const char* export_dir) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    Ctx& c = h->ctx;
+    BTensor<S> psi;
+    S_.heff = std::make_unique<HeffPlan<S>>(S_.chain->freeze(il, psi));
+    S_.io.alloc(sizeof(S) * 2 * std::max<long long>(S_.heff->n, 1), c.stream);
+    S_.staged[0] = std::move(psi);
+    if (export_dir && export_dir[0]) S_.chain->export_problem(il, S_.staged[0], export_dir);
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
 int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
@@ -307,9 +342,10 @@ int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     const Timers& t = S_.chain->timers;
-    const double v[9] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
-                         (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded};
-    for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
+    const double v[10] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
+                          (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded,
+                          (double)S_.chain->near_ties};
+    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
   });
 }
 

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <numeric>
 
 namespace sadmrg {
@@ -43,6 +45,25 @@ HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, con
     if (base[i] >= 0) cp(opl[i], base[i]);
 
   GemmPlan& p = H.plan;
+  const Struct& ps0 = psi.st;
+  auto same = [](const Bond& a, const Bond& b) { return a.q == b.q && a.d == b.d; };
+  SADMRG_REQUIRE(ps0.nbond() == 2, SADMRG_ERR_ARG, "heff: psi must have two bonds");
+  if (hl >= 0)
+    SADMRG_REQUIRE(hhL->st.nbond() == 2 && same(hhL->st.bonds[0], ps0.bonds[0]) && same(hhL->st.bonds[1], ps0.bonds[0]),
+                   SADMRG_ERR_ARG, "heff: left block Hamiltonian does not match psi");
+  if (hr >= 0)
+    SADMRG_REQUIRE(hhR->st.nbond() == 2 && same(hhR->st.bonds[0], ps0.bonds[1]) && same(hhR->st.bonds[1], ps0.bonds[1]),
+                   SADMRG_ERR_ARG, "heff: right block Hamiltonian does not match psi");
+  for (auto& t : terms) {
+    const BTensor<S>* a = opl[t.op1];
+    const BTensor<S>* b = opl[t.op2];
+    if (!a || !b || a->null() || b->null()) continue;
+    SADMRG_REQUIRE(a->st.nbond() == 3 && b->st.nbond() == 3 && same(a->st.bonds[0], ps0.bonds[0]) &&
+                       same(a->st.bonds[2], ps0.bonds[0]) && same(b->st.bonds[0], ps0.bonds[1]) &&
+                       same(b->st.bonds[2], ps0.bonds[1]) && a->st.bonds[1].q == b->st.bonds[1].q &&
+                       a->st.bonds[1].d == b->st.bonds[1].d,
+                   SADMRG_ERR_ARG, "heff: operator bonds do not match psi");
+  }
   const std::vector<Blk> P = blocks_of(psi);
   std::vector<int> job_of(psi.nten(), -1);
   for (auto& b : P) job_of[b.idx] = p.add_job(1, 1, b.off, b.d[0], b.d[1], b.d[0], 0);
@@ -442,6 +463,7 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   }
   const int ntot = (int)wsort.size();
   const int dcut = ntot > max_dcut ? max_dcut : ntot;
+  if (dcut < ntot && dcut > 0 && std::fabs(wsort[dcut - 1] - wsort[dcut]) <= 1e-8 * wsort[dcut - 1]) out.near_tie = true;
   std::vector<int> dim(nm1, 0);
   for (int k = 0; k < dcut; ++k) dim[isort[k]]++;
   std::vector<int> amom, bdim;
@@ -801,6 +823,9 @@ void Chain<S>::lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec) {
   HeffPlan<S> H = heff_plan(il, ir, vec);
   LanczosStats st = lanczos_solve<S>(c, H, vec.data(), mlanc, prec);
   gs_enr = st.energy;
+  if (std::getenv("SADMRG_VERBOSE"))
+    std::fprintf(stderr, "lanczos (%d,%d) E=%.15f matvecs=%d ov=%.3e n=%lld\n", il, ir, st.energy, st.matvecs,
+                 st.overlap, (long long)vec.nelem);
   timers.matvecs += st.matvecs;
   timers.heff_flops += (double)H.flops * st.matvecs;
   timers.lanczos += now_s() - t0;
@@ -819,6 +844,13 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   const double t0 = now_s();
   SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &ww);
   last_discarded = s.discarded_weight;
+  if (s.near_tie) ++near_ties;
+  if (std::getenv("SADMRG_VERBOSE")) {
+    std::fprintf(stderr, "svd (%d,%d) kept=%d dw=%.3e sectors:", il, ir, s.kept, s.discarded_weight);
+    const Bond& b = uu[il].st.bonds[2];
+    for (int k = 0; k < b.nmom(); ++k) std::fprintf(stderr, " %d:%d", b.q[k], b.d[k]);
+    std::fprintf(stderr, "\n");
+  }
   timers.svd += now_s() - t0;
 }
 
@@ -912,6 +944,146 @@ void Chain<S>::sweep() {
     lanczos_solve_eigenvector(i - 2, i - 1, vec);
     svd_step(vec, i - 2, i - 1, 1.0, 0.0);
   }
+}
+
+template <class S>
+bool Chain<S>::read_mps(const std::string& dir, int bond_read) {
+  for (int i = 0; i < ns; ++i) {
+    const std::string base = dir + "/uu-" + std::to_string(ns) + "-" + std::to_string(bond_read) + "-" +
+                             std::to_string(totspin) + "-0-" + std::to_string(i);
+    FILE* f = std::fopen((base + ".dat").c_str(), "r");
+    if (!f) return false;
+    int nb = 0, lc = 0;
+    std::vector<Bond> bonds;
+    bool ok = std::fscanf(f, "%d %d", &nb, &lc) == 2 && nb >= 1 && nb <= 4;
+    for (int b = 0; ok && b < nb; ++b) {
+      int dir_ = 0, nc = 0;
+      ok = std::fscanf(f, "%d %d", &dir_, &nc) == 2 && nc >= 1;
+      std::vector<int> q(nc), d(nc);
+      for (int k = 0; ok && k < nc; ++k) ok = std::fscanf(f, "%d", &q[k]) == 1;
+      for (int k = 0; ok && k < nc; ++k) ok = std::fscanf(f, "%d", &d[k]) == 1;
+      if (ok) bonds.push_back(Bond(dir_, q, d));
+    }
+    std::fclose(f);
+    SADMRG_REQUIRE(ok, SADMRG_ERR_ARG, "read_mps: malformed " + base + ".dat");
+    Struct st(c.sym, lc, bonds);
+    std::vector<char> pres(st.nten(), 0);
+    long long ndata = 0;
+    int q[8], d[8];
+    for (long b = 0; b < st.nten(); ++b)
+      if (st.block(b, q, d)) { pres[b] = 1; ndata += st.block_elems(b); }
+    std::vector<S> data(ndata);
+    FILE* fb = std::fopen((base + ".bin").c_str(), "rb");
+    if (!fb) return false;
+    const size_t got = std::fread(data.data(), sizeof(S), ndata, fb);
+    std::fclose(fb);
+    SADMRG_REQUIRE((long long)got == ndata, SADMRG_ERR_ARG, "read_mps: short " + base + ".bin");
+    uu[i] = ops::from_host<S>(c, st, pres, data.data());
+  }
+  return true;
+}
+
+template <class S>
+void Chain<S>::save_mps(const std::string& dir) const {
+  for (int i = 0; i < ns; ++i) {
+    const BTensor<S>& t = uu[i];
+    const std::string base = dir + "/uu-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
+                             std::to_string(totspin) + "-0-" + std::to_string(i);
+    FILE* f = std::fopen((base + ".dat").c_str(), "w");
+    SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "save_mps: cannot write " + base + ".dat");
+    std::fprintf(f, "%d\t%d\n", t.st.nbond(), t.st.locspin);
+    for (auto& b : t.st.bonds) {
+      std::fprintf(f, "%d\t%d\n", b.dir, b.nmom());
+      for (int k = 0; k < b.nmom(); ++k) std::fprintf(f, "%d\t", b.q[k]);
+      std::fprintf(f, "\n");
+      for (int k = 0; k < b.nmom(); ++k) std::fprintf(f, "%d\t", b.d[k]);
+      std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+    // data of the allowed blocks (null ones written as zeros), then the SU(2) CGC blocks
+    std::vector<S> h = ops::to_host<S>(c, t);
+    FILE* fb = std::fopen((base + ".bin").c_str(), "wb");
+    SADMRG_REQUIRE(fb, SADMRG_ERR_ARG, "save_mps: cannot write " + base + ".bin");
+    int q[8], d[8];
+    std::vector<double> cg;
+    for (long b = 0; b < t.nten(); ++b) {
+      if (!t.st.block(b, q, d)) continue;
+      const long long n = t.st.block_elems(b);
+      if (t.present(b)) std::fwrite(h.data() + t.off[b], sizeof(S), n, fb);
+      else { std::vector<S> z(n, S(0)); std::fwrite(z.data(), sizeof(S), n, fb); }
+      if (c.sym == Sym::SU2 && t.st.nbond() == 3) {
+        HDense cc;
+        cc.make_cgc(q[0], q[1], q[2]);
+        cg.insert(cg.end(), cc.v.begin(), cc.v.end());
+      }
+    }
+    if (!cg.empty()) std::fwrite(cg.data(), sizeof(double), cg.size(), fb);
+    std::fclose(fb);
+  }
+}
+
+template <class S>
+HeffPlan<S> Chain<S>::freeze(int il, BTensor<S>& psi) {
+  SADMRG_REQUIRE(il >= 1 && il + 2 < ns, SADMRG_ERR_ARG, "freeze: bond out of range");
+  const int ir = il + 1;
+  prepare_input_vector(il, ir, psi);
+  prepare_site_operator_from_left(il, false);
+  prepare_site_operator_from_right(ir, false);
+  return heff_plan(il, ir, psi);
+}
+
+template <class S>
+static void write_tensor(Ctx& c, const BTensor<S>& t, const std::string& base) {
+  FILE* f = std::fopen((base + ".txt").c_str(), "w");
+  SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "export: cannot write " + base);
+  std::fprintf(f, "nbond %d locspin %d nten %ld\n", t.st.nbond(), t.st.locspin, t.nten());
+  for (int b = 0; b < t.st.nbond(); ++b) {
+    const Bond& bd = t.st.bonds[b];
+    std::fprintf(f, "bond %d dir %d nmom %d q", b, bd.dir, bd.nmom());
+    for (int k = 0; k < bd.nmom(); ++k) std::fprintf(f, " %d", bd.q[k]);
+    std::fprintf(f, " d");
+    for (int k = 0; k < bd.nmom(); ++k) std::fprintf(f, " %d", bd.d[k]);
+    std::fprintf(f, "\n");
+  }
+  int q[8], d[8];
+  for (long i = 0; i < t.nten(); ++i) {
+    if (!t.present(i)) continue;
+    t.st.block(i, q, d);
+    std::fprintf(f, "block %ld q", i);
+    for (int b = 0; b < t.st.nbond(); ++b) std::fprintf(f, " %d", q[b]);
+    std::fprintf(f, " d");
+    for (int b = 0; b < t.st.nbond(); ++b) std::fprintf(f, " %d", d[b]);
+    std::fprintf(f, " off %lld n %lld\n", t.off[i], t.st.block_elems(i));
+  }
+  std::fclose(f);
+  std::vector<S> h = ops::to_host<S>(c, t);
+  FILE* fb = std::fopen((base + ".bin").c_str(), "wb");
+  SADMRG_REQUIRE(fb, SADMRG_ERR_ARG, "export: cannot write " + base);
+  if (!h.empty()) std::fwrite(h.data(), sizeof(S), h.size(), fb);
+  std::fclose(fb);
+}
+
+template <class S>
+void Chain<S>::export_problem(int il, const BTensor<S>& psi, const std::string& dir) const {
+  const int ir = il + 1;
+  write_tensor(c, psi, dir + "/psi");
+  if (!hh[il].null()) write_tensor(c, hh[il], dir + "/hh_il");
+  if (!hh[ir].null()) write_tensor(c, hh[ir], dir + "/hh_ir");
+  for (int k = 0; k < ns; ++k) {
+    if (k <= il && !opr[il][k].null()) write_tensor(c, opr[il][k], dir + "/opr_il_" + std::to_string(k));
+    if (k >= ir && !opr[ir][k].null()) write_tensor(c, opr[ir][k], dir + "/opr_ir_" + std::to_string(k));
+  }
+  FILE* f = std::fopen((dir + "/meta.txt").c_str(), "w");
+  SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "export: cannot write meta");
+  std::fprintf(f, "sym %d cplx %d ns %d lx %d ly %d D %d sec %d il %d ir %d J2 %.17g open 1 maxangm 0\n",
+               c.sym == Sym::SU2 ? 1 : 0, kCx<S> ? 1 : 0, ns, lx, ly, bondd, totspin, il, ir, coup[2]);
+  std::fprintf(f, "coup");
+  for (int k = 0; k <= ns / 2; ++k) std::fprintf(f, " %.17g", coup[k]);
+  std::fprintf(f, "\n");
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b)
+      if (hmap[a][b]) std::fprintf(f, "hmap %d %d %d\n", a, b, hmap[a][b]);
+  std::fclose(f);
 }
 
 template struct HeffPlan<double>;

@@ -60,6 +60,7 @@ struct SvdStats {
   int kept = 0;
   double discarded_weight = 0.0;
   int sweeps_max = 0;
+  bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative)
 };
 
 // BlockTensor::svd (src/block_tensor_inst.cpp:501-637)
@@ -90,6 +91,14 @@ class Chain {
   HeffPlan<S> heff_plan(int il, int ir, const BTensor<S>& vec);
   void lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec);
   void wavefunc_transformation(int i, int dir);
+  // DMRG::read_mps / save_mps2 checkpoint format (src/dmrg_inst.cpp:947-1079)
+  bool read_mps(const std::string& dir, int bond_read);
+  void save_mps(const std::string& dir) const;
+  // the two-site problem at bond (il, il+1): psi from the current site tensors and
+  // the H_eff plan of DMRG::hamiltonian_vector_multiplication_idmrg
+  HeffPlan<S> freeze(int il, BTensor<S>& psi);
+  // the same problem written as text-structure + binary-data files (one pair per tensor)
+  void export_problem(int il, const BTensor<S>& psi, const std::string& dir) const;
 
   Ctx& c;
   int lx, ly, ns, bondd, physpn, totspin, nfree = 2;
@@ -102,6 +111,7 @@ class Chain {
   double gs_enr = 0.0;
   std::vector<double> ww;
   double last_discarded = 0.0;
+  int near_ties = 0;          // truncations whose cut fell inside a near-degenerate pair
   // Lanczos settings (reference constants at src/dmrg_inst.cpp:267,1289,1338)
   int mlanc_max = 40;
   int prec = PREC_FP64;

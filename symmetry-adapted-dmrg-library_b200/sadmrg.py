@@ -29,7 +29,7 @@ EXPORTED = [
     "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device",
     "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
     "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
-    "sadmrg_chain_sweep", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
+    "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
 ]
 
@@ -74,6 +74,9 @@ def load(path: str = LIB_PATH):
         "sadmrg_chain_prepare_sweep": ([vp], C.c_int),
         "sadmrg_chain_sweep": ([vp, dp], C.c_int),
         "sadmrg_chain_bond": ([vp, C.c_int, C.c_int, ip, ip, ip], C.c_int),
+        "sadmrg_chain_read_mps": ([vp, C.c_char_p, C.c_int], C.c_int),
+        "sadmrg_chain_save_mps": ([vp, C.c_char_p], C.c_int),
+        "sadmrg_chain_freeze": ([vp, C.c_int, C.c_char_p], C.c_int),
         "sadmrg_chain_stats": ([vp, dp, C.c_int], C.c_int),
         "sadmrg_chain_set_tensor": ([vp, C.c_int, C.c_int, C.c_int, td], C.c_int),
         "sadmrg_chain_stage_tensor": ([vp, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -276,6 +279,17 @@ class Handle:
         self._check(self.lib.sadmrg_chain_sweep(self.h, C.byref(e)), "chain_sweep")
         return e.value
 
+    def chain_read_mps(self, directory: str, bond_read: int):
+        self._check(self.lib.sadmrg_chain_read_mps(self.h, directory.encode(), int(bond_read)), "chain_read_mps")
+
+    def chain_save_mps(self, directory: str):
+        self._check(self.lib.sadmrg_chain_save_mps(self.h, directory.encode()), "chain_save_mps")
+
+    def chain_freeze(self, il: int, export_dir: Optional[str] = None) -> BlockTensorData:
+        """Freeze the two-site problem at (il, il+1) as the handle's H_eff plan; returns psi."""
+        self._check(self.lib.sadmrg_chain_freeze(self.h, int(il), (export_dir or "").encode()), "chain_freeze")
+        return self.staged(0)
+
     def chain_bond(self, site: int):
         cap = 4096
         n = C.c_int()
@@ -287,10 +301,10 @@ class Handle:
         return [(int(q[i]), int(d[i])) for i in range(n.value)]
 
     def chain_stats(self):
-        out = np.zeros(9)
-        self._check(self.lib.sadmrg_chain_stats(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), 9), "chain_stats")
+        out = np.zeros(10)
+        self._check(self.lib.sadmrg_chain_stats(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), 10), "chain_stats")
         keys = ["lanczos_s", "env_s", "svd_s", "prep_s", "matvecs", "heff_flops", "gemm_flops", "launches",
-                "discarded"]
+                "discarded", "near_ties"]
         return dict(zip(keys, out.tolist()))
 
     def chain_set_tensor(self, kind: int, site: int, k: int, t: Optional[BlockTensorData]):

@@ -120,15 +120,24 @@ def main():
             np.savez_compressed(os.path.join(HERE, f"centre_{name}.npz"), **arrays)
             print("wrote", name, len(arrays))
     for name, args in SWEEP_CASES.items():
+        ck = {}
         with tempfile.TemporaryDirectory() as wd:
-            stdout = run(args, wd)
+            # the MPS after the reference's iDMRG, in its save_mps2 format: both sides sweep from it
+            stdout = run(args + ["-save", os.path.join(wd, "ck")], wd)
+            L = int(args[args.index("-L") + 1]) if "-L" in args else \
+                int(args[args.index("-lx") + 1]) * int(args[args.index("-ly") + 1])
+            if L <= 16:
+                for fn in sorted(os.listdir(os.path.join(wd, "ck"))):
+                    raw = open(os.path.join(wd, "ck", fn), "rb").read()
+                    ck["ck__" + fn] = np.frombuffer(raw, dtype=np.uint8)
         e_idmrg, energies, bonds = parse_sweeps(stdout)
-        last = bonds[max(bonds)] if bonds else {}
-        sites = sorted(last)
-        flat = [f"{s}:" + ",".join(f"{q}x{d}" for q, d in last[s]) for s in sites]
+        per_sweep = []
+        for s_ in sorted(k for k in bonds if k >= 0):
+            per_sweep.append([f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])])
         np.savez_compressed(os.path.join(HERE, f"sweeps_{name}.npz"), args=np.array(" ".join(args)),
-                            e_idmrg=np.float64(e_idmrg), energies=np.array(energies), bonds=np.array(flat))
-        print("wrote", name, e_idmrg, energies)
+                            e_idmrg=np.float64(e_idmrg), energies=np.array(energies),
+                            bonds=np.array(per_sweep[-1]), bonds_per_sweep=np.array(per_sweep), **ck)
+        print("wrote", name, e_idmrg, energies, len(ck))
 
 
 if __name__ == "__main__":
