@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""bench.py -- H_eff*psi throughput of the two-site DMRG hot path on B200.
+
+Workload (default): SU(2) spin-1/2 Heisenberg chain, open boundaries, L = 100,
+D = 512 kept multiplets.  The chain is grown on the GPU by the library's iDMRG
+(seeded like the reference, mt19937_64(42)) and the two-site problem at the
+centre bond is frozen; one benchmark step is one application of H_eff to psi on
+that problem (all sector products of one matvec, two grouped launches).
+
+Arms
+  ours (default)      3xTF32 split-precision matvec (value), FP64 matvec, end to
+                      end through the C ABI with host buffers (e2e), Lanczos
+                      mixed vs FP64 energies, the reference CPU build on the same
+                      problem (cpu_baseline), roofline of the dominant launch.
+  --impl reference    the reference's own DMRG::hamiltonian_vector_multiplication_idmrg
+                      (oracle/_ref, built from the reference sources) on the same
+                      problem, all host threads.
+
+Timing: CUDA events on the library's stream, one event pair per launch, L2
+flushed (256 MiB write) between timed steps; the problem is ~20 MB, so without
+the flush it would sit in the 126 MB L2.  Multi-GPU runs are independent
+replicas (the path has no exchange step); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "symmetry-adapted-dmrg-library_b200")
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+sys.path.insert(0, PKG)
+
+WORKLOADS = {
+    "su2_heisenberg_L100_D512": dict(sym=1, cplx=False, lx=1, ly=100, D=512, J2=0.0),
+    "su2_ladder_2x32_D1024": dict(sym=1, cplx=False, lx=32, ly=2, D=1024, J2=0.0),
+    "u1_heisenberg_L32_D64": dict(sym=0, cplx=False, lx=1, ly=32, D=64, J2=0.0),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="su2_heisenberg_L100_D512", choices=sorted(WORKLOADS))
+    ap.add_argument("--sweeps", type=int, default=1, help="timed finite sweeps before freezing")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def reduce_max(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def measured_peaks():
+    """cuBLAS FP64 and TF32 GEMM throughput on this GPU (8192^3, best of 3), and the
+    driver-measured HBM / bf16 peaks when present."""
+    import torch
+    out = {}
+    n = 8192
+    for name, dt, tf32 in (("fp64_tflops", torch.float64, False), ("tf32_tflops", torch.float32, True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, dtype=dt, device="cuda")
+        b = torch.randn(n, n, dtype=dt, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(3):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) / 1e3)
+        out[name] = 2 * n ** 3 / best / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mp = json.load(f)
+        out["hbm_gbs"] = mp.get("hbm_gbs")
+        out["bf16_tflops"] = mp.get("bf16_tflops")
+    except Exception:
+        pass
+    return out
+
+
+def build_problem(wl: dict, device: int, sweeps: int, export_dir: str | None):
+    import sadmrg
+    h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=device)
+    h.chain_create(wl["lx"], wl["ly"], wl["D"], 1, 0, True, wl["J2"])
+    t0 = time.perf_counter()
+    e_idmrg = h.chain_idmrg()
+    t_idmrg = time.perf_counter() - t0
+    sweep_times, sweep_e = [], []
+    for _ in range(sweeps):
+        t0 = time.perf_counter()
+        sweep_e.append(h.chain_sweep())
+        sweep_times.append(time.perf_counter() - t0)
+    stats = h.chain_stats()
+    ns = wl["lx"] * wl["ly"]
+    psi = h.chain_freeze(ns // 2 - 1, export_dir)
+    return h, psi, dict(idmrg_s=round(t_idmrg, 3), idmrg_E=e_idmrg, sweep_s=[round(x, 3) for x in sweep_times],
+                        sweep_E=sweep_e, chain_stats=stats)
+
+
+def run_reference_harness(export_dir: str, wl: dict, calls: int, threads: int):
+    sym = "su2" if wl["sym"] else "u1"
+    env = dict(os.environ)
+    env.pop("OPENBLAS_NUM_THREADS", None)
+    out = subprocess.run([HARNESS, "-sym", sym, "-cplx", str(int(wl["cplx"])), "-load", export_dir,
+                          "-bench_heff", str(calls), "-threads", str(threads)], capture_output=True, text=True,
+                         env=env, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference harness failed: {out.stderr[-300:]}")
+    for line in out.stdout.splitlines():
+        t = line.split()
+        if t and t[0] == "BENCH_HEFF":
+            return float(t[4])
+    raise RuntimeError("reference harness printed no timing")
+
+
+def main():
+    a = parse()
+    wl = WORKLOADS[a.workload]
+    ws, rank, local = dist_init()
+    cores = os.cpu_count() or 1
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        if not os.path.exists(HARNESS):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
+            return
+        with tempfile.TemporaryDirectory() as td:
+            # inputs: the same frozen problem (built on the GPU, written as files); the timed
+            # path is the reference's own H_eff*psi on the host cores
+            h, psi, meta = build_problem(wl, local, a.sweeps, td)
+            info = h.heff_info()
+            h.close()
+            run_reference_harness(td, wl, max(1, a.warmup), cores)
+            secs = run_reference_harness(td, wl, a.steps, cores)
+        v = info["flops"] * a.steps / secs / 1e12
+        line = {"metric": "H_eff*psi TFLOP/s", "value": v, "unit": "TFLOP/s", "n_gpus": ws, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": secs / a.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": a.workload, "L": wl["lx"] * wl["ly"], "D": wl["D"],
+                           "symmetry": "SU2" if wl["sym"] else "U1", "psi_elems": info["n"],
+                           "flops_per_step": info["flops"], "l2": "host run"},
+                "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                 "sample": f"{a.steps} H_eff*psi calls of the reference build on the frozen centre problem"},
+                "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import sadmrg
+    torch.cuda.set_device(local)
+    export_dir = tempfile.mkdtemp(prefix="sadmrg_bench_") if rank == 0 else None
+    h, psi, meta = build_problem(wl, local, a.sweeps, export_dir)
+    info = h.heff_info()
+    n = info["n"]
+    cplx = wl["cplx"]
+    dt = torch.complex128 if cplx else torch.float64
+    x = torch.from_numpy(np.asarray(psi.data)).to("cuda")
+    y = torch.empty_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    peaks = measured_peaks()
+
+    def timed(prec, steps):
+        ms = np.zeros(2)
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            m, fl = h.heff_profile(prec, 1, x.data_ptr(), y.data_ptr())
+            ms += m
+        return ms / steps, fl
+
+    for prec in (sadmrg.PREC_FP64, sadmrg.PREC_TF32X3):
+        timed(prec, a.warmup)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed")
+        ms_mix, fl = timed(sadmrg.PREC_TF32X3, a.steps)
+        ms_64, _ = timed(sadmrg.PREC_FP64, a.steps)
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    barrier(ws)
+    step_mix = reduce_max(float(ms_mix.sum()), ws)
+    step_64 = reduce_max(float(ms_64.sum()), ws)
+    flops = info["flops"]
+    value = flops * ws / (step_mix / 1e3) / 1e12
+    value64 = flops * ws / (step_64 / 1e3) / 1e12
+    # end to end through the C ABI with host buffers (H2D of psi, matvec, D2H of H psi)
+    psi_host = np.ascontiguousarray(psi.data)
+    h.heff_apply(psi_host, sadmrg.PREC_TF32X3)
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        out = h.heff_apply(psi_host, sadmrg.PREC_TF32X3)
+    e2e_s = reduce_max((time.perf_counter() - t0) / a.steps, ws)
+    e2e = flops * ws / e2e_s / 1e12
+    # accuracy of the split-precision matvec and of the mixed Lanczos
+    y64 = h.heff_apply(psi_host, sadmrg.PREC_FP64)
+    mv_err = float(np.abs(out - y64).max() / np.abs(y64).max())
+    # Lanczos to a tight stop (|<v|Hv>|/|Hv| within 1e-14 of 1, <= 100 steps) from the frozen psi
+    h.set_lanczos_tol(1e-14)
+    t0 = time.perf_counter()
+    e64, _, mv64 = h.heff_lanczos(psi_host, 100, sadmrg.PREC_FP64)
+    t_l64 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    emx, _, mvmx = h.heff_lanczos(psi_host, 100, sadmrg.PREC_TF32X3)
+    t_lmx = time.perf_counter() - t0
+    # dominant launch and its roofline (3xTF32: three TF32 products per useful product)
+    k = int(np.argmax(ms_mix))
+    achieved = fl[k] / (ms_mix[k] / 1e3) / 1e12
+    peak = peaks["tf32_tflops"] / 3.0
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj.get(a.workload, {}).get(f"stage{k}")
+    except Exception:
+        pass
+    line = {
+        "metric": "H_eff*psi TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": step_mix, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "tf32x3 (f32 partial sums, f64 accumulation)", "data": "synthetic",
+        "config": {"workload": a.workload, "L": wl["lx"] * wl["ly"], "D": wl["D"],
+                   "symmetry": "SU2" if wl["sym"] else "U1", "bond": f"centre ({n} psi elements)",
+                   "flops_per_step": flops, "tasks": info["ntasks"], "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": value64, "ms_per_step": step_64, "speedup_mixed_over_fp64": value / value64},
+        "accuracy": {"matvec_rel_err_tf32x3": mv_err, "lanczos_E_fp64": e64, "lanczos_E_mixed": emx,
+                     "abs_dE": abs(emx - e64), "lanczos_s_fp64": t_l64, "lanczos_s_mixed": t_lmx,
+                     "matvecs_fp64": mv64, "matvecs_mixed": mvmx},
+        "chain": meta,
+        "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": int(n * (16 if cplx else 8)),
+                "d2h_bytes_per_step": int(n * (16 if cplx else 8))},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": f"grouped_gemm_tf32x3 stage {k}",
+                     "peak_source": "cuBLAS TF32 GEMM measured in this run / 3 (3xTF32)",
+                     "stage_ms": ms_mix.tolist(), "stage_flops": list(fl)},
+        "peaks_measured": peaks,
+        "gpu_launches": 2 * a.steps * 2,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not a.no_cpu and os.path.exists(HARNESS):
+        try:
+            t1 = run_reference_harness(export_dir, wl, 1, cores)
+            calls = int(max(2, min(400, 15.0 / max(t1, 1e-3))))
+            secs = run_reference_harness(export_dir, wl, calls, cores)
+            ref = np.fromfile(os.path.join(export_dir, "hpsi_ref.bin"), dtype=np.complex128 if cplx else np.float64)
+            par = float(np.abs(ref - y64).max() / np.abs(ref).max()) if ref.size == y64.size else None
+            line["cpu_baseline"] = {"value": flops * calls / secs / 1e12, "unit": "TFLOP/s", "cores": cores,
+                                    "kind": "reference",
+                                    "sample": f"{calls} H_eff*psi calls of the reference build on the same problem",
+                                    "ms_per_call": secs / calls * 1e3, "fp64_gpu_vs_reference_rel_diff": par}
+        except Exception as ex:
+            line["cpu_baseline"] = {"value": None, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                    "sample": f"failed: {ex}"}
+    if rank == 0:
+        print(json.dumps(line))
+    h.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -68,6 +68,10 @@ int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out);
 int sadmrg_destroy(sadmrg_handle* h);
 const char* sadmrg_last_error(const sadmrg_handle* h);
 
+/* Lanczos convergence: stop at a check (every 4 steps) once |<v|Hv>|/|Hv| is
+ * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338). */
+int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol);
+
 /* ---- frozen two-site problem: H_eff * psi ---------------------------------
  * ops[] holds every block operator once; term i pairs ops[op1[i]] (left block,
  * legs (a, channel, a')) with ops[op2[i]] (right block, legs (b, channel, b')),
@@ -84,6 +88,12 @@ int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* byte
 int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision);
 /* out = H_eff psi with device pointers (no copies) */
 int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision);
+/* Per-stage device time of one H_eff*psi (CUDA events on the handle's stream,
+ * averaged over reps): ms[0] stage 0 (X = op1^T psi products), ms[1] stage 1
+ * (the output accumulation lists); flops[] the algorithmic flops of each stage.
+ * psi_dev / out_dev may be NULL (the handle's own buffers are used). */
+int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, double* ms,
+                        double* flops);
 /* Lanczos ground state (lanczos1) from psi; psi is overwritten by the Ritz vector.
  * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
  * FP64 restart from its result. */

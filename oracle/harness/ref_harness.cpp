@@ -32,6 +32,7 @@
 #include <unistd.h>
 #include <sstream>
 #include <vector>
+#include <map>
 
 #define private public
 #define protected public
@@ -46,6 +47,9 @@ int myrank = 0;
 CGCTables* g_cgc_tables = nullptr;
 void makeup_clebsch_gordan_coefficient_tensors(int physpn, int max_angm, CGCTables& t);
 
+struct Opts;
+template <class S, class Sym> static int run_load(const Opts& o);
+
 struct Opts {
   int sym = 0;       // 0 = U1, 1 = SU2
   int cplx = 0;      // 0 = double, 1 = dcmplex
@@ -56,6 +60,7 @@ struct Opts {
   std::string save;  // directory: save_mps2 after iDMRG (checkpoint files)
   std::string read;  // directory: read_mps + prepare_sweep instead of iDMRG
   int bench_heff = 0;  // time this many H*v calls on the centre problem
+  std::string load;    // directory with an exported two-site problem (time / check H*v on it)
   int quiet = 1;
 };
 
@@ -291,6 +296,155 @@ static int run(const Opts& o) {
   return 0;
 }
 
+// ---- exported two-site problem ---------------------------------------------
+// Reads the <name>.txt / <name>.bin pairs written by the GPU library's problem
+// export into the reference's own BlockTensors and runs the reference's
+// DMRG::hamiltonian_vector_multiplication_idmrg on them.
+template <class S, class Sym>
+static bool load_tensor(const std::string& dir, const std::string& name, BlockTensor<S, Sym>& t, bool psi) {
+  std::ifstream ft(dir + "/" + name + ".txt");
+  if (!ft) return false;
+  std::string line, w;
+  int nb = 0, ls = 0;
+  // BondType has no copy constructor: keep the raw labels and set the bonds in place
+  std::vector<std::vector<int>> bq, bdm;
+  std::vector<int> bdir;
+  struct B { long idx; std::vector<int> dims; long off, n; };
+  std::vector<B> blocks;
+  while (std::getline(ft, line)) {
+    std::istringstream is(line);
+    is >> w;
+    if (w == "nbond") { long nten; std::string a, b; is >> nb >> a >> ls >> b >> nten; }
+    else if (w == "bond") {
+      int bi, dir, nm; std::string a, c, q;
+      is >> bi >> a >> dir >> c >> nm >> q;
+      std::vector<int> qs(nm), ds(nm);
+      for (int k = 0; k < nm; ++k) is >> qs[k];
+      is >> q;
+      for (int k = 0; k < nm; ++k) is >> ds[k];
+      bq.push_back(qs);
+      bdm.push_back(ds);
+      bdir.push_back(dir);
+    } else if (w == "block") {
+      B b; std::string x;
+      is >> b.idx >> x;
+      for (int k = 0; k < nb; ++k) { int qq; is >> qq; }
+      is >> x;
+      b.dims.resize(nb);
+      for (int k = 0; k < nb; ++k) is >> b.dims[k];
+      is >> x >> b.off >> x >> b.n;
+      blocks.push_back(b);
+    }
+  }
+  typename Sym::BondType* bonds = new typename Sym::BondType[nb];
+  for (int b = 0; b < nb; ++b) bonds[b].set(bdir[b], (int)bq[b].size(), bq[b].data(), bdm[b].data());
+  typename Sym::StructType st;
+  st.set_struct(nb, ls, bonds);
+  delete[] bonds;
+  t.set(st, nullptr, nullptr);
+  std::ifstream fb(dir + "/" + name + ".bin", std::ios::binary);
+  fb.seekg(0, std::ios::end);
+  const long nbytes = fb.tellg();
+  fb.seekg(0);
+  std::vector<S> data(nbytes / sizeof(S));
+  fb.read(reinterpret_cast<char*>(data.data()), nbytes);
+  for (auto& b : blocks) t.data_blocks[b.idx].copy(nb, b.dims.data(), data.data() + b.off);
+  if constexpr (Sym::has_cgc) {
+    if (psi) {  // the two-site vector carries singlet CGC blocks (makeup_input_vector)
+      std::vector<int> angm(nb), bdim(nb);
+      for (int i = 0; i < t.nten; ++i)
+        if (t.cgc.get_tensor_argument(i, angm.data(), bdim.data())) t.cgc_blocks[i].make_singlet(angm[0]);
+    }
+  }
+  return true;
+}
+
+template <class S, class Sym>
+static int run_load(const Opts& o) {
+  std::ifstream fm(o.load + "/meta.txt");
+  if (!fm) { std::cerr << "no meta.txt in " << o.load << "\n"; return 3; }
+  std::map<std::string, double> meta;
+  std::string line;
+  std::getline(fm, line);
+  {
+    std::istringstream is(line);
+    std::string k;
+    double v;
+    while (is >> k >> v) meta[k] = v;
+  }
+  const int lx = (int)meta["lx"], ly = (int)meta["ly"], il = (int)meta["il"], ir = (int)meta["ir"];
+  psize = o.threads;
+  omp_set_num_threads(o.threads);
+  std::streambuf* saved = std::cout.rdbuf();
+  std::ostringstream sink;
+  std::cout.rdbuf(sink.rdbuf());
+  DMRG<S, Sym> chain(lx, ly, (int)meta["D"], 1, (int)meta["sec"], 0);
+  std::cout.rdbuf(saved);
+  Opts g = o;
+  g.open = (int)meta["open"];
+  g.J2 = meta["J2"];
+  patch_geometry(chain, g);
+  if constexpr (Sym::has_cgc) {
+    // fac_hamilt_vec for 2J beyond the constructor's max_angm = 20, computed with the
+    // reference's own Dense / CGCTable code by the formula of src/cgc_tables.cpp:153-164
+    const int M = 64;
+    double*** f = new double**[M];
+    Dense<double> sg[M], c, t1, t2;
+    for (int i = 0; i < M; ++i) sg[i].make_singlet(i);
+    for (int i = 0; i < M; ++i) {
+      f[i] = new double*[M];
+      for (int j = 0; j < M; ++j) {
+        f[i][j] = new double[M]();
+        for (int k = 0; k < M; ++k)
+          if (j <= 6 && k >= std::abs(i - j) && k <= i + j && (i % 2 == k % 2)) {
+            c.make_cgc(i, j, k);
+            t1.contract(c, 0, sg[i], 1);
+            t2.contract(t1, 0, sg[j], 1);
+            t1.contract(t2, 0, sg[k], 1);
+            f[i][j][k] = c.inner_prod_u(t1) * std::sqrt((double)(j + 1));
+          }
+      }
+    }
+    g_cgc_tables->fac_hamilt_vec = f;  // the old 20^3 table is left allocated
+  }
+  BlockTensor<S, Sym> vec, out;
+  bool ok = load_tensor(o.load, "psi", vec, true);
+  load_tensor(o.load, "hh_il", chain.hh[il], false);
+  load_tensor(o.load, "hh_ir", chain.hh[ir], false);
+  for (int k = 0; k < chain.ns; ++k) {
+    load_tensor(o.load, "opr_il_" + std::to_string(k), chain.opr[il][k], false);
+    load_tensor(o.load, "opr_ir_" + std::to_string(k), chain.opr[ir][k], false);
+  }
+  if (!ok) { std::cerr << "no psi in " << o.load << "\n"; return 3; }
+  std::cout.rdbuf(sink.rdbuf());
+  chain.hamiltonian_vector_multiplication_idmrg(il, ir, vec, out);
+  std::cout.rdbuf(saved);
+  {
+    // result in the block order of psi (missing blocks written as zeros)
+    std::ofstream fo(o.load + "/hpsi_ref.bin", std::ios::binary);
+    std::vector<int> angm(2), bdim(2);
+    for (int i = 0; i < vec.nten; ++i) {
+      if (vec.data_blocks[i].check_null()) continue;
+      const long n = vec.data_blocks[i].get_nelem();
+      if (i < out.nten && !out.data_blocks[i].check_null())
+        fo.write(reinterpret_cast<const char*>(out.data_blocks[i].getptr()), sizeof(S) * n);
+      else {
+        std::vector<S> z(n, S(0));
+        fo.write(reinterpret_cast<const char*>(z.data()), sizeof(S) * n);
+      }
+    }
+  }
+  const int reps = std::max(o.bench_heff, 1);
+  std::cout.rdbuf(sink.rdbuf());
+  auto a = std::chrono::steady_clock::now();
+  for (int r = 0; r < reps; ++r) chain.hamiltonian_vector_multiplication_idmrg(il, ir, vec, out);
+  auto b = std::chrono::steady_clock::now();
+  std::cout.rdbuf(saved);
+  std::cout << std::setprecision(10) << "BENCH_HEFF calls " << reps << " seconds "
+            << std::chrono::duration<double>(b - a).count() << " threads " << o.threads << "\n";
+  return 0;
+}
+
 int main(int argc, char** argv) {
   Opts o;
   for (int i = 1; i < argc; ++i) {
@@ -311,9 +465,16 @@ int main(int argc, char** argv) {
     else if (a == "-dump") o.dump = nxt();
     else if (a == "-save") o.save = nxt();
     else if (a == "-read") o.read = nxt();
+    else if (a == "-load") o.load = nxt();
     else if (a == "-bench_heff") o.bench_heff = std::stoi(nxt());
     else if (a == "-verbose") o.quiet = 0;
     else { std::cerr << "unknown option " << a << "\n"; return 2; }
+  }
+  if (!o.load.empty()) {
+    if (o.sym == 0 && o.cplx == 0) return run_load<double, U1Symmetry>(o);
+    if (o.sym == 0 && o.cplx == 1) return run_load<dcmplex, U1Symmetry>(o);
+    if (o.sym == 1 && o.cplx == 0) return run_load<double, SU2Symmetry>(o);
+    return run_load<dcmplex, SU2Symmetry>(o);
   }
   if (o.sym == 0 && o.cplx == 0) return run<double, U1Symmetry>(o);
   if (o.sym == 0 && o.cplx == 1) return run<dcmplex, U1Symmetry>(o);

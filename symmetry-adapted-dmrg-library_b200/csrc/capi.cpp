@@ -162,6 +162,13 @@ int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadm
   });
 }
 
+int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(ov_tol > 0.0 && ov_tol < 1.0, SADMRG_ERR_ARG, "set_lanczos_tol: tolerance out of range");
+    h->ctx.lanczos_ov_tol = ov_tol;
+  });
+}
+
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
@@ -198,6 +205,52 @@ int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_de
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply_device: no plan");
     SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_apply: precision");
     S_.heff->apply(h->ctx, static_cast<const S*>(psi_dev), static_cast<S*>(out_dev), precision);
+  });
+}
+
+int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, double* ms,
+                        double* flops) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_profile: no plan");
+    SADMRG_REQUIRE(reps >= 1, SADMRG_ERR_ARG, "heff_profile: reps");
+    const HeffPlan<S>& H = *S_.heff;
+    const S* in = psi_dev ? static_cast<const S*>(psi_dev) : S_.io.template as<S>();
+    S* out = out_dev ? static_cast<S*>(out_dev) : S_.io.template as<S>() + H.n;
+    Bases b{};
+    b.p[0] = const_cast<S*>(in);
+    b.p[1] = out;
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = H.scratch->get();
+    cudaEvent_t ev[3];
+    for (auto& e : ev) SADMRG_CUDA(cudaEventCreate(&e));
+    double acc[2] = {0.0, 0.0};
+    for (int r = 0; r < reps; ++r) {
+      SADMRG_CUDA(cudaEventRecord(ev[0], c.stream));
+      H.plan.run(c, ScalarInfo<S>::cplx, precision, b, 0, 1);
+      SADMRG_CUDA(cudaEventRecord(ev[1], c.stream));
+      H.plan.run(c, ScalarInfo<S>::cplx, precision, b, 1, 2);
+      SADMRG_CUDA(cudaEventRecord(ev[2], c.stream));
+      SADMRG_CUDA(cudaEventSynchronize(ev[2]));
+      float t0 = 0.f, t1 = 0.f;
+      SADMRG_CUDA(cudaEventElapsedTime(&t0, ev[0], ev[1]));
+      SADMRG_CUDA(cudaEventElapsedTime(&t1, ev[1], ev[2]));
+      acc[0] += t0;
+      acc[1] += t1;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    ms[0] = acc[0] / reps;
+    ms[1] = acc[1] / reps;
+    // algorithmic flops per stage
+    double f[2] = {0.0, 0.0};
+    const auto& P = H.plan;
+    for (size_t j = 0; j < P.jobs.size(); ++j)
+      for (auto& t : P.job_terms[j])
+        f[P.job_stage[j]] += (ScalarInfo<S>::cplx ? 8.0 : 2.0) * P.jobs[j].m * (double)P.jobs[j].n * t.k;
+    flops[0] = f[0];
+    flops[1] = f[1];
   });
 }
 

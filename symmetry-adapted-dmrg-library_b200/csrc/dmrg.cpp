@@ -363,7 +363,7 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
     if (m % 4 == 0) {
       ritz_vec(m);
       check(ee, ov);
-      if (std::fabs(ov - 1.0) < 1e-8) { st.energy = eig[0]; return st; }
+      if (std::fabs(ov - 1.0) < c.lanczos_ov_tol) { st.energy = eig[0]; return st; }
     }
   }
   matvec(K.F(mlanc - 1), K.F(mlanc));

@@ -1,9 +1,6 @@
 // kernels.cu -- sm_100a kernels for the two-site DMRG hot path.
 //
-//  * grouped_gemm_f64 / grouped_gemm_z64: one launch runs every sector GEMM of
-//    a task list (H_eff*psi, environment updates, projector products).  FP64
-//    products run on the double-precision tensor path (mma.sync m8n8k4 .f64);
-//    tcgen05 has no f64 kind on sm_100a.
+//  (the grouped block-GEMM executor is in gemm.cu)
 //  * block utilities (segment axpy, block transpose, fuse fill, SVD gather);
 //  * Krylov vector kernels with deterministic two-pass reductions;
 //  * one-sided (Hestenes) block Jacobi SVD, column blocks staged in shared
@@ -14,209 +11,6 @@
 #include "kernels.cuh"
 
 namespace sadmrg {
-
-// --------------------------------------------------------------------------
-// FP64 tensor-core MMA: D(8x8) += A(8x4, row) * B(4x8, col)
-// A frag: a = A[lane>>2][lane&3];  B frag: b = B[lane&3][lane>>2]
-// C frag: c0,c1 = C[lane>>2][2*(lane&3) + {0,1}]
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-constexpr int kGemmThreads = 128;
-
-template <int BM, int BN, int BK>
-__global__ void __launch_bounds__(kGemmThreads) grouped_gemm_f64(const GemmTerm* __restrict__ terms,
-                                                                 const GemmJob* __restrict__ jobs,
-                                                                 const GemmTile* __restrict__ tiles, Bases bases) {
-  constexpr int PAD = 4;
-  __shared__ double As[BK][BM + PAD];
-  __shared__ double Bs[BK][BN + PAD];
-  const GemmTile t = tiles[blockIdx.x];
-  const GemmJob J = jobs[t.job];
-  const int row0 = t.tm * BM, col0 = t.tn * BN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
-  double acc[MT][NT][2];
-#pragma unroll
-  for (int i = 0; i < MT; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  for (int ti = 0; ti < J.nt; ++ti) {
-    const GemmTerm T = terms[J.t0 + ti];
-    const double* __restrict__ A = static_cast<const double*>(bases.p[T.abuf]) + T.aoff;
-    const double* __restrict__ B = static_cast<const double*>(bases.p[T.bbuf]) + T.boff;
-    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
-    const double alpha = T.ar;
-    for (int k0 = 0; k0 < T.k; k0 += BK) {
-#pragma unroll 4
-      for (int e = tid; e < BM * BK; e += kGemmThreads) {
-        int i, kk;
-        if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
-        const int gi = row0 + i, gk = k0 + kk;
-        double v = 0.0;
-        if (gi < J.m && gk < T.k) v = ta ? A[gk + (long long)gi * T.lda] : A[gi + (long long)gk * T.lda];
-        As[kk][i] = v * alpha;
-      }
-#pragma unroll 4
-      for (int e = tid; e < BK * BN; e += kGemmThreads) {
-        int j, kk;
-        if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
-        const int gj = col0 + j, gk = k0 + kk;
-        double v = 0.0;
-        if (gj < J.n && gk < T.k) v = tb ? B[gj + (long long)gk * T.ldb] : B[gk + (long long)gj * T.ldb];
-        Bs[kk][j] = v;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k4 = 0; k4 < BK; k4 += 4) {
-        double af[MT], bf[NT];
-#pragma unroll
-        for (int mi = 0; mi < MT; ++mi) af[mi] = As[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
-#pragma unroll
-        for (int ni = 0; ni < NT; ++ni) bf[ni] = Bs[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
-#pragma unroll
-        for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-          for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
-      }
-      __syncthreads();
-    }
-  }
-  double* __restrict__ C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
-  const bool accum = J.flags & JF_ACCUM;
-#pragma unroll
-  for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < NT; ++ni)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = row0 + wm * WM + mi * 8 + (lane >> 2);
-        const int c = col0 + wn * WN + ni * 8 + 2 * (lane & 3) + e;
-        if (r < J.m && c < J.n) {
-          const long long idx = r + (long long)c * J.ldc;
-          C[idx] = accum ? C[idx] + acc[mi][ni][e] : acc[mi][ni][e];
-        }
-      }
-}
-
-// complex (interleaved re,im): products split into real DMMAs,
-// rr = Re*Re, ii = Im*Im, im = Re*Im + Im*Re;  C = (rr - ii) + i*im
-template <int BM, int BN, int BK>
-__global__ void __launch_bounds__(kGemmThreads) grouped_gemm_z64(const GemmTerm* __restrict__ terms,
-                                                                 const GemmJob* __restrict__ jobs,
-                                                                 const GemmTile* __restrict__ tiles, Bases bases) {
-  constexpr int PAD = 4;
-  __shared__ double Ar[BK][BM + PAD], Ai[BK][BM + PAD];
-  __shared__ double Br[BK][BN + PAD], Bi[BK][BN + PAD];
-  const GemmTile t = tiles[blockIdx.x];
-  const GemmJob J = jobs[t.job];
-  const int row0 = t.tm * BM, col0 = t.tn * BN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
-  double rr[MT][NT][2], ii[MT][NT][2], im[MT][NT][2];
-#pragma unroll
-  for (int i = 0; i < MT; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) rr[i][j][e] = ii[i][j][e] = im[i][j][e] = 0.0;
-
-  for (int ti = 0; ti < J.nt; ++ti) {
-    const GemmTerm T = terms[J.t0 + ti];
-    const double2* __restrict__ A = static_cast<const double2*>(bases.p[T.abuf]) + T.aoff;
-    const double2* __restrict__ B = static_cast<const double2*>(bases.p[T.bbuf]) + T.boff;
-    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
-    const double ca = (T.flags & TF_CA) ? -1.0 : 1.0, cb = (T.flags & TF_CB) ? -1.0 : 1.0;
-    for (int k0 = 0; k0 < T.k; k0 += BK) {
-      for (int e = tid; e < BM * BK; e += kGemmThreads) {
-        int i, kk;
-        if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
-        const int gi = row0 + i, gk = k0 + kk;
-        double2 v = make_double2(0.0, 0.0);
-        if (gi < J.m && gk < T.k) v = ta ? A[gk + (long long)gi * T.lda] : A[gi + (long long)gk * T.lda];
-        v.y *= ca;
-        Ar[kk][i] = v.x * T.ar - v.y * T.ai;
-        Ai[kk][i] = v.x * T.ai + v.y * T.ar;
-      }
-      for (int e = tid; e < BK * BN; e += kGemmThreads) {
-        int j, kk;
-        if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
-        const int gj = col0 + j, gk = k0 + kk;
-        double2 v = make_double2(0.0, 0.0);
-        if (gj < J.n && gk < T.k) v = tb ? B[gj + (long long)gk * T.ldb] : B[gk + (long long)gj * T.ldb];
-        Br[kk][j] = v.x;
-        Bi[kk][j] = v.y * cb;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k4 = 0; k4 < BK; k4 += 4) {
-        double ar[MT], ai[MT], br[NT], bi[NT];
-#pragma unroll
-        for (int mi = 0; mi < MT; ++mi) {
-          ar[mi] = Ar[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
-          ai[mi] = Ai[k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
-        }
-#pragma unroll
-        for (int ni = 0; ni < NT; ++ni) {
-          br[ni] = Br[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
-          bi[ni] = Bi[k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
-        }
-#pragma unroll
-        for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-          for (int ni = 0; ni < NT; ++ni) {
-            dmma884(rr[mi][ni][0], rr[mi][ni][1], ar[mi], br[ni]);
-            dmma884(ii[mi][ni][0], ii[mi][ni][1], ai[mi], bi[ni]);
-            dmma884(im[mi][ni][0], im[mi][ni][1], ar[mi], bi[ni]);
-            dmma884(im[mi][ni][0], im[mi][ni][1], ai[mi], br[ni]);
-          }
-      }
-      __syncthreads();
-    }
-  }
-  double2* __restrict__ C = static_cast<double2*>(bases.p[J.cbuf]) + J.coff;
-  const bool accum = J.flags & JF_ACCUM;
-#pragma unroll
-  for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < NT; ++ni)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = row0 + wm * WM + mi * 8 + (lane >> 2);
-        const int c = col0 + wn * WN + ni * 8 + 2 * (lane & 3) + e;
-        if (r < J.m && c < J.n) {
-          const long long idx = r + (long long)c * J.ldc;
-          double2 v = make_double2(rr[mi][ni][e] - ii[mi][ni][e], im[mi][ni][e]);
-          if (accum) { double2 o = C[idx]; v.x += o.x; v.y += o.y; }
-          C[idx] = v;
-        }
-      }
-}
-
-constexpr int kRealBM = 64, kRealBN = 64, kRealBK = 16;
-constexpr int kCplxBM = 32, kCplxBN = 32, kCplxBK = 16;
-
-int gemm_tile_m(bool cplx, int /*prec*/) { return cplx ? kCplxBM : kRealBM; }
-int gemm_tile_n(bool cplx, int /*prec*/) { return cplx ? kCplxBN : kRealBN; }
-
-void launch_grouped_gemm_tf32x3(bool cplx, const GemmTerm* terms, const GemmJob* jobs, const GemmTile* tiles,
-                                int ntiles, const Bases& b, cudaStream_t s);
-
-void launch_grouped_gemm(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const GemmTile* tiles,
-                         int ntiles, const Bases& b, cudaStream_t s) {
-  if (ntiles <= 0) return;
-  if (prec == PREC_TF32X3) { launch_grouped_gemm_tf32x3(cplx, terms, jobs, tiles, ntiles, b, s); return; }
-  if (cplx)
-    grouped_gemm_z64<kCplxBM, kCplxBN, kCplxBK><<<ntiles, kGemmThreads, 0, s>>>(terms, jobs, tiles, b);
-  else
-    grouped_gemm_f64<kRealBM, kRealBN, kRealBK><<<ntiles, kGemmThreads, 0, s>>>(terms, jobs, tiles, b);
-}
 
 // --------------------------------------------------------------------------
 // block utilities

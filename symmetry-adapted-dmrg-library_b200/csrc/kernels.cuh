@@ -31,14 +31,23 @@ struct GemmJob {              // C (m x n, column-major, ldc) receives its terms
 struct GemmTile {
   int job, tm, tn;
 };
+struct WorkItem {             // one output tile x a contiguous range of the job's concatenated k
+  int job, tm, tn;
+  int t0, k0, kcount;         // first term (relative to the job's t0), offset in it, total k
+  int slot;                   // < 0: write C directly; otherwise the partial-tile slot
+};
+struct RedItem {              // C tile = sum of slots [slot0, slot0 + nslot) (fixed order)
+  int job, tm, tn, slot0, nslot;
+};
 struct Bases {
   void* p[kMaxBases];
 };
 
-// Grouped GEMM over a tile table (one CTA per output tile, terms accumulated in
-// registers, no atomics: each output element is written by exactly one CTA).
-void launch_grouped_gemm(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs,
-                         const GemmTile* tiles, int ntiles, const Bases& b, cudaStream_t s);
+// Grouped GEMM over work items (deterministic split-K; see gemm.cu).
+void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
+                  const Bases& b, void* work, cudaStream_t s);
+void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
+                   cudaStream_t s);
 int gemm_tile_m(bool cplx, int prec);
 int gemm_tile_n(bool cplx, int prec);
 

@@ -95,51 +95,115 @@ void GemmPlan::finalize(Ctx& c, bool cplx) {
     }
   }
   const int BM = gemm_tile_m(cplx, 0), BN = gemm_tile_n(cplx, 0);
-  std::vector<std::vector<std::pair<long long, GemmTile>>> per(nstage);
-  for (size_t j = 0; j < jobs.size(); ++j) {
-    long long cost = 1;
-    for (auto& t : job_terms[j]) cost += t.k;
-    const int tm = (jobs[j].m + BM - 1) / BM, tn = (jobs[j].n + BN - 1) / BN;
-    for (int a = 0; a < tm; ++a)
-      for (int b = 0; b < tn; ++b) per[job_stage[j]].push_back({cost, GemmTile{(int)j, a, b}});
-  }
-  tiles.clear();
-  stage_tiles.assign(nstage + 1, 0);
+  items.clear();
+  reds.clear();
+  stage_items.assign(nstage + 1, 0);
+  stage_reds.assign(nstage + 1, 0);
+  int nslot = 0;
   for (int s = 0; s < nstage; ++s) {
-    stage_tiles[s] = (int)tiles.size();
-    // longest work first, so the long accumulation lists start early
-    std::stable_sort(per[s].begin(), per[s].end(),
-                     [](const std::pair<long long, GemmTile>& a, const std::pair<long long, GemmTile>& b) {
-                       return a.first > b.first;
-                     });
-    for (auto& p : per[s]) tiles.push_back(p.second);
+    // split-K chunk: enough items to fill the GPU, never below 128 of k
+    long long total = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      if (job_stage[j] != s) continue;
+      long long kt = 0;
+      for (auto& t : job_terms[j]) kt += t.k;
+      total += (long long)((jobs[j].m + BM - 1) / BM) * ((jobs[j].n + BN - 1) / BN) * std::max<long long>(kt, 1);
+    }
+    long long ntile = 0;
+    for (size_t j = 0; j < jobs.size(); ++j)
+      if (job_stage[j] == s)
+        ntile += (long long)((jobs[j].m + BM - 1) / BM) * ((jobs[j].n + BN - 1) / BN);
+    // split the reduction only when the output tiles alone cannot fill the GPU
+    long long kc = (total + target_items - 1) / std::max(target_items, 1);
+    kc = std::max<long long>(128, (kc + 15) / 16 * 16);
+    if (ntile >= target_items / 2) kc = (long long)1 << 40;
+    std::vector<std::pair<long long, WorkItem>> its;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      if (job_stage[j] != s) continue;
+      long long kt = 0;
+      for (auto& t : job_terms[j]) kt += t.k;
+      if (kt == 0 && (jobs[j].flags & JF_ACCUM)) continue;
+      const int tm = (jobs[j].m + BM - 1) / BM, tn = (jobs[j].n + BN - 1) / BN;
+      const long long nch = std::max<long long>(1, (kt + kc - 1) / kc);
+      for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) {
+          if (nch == 1) {
+            its.push_back({kt, WorkItem{(int)j, a, b, 0, 0, (int)kt, -1}});
+            continue;
+          }
+          const int slot0 = nslot;
+          long long pos = 0;
+          int t = 0, k = 0;
+          for (long long ch = 0; ch < nch; ++ch) {
+            const long long len = std::min(kc, kt - pos);
+            its.push_back({len, WorkItem{(int)j, a, b, t, k, (int)len, nslot++}});
+            // advance (t, k) by len along the concatenated k
+            long long left = len;
+            while (left > 0) {
+              const int avail = job_terms[j][t].k - k;
+              if (left < avail) { k += (int)left; left = 0; }
+              else { left -= avail; ++t; k = 0; }
+            }
+            pos += len;
+          }
+          reds.push_back(RedItem{(int)j, a, b, slot0, (int)nch});
+        }
+    }
+    // longest work first
+    std::stable_sort(its.begin(), its.end(), [](const std::pair<long long, WorkItem>& x,
+                                                const std::pair<long long, WorkItem>& y) { return x.first > y.first; });
+    stage_items[s] = (int)items.size();
+    for (auto& p : its) items.push_back(p.second);
+    stage_items[s + 1] = (int)items.size();
+    stage_reds[s + 1] = (int)reds.size();
   }
-  stage_tiles[nstage] = (int)tiles.size();
+  for (int s = 0; s < nstage; ++s) {
+    stage_items[s + 1] = std::max(stage_items[s + 1], stage_items[s]);
+    stage_reds[s + 1] = std::max(stage_reds[s + 1], stage_reds[s]);
+  }
   const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size(),
-               bl = sizeof(GemmTile) * tiles.size();
+               bi = sizeof(WorkItem) * items.size(), br = sizeof(RedItem) * reds.size();
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t total = al(bt) + al(bj) + al(bl) + 256;
+  const size_t total = al(bt) + al(bj) + al(bi) + al(br) + 256;
   std::vector<unsigned char> h(total, 0);
   if (bt) std::memcpy(h.data(), flat_terms.data(), bt);
   if (bj) std::memcpy(h.data() + al(bt), jobs.data(), bj);
-  if (bl) std::memcpy(h.data() + al(bt) + al(bj), tiles.data(), bl);
+  if (bi) std::memcpy(h.data() + al(bt) + al(bj), items.data(), bi);
+  if (br) std::memcpy(h.data() + al(bt) + al(bj) + al(bi), reds.data(), br);
   dev = std::make_shared<DevBuf>(total, c.stream);
   SADMRG_CUDA(cudaMemcpyAsync(dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
   unsigned char* base = dev->as<unsigned char>();
   d_terms = reinterpret_cast<GemmTerm*>(base);
   d_jobs = reinterpret_cast<GemmJob*>(base + al(bt));
-  d_tiles = reinterpret_cast<GemmTile*>(base + al(bt) + al(bj));
+  d_items = reinterpret_cast<WorkItem*>(base + al(bt) + al(bj));
+  d_reds = reinterpret_cast<RedItem*>(base + al(bt) + al(bj) + al(bi));
+  work = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * BM * BN * (cplx ? 16 : 8), c.stream);
   // the host copy must stay alive until the async copy completes
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+int GemmPlan::launches_per_run() const {
+  int n = 0;
+  for (int s = 0; s < nstage; ++s) {
+    if (stage_items[s + 1] > stage_items[s]) ++n;
+    if (stage_reds[s + 1] > stage_reds[s]) ++n;
+  }
+  return n;
 }
 
 void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi) const {
   if (stage_hi < 0) stage_hi = nstage;
   for (int s = stage_lo; s < stage_hi; ++s) {
-    const int nt = stage_tiles[s + 1] - stage_tiles[s];
-    if (nt <= 0) continue;
-    launch_grouped_gemm(cplx, prec, d_terms, d_jobs, d_tiles + stage_tiles[s], nt, b, c.stream);
-    ++c.launches;
+    const int ni = stage_items[s + 1] - stage_items[s];
+    if (ni > 0) {
+      launch_items(cplx, prec, d_terms, d_jobs, d_items + stage_items[s], ni, b, work->get(), c.stream);
+      ++c.launches;
+    }
+    const int nr = stage_reds[s + 1] - stage_reds[s];
+    if (nr > 0) {
+      launch_reduce(cplx, d_jobs, d_reds + stage_reds[s], nr, b, work->get(), c.stream);
+      ++c.launches;
+    }
   }
   SADMRG_CUDA(cudaGetLastError());
   c.gemm_flops += flops;

@@ -29,6 +29,7 @@ struct Ctx {
   double* d_scalars = nullptr;   // small device scratch for reductions
   double* d_partial = nullptr;
   int npart = 296;
+  double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
   ~Ctx();
@@ -71,14 +72,19 @@ struct GemmPlan {
   long long scratch_elems = 0;
   int nstage = 2;
   // device copy
-  std::vector<GemmTile> tiles;
-  std::vector<int> stage_tiles;   // tile offsets per stage (size nstage+1)
+  std::vector<WorkItem> items;
+  std::vector<RedItem> reds;
+  std::vector<int> stage_items;   // item offsets per stage (size nstage+1)
+  std::vector<int> stage_reds;    // reduction offsets per stage (size nstage+1)
   std::vector<GemmTerm> flat_terms;
   std::shared_ptr<DevBuf> dev;
+  std::shared_ptr<DevBuf> work;   // split-K partial tiles
   GemmTerm* d_terms = nullptr;
   GemmJob* d_jobs = nullptr;
-  GemmTile* d_tiles = nullptr;
+  WorkItem* d_items = nullptr;
+  RedItem* d_reds = nullptr;
   long long flops = 0;            // algorithmic flops of one execution (real multiply-adds * 2)
+  int target_items = 148 * 8;     // work items per stage the split-K aims for
 
   int add_job(int stage, int cbuf, long long coff, int m, int n, int ldc, int flags);
   void add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
@@ -86,6 +92,7 @@ struct GemmPlan {
   long long alloc_scratch(long long elems) { long long o = scratch_elems; scratch_elems += elems; return o; }
   void finalize(Ctx& c, bool cplx);
   void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1) const;
+  int launches_per_run() const;
   bool empty() const { return jobs.empty(); }
 };
 

@@ -26,8 +26,8 @@ PREC_FP64, PREC_TF32X3 = 0, 1
 
 EXPORTED = [
     "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
-    "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device",
-    "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
+    "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device",
+    "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
     "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
@@ -63,10 +63,12 @@ def load(path: str = LIB_PATH):
         "sadmrg_destroy": ([vp], C.c_int),
         "sadmrg_last_error": ([vp], C.c_char_p),
         "sadmrg_heff_plan": ([vp, td, td, td, C.c_int, td, C.c_int, ip, ip], C.c_int),
+        "sadmrg_set_lanczos_tol": ([vp, C.c_double], C.c_int),
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
+        "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -179,6 +181,9 @@ class Handle:
             msg = self.lib.sadmrg_last_error(self.h)
             raise SadmrgError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
 
+    def set_lanczos_tol(self, ov_tol: float):
+        self._check(self.lib.sadmrg_set_lanczos_tol(self.h, float(ov_tol)), "set_lanczos_tol")
+
     # -- frozen two-site problem -------------------------------------------
     def heff_plan(self, psi: BlockTensorData, hh_left: Optional[BlockTensorData],
                   hh_right: Optional[BlockTensorData], ops: Sequence[BlockTensorData],
@@ -213,6 +218,14 @@ class Handle:
     def heff_apply_device(self, psi_ptr: int, out_ptr: int, precision: int = PREC_FP64):
         self._check(self.lib.sadmrg_heff_apply_device(self.h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
                                                       int(precision)), "heff_apply_device")
+
+    def heff_profile(self, precision: int = PREC_FP64, reps: int = 10, psi_ptr: int = 0, out_ptr: int = 0):
+        """per-stage device milliseconds and algorithmic flops of one H_eff*psi"""
+        ms = (C.c_double * 2)()
+        fl = (C.c_double * 2)()
+        self._check(self.lib.sadmrg_heff_profile(self.h, int(precision), int(reps), C.c_void_p(psi_ptr or None),
+                                                 C.c_void_p(out_ptr or None), ms, fl), "heff_profile")
+        return [ms[0], ms[1]], [fl[0], fl[1]]
 
     def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         x = np.array(psi, dtype=self.dtype, copy=True)
@@ -318,3 +331,73 @@ class Handle:
     def chain_env_update(self, site: int, direction: int, real_env: bool):
         self._check(self.lib.sadmrg_chain_env_update(self.h, int(site), int(direction), int(bool(real_env))),
                     "chain_env_update")
+
+
+def read_exported_tensor(directory: str, name: str, cplx: bool) -> Optional[BlockTensorData]:
+    """A tensor written by sadmrg_chain_freeze(..., export_dir): <name>.txt + <name>.bin."""
+    path = os.path.join(directory, name + ".txt")
+    if not os.path.exists(path):
+        return None
+    dirs, qs, ds, blocks, ls = [], [], [], [], 0
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "nbond":
+                ls = int(t[3])
+            elif t[0] == "bond":
+                qi, di = t.index("q"), t.index("d")
+                dirs.append(int(t[3]))
+                qs.append([int(x) for x in t[qi + 1:di]])
+                ds.append([int(x) for x in t[di + 1:]])
+            elif t[0] == "block":
+                blocks.append(int(t[1]))
+    data = np.fromfile(os.path.join(directory, name + ".bin"), dtype=np.complex128 if cplx else np.float64)
+    return BlockTensorData(dirs, qs, ds, ls, np.array(blocks, np.int64), data)
+
+
+def load_exported_problem(h: "Handle", directory: str) -> BlockTensorData:
+    """Plan H_eff*psi on a problem exported by sadmrg_chain_freeze (the reference's operator set)."""
+    meta = open(os.path.join(directory, "meta.txt")).read().split("\n")
+    kv = meta[0].split()
+    m = {kv[i]: kv[i + 1] for i in range(0, len(kv) - 1, 2)}
+    il, ir, ns = int(m["il"]), int(m["ir"]), int(m["ns"])
+    coup = [float(x) for x in meta[1].split()[1:]]
+    hmap = {}
+    for line in meta[2:]:
+        t = line.split()
+        if t and t[0] == "hmap":
+            hmap[(int(t[1]), int(t[2]))] = int(t[3])
+    cplx = h.cplx
+    psi = read_exported_tensor(directory, "psi", cplx)
+    hl = read_exported_tensor(directory, "hh_il", cplx)
+    hr = read_exported_tensor(directory, "hh_ir", cplx)
+    ops, terms = [], []
+    left = il < ns // 2
+    m1, m4 = (il + 1, ns - ir) if left else (ns - ir, il + 1)
+    for m0 in range(m1):
+        acc = None
+        for mm in range(m4):
+            j, k = (m0, ir + mm) if left else (mm, ir + m0)
+            hv = hmap.get((j, k), 0)
+            if hv <= 0:
+                continue
+            t = read_exported_tensor(directory, f"opr_ir_{k}" if left else f"opr_il_{j}", cplx)
+            if t is None:
+                continue
+            if acc is None:
+                acc = BlockTensorData(t.dirs, t.qs, t.ds, t.locspin, t.blocks.copy(), coup[hv] * t.data)
+            else:
+                if list(acc.blocks) != list(t.blocks):
+                    raise ValueError("summed operators with different block sets are not supported here")
+                acc.data = acc.data + coup[hv] * t.data
+        if acc is None:
+            continue
+        fixed = read_exported_tensor(directory, f"opr_il_{m0}" if left else f"opr_ir_{ir + m0}", cplx)
+        if fixed is None:
+            continue
+        ops += [fixed, acc]
+        terms.append((len(ops) - 2, len(ops) - 1) if left else (len(ops) - 1, len(ops) - 2))
+    h.heff_plan(psi, hl, hr, ops, terms)
+    return psi
