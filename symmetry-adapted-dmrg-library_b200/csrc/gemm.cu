@@ -202,6 +202,294 @@ __global__ void __launch_bounds__(kThreads) items_f64(const GemmTerm* __restrict
       }
 }
 
+
+// ---------------------------------------------------------------------------
+// FP64, real, multistage: slabs are copied global -> shared with cp.async (8-byte,
+// zero-filled outside the block), STAGES-1 slabs in flight while the tensor cores
+// consume one.  Each operand slab is kept in the layout its global copy is
+// contiguous in (k-major for A, n-major for B when not transposed; the other way
+// when transposed), and the fragment loads follow that layout; row strides of
+// 68 / 20 doubles keep both the copies and the fragment loads conflict free.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int BM, int BN, int BK, int STAGES>
+__global__ void __launch_bounds__(kThreads, 3) items_f64_ms(const GemmTerm* __restrict__ terms,
+                                                            const GemmJob* __restrict__ jobs,
+                                                            const WorkItem* __restrict__ items, Bases bases,
+                                                            double* __restrict__ work) {
+  static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
+  constexpr int SK = BM + 4;        // k-major row stride (rows of m or n)
+  constexpr int SM = BK + 4;        // m/n-major row stride (rows of k)
+  constexpr int ABUF = (BM * SM > BK * SK) ? BM * SM : BK * SK;
+  constexpr int BBUF = (BN * SM > BK * SK) ? BN * SM : BK * SK;
+  extern __shared__ __align__(16) double smem_ms[];
+  double* As = smem_ms;                         // STAGES x ABUF
+  double* Bs = smem_ms + STAGES * ABUF;         // STAGES x BBUF
+  __shared__ double sh_alpha[STAGES];
+  __shared__ int sh_flags[STAGES];
+  const WorkItem it = items[blockIdx.x];
+  const GemmJob J = jobs[it.job];
+  const int row0 = it.tm * BM, col0 = it.tn * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
+  constexpr int EA = BM * BK / kThreads, EB = BK * BN / kThreads;
+  double acc[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  SlabWalk w{J.t0 + it.t0, it.k0, it.kcount};
+
+  auto issue = [&](int st, int tt, int k0, int kt) {
+    const GemmTerm T = terms[tt];
+    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
+    const double* A = static_cast<const double*>(bases.p[T.abuf]) + T.aoff;
+    const double* B = static_cast<const double*>(bases.p[T.bbuf]) + T.boff;
+    double* as = As + st * ABUF;
+    double* bs = Bs + st * BBUF;
+#pragma unroll
+    for (int q = 0; q < EA; ++q) {
+      const int e = tid + q * kThreads;
+      int i, kk;
+      if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
+      const int gi = row0 + i;
+      const bool ok = gi < J.m && kk < kt;
+      const double* src = ok ? (ta ? A + (k0 + kk) + (long long)gi * T.lda : A + gi + (long long)(k0 + kk) * T.lda) : A;
+      cp_async8(ta ? as + i * SM + kk : as + kk * SK + i, src, ok);
+    }
+#pragma unroll
+    for (int q = 0; q < EB; ++q) {
+      const int e = tid + q * kThreads;
+      int j, kk;
+      if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+      const int gj = col0 + j;
+      const bool ok = gj < J.n && kk < kt;
+      const double* src = ok ? (tb ? B + gj + (long long)(k0 + kk) * T.ldb : B + (k0 + kk) + (long long)gj * T.ldb) : B;
+      cp_async8(tb ? bs + kk * SK + j : bs + j * SM + kk, src, ok);
+    }
+    if (tid == 0) { sh_alpha[st] = T.ar; sh_flags[st] = T.flags; }
+  };
+
+  int issued = 0;
+#pragma unroll
+  for (int st = 0; st < STAGES - 1; ++st) {
+    int tt, kk, kt;
+    if (w.next(terms, BK, tt, kk, kt)) { issue(st, tt, kk, kt); ++issued; }
+    cp_async_commit();
+  }
+  for (int c = 0; c < issued; ++c) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int st = c % STAGES;
+    const double alpha = sh_alpha[st];
+    const int fl = sh_flags[st];
+    const bool ta = fl & TF_TA, tb = fl & TF_TB;
+    const double* as = As + st * ABUF;
+    const double* bs = Bs + st * BBUF;
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      const int k = k4 + (lane & 3);
+      double af[MT], bf[NT];
+#pragma unroll
+      for (int mi = 0; mi < MT; ++mi) {
+        const int r = wm * WM + mi * 8 + (lane >> 2);
+        af[mi] = (ta ? as[r * SM + k] : as[k * SK + r]) * alpha;
+      }
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) {
+        const int cc = wn * WN + ni * 8 + (lane >> 2);
+        bf[ni] = tb ? bs[k * SK + cc] : bs[cc * SM + k];
+      }
+#pragma unroll
+      for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
+    }
+    int tt, kk, kt;
+    if (w.next(terms, BK, tt, kk, kt)) { issue((c + STAGES - 1) % STAGES, tt, kk, kt); ++issued; }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  const bool direct = it.slot < 0;
+  double* C = direct ? static_cast<double*>(bases.p[J.cbuf]) + J.coff : work + (long long)it.slot * BM * BN;
+  const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = wm * WM + mi * 8 + (lane >> 2);
+        const int c = wn * WN + ni * 8 + 2 * (lane & 3) + e;
+        if (direct) {
+          if (row0 + r < J.m && col0 + c < J.n) {
+            const long long idx = (row0 + r) + (long long)(col0 + c) * J.ldc;
+            C[idx] = accum ? C[idx] + acc[mi][ni][e] : acc[mi][ni][e];
+          }
+        } else {
+          C[r + c * BM] = acc[mi][ni][e];
+        }
+      }
+}
+constexpr int kF64Stages = 3;
+constexpr size_t kF64MsSmem = (size_t)kF64Stages * 2 * (64 * 20) * sizeof(double);
+
+
+// 3xTF32, real, multistage: the same FP64 slabs as items_f64_ms; operands are
+// rounded to FP32 and split into TF32 hi/lo while the fragments are read.
+template <int BM, int BN, int BK, int STAGES>
+__global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* __restrict__ terms,
+                                                               const GemmJob* __restrict__ jobs,
+                                                               const WorkItem* __restrict__ items, Bases bases,
+                                                               double* __restrict__ work) {
+  static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
+  constexpr int SK = BM + 4, SM = BK + 4;
+  constexpr int ABUF = (BM * SM > BK * SK) ? BM * SM : BK * SK;
+  constexpr int BBUF = (BN * SM > BK * SK) ? BN * SM : BK * SK;
+  extern __shared__ __align__(16) double smem_ms[];
+  double* As = smem_ms;
+  double* Bs = smem_ms + STAGES * ABUF;
+  __shared__ double sh_alpha[STAGES];
+  __shared__ int sh_flags[STAGES];
+  const WorkItem it = items[blockIdx.x];
+  const GemmJob J = jobs[it.job];
+  const int row0 = it.tm * BM, col0 = it.tn * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, tg = lane & 3;
+  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 16, NT = WN / 8;
+  constexpr int EA = BM * BK / kThreads, EB = BK * BN / kThreads;
+  double accd[MT][NT][4];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) accd[i][j][e] = 0.0;
+  SlabWalk w{J.t0 + it.t0, it.k0, it.kcount};
+  auto issue = [&](int st, int tt, int k0, int kt) {
+    const GemmTerm T = terms[tt];
+    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
+    const double* A = static_cast<const double*>(bases.p[T.abuf]) + T.aoff;
+    const double* B = static_cast<const double*>(bases.p[T.bbuf]) + T.boff;
+    double* as = As + st * ABUF;
+    double* bs = Bs + st * BBUF;
+#pragma unroll
+    for (int q = 0; q < EA; ++q) {
+      const int e = tid + q * kThreads;
+      int i, kk;
+      if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
+      const int gi = row0 + i;
+      const bool ok = gi < J.m && kk < kt;
+      const double* src = ok ? (ta ? A + (k0 + kk) + (long long)gi * T.lda : A + gi + (long long)(k0 + kk) * T.lda) : A;
+      cp_async8(ta ? as + i * SM + kk : as + kk * SK + i, src, ok);
+    }
+#pragma unroll
+    for (int q = 0; q < EB; ++q) {
+      const int e = tid + q * kThreads;
+      int j, kk;
+      if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+      const int gj = col0 + j;
+      const bool ok = gj < J.n && kk < kt;
+      const double* src = ok ? (tb ? B + gj + (long long)(k0 + kk) * T.ldb : B + (k0 + kk) + (long long)gj * T.ldb) : B;
+      cp_async8(tb ? bs + kk * SK + j : bs + j * SM + kk, src, ok);
+    }
+    if (tid == 0) { sh_alpha[st] = T.ar; sh_flags[st] = T.flags; }
+  };
+  int issued = 0;
+#pragma unroll
+  for (int st = 0; st < STAGES - 1; ++st) {
+    int tt, kk, kt;
+    if (w.next(terms, BK, tt, kk, kt)) { issue(st, tt, kk, kt); ++issued; }
+    cp_async_commit();
+  }
+  for (int c = 0; c < issued; ++c) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int st = c % STAGES;
+    const double alpha = sh_alpha[st];
+    const int fl = sh_flags[st];
+    const bool ta = fl & TF_TA, tb = fl & TF_TB;
+    const double* as = As + st * ABUF;
+    const double* bs = Bs + st * BBUF;
+    float acc[MT][NT][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+#pragma unroll
+    for (int k8 = 0; k8 < BK; k8 += 8) {
+      uint32_t ah[MT][4], al[MT][4], bh[NT][2], bl[NT][2];
+#pragma unroll
+      for (int mi = 0; mi < MT; ++mi) {
+        const int r = wm * WM + mi * 16 + g;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int rr = r + ((e & 1) ? 8 : 0), k = k8 + tg + ((e & 2) ? 4 : 0);
+          split3((ta ? as[rr * SM + k] : as[k * SK + rr]) * alpha, ah[mi][e], al[mi][e]);
+        }
+      }
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) {
+        const int cc = wn * WN + ni * 8 + g;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int k = k8 + tg + (e ? 4 : 0);
+          split3(tb ? bs[k * SK + cc] : bs[cc * SM + k], bh[ni][e], bl[ni][e]);
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni) {
+          mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) accd[i][j][e] += (double)acc[i][j][e];
+    int tt, kk, kt;
+    if (w.next(terms, BK, tt, kk, kt)) { issue((c + STAGES - 1) % STAGES, tt, kk, kt); ++issued; }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  const bool direct = it.slot < 0;
+  double* C = direct ? static_cast<double*>(bases.p[J.cbuf]) + J.coff : work + (long long)it.slot * BM * BN;
+  const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = wm * WM + mi * 16 + g + (e >= 2 ? 8 : 0);
+        const int c = wn * WN + ni * 8 + 2 * tg + (e & 1);
+        if (direct) {
+          if (row0 + r < J.m && col0 + c < J.n) {
+            const long long idx = (row0 + r) + (long long)(col0 + c) * J.ldc;
+            C[idx] = accum ? C[idx] + accd[mi][ni][e] : accd[mi][ni][e];
+          }
+        } else {
+          C[r + c * BM] = accd[mi][ni][e];
+        }
+      }
+}
+
 // ---------------------------------------------------------------------------
 // FP64, complex: rr = Re*Re, ii = Im*Im, im = Re*Im + Im*Re; C = rr - ii + i im
 template <int BM, int BN, int BK>
@@ -529,11 +817,31 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
                   const Bases& b, void* work, cudaStream_t s) {
   if (nitems <= 0) return;
   if (prec == PREC_TF32X3) {
-    if (cplx) items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work);
-    else items_tf32x3<false, 64, 64, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work);
+    if (cplx) {
+      items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work);
+    } else {
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(items_tf32x3_ms<64, 64, 16, kF64Stages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kF64MsSmem);
+        attr = true;
+      }
+      items_tf32x3_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
+                                                                                 static_cast<double*>(work));
+    }
   } else {
-    if (cplx) items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work));
-    else items_f64<64, 64, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double*>(work));
+    if (cplx) {
+      items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work));
+    } else {
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(items_f64_ms<64, 64, 16, kF64Stages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kF64MsSmem);
+        attr = true;
+      }
+      items_f64_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
+                                                                              static_cast<double*>(work));
+    }
   }
 }
 
