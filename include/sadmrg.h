@@ -88,6 +88,18 @@ int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* byte
 int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision);
 /* out = H_eff psi with device pointers (no copies) */
 int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision);
+/* out = H_eff psi with device pointers, allocating nothing.  No counterpart in
+ * the reference (its H*v allocates per call).  For callers that cannot allocate
+ * device memory when they apply the operator -- a host whose memory pool is
+ * capped or fully reserved, or a solver loop that must not touch the allocator
+ * between steps.  The plan (sadmrg_heff_plan) must exist already; the stage-0
+ * products and split-K partial tiles go to one fixed 32 MiB device array
+ * compiled into the library, and a plan that needs more is refused with
+ * SADMRG_ERR_LIMIT.  The first call on a device looks that array's device
+ * address up (cudaGetSymbolAddress); make it before any stream capture.  Every
+ * call shares the array and overwrites it, so calls that overlap on the GPU
+ * (two streams, two handles on one device) race. */
+int sadmrg_heff_apply_noalloc(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision);
 /* Per-stage device time of one H_eff*psi (CUDA events on the handle's stream,
  * averaged over reps): ms[0] stage 0 (X = op1^T psi products), ms[1] stage 1
  * (the output accumulation lists); flops[] the algorithmic flops of each stage.

@@ -208,6 +208,38 @@ int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_de
   });
 }
 
+// Same matvec as sadmrg_heff_apply_device, but the products of stage 0 and the
+// split-K partial tiles go to the library's fixed device scratch instead of the
+// plan's buffers, so this call allocates nothing (see include/sadmrg.h).
+int sadmrg_heff_apply_noalloc(sadmrg_handle* h, const void* psi_dev, void* out_dev, int precision) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply_noalloc: no plan");
+    SADMRG_REQUIRE(psi_dev && out_dev, SADMRG_ERR_ARG, "heff_apply_noalloc: null device pointer");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG,
+                   "heff_apply_noalloc: precision");
+    const HeffPlan<S>& H = *S_.heff;
+    const size_t xbytes = ((size_t)H.plan.scratch_elems * sizeof(S) + 255) & ~size_t(255);
+    const size_t need = xbytes + H.plan.work_bytes();
+    if (need > kNoAllocScratchBytes)
+      throw Error(SADMRG_ERR_LIMIT, "heff_apply_noalloc: the plan needs " + std::to_string(need) +
+                                        " bytes of scratch, more than the fixed " +
+                                        std::to_string(kNoAllocScratchBytes) + " bytes");
+    void* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != 0)
+      throw Error(SADMRG_ERR_CUDA, std::string("heff_apply_noalloc: cudaGetSymbolAddress: ") +
+                                       cudaGetErrorString((cudaError_t)rc));
+    Bases b{};
+    b.p[0] = const_cast<void*>(psi_dev);
+    b.p[1] = out_dev;
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = scratch;
+    H.plan.run(h->ctx, ScalarInfo<S>::cplx, precision, b, 0, -1, static_cast<unsigned char*>(scratch) + xbytes);
+  });
+}
+
 int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, double* ms,
                         double* flops) {
   return dispatch(h, [&](auto* tag) {

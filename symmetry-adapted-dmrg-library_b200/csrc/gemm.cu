@@ -20,6 +20,7 @@
 //            Yokota 2022).
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -843,6 +844,31 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
                                                                               static_cast<double*>(work));
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fixed scratch for the allocation-free H_eff*psi entry point.  It lives for the
+// life of the process on every device that loads the library.  Host code must not
+// use the symbol's host-side name as a device address: the device address is
+// looked up once per device with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+int noalloc_scratch(void** ptr) {
+  static std::mutex mu;
+  static void* cache[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(mu);
+  if (!cache[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return (int)e;
+    cache[dev] = p;
+  }
+  *ptr = cache[dev];
+  return 0;
 }
 
 void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,

@@ -48,6 +48,11 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
                   const Bases& b, void* work, cudaStream_t s);
 void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
                    cudaStream_t s);
+// Fixed device scratch of the allocation-free H_eff*psi entry point (gemm.cu).
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
+// Device address of that scratch on the current device (looked up once per
+// device); returns 0 or a cudaError_t value.
+int noalloc_scratch(void** ptr);
 int gemm_tile_m(bool cplx, int prec);
 int gemm_tile_n(bool cplx, int prec);
 

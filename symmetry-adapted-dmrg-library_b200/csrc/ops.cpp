@@ -191,17 +191,19 @@ int GemmPlan::launches_per_run() const {
   return n;
 }
 
-void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi) const {
+void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi,
+                   void* work_override) const {
   if (stage_hi < 0) stage_hi = nstage;
+  void* wk = work_override ? work_override : work->get();
   for (int s = stage_lo; s < stage_hi; ++s) {
     const int ni = stage_items[s + 1] - stage_items[s];
     if (ni > 0) {
-      launch_items(cplx, prec, d_terms, d_jobs, d_items + stage_items[s], ni, b, work->get(), c.stream);
+      launch_items(cplx, prec, d_terms, d_jobs, d_items + stage_items[s], ni, b, wk, c.stream);
       ++c.launches;
     }
     const int nr = stage_reds[s + 1] - stage_reds[s];
     if (nr > 0) {
-      launch_reduce(cplx, d_jobs, d_reds + stage_reds[s], nr, b, work->get(), c.stream);
+      launch_reduce(cplx, d_jobs, d_reds + stage_reds[s], nr, b, wk, c.stream);
       ++c.launches;
     }
   }

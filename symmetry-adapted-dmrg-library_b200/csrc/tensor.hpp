@@ -91,7 +91,9 @@ struct GemmPlan {
                 double ar, double ai);
   long long alloc_scratch(long long elems) { long long o = scratch_elems; scratch_elems += elems; return o; }
   void finalize(Ctx& c, bool cplx);
-  void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1) const;
+  void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1,
+           void* work_override = nullptr) const;
+  size_t work_bytes() const { return work ? work->bytes() : 0; }
   int launches_per_run() const;
   bool empty() const { return jobs.empty(); }
 };

@@ -26,7 +26,7 @@ PREC_FP64, PREC_TF32X3 = 0, 1
 
 EXPORTED = [
     "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
-    "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device",
+    "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device", "sadmrg_heff_apply_noalloc",
     "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
     "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
@@ -67,6 +67,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
+        "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
         "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
@@ -226,6 +227,11 @@ class Handle:
         self._check(self.lib.sadmrg_heff_profile(self.h, int(precision), int(reps), C.c_void_p(psi_ptr or None),
                                                  C.c_void_p(out_ptr or None), ms, fl), "heff_profile")
         return [ms[0], ms[1]], [fl[0], fl[1]]
+
+    def heff_apply_noalloc(self, psi_ptr: int, out_ptr: int, precision: int = PREC_FP64):
+        """H_eff*psi on device pointers without allocating (library's fixed device scratch)."""
+        self._check(self.lib.sadmrg_heff_apply_noalloc(self.h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
+                                                       int(precision)), "heff_apply_noalloc")
 
     def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         x = np.array(psi, dtype=self.dtype, copy=True)
