@@ -68,6 +68,15 @@ int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out);
 int sadmrg_destroy(sadmrg_handle* h);
 const char* sadmrg_last_error(const sadmrg_handle* h);
 
+/* Device status of the tcgen05 GEMM kernels (no counterpart in the reference,
+ * whose CPU code has nothing to wait on).  Synchronises the handle's stream,
+ * stores 0 if every bounded wait since the last query completed, otherwise a
+ * nonzero code (the tiles those waits guarded were left unwritten), and clears
+ * it.  The calls that synchronise anyway (heff_apply, heff_lanczos,
+ * heff_profile, chain_idmrg, chain_sweep) check it themselves and fail with
+ * SADMRG_ERR_CUDA. */
+int sadmrg_device_status(sadmrg_handle* h, int* status);
+
 /* Lanczos convergence: stop at a check (every 4 steps) once |<v|Hv>|/|Hv| is
  * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338). */
 int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol);

@@ -81,6 +81,16 @@ static State<S>& st_of(sadmrg_handle* h);
 template <> State<double>& st_of<double>(sadmrg_handle* h) { return h->sd; }
 template <> State<dcmplex>& st_of<dcmplex>(sadmrg_handle* h) { return h->sz; }
 
+// A tcgen05 item kernel whose bounded wait ran out leaves its tile unwritten and
+// raises a device status word; calls that synchronise anyway check it.
+static void check_device_status() {
+  const int v = umma_status(true);
+  if (v < 0) throw Error(SADMRG_ERR_CUDA, "cannot read the tcgen05 status word");
+  if (v != 0)
+    throw Error(SADMRG_ERR_CUDA, "tcgen05 GEMM: a bounded wait ran out (status " + std::to_string(v) +
+                                     "); the results of this call are invalid");
+}
+
 template <class F>
 static int dispatch(sadmrg_handle* h, F&& f) {
   return guard(h, [&]() {
@@ -92,6 +102,16 @@ static int dispatch(sadmrg_handle* h, F&& f) {
 extern "C" {
 
 int sadmrg_version(void) { return 10000; }
+
+int sadmrg_device_status(sadmrg_handle* h, int* status) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(status, SADMRG_ERR_ARG, "device_status: null output");
+    SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+    const int v = umma_status(true);
+    SADMRG_REQUIRE(v >= 0, SADMRG_ERR_CUDA, "device_status: cannot read the status word");
+    *status = v;
+  });
+}
 
 int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out) {
   if (!out || (sym != 0 && sym != 1)) return SADMRG_ERR_ARG;
@@ -195,6 +215,7 @@ int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, in
     S_.heff->apply(c, din, dout, precision);
     SADMRG_CUDA(cudaMemcpyAsync(out_host, dout, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_status();
   });
 }
 
@@ -221,7 +242,7 @@ int sadmrg_heff_apply_noalloc(sadmrg_handle* h, const void* psi_dev, void* out_d
                    "heff_apply_noalloc: precision");
     const HeffPlan<S>& H = *S_.heff;
     const size_t xbytes = ((size_t)H.plan.scratch_elems * sizeof(S) + 255) & ~size_t(255);
-    const size_t need = xbytes + H.plan.work_bytes();
+    const size_t need = xbytes + H.plan.work_bytes(ScalarInfo<S>::cplx, precision);
     if (need > kNoAllocScratchBytes)
       throw Error(SADMRG_ERR_LIMIT, "heff_apply_noalloc: the plan needs " + std::to_string(need) +
                                         " bytes of scratch, more than the fixed " +
@@ -273,6 +294,7 @@ int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* p
       acc[1] += t1;
     }
     for (auto& e : ev) cudaEventDestroy(e);
+    check_device_status();
     ms[0] = acc[0] / reps;
     ms[1] = acc[1] / reps;
     // algorithmic flops per stage
@@ -299,6 +321,7 @@ int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precisi
     LanczosStats st = lanczos_solve<S>(c, *S_.heff, dv, mlanc, precision);
     SADMRG_CUDA(cudaMemcpyAsync(psi_host, dv, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_status();
     if (energy) *energy = st.energy;
     if (matvecs) *matvecs = st.matvecs;
   });
@@ -346,6 +369,7 @@ int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy) {
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     S_.chain->do_idmrg();
     SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+    check_device_status();
     if (energy) *energy = S_.chain->energy();
   });
 }
@@ -367,6 +391,7 @@ int sadmrg_chain_sweep(sadmrg_handle* h, double* energy) {
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     S_.chain->sweep();
     SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+    check_device_status();
     if (energy) *energy = S_.chain->energy();
   });
 }

@@ -140,7 +140,7 @@ HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, con
         }
       }
   }
-  p.finalize(c, kCx<S>);
+  p.finalize(c, kCx<S>, /*mixed=*/true);
   H.scratch = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(p.scratch_elems, 1), c.stream);
   H.flops = p.flops;
   H.bytes = (2 * H.n + tot) * (long long)sizeof(S);

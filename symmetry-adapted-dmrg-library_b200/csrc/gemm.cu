@@ -872,9 +872,8 @@ int noalloc_scratch(void** ptr) {
 }
 
 void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
-                   cudaStream_t s) {
+                   int BM, int BN, cudaStream_t s) {
   if (nred <= 0) return;
-  const int BM = gemm_tile_m(cplx, 0), BN = gemm_tile_n(cplx, 0);
   if (cplx) reduce_slots<true><<<nred, 256, 0, s>>>(jobs, red, b, work, BM, BN);
   else reduce_slots<false><<<nred, 256, 0, s>>>(jobs, red, b, work, BM, BN);
 }

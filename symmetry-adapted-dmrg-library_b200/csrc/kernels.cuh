@@ -43,11 +43,23 @@ struct Bases {
   void* p[kMaxBases];
 };
 
+// Item kernel families.  GEMM_MMA_SYNC: FP64 DMMA and the mma.sync 3xTF32
+// (gemm.cu); GEMM_UMMA: tcgen05 3xTF32 with the accumulator in tensor memory,
+// real data only (umma.cu).
+enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
+constexpr int kUmmaTileM = 128;
+
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
                   const Bases& b, void* work, cudaStream_t s);
+void launch_items_umma(const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems, const Bases& b,
+                       void* work, cudaStream_t s);
+int umma_tile_n();
+// status word of the tcgen05 kernels: 0 = fine, otherwise a wait ran out (the
+// tile it guarded was not written); reset clears it.  -1 if it cannot be read.
+int umma_status(bool reset);
 void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
-                   cudaStream_t s);
+                   int bm, int bn, cudaStream_t s);
 // Fixed device scratch of the allocation-free H_eff*psi entry point (gemm.cu).
 constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 // Device address of that scratch on the current device (looked up once per

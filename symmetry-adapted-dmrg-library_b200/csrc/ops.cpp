@@ -83,22 +83,12 @@ void GemmPlan::add_term(int job, int abuf, long long aoff, int lda, int bbuf, lo
   job_terms[job].push_back(t);
 }
 
-void GemmPlan::finalize(Ctx& c, bool cplx) {
-  flat_terms.clear();
-  flops = 0;
-  for (size_t j = 0; j < jobs.size(); ++j) {
-    jobs[j].t0 = (int)flat_terms.size();
-    jobs[j].nt = (int)job_terms[j].size();
-    for (auto& t : job_terms[j]) {
-      flat_terms.push_back(t);
-      flops += (cplx ? 8LL : 2LL) * jobs[j].m * (long long)jobs[j].n * t.k;
-    }
-  }
-  const int BM = gemm_tile_m(cplx, 0), BN = gemm_tile_n(cplx, 0);
-  items.clear();
-  reds.clear();
-  stage_items.assign(nstage + 1, 0);
-  stage_reds.assign(nstage + 1, 0);
+void GemmPlan::build_schedule(GemmSchedule& sc, bool cplx) {
+  const int BM = sc.bm, BN = sc.bn;
+  sc.items.clear();
+  sc.reds.clear();
+  sc.stage_items.assign(nstage + 1, 0);
+  sc.stage_reds.assign(nstage + 1, 0);
   int nslot = 0;
   for (int s = 0; s < nstage; ++s) {
     // split-K chunk: enough items to fill the GPU, never below 128 of k
@@ -146,47 +136,93 @@ void GemmPlan::finalize(Ctx& c, bool cplx) {
             }
             pos += len;
           }
-          reds.push_back(RedItem{(int)j, a, b, slot0, (int)nch});
+          sc.reds.push_back(RedItem{(int)j, a, b, slot0, (int)nch});
         }
     }
     // longest work first
     std::stable_sort(its.begin(), its.end(), [](const std::pair<long long, WorkItem>& x,
                                                 const std::pair<long long, WorkItem>& y) { return x.first > y.first; });
-    stage_items[s] = (int)items.size();
-    for (auto& p : its) items.push_back(p.second);
-    stage_items[s + 1] = (int)items.size();
-    stage_reds[s + 1] = (int)reds.size();
+    sc.stage_items[s] = (int)sc.items.size();
+    for (auto& p : its) sc.items.push_back(p.second);
+    sc.stage_items[s + 1] = (int)sc.items.size();
+    sc.stage_reds[s + 1] = (int)sc.reds.size();
   }
   for (int s = 0; s < nstage; ++s) {
-    stage_items[s + 1] = std::max(stage_items[s + 1], stage_items[s]);
-    stage_reds[s + 1] = std::max(stage_reds[s + 1], stage_reds[s]);
+    sc.stage_items[s + 1] = std::max(sc.stage_items[s + 1], sc.stage_items[s]);
+    sc.stage_reds[s + 1] = std::max(sc.stage_reds[s + 1], sc.stage_reds[s]);
   }
-  const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size(),
-               bi = sizeof(WorkItem) * items.size(), br = sizeof(RedItem) * reds.size();
+  sc.nslot = nslot;
+  (void)cplx;
+}
+
+void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed) {
+  flat_terms.clear();
+  flops = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    jobs[j].t0 = (int)flat_terms.size();
+    jobs[j].nt = (int)job_terms[j].size();
+    for (auto& t : job_terms[j]) {
+      flat_terms.push_back(t);
+      flops += (cplx ? 8LL : 2LL) * jobs[j].m * (long long)jobs[j].n * t.k;
+    }
+  }
+  sched.clear();
+  sched.emplace_back();
+  sched[0].kind = GEMM_MMA_SYNC;
+  sched[0].bm = gemm_tile_m(cplx, 0);
+  sched[0].bn = gemm_tile_n(cplx, 0);
+  if (mixed && !cplx) {
+    sched.emplace_back();
+    sched[1].kind = GEMM_UMMA;
+    sched[1].bm = kUmmaTileM;
+    sched[1].bn = umma_tile_n();
+  }
+  for (auto& sc : sched) build_schedule(sc, cplx);
+
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t total = al(bt) + al(bj) + al(bi) + al(br) + 256;
+  const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size();
+  size_t total = al(bt) + al(bj) + 256;
+  for (auto& sc : sched) total += al(sizeof(WorkItem) * sc.items.size()) + al(sizeof(RedItem) * sc.reds.size());
   std::vector<unsigned char> h(total, 0);
   if (bt) std::memcpy(h.data(), flat_terms.data(), bt);
   if (bj) std::memcpy(h.data() + al(bt), jobs.data(), bj);
-  if (bi) std::memcpy(h.data() + al(bt) + al(bj), items.data(), bi);
-  if (br) std::memcpy(h.data() + al(bt) + al(bj) + al(bi), reds.data(), br);
+  std::vector<size_t> io(sched.size()), ro(sched.size());
+  size_t pos = al(bt) + al(bj);
+  for (size_t i = 0; i < sched.size(); ++i) {
+    const size_t bi = sizeof(WorkItem) * sched[i].items.size(), br = sizeof(RedItem) * sched[i].reds.size();
+    io[i] = pos;
+    if (bi) std::memcpy(h.data() + pos, sched[i].items.data(), bi);
+    pos += al(bi);
+    ro[i] = pos;
+    if (br) std::memcpy(h.data() + pos, sched[i].reds.data(), br);
+    pos += al(br);
+  }
   dev = std::make_shared<DevBuf>(total, c.stream);
   SADMRG_CUDA(cudaMemcpyAsync(dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
   unsigned char* base = dev->as<unsigned char>();
   d_terms = reinterpret_cast<GemmTerm*>(base);
   d_jobs = reinterpret_cast<GemmJob*>(base + al(bt));
-  d_items = reinterpret_cast<WorkItem*>(base + al(bt) + al(bj));
-  d_reds = reinterpret_cast<RedItem*>(base + al(bt) + al(bj) + al(bi));
-  work = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * BM * BN * (cplx ? 16 : 8), c.stream);
+  for (size_t i = 0; i < sched.size(); ++i) {
+    auto& sc = sched[i];
+    sc.d_items = reinterpret_cast<WorkItem*>(base + io[i]);
+    sc.d_reds = reinterpret_cast<RedItem*>(base + ro[i]);
+    sc.work = std::make_shared<DevBuf>((size_t)std::max(sc.nslot, 1) * sc.bm * sc.bn * (cplx ? 16 : 8), c.stream);
+  }
   // the host copy must stay alive until the async copy completes
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-int GemmPlan::launches_per_run() const {
+const GemmSchedule& GemmPlan::schedule(bool cplx, int prec) const {
+  if (prec == PREC_TF32X3 && !cplx && sched.size() > 1) return sched[1];
+  return sched.at(0);
+}
+
+int GemmPlan::launches_per_run(bool cplx, int prec) const {
+  const GemmSchedule& sc = schedule(cplx, prec);
   int n = 0;
   for (int s = 0; s < nstage; ++s) {
-    if (stage_items[s + 1] > stage_items[s]) ++n;
-    if (stage_reds[s + 1] > stage_reds[s]) ++n;
+    if (sc.stage_items[s + 1] > sc.stage_items[s]) ++n;
+    if (sc.stage_reds[s + 1] > sc.stage_reds[s]) ++n;
   }
   return n;
 }
@@ -194,16 +230,18 @@ int GemmPlan::launches_per_run() const {
 void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi,
                    void* work_override) const {
   if (stage_hi < 0) stage_hi = nstage;
-  void* wk = work_override ? work_override : work->get();
+  const GemmSchedule& sc = schedule(cplx, prec);
+  void* wk = work_override ? work_override : sc.work->get();
   for (int s = stage_lo; s < stage_hi; ++s) {
-    const int ni = stage_items[s + 1] - stage_items[s];
+    const int ni = sc.stage_items[s + 1] - sc.stage_items[s];
     if (ni > 0) {
-      launch_items(cplx, prec, d_terms, d_jobs, d_items + stage_items[s], ni, b, wk, c.stream);
+      if (sc.kind == GEMM_UMMA) launch_items_umma(d_terms, d_jobs, sc.d_items + sc.stage_items[s], ni, b, wk, c.stream);
+      else launch_items(cplx, prec, d_terms, d_jobs, sc.d_items + sc.stage_items[s], ni, b, wk, c.stream);
       ++c.launches;
     }
-    const int nr = stage_reds[s + 1] - stage_reds[s];
+    const int nr = sc.stage_reds[s + 1] - sc.stage_reds[s];
     if (nr > 0) {
-      launch_reduce(cplx, d_jobs, d_reds + stage_reds[s], nr, b, wk, c.stream);
+      launch_reduce(cplx, d_jobs, sc.d_reds + sc.stage_reds[s], nr, b, wk, sc.bm, sc.bn, c.stream);
       ++c.launches;
     }
   }

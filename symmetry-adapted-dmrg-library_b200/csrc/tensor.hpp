@@ -64,6 +64,21 @@ template <class S> std::vector<Blk> blocks_of(const BTensor<S>& t);
 template <class S> BTensor<S> alloc_tensor(Ctx& c, const Struct& st, const std::vector<char>& present);
 template <class S> BTensor<S> clone(Ctx& c, const BTensor<S>& t);
 
+// Work items and split-K reductions of a plan for one output-tile shape.
+struct GemmSchedule {
+  int kind = GEMM_MMA_SYNC;       // which item kernel family runs it
+  int bm = 64, bn = 64;
+  std::vector<WorkItem> items;
+  std::vector<RedItem> reds;
+  std::vector<int> stage_items;   // item offsets per stage (size nstage+1)
+  std::vector<int> stage_reds;    // reduction offsets per stage (size nstage+1)
+  WorkItem* d_items = nullptr;
+  RedItem* d_reds = nullptr;
+  std::shared_ptr<DevBuf> work;   // split-K partial tiles
+  int nslot = 0;
+  size_t work_bytes() const { return work ? work->bytes() : 0; }
+};
+
 // A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.
 struct GemmPlan {
   std::vector<std::vector<GemmTerm>> job_terms;
@@ -72,17 +87,11 @@ struct GemmPlan {
   long long scratch_elems = 0;
   int nstage = 2;
   // device copy
-  std::vector<WorkItem> items;
-  std::vector<RedItem> reds;
-  std::vector<int> stage_items;   // item offsets per stage (size nstage+1)
-  std::vector<int> stage_reds;    // reduction offsets per stage (size nstage+1)
   std::vector<GemmTerm> flat_terms;
+  std::vector<GemmSchedule> sched;   // [0]: mma.sync tiles; [1] (real mixed plans): tcgen05 tiles
   std::shared_ptr<DevBuf> dev;
-  std::shared_ptr<DevBuf> work;   // split-K partial tiles
   GemmTerm* d_terms = nullptr;
   GemmJob* d_jobs = nullptr;
-  WorkItem* d_items = nullptr;
-  RedItem* d_reds = nullptr;
   long long flops = 0;            // algorithmic flops of one execution (real multiply-adds * 2)
   int target_items = 148 * 8;     // work items per stage the split-K aims for
 
@@ -90,12 +99,18 @@ struct GemmPlan {
   void add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
                 double ar, double ai);
   long long alloc_scratch(long long elems) { long long o = scratch_elems; scratch_elems += elems; return o; }
-  void finalize(Ctx& c, bool cplx);
+  // mixed: also schedule the tcgen05 3xTF32 tiles (real plans that run PREC_TF32X3)
+  void finalize(Ctx& c, bool cplx, bool mixed = false);
+  // the schedule a run at this precision uses
+  const GemmSchedule& schedule(bool cplx, int prec) const;
   void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1,
            void* work_override = nullptr) const;
-  size_t work_bytes() const { return work ? work->bytes() : 0; }
-  int launches_per_run() const;
+  size_t work_bytes(bool cplx, int prec) const { return schedule(cplx, prec).work_bytes(); }
+  int launches_per_run(bool cplx, int prec) const;
   bool empty() const { return jobs.empty(); }
+
+ private:
+  void build_schedule(GemmSchedule& s, bool cplx);
 };
 
 }  // namespace sadmrg

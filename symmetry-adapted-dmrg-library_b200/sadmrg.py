@@ -62,6 +62,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_create": ([C.c_int, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
         "sadmrg_destroy": ([vp], C.c_int),
         "sadmrg_last_error": ([vp], C.c_char_p),
+        "sadmrg_device_status": ([vp, ip], C.c_int),
         "sadmrg_heff_plan": ([vp, td, td, td, C.c_int, td, C.c_int, ip, ip], C.c_int),
         "sadmrg_set_lanczos_tol": ([vp, C.c_double], C.c_int),
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
@@ -219,6 +220,12 @@ class Handle:
     def heff_apply_device(self, psi_ptr: int, out_ptr: int, precision: int = PREC_FP64):
         self._check(self.lib.sadmrg_heff_apply_device(self.h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
                                                       int(precision)), "heff_apply_device")
+
+    def device_status(self) -> int:
+        """Status word of the tcgen05 kernels since the last query (0 = fine); clears it."""
+        v = C.c_int(0)
+        self._check(self.lib.sadmrg_device_status(self.h, C.byref(v)), "device_status")
+        return v.value
 
     def heff_profile(self, precision: int = PREC_FP64, reps: int = 10, psi_ptr: int = 0, out_ptr: int = 0):
         """per-stage device milliseconds and algorithmic flops of one H_eff*psi"""
