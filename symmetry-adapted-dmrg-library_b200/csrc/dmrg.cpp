@@ -140,7 +140,9 @@ HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, con
         }
       }
   }
-  p.finalize(c, kCx<S>, /*mixed=*/true);
+  Bases cb{};
+  cb.p[2] = H.opsbuf->get();
+  p.finalize(c, kCx<S>, /*mixed=*/true, &cb);
   H.scratch = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(p.scratch_elems, 1), c.stream);
   H.flops = p.flops;
   H.bytes = (2 * H.n + tot) * (long long)sizeof(S);

@@ -44,20 +44,62 @@ struct Bases {
 };
 
 // Item kernel families.  GEMM_MMA_SYNC: FP64 DMMA and the mma.sync 3xTF32
-// (gemm.cu); GEMM_UMMA: tcgen05 3xTF32 with the accumulator in tensor memory,
-// real data only (umma.cu).
+// (gemm.cu); GEMM_UMMA: tcgen05 3xTF32 over pre-split operand panels with the
+// accumulator in tensor memory, real data only (umma.cu).
 enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
-constexpr int kUmmaTileM = 128;
 
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
                   const Bases& b, void* work, cudaStream_t s);
-void launch_items_umma(const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems, const Bases& b,
-                       void* work, cudaStream_t s);
-int umma_tile_n();
-// status word of the tcgen05 kernels: 0 = fine, otherwise a wait ran out (the
-// tile it guarded was not written); reset clears it.  -1 if it cannot be read.
+
+// ---- tcgen05 3xTF32 over TF32 hi/lo operand panels (umma.cu) --------------
+// An operand (rows x K after op) is stored as panels: panel (p, s) holds rows
+// [p*T, p*T + T) and k [32 s, 32 s + 32) as a hi plane then a lo plane, each
+// [kg = 0..7][row = 0..T-1][4 consecutive k] of TF32 bit patterns (x ~ hi + lo),
+// zero padded; it starts at dst + (p * nslab + s) * T * 256 bytes.  This is the
+// K-major, no-swizzle core-matrix layout tcgen05.mma reads, so a panel moves
+// into shared memory as one contiguous bulk copy.
+constexpr int kPanelK = 32;
+constexpr int kUmmaTileM = 128;
+struct PackJob {              // FP64 matrix -> panels
+  long long src;              // element offset in its source buffer
+  long long dst;              // byte offset of panel (0, 0) in the packed buffer
+  long long chunk0;           // first 16-byte chunk of this job in the launch (prefix sum)
+  int srcbuf, ld, rows, K, trans, T;   // trans 0: (r, k) at src[r + k*ld]; 1: at src[k + r*ld]
+};
+struct UTerm {                // a term's operands as panel sets: A (T = 128), B (T = BN)
+  long long a, b;             // byte offsets of panel (0, 0)
+  int abuf, bbuf;             // 0: constant panels, 1: per-apply panels
+  int nslab, klast;           // k slabs, k of the last slab (1..32)
+};
+struct UJob {                 // output tile grid of one job
+  long long coff;             // FP64 output: bases.p[cbuf] + coff, column-major, ldc
+  long long pack;             // >= 0: the result becomes A panels (T = 128) at this byte offset of the
+                              // per-apply buffer, scaled by alpha, with pack_nslab slabs per panel
+  double alpha;
+  int cbuf, m, n, ldc, flags, t0, nt, pack_nslab;
+};
+struct UItem {                // one output tile x a run of consecutive slabs
+  int job, tm, tn, t0, s0, nslab, slot;   // t0: first term (absolute), s0: its first slab; slot < 0: direct
+};
+struct URed {                 // C tile = sum of FP32 partial slots [slot0, slot0 + nslot) in fixed order
+  int job, tm, tn, slot0, nslot;
+};
+struct UBufs {
+  const unsigned char* pconst;
+  unsigned char* pvar;
+  float* slots;
+};
+void launch_pack(const PackJob* jobs, int njobs, long long nchunks, const Bases& b, unsigned char* dst,
+                 cudaStream_t s);
+void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
+                       const UBufs& u, cudaStream_t s);
+void launch_umma_reduce(int bn, const UJob* jobs, const URed* red, int nred, const Bases& b, const UBufs& u,
+                        cudaStream_t s);
+// status word of the tcgen05 kernels: 0 = fine, otherwise a bounded wait ran out
+// (the tiles it guarded were not written); reset clears it.  -1 if unreadable.
 int umma_status(bool reset);
+int device_sm_count();
 void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
                    int bm, int bn, cudaStream_t s);
 // Fixed device scratch of the allocation-free H_eff*psi entry point (gemm.cu).

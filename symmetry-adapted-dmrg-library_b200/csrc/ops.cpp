@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <tuple>
 
 namespace sadmrg {
 
@@ -155,7 +157,7 @@ void GemmPlan::build_schedule(GemmSchedule& sc, bool cplx) {
   (void)cplx;
 }
 
-void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed) {
+void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed, const Bases* const_bases) {
   flat_terms.clear();
   flops = 0;
   for (size_t j = 0; j < jobs.size(); ++j) {
@@ -166,63 +168,288 @@ void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed) {
       flops += (cplx ? 8LL : 2LL) * jobs[j].m * (long long)jobs[j].n * t.k;
     }
   }
-  sched.clear();
-  sched.emplace_back();
-  sched[0].kind = GEMM_MMA_SYNC;
-  sched[0].bm = gemm_tile_m(cplx, 0);
-  sched[0].bn = gemm_tile_n(cplx, 0);
-  if (mixed && !cplx) {
-    sched.emplace_back();
-    sched[1].kind = GEMM_UMMA;
-    sched[1].bm = kUmmaTileM;
-    sched[1].bn = umma_tile_n();
-  }
-  for (auto& sc : sched) build_schedule(sc, cplx);
+  sched = GemmSchedule{};
+  sched.bm = gemm_tile_m(cplx, 0);
+  sched.bn = gemm_tile_n(cplx, 0);
+  build_schedule(sched, cplx);
 
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size();
-  size_t total = al(bt) + al(bj) + 256;
-  for (auto& sc : sched) total += al(sizeof(WorkItem) * sc.items.size()) + al(sizeof(RedItem) * sc.reds.size());
+  const size_t bt = sizeof(GemmTerm) * flat_terms.size(), bj = sizeof(GemmJob) * jobs.size(),
+               bi = sizeof(WorkItem) * sched.items.size(), br = sizeof(RedItem) * sched.reds.size();
+  const size_t total = al(bt) + al(bj) + al(bi) + al(br) + 256;
   std::vector<unsigned char> h(total, 0);
   if (bt) std::memcpy(h.data(), flat_terms.data(), bt);
   if (bj) std::memcpy(h.data() + al(bt), jobs.data(), bj);
-  std::vector<size_t> io(sched.size()), ro(sched.size());
-  size_t pos = al(bt) + al(bj);
-  for (size_t i = 0; i < sched.size(); ++i) {
-    const size_t bi = sizeof(WorkItem) * sched[i].items.size(), br = sizeof(RedItem) * sched[i].reds.size();
-    io[i] = pos;
-    if (bi) std::memcpy(h.data() + pos, sched[i].items.data(), bi);
-    pos += al(bi);
-    ro[i] = pos;
-    if (br) std::memcpy(h.data() + pos, sched[i].reds.data(), br);
-    pos += al(br);
-  }
+  if (bi) std::memcpy(h.data() + al(bt) + al(bj), sched.items.data(), bi);
+  if (br) std::memcpy(h.data() + al(bt) + al(bj) + al(bi), sched.reds.data(), br);
   dev = std::make_shared<DevBuf>(total, c.stream);
   SADMRG_CUDA(cudaMemcpyAsync(dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
   unsigned char* base = dev->as<unsigned char>();
   d_terms = reinterpret_cast<GemmTerm*>(base);
   d_jobs = reinterpret_cast<GemmJob*>(base + al(bt));
-  for (size_t i = 0; i < sched.size(); ++i) {
-    auto& sc = sched[i];
-    sc.d_items = reinterpret_cast<WorkItem*>(base + io[i]);
-    sc.d_reds = reinterpret_cast<RedItem*>(base + ro[i]);
-    sc.work = std::make_shared<DevBuf>((size_t)std::max(sc.nslot, 1) * sc.bm * sc.bn * (cplx ? 16 : 8), c.stream);
-  }
-  // the host copy must stay alive until the async copy completes
+  sched.d_items = reinterpret_cast<WorkItem*>(base + al(bt) + al(bj));
+  sched.d_reds = reinterpret_cast<RedItem*>(base + al(bt) + al(bj) + al(bi));
+  sched.work = std::make_shared<DevBuf>((size_t)std::max(sched.nslot, 1) * sched.bm * sched.bn * (cplx ? 16 : 8),
+                                        c.stream);
+  umma.reset();
+  if (mixed && !cplx && const_bases) build_umma(c, *const_bases);
+  // the host copies must stay alive until the async copies complete
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-const GemmSchedule& GemmPlan::schedule(bool cplx, int prec) const {
-  if (prec == PREC_TF32X3 && !cplx && sched.size() > 1) return sched[1];
-  return sched.at(0);
+// tcgen05 schedule (see UmmaSchedule).  Returns false, leaving umma empty, when
+// some term does not fit the panel scheme; the plan then runs 3xTF32 on the
+// mma.sync kernels.
+bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
+  auto U = std::make_shared<UmmaSchedule>();
+  const int nsm = device_sm_count();
+  // tile width: 128 when the 128-wide output tiles alone fill the GPU twice per stage
+  long long t128 = 0;
+  for (size_t j = 0; j < jobs.size(); ++j)
+    t128 += (long long)((jobs[j].m + 127) / 128) * ((jobs[j].n + 127) / 128);
+  U->bn = (t128 >= 2LL * nsm * std::max(nstage, 1)) ? 128 : 64;
+  const int BN = U->bn;
+
+  struct Key {
+    int buf;
+    long long src;
+    int ld, rows, K, trans, T;
+    bool operator<(const Key& o) const {
+      return std::tie(buf, src, ld, rows, K, trans, T) < std::tie(o.buf, o.src, o.ld, o.rows, o.K, o.trans, o.T);
+    }
+  };
+  struct Pk {
+    Key k;
+    int cls;         // 0: constant (buffer 2), 1: psi (buffer 0), 2: stage-0 result (buffer 3)
+    long long dst;
+  };
+  std::map<Key, int> index;
+  std::vector<Pk> packs;
+  auto get = [&](int buf, long long src, int ld, int rows, int K, int trans, int T) -> int {
+    const Key k{buf, src, ld, rows, K, trans, T};
+    auto it = index.find(k);
+    if (it != index.end()) return it->second;
+    const int cls = buf == 2 ? 0 : buf == 0 ? 1 : buf == 3 ? 2 : -1;
+    if (cls < 0) return -1;
+    packs.push_back(Pk{k, cls, 0});
+    index[k] = (int)packs.size() - 1;
+    return (int)packs.size() - 1;
+  };
+  auto nslab_of = [](int K) { return (K + kPanelK - 1) / kPanelK; };
+  auto panel_bytes = [&](const Key& k) {
+    return (long long)((k.rows + k.T - 1) / k.T) * nslab_of(k.K) * k.T * 256;
+  };
+  std::vector<int> ta(flat_terms.size(), -1), tb(flat_terms.size(), -1);
+  std::map<long long, double> xalpha;   // stage-0 result offset -> the one alpha its readers use
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const GemmJob& J = jobs[j];
+    for (int t = J.t0; t < J.t0 + J.nt; ++t) {
+      const GemmTerm& T = flat_terms[t];
+      if (T.k == 0) continue;
+      const int a = get(T.abuf, T.aoff, T.lda, J.m, T.k, (T.flags & TF_TA) ? 1 : 0, kUmmaTileM);
+      const int b = get(T.bbuf, T.boff, T.ldb, J.n, T.k, (T.flags & TF_TB) ? 0 : 1, BN);
+      if (a < 0 || b < 0 || packs[b].cls == 2) return false;
+      if (packs[a].cls == 2) {
+        if (T.flags & TF_TA) return false;
+        auto it = xalpha.find(T.aoff);
+        if (it == xalpha.end()) xalpha[T.aoff] = T.ar;
+        else if (it->second != T.ar) return false;
+      } else if (T.ar != 1.0) {
+        return false;
+      }
+      ta[t] = a;
+      tb[t] = b;
+    }
+  }
+  long long cbytes = 0, vbytes = 0;
+  for (auto& p : packs) {
+    long long& tot = p.cls == 0 ? cbytes : vbytes;
+    p.dst = tot;
+    tot += (panel_bytes(p.k) + 255) & ~255LL;
+  }
+  for (auto& p : packs) {
+    if (p.cls == 2) continue;
+    PackJob P{};
+    P.src = p.k.src;
+    P.dst = p.dst;
+    P.srcbuf = p.k.buf;
+    P.ld = p.k.ld;
+    P.rows = p.k.rows;
+    P.K = p.k.K;
+    P.trans = p.k.trans;
+    P.T = p.k.T;
+    const long long nch = (long long)((P.rows + P.T - 1) / P.T) * P.T * nslab_of(P.K) * 8;
+    long long& cc = p.cls == 0 ? U->cchunks : U->vchunks;
+    P.chunk0 = cc;
+    cc += nch;
+    (p.cls == 0 ? U->cpack : U->vpack).push_back(P);
+  }
+  U->terms.resize(flat_terms.size());
+  for (size_t t = 0; t < flat_terms.size(); ++t) {
+    UTerm u{};
+    const int K = flat_terms[t].k;
+    if (K > 0) {
+      u.a = packs[ta[t]].dst;
+      u.b = packs[tb[t]].dst;
+      u.abuf = packs[ta[t]].cls ? 1 : 0;
+      u.bbuf = packs[tb[t]].cls ? 1 : 0;
+      u.nslab = nslab_of(K);
+      u.klast = K - (u.nslab - 1) * kPanelK;
+    }
+    U->terms[t] = u;
+  }
+  // jobs: stage-0 results become the A panels their readers use
+  std::map<long long, int> xreader;   // stage-0 result offset -> its pack
+  for (size_t i = 0; i < packs.size(); ++i)
+    if (packs[i].cls == 2) {
+      if (xreader.count(packs[i].k.src)) return false;
+      xreader[packs[i].k.src] = (int)i;
+    }
+  int produced = 0;
+  U->jobs.resize(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const GemmJob& J = jobs[j];
+    UJob u{};
+    u.coff = J.coff;
+    u.pack = -1;
+    u.alpha = 1.0;
+    u.cbuf = J.cbuf;
+    u.m = J.m;
+    u.n = J.n;
+    u.ldc = J.ldc;
+    u.flags = J.flags;
+    u.t0 = J.t0;
+    u.nt = J.nt;
+    if (J.cbuf == 3) {
+      auto it = xreader.find(J.coff);
+      if (it == xreader.end() || job_stage[j] != 0 || (J.flags & JF_ACCUM)) return false;
+      const Key& k = packs[it->second].k;
+      if (k.rows != J.m || k.K != J.n || k.ld != J.ldc || k.trans != 0 || k.T != kUmmaTileM) return false;
+      u.pack = packs[it->second].dst;
+      u.alpha = xalpha[J.coff];
+      u.pack_nslab = nslab_of(J.n);
+      ++produced;
+    } else if (J.cbuf != 1) {
+      return false;
+    }
+    U->jobs[j] = u;
+  }
+  if (produced != (int)xreader.size()) return false;
+
+  // slab-granular items, longest first; split the reduction only when the
+  // output tiles cannot keep every SM busy
+  const int target = 4 * nsm;
+  U->stage_items.assign(nstage + 1, 0);
+  U->stage_reds.assign(nstage + 1, 0);
+  int nslot = 0;
+  for (int s = 0; s < nstage; ++s) {
+    long long total = 0, ntile = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      if (job_stage[j] != s) continue;
+      long long ns = 0;
+      for (int t = jobs[j].t0; t < jobs[j].t0 + jobs[j].nt; ++t) ns += U->terms[t].nslab;
+      const long long tiles = (long long)((jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);
+      ntile += tiles;
+      total += tiles * std::max<long long>(ns, 1);
+    }
+    long long kc = std::max<long long>(4, (total + target - 1) / target);
+    if (ntile >= target / 2) kc = (long long)1 << 40;
+    std::vector<std::pair<long long, UItem>> its;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      if (job_stage[j] != s) continue;
+      const GemmJob& J = jobs[j];
+      long long ns = 0;
+      for (int t = J.t0; t < J.t0 + J.nt; ++t) ns += U->terms[t].nslab;
+      if (ns == 0 && (J.flags & JF_ACCUM)) continue;
+      const int tm = (J.m + kUmmaTileM - 1) / kUmmaTileM, tn = (J.n + BN - 1) / BN;
+      const long long nch = std::max<long long>(1, (ns + kc - 1) / kc);
+      for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) {
+          if (nch == 1) {
+            its.push_back({ns, UItem{(int)j, a, b, J.t0, 0, (int)ns, -1}});
+            continue;
+          }
+          const int slot0 = nslot;
+          long long pos = 0;
+          int t = J.t0, s0 = 0;
+          for (long long ch = 0; ch < nch; ++ch) {
+            const long long len = std::min(kc, ns - pos);
+            its.push_back({len, UItem{(int)j, a, b, t, s0, (int)len, nslot++}});
+            long long left = len;
+            while (left > 0) {
+              const int avail = U->terms[t].nslab - s0;
+              if (left < avail) { s0 += (int)left; left = 0; }
+              else { left -= avail; ++t; s0 = 0; }
+            }
+            pos += len;
+          }
+          U->reds.push_back(URed{(int)j, a, b, slot0, (int)nch});
+        }
+    }
+    std::stable_sort(its.begin(), its.end(),
+                     [](const std::pair<long long, UItem>& x, const std::pair<long long, UItem>& y) {
+                       return x.first > y.first;
+                     });
+    U->stage_items[s] = (int)U->items.size();
+    for (auto& p : its) U->items.push_back(p.second);
+    U->stage_items[s + 1] = (int)U->items.size();
+    U->stage_reds[s + 1] = (int)U->reds.size();
+  }
+  for (int s = 0; s < nstage; ++s) {
+    U->stage_items[s + 1] = std::max(U->stage_items[s + 1], U->stage_items[s]);
+    U->stage_reds[s + 1] = std::max(U->stage_reds[s + 1], U->stage_reds[s]);
+  }
+  U->nslot = nslot;
+
+  // device copies: [cpack | vpack | terms | jobs | items | reds]
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t b0 = sizeof(PackJob) * U->cpack.size(), b1 = sizeof(PackJob) * U->vpack.size(),
+               b2 = sizeof(UTerm) * U->terms.size(), b3 = sizeof(UJob) * U->jobs.size(),
+               b4 = sizeof(UItem) * U->items.size(), b5 = sizeof(URed) * U->reds.size();
+  const size_t o1 = al(b0), o2 = o1 + al(b1), o3 = o2 + al(b2), o4 = o3 + al(b3), o5 = o4 + al(b4),
+               total = o5 + al(b5) + 256;
+  std::vector<unsigned char> h(total, 0);
+  if (b0) std::memcpy(h.data(), U->cpack.data(), b0);
+  if (b1) std::memcpy(h.data() + o1, U->vpack.data(), b1);
+  if (b2) std::memcpy(h.data() + o2, U->terms.data(), b2);
+  if (b3) std::memcpy(h.data() + o3, U->jobs.data(), b3);
+  if (b4) std::memcpy(h.data() + o4, U->items.data(), b4);
+  if (b5) std::memcpy(h.data() + o5, U->reds.data(), b5);
+  U->dev = std::make_shared<DevBuf>(total, c.stream);
+  SADMRG_CUDA(cudaMemcpyAsync(U->dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
+  unsigned char* base = U->dev->as<unsigned char>();
+  const PackJob* d_cpack = reinterpret_cast<PackJob*>(base);
+  U->d_vpack = reinterpret_cast<PackJob*>(base + o1);
+  U->d_terms = reinterpret_cast<UTerm*>(base + o2);
+  U->d_jobs = reinterpret_cast<UJob*>(base + o3);
+  U->d_items = reinterpret_cast<UItem*>(base + o4);
+  U->d_reds = reinterpret_cast<URed*>(base + o5);
+  U->pconst = std::make_shared<DevBuf>((size_t)std::max<long long>(cbytes, 256), c.stream);
+  U->pvar = std::make_shared<DevBuf>((size_t)std::max<long long>(vbytes, 256), c.stream);
+  U->slots = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * kUmmaTileM * BN * sizeof(float), c.stream);
+  launch_pack(d_cpack, (int)U->cpack.size(), U->cchunks, cb, U->pconst->as<unsigned char>(), c.stream);
+  ++c.launches;
+  SADMRG_CUDA(cudaGetLastError());
+  // the host image must outlive the async copy
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  umma = U;
+  return true;
 }
 
 int GemmPlan::launches_per_run(bool cplx, int prec) const {
-  const GemmSchedule& sc = schedule(cplx, prec);
   int n = 0;
+  if (uses_umma(cplx, prec)) {
+    const UmmaSchedule& U = *umma;
+    if (!U.vpack.empty()) ++n;
+    for (int s = 0; s < nstage; ++s) {
+      if (U.stage_items[s + 1] > U.stage_items[s]) ++n;
+      if (U.stage_reds[s + 1] > U.stage_reds[s]) ++n;
+    }
+    return n;
+  }
   for (int s = 0; s < nstage; ++s) {
-    if (sc.stage_items[s + 1] > sc.stage_items[s]) ++n;
-    if (sc.stage_reds[s + 1] > sc.stage_reds[s]) ++n;
+    if (sched.stage_items[s + 1] > sched.stage_items[s]) ++n;
+    if (sched.stage_reds[s + 1] > sched.stage_reds[s]) ++n;
   }
   return n;
 }
@@ -230,18 +457,40 @@ int GemmPlan::launches_per_run(bool cplx, int prec) const {
 void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi,
                    void* work_override) const {
   if (stage_hi < 0) stage_hi = nstage;
-  const GemmSchedule& sc = schedule(cplx, prec);
-  void* wk = work_override ? work_override : sc.work->get();
-  for (int s = stage_lo; s < stage_hi; ++s) {
-    const int ni = sc.stage_items[s + 1] - sc.stage_items[s];
-    if (ni > 0) {
-      if (sc.kind == GEMM_UMMA) launch_items_umma(d_terms, d_jobs, sc.d_items + sc.stage_items[s], ni, b, wk, c.stream);
-      else launch_items(cplx, prec, d_terms, d_jobs, sc.d_items + sc.stage_items[s], ni, b, wk, c.stream);
+  if (uses_umma(cplx, prec)) {
+    const UmmaSchedule& U = *umma;
+    UBufs ub{U.pconst->as<unsigned char>(), U.pvar->as<unsigned char>(),
+             work_override ? static_cast<float*>(work_override) : U.slots->as<float>()};
+    if (stage_lo == 0 && !U.vpack.empty()) {
+      launch_pack(U.d_vpack, (int)U.vpack.size(), U.vchunks, b, ub.pvar, c.stream);
       ++c.launches;
     }
-    const int nr = sc.stage_reds[s + 1] - sc.stage_reds[s];
+    for (int s = stage_lo; s < stage_hi; ++s) {
+      const int ni = U.stage_items[s + 1] - U.stage_items[s];
+      if (ni > 0) {
+        launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items + U.stage_items[s], ni, b, ub, c.stream);
+        ++c.launches;
+      }
+      const int nr = U.stage_reds[s + 1] - U.stage_reds[s];
+      if (nr > 0) {
+        launch_umma_reduce(U.bn, U.d_jobs, U.d_reds + U.stage_reds[s], nr, b, ub, c.stream);
+        ++c.launches;
+      }
+    }
+    SADMRG_CUDA(cudaGetLastError());
+    c.gemm_flops += flops;
+    return;
+  }
+  void* wk = work_override ? work_override : sched.work->get();
+  for (int s = stage_lo; s < stage_hi; ++s) {
+    const int ni = sched.stage_items[s + 1] - sched.stage_items[s];
+    if (ni > 0) {
+      launch_items(cplx, prec, d_terms, d_jobs, sched.d_items + sched.stage_items[s], ni, b, wk, c.stream);
+      ++c.launches;
+    }
+    const int nr = sched.stage_reds[s + 1] - sched.stage_reds[s];
     if (nr > 0) {
-      launch_reduce(cplx, d_jobs, sc.d_reds + sc.stage_reds[s], nr, b, wk, sc.bm, sc.bn, c.stream);
+      launch_reduce(cplx, d_jobs, sched.d_reds + sched.stage_reds[s], nr, b, wk, sched.bm, sched.bn, c.stream);
       ++c.launches;
     }
   }

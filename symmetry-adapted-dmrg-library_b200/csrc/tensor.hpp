@@ -64,9 +64,8 @@ template <class S> std::vector<Blk> blocks_of(const BTensor<S>& t);
 template <class S> BTensor<S> alloc_tensor(Ctx& c, const Struct& st, const std::vector<char>& present);
 template <class S> BTensor<S> clone(Ctx& c, const BTensor<S>& t);
 
-// Work items and split-K reductions of a plan for one output-tile shape.
+// Work items and split-K reductions of a plan for the mma.sync item kernels.
 struct GemmSchedule {
-  int kind = GEMM_MMA_SYNC;       // which item kernel family runs it
   int bm = 64, bn = 64;
   std::vector<WorkItem> items;
   std::vector<RedItem> reds;
@@ -79,6 +78,29 @@ struct GemmSchedule {
   size_t work_bytes() const { return work ? work->bytes() : 0; }
 };
 
+// The tcgen05 schedule of a real plan: operand panels, panel-addressed terms,
+// jobs, slab-granular items (umma.cu).  Built only when every term fits the
+// panel scheme (constant operands in buffer 2, psi in buffer 0, stage-0 results
+// in buffer 3 consumed only as untransposed A operands with one alpha each).
+struct UmmaSchedule {
+  int bn = 64;
+  std::vector<PackJob> cpack, vpack;       // constant panels (packed once), psi panels (every apply)
+  long long cchunks = 0, vchunks = 0;
+  std::vector<UTerm> terms;
+  std::vector<UJob> jobs;
+  std::vector<UItem> items;
+  std::vector<URed> reds;
+  std::vector<int> stage_items, stage_reds;
+  std::shared_ptr<DevBuf> dev, pconst, pvar, slots;
+  PackJob* d_vpack = nullptr;
+  UTerm* d_terms = nullptr;
+  UJob* d_jobs = nullptr;
+  UItem* d_items = nullptr;
+  URed* d_reds = nullptr;
+  int nslot = 0;
+  size_t slot_bytes() const { return slots ? slots->bytes() : 0; }
+};
+
 // A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.
 struct GemmPlan {
   std::vector<std::vector<GemmTerm>> job_terms;
@@ -88,7 +110,8 @@ struct GemmPlan {
   int nstage = 2;
   // device copy
   std::vector<GemmTerm> flat_terms;
-  std::vector<GemmSchedule> sched;   // [0]: mma.sync tiles; [1] (real mixed plans): tcgen05 tiles
+  GemmSchedule sched;                  // mma.sync items (FP64, and 3xTF32 when there is no tcgen05 schedule)
+  std::shared_ptr<UmmaSchedule> umma;  // tcgen05 3xTF32 (real plans finalised with mixed = true)
   std::shared_ptr<DevBuf> dev;
   GemmTerm* d_terms = nullptr;
   GemmJob* d_jobs = nullptr;
@@ -99,18 +122,22 @@ struct GemmPlan {
   void add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
                 double ar, double ai);
   long long alloc_scratch(long long elems) { long long o = scratch_elems; scratch_elems += elems; return o; }
-  // mixed: also schedule the tcgen05 3xTF32 tiles (real plans that run PREC_TF32X3)
-  void finalize(Ctx& c, bool cplx, bool mixed = false);
-  // the schedule a run at this precision uses
-  const GemmSchedule& schedule(bool cplx, int prec) const;
+  // mixed: also build the tcgen05 schedule; its constant panels are packed from
+  // const_bases (buffer 2) on the context's stream.
+  void finalize(Ctx& c, bool cplx, bool mixed = false, const Bases* const_bases = nullptr);
+  bool uses_umma(bool cplx, int prec) const { return prec == PREC_TF32X3 && !cplx && umma != nullptr; }
   void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1,
            void* work_override = nullptr) const;
-  size_t work_bytes(bool cplx, int prec) const { return schedule(cplx, prec).work_bytes(); }
+  // bytes of split-K workspace a run at this precision uses
+  size_t work_bytes(bool cplx, int prec) const {
+    return uses_umma(cplx, prec) ? umma->slot_bytes() : sched.work_bytes();
+  }
   int launches_per_run(bool cplx, int prec) const;
   bool empty() const { return jobs.empty(); }
 
  private:
   void build_schedule(GemmSchedule& s, bool cplx);
+  bool build_umma(Ctx& c, const Bases& cb);
 };
 
 }  // namespace sadmrg

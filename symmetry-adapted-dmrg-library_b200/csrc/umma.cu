@@ -1,31 +1,30 @@
 // umma.cu -- 3xTF32 grouped block-GEMM on the fifth-generation tensor cores
-// (tcgen05.mma .kind::tf32, FP32 accumulator in tensor memory), real data.
+// (tcgen05.mma .kind::tf32, FP32 accumulators in tensor memory), real data.
 //
-// Same work-item contract as gemm.cu: an item is one output tile of a job and a
-// contiguous range of the job's concatenated reduction dimension; an item that
-// covers the whole range writes C (optionally accumulating), otherwise it writes
-// its partial tile to a workspace slot that the fixed-order reduction sums.
-// Output tiles are 128 x BN (one tcgen05.mma M=128, N=BN), k slabs are 32 wide.
+// Operands are pre-split into TF32 hi/lo panels (layout in kernels.cuh): the
+// constant operators once per plan, psi once per matvec (pack_kernel), and the
+// intermediate X = op1^T psi directly by the epilogue of the stage that makes
+// it.  The GEMM then does no per-element work in its main loop:
 //
-// Per slab, 256 threads:
-//   1. read the FP64 operands of the slab from global memory into registers
-//      (one slab ahead, so the loads overlap the tensor-core work of the slab
-//      before), coalesced along whichever index is contiguous in memory;
-//   2. multiply A by the term's alpha, split every value into TF32 hi and lo
-//      (x = hi + lo + O(2^-22 |x|)), and store four planes A_hi, A_lo, B_hi,
-//      B_lo into shared memory in the K-major, no-swizzle core-matrix layout:
-//      plane[kg][row][4] with kg = k / 4, i.e. 16-byte rows of 4 k values,
-//      8-row core matrices 128 bytes apart (SBO), k halves of an 8-wide MMA
-//      step R * 16 bytes apart (LBO);
-//   3. one thread issues per 8-wide k step three tcgen05.mma (lo*hi, hi*lo,
-//      hi*hi) into the same FP32 accumulator and commits them to the slab
-//      buffer's mbarrier; two buffers, so step 2 of the next slab overlaps.
-// Epilogue: each warp reads its 32 TMEM lanes x BN/2 columns with tcgen05.ld,
-// widens to FP64 and stores (coalesced down each column).
+//   warp 0 (one lane)  producer: per slab, two cp.async.bulk copies (A panel
+//                      128 x 32, B panel BN x 32, hi + lo) into a ring of
+//                      shared-memory stages, completion tracked by the stage's
+//                      mbarrier (expect_tx);
+//   warp 1 (one lane)  issuer: per 8-wide k step three tcgen05.mma (lo*hi,
+//                      hi*lo, hi*hi) into the item's accumulator; tcgen05.commit
+//                      frees the stage, and after the item's last slab signals
+//                      the accumulator full;
+//   warps 2-5          epilogue: tcgen05.ld of the 128 x BN accumulator (each
+//                      warp its 32 lanes), then FP64 store (optionally adding),
+//                      FP32 split-K partial tile, or hi/lo panels of X.
+// Two accumulators (2 x BN TMEM columns) let the epilogue of one item overlap
+// the MMAs of the next; the kernel is persistent (one CTA per SM, static
+// round-robin over the longest-first item list).
 //
-// Every wait on an mbarrier is bounded (time and iterations).  A wait that runs
-// out sets a device status word (read by umma_status), drains what this CTA
-// issued (again bounded), frees its tensor memory and leaves the tile unwritten.
+// Every mbarrier wait is bounded (time and iterations) and also gives up when
+// another role has failed.  A wait that runs out sets a device status word
+// (umma_status) and the CTA stops; before it frees its tensor memory and exits
+// it waits, again bounded, for the copies and MMAs it issued.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -34,11 +33,9 @@
 namespace sadmrg {
 namespace {
 
-constexpr int kUBM = 128;             // tile rows = tcgen05.mma M
-constexpr int kUBK = 32;              // k per slab
-constexpr int kUThreads = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait
 constexpr long long kWaitIters = 1ll << 26;
+constexpr int kGThreads = 192;                          // 6 warps: producer, issuer, 4 x epilogue
 
 __device__ int g_umma_status = 0;
 
@@ -55,15 +52,15 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return r;
 }
-// x ~ hi + lo, both TF32 (the same split as the mma.sync 3xTF32 path)
+// x ~ hi + lo, both TF32 (the split of the mma.sync 3xTF32 path)
 __device__ __forceinline__ void split_hl(double v, uint32_t& hi, uint32_t& lo) {
   const float f = (float)v;
   hi = tf32_rna(f);
   lo = tf32_rna(f - __uint_as_float(hi));
 }
-
-__device__ __forceinline__ void st_shared_v4(uint32_t a, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(a), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+__device__ __forceinline__ void split_hl_f(float f, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_rna(f);
+  lo = tf32_rna(f - __uint_as_float(hi));
 }
 
 // shared-memory matrix descriptor: K-major, no swizzle, version 1
@@ -91,14 +88,26 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+// one contiguous global -> shared copy, completion counted on the mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
 
-// bounded wait for the phase with the given parity; false if it ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity.  Gives up (false) after
+// kWaitNs, or as soon as *abort is set when abort is non-null.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort) {
   const unsigned long long t0 = gtime();
   for (long long i = 0; i < kWaitIters; ++i) {
     uint32_t ok;
@@ -109,7 +118,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (ok) return true;
-    if ((i & 63) == 63 && gtime() - t0 > kWaitNs) break;
+    if ((i & 63) == 63) {
+      if (abort && *abort) return false;
+      if (gtime() - t0 > kWaitNs) return false;
+    }
   }
   return false;
 }
@@ -128,80 +140,91 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// Slab walk over an item's concatenated k (slabs never straddle a term).
-struct UWalk {
-  int t, k, rem;
-  __device__ bool next(const GemmTerm* terms, int& tt, int& kk, int& kt) {
-    if (rem <= 0) return false;
-    int tk = terms[t].k;
-    while (k >= tk) { ++t; k = 0; tk = terms[t].k; }
-    tt = t;
-    kk = k;
-    kt = min(kUBK, min(tk - k, rem));
-    k += kt;
-    rem -= kt;
-    return true;
-  }
-};
-
-// Position (row, kg) of the q-th 16-byte chunk of this thread in an R-row plane.
-// kcontig: k is the contiguous global index (a warp covers 8 rows x 4 chunks);
-// otherwise the row index is (a warp covers 32 rows of one chunk column).
-// Both give conflict-free 16-byte shared stores.
-template <int R>
-__device__ __forceinline__ void chunk_pos(bool kcontig, int q, int& row, int& kg) {
-  const int e = (int)threadIdx.x + q * kUThreads;
-  if (kcontig) {
-    row = (e >> 2) % R;
-    kg = (e & 3) + 4 * ((e >> 2) / R);
-  } else {
-    row = e % R;
-    kg = e / R;
-  }
+__device__ __forceinline__ void st_global_v4(void* p, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+  *reinterpret_cast<uint4*>(p) = make_uint4(x, y, z, w);
 }
 
-template <int BN>
-struct UCfg {
-  static constexpr int KG = kUBK / 4;                        // 16-byte chunks along k
-  static constexpr int APER = kUBM * KG / kUThreads;         // A chunks per thread
-  static constexpr int BPER = BN * KG / kUThreads;           // B chunks per thread
-  static constexpr uint32_t PA = kUBM * kUBK * 4;            // bytes of one A plane
-  static constexpr uint32_t PB = BN * kUBK * 4;              // bytes of one B plane
-  static constexpr uint32_t BUF = 2 * PA + 2 * PB;           // one slab buffer
-  static constexpr uint32_t SMEM = 2 * BUF + 128;            // two buffers + alignment slack
-  static constexpr uint32_t TCOLS = BN < 32 ? 32 : BN;       // TMEM columns (power of two >= 32)
-  static_assert(APER * kUThreads == kUBM * KG && BPER * kUThreads == BN * KG, "chunk split");
+// ---------------------------------------------------------------------------
+// FP64 matrices -> TF32 hi/lo panels.  One thread per 16-byte chunk (4 k of one
+// row); consecutive threads take consecutive rows of one (slab, kg) column, so
+// the stores are contiguous and the loads coalesce along rows (trans 0) or read
+// one 32-byte sector per thread (trans 1).
+__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, int njobs, long long nchunks,
+                                                   Bases bases, unsigned char* __restrict__ dst) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchunks) return;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].chunk0 <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  const PackJob P = jobs[lo];
+  const long long local = c - P.chunk0;
+  const int nslab = (P.K + kPanelK - 1) / kPanelK;
+  const long long Rp = (long long)((P.rows + P.T - 1) / P.T) * P.T;
+  const int r = (int)(local % Rp);
+  const int kgs = (int)(local / Rp);
+  const int s = kgs >> 3, kg = kgs & 7;
+  const int p = r / P.T, rr = r % P.T;
+  const double* src = static_cast<const double*>(bases.p[P.srcbuf]) + P.src;
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int k = s * kPanelK + kg * 4 + u;
+    double v = 0.0;
+    if (r < P.rows && k < P.K) v = P.trans ? src[k + (long long)r * P.ld] : src[r + (long long)k * P.ld];
+    split_hl(v, h[u], l[u]);
+  }
+  unsigned char* panel = dst + P.dst + ((long long)p * nslab + s) * P.T * 256;
+  const long long off = ((long long)kg * P.T + rr) * 16;
+  st_global_v4(panel + off, h[0], h[1], h[2], h[3]);
+  st_global_v4(panel + (long long)P.T * 128 + off, l[0], l[1], l[2], l[3]);
+}
+
+// ---------------------------------------------------------------------------
+template <int BN, int ST>
+struct UG {
+  static constexpr uint32_t ABYTES = kUmmaTileM * 256;   // A panel: hi + lo planes
+  static constexpr uint32_t BBYTES = BN * 256;
+  static constexpr uint32_t SBYTES = ABYTES + BBYTES;    // one stage
+  static constexpr uint32_t SMEM = ST * SBYTES + 1024;
+  static constexpr uint32_t TCOLS = 2 * BN;              // two accumulators
   static_assert(BN == 64 || BN == 128, "tile width");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-template <int BN>
-__global__ void __launch_bounds__(kUThreads, 2)
-    items_umma_tf32x3(const GemmTerm* __restrict__ terms, const GemmJob* __restrict__ jobs,
-                      const WorkItem* __restrict__ items, Bases bases, double* __restrict__ work) {
-  using C = UCfg<BN>;
-  constexpr int BM = kUBM;
-  extern __shared__ unsigned char usmem_raw[];
-  __shared__ __align__(8) unsigned long long mbar[2];
+template <int BN, int ST>
+__global__ void __launch_bounds__(kGThreads, 1)
+    umma_gemm(const UTerm* __restrict__ terms, const UJob* __restrict__ jobs, const UItem* __restrict__ items,
+              int nitems, Bases bases, UBufs ub) {
+  using G = UG<BN, ST>;
+  constexpr int BM = kUmmaTileM;
+  extern __shared__ unsigned char usm_raw[];
+  __shared__ __align__(8) unsigned long long full[ST], empty[ST], tfull[2], tempty[2];
   __shared__ uint32_t tmem_sh;
-  __shared__ int abort_sh;
+  __shared__ volatile int abort_sh;
 
-  unsigned char* usmem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usmem_raw) + 127) & ~uintptr_t(127));
-  const uint32_t sbase = saddr(usmem);
-  const WorkItem it = items[blockIdx.x];
-  const GemmJob J = jobs[it.job];
-  const int row0 = it.tm * BM, col0 = it.tn * BN;
+  unsigned char* usm =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm_raw) + 127) & ~uintptr_t(127));
+  const uint32_t sbase = saddr(usm);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar0 = saddr(&mbar[0]), bar1 = saddr(&mbar[1]);
 
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(&tmem_sh)),
-                 "r"(C::TCOLS)
+                 "r"(G::TCOLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(bar0, 1);
-    mbar_init(bar1, 1);
+    for (int i = 0; i < ST; ++i) {
+      mbar_init(saddr(&full[i]), 1);
+      mbar_init(saddr(&empty[i]), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(saddr(&tfull[i]), 1);
+      mbar_init(saddr(&tempty[i]), 4 * 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     abort_sh = 0;
   }
@@ -210,178 +233,264 @@ __global__ void __launch_bounds__(kUThreads, 2)
   fence_after();
   const uint32_t tmem = tmem_sh;
 
-  double ra[C::APER][4], rb[C::BPER][4];
-  double s_alpha = 0.0;
-  int s_flags = 0, s_kt = 0;
-
-  auto load = [&](int tt, int k0, int kt) {
-    const GemmTerm& T = terms[tt];
-    const double* A = static_cast<const double*>(bases.p[T.abuf]) + T.aoff;
-    const double* B = static_cast<const double*>(bases.p[T.bbuf]) + T.boff;
-    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
-    const int lda = T.lda, ldb = T.ldb;
-#pragma unroll
-    for (int q = 0; q < C::APER; ++q) {
-      int row, kg;
-      chunk_pos<BM>(ta, q, row, kg);
-      const int gi = row0 + row;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int kk = 4 * kg + u;
-        double v = 0.0;
-        if (gi < J.m && kk < kt) v = ta ? A[(k0 + kk) + (long long)gi * lda] : A[gi + (long long)(k0 + kk) * lda];
-        ra[q][u] = v;
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      long long g = 0;
+      uint32_t last_bar = 0, last_par = 0;
+      bool issued_any = false;
+      for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x) {
+        const UItem it = items[ii];
+        int t = it.t0, s = it.s0;
+        for (int q = 0; q < it.nslab; ++q) {
+          while (s >= terms[t].nslab) { ++t; s = 0; }
+          const UTerm T = terms[t];
+          const int st = (int)(g % ST);
+          const uint32_t n = (uint32_t)(g / ST);
+          if (!mbar_wait(saddr(&empty[st]), (n & 1u) ^ 1u, &abort_sh)) {
+            if (!abort_sh) atomicExch(&g_umma_status, 3);
+            abort_sh = 1;
+            break;
+          }
+          const uint32_t fb = saddr(&full[st]);
+          mbar_expect_tx(fb, G::SBYTES);
+          const unsigned char* A = (T.abuf ? ub.pvar : ub.pconst) + T.a + ((long long)it.tm * T.nslab + s) * G::ABYTES;
+          const unsigned char* B = (T.bbuf ? ub.pvar : ub.pconst) + T.b + ((long long)it.tn * T.nslab + s) * G::BBYTES;
+          const uint32_t sa = sbase + (uint32_t)st * G::SBYTES;
+          bulk_g2s(sa, A, G::ABYTES, fb);
+          bulk_g2s(sa + G::ABYTES, B, G::BBYTES, fb);
+          last_bar = fb;
+          last_par = n & 1u;
+          issued_any = true;
+          ++g;
+          ++s;
+        }
       }
+      // the copies this thread issued have landed before the CTA can exit
+      if (issued_any && !mbar_wait(last_bar, last_par, nullptr)) atomicExch(&g_umma_status, 4);
     }
-#pragma unroll
-    for (int q = 0; q < C::BPER; ++q) {
-      int row, kg;
-      chunk_pos<BN>(!tb, q, row, kg);
-      const int gj = col0 + row;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int kk = 4 * kg + u;
-        double v = 0.0;
-        if (gj < J.n && kk < kt) v = tb ? B[gj + (long long)(k0 + kk) * ldb] : B[(k0 + kk) + (long long)gj * ldb];
-        rb[q][u] = v;
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = tf32_idesc(BM, BN);
+      long long g = 0;
+      int il = 0;
+      uint32_t last_bar = 0, last_par = 0;
+      bool committed = false;
+      for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x, ++il) {
+        const UItem it = items[ii];
+        const int acc = il & 1;
+        if (!mbar_wait(saddr(&tempty[acc]), (((uint32_t)il >> 1) & 1u) ^ 1u, &abort_sh)) {
+          if (!abort_sh) atomicExch(&g_umma_status, 5);
+          abort_sh = 1;
+          break;
+        }
+        fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * BN);
+        int t = it.t0, s = it.s0;
+        bool ok = true;
+        for (int q = 0; q < it.nslab; ++q) {
+          while (s >= terms[t].nslab) { ++t; s = 0; }
+          const UTerm T = terms[t];
+          const int kt = (s == T.nslab - 1) ? T.klast : kPanelK;
+          const int st = (int)(g % ST);
+          const uint32_t n = (uint32_t)(g / ST);
+          if (!mbar_wait(saddr(&full[st]), n & 1u, &abort_sh)) {
+            if (!abort_sh) atomicExch(&g_umma_status, 6);
+            abort_sh = 1;
+            ok = false;
+            break;
+          }
+          fence_after();
+          const uint32_t a0 = sbase + (uint32_t)st * G::SBYTES, b0 = a0 + G::ABYTES;
+          const int nks = (kt + 7) >> 3;
+          for (int ks = 0; ks < nks; ++ks) {
+            const uint32_t ao = (uint32_t)ks * 2u * BM * 16u, bo = (uint32_t)ks * 2u * BN * 16u;
+            const uint64_t ah = kmajor_desc(a0 + ao, BM * 16, 128);
+            const uint64_t al = kmajor_desc(a0 + BM * 128 + ao, BM * 16, 128);
+            const uint64_t bh = kmajor_desc(b0 + bo, BN * 16, 128);
+            const uint64_t bl = kmajor_desc(b0 + BN * 128 + bo, BN * 16, 128);
+            umma_tf32(d, al, bh, idesc, (q > 0 || ks > 0) ? 1u : 0u);
+            umma_tf32(d, ah, bl, idesc, 1u);
+            umma_tf32(d, ah, bh, idesc, 1u);
+          }
+          umma_commit(saddr(&empty[st]));
+          last_bar = saddr(&empty[st]);
+          last_par = n & 1u;
+          committed = true;
+          ++g;
+          ++s;
+        }
+        if (!ok) break;
+        umma_commit(saddr(&tfull[acc]));
+        last_bar = saddr(&tfull[acc]);
+        last_par = ((uint32_t)il >> 1) & 1u;
+        committed = true;
       }
+      // every MMA this thread issued has finished before tensor memory is freed
+      if (committed && !mbar_wait(last_bar, last_par, nullptr)) atomicExch(&g_umma_status, 7);
     }
-    s_alpha = T.ar;
-    s_flags = T.flags;
-    s_kt = kt;
-  };
-
-  auto store = [&](int buf) {
-    const uint32_t pa = sbase + buf * C::BUF, pb = pa + 2 * C::PA;
-    const bool ta = s_flags & TF_TA, tb = s_flags & TF_TB;
-#pragma unroll
-    for (int q = 0; q < C::APER; ++q) {
-      int row, kg;
-      chunk_pos<BM>(ta, q, row, kg);
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) split_hl(ra[q][u] * s_alpha, h[u], l[u]);
-      const uint32_t off = (uint32_t)(kg * BM + row) * 16u;
-      st_shared_v4(pa + off, h[0], h[1], h[2], h[3]);
-      st_shared_v4(pa + C::PA + off, l[0], l[1], l[2], l[3]);
-    }
-#pragma unroll
-    for (int q = 0; q < C::BPER; ++q) {
-      int row, kg;
-      chunk_pos<BN>(!tb, q, row, kg);
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) split_hl(rb[q][u], h[u], l[u]);
-      const uint32_t off = (uint32_t)(kg * BN + row) * 16u;
-      st_shared_v4(pb + off, h[0], h[1], h[2], h[3]);
-      st_shared_v4(pb + C::PB + off, l[0], l[1], l[2], l[3]);
-    }
-  };
-
-  constexpr uint32_t idesc = tf32_idesc(BM, BN);
-  UWalk w{J.t0 + it.t0, it.k0, it.kcount};
-  int tt, kk, kt;
-  bool have = w.next(terms, tt, kk, kt);
-  if (have) load(tt, kk, kt);
-  int issued = 0;        // slabs whose MMAs were committed
-  bool failed = false;
-  for (int c = 0; have; ++c) {
-    const int buf = c & 1;
-    if (c >= 2 && !mbar_wait(buf ? bar1 : bar0, ((c - 2) >> 1) & 1)) {
-      abort_sh = 1;
-      atomicExch(&g_umma_status, 1);
-    }
-    store(buf);
-    const int ktc = s_kt;
-    have = w.next(terms, tt, kk, kt);
-    if (have) load(tt, kk, kt);
-    fence_proxy_async();
-    __syncthreads();
-    if (abort_sh) { failed = true; break; }
-    if (tid == 0) {
+  } else {
+    // ---------------- epilogue: warps 2..5 ----------------
+    const int quarter = warp & 3;           // TMEM lanes 32*quarter .. +31
+    const int r = 32 * quarter + lane;      // tile row
+    int il = 0;
+    for (int ii = blockIdx.x; ii < nitems; ii += gridDim.x, ++il) {
+      if (__shfl_sync(0xffffffffu, abort_sh, 0)) break;
+      const UItem it = items[ii];
+      const UJob J = jobs[it.job];
+      const int acc = il & 1;
+      const bool got = mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh);
+      if (!__all_sync(0xffffffffu, got)) {
+        if (lane == 0) {
+          if (!abort_sh) atomicExch(&g_umma_status, 8);
+          abort_sh = 1;
+        }
+        break;
+      }
       fence_after();
-      const uint32_t pa = sbase + buf * C::BUF, pb = pa + 2 * C::PA;
-      const int nks = (ktc + 7) / 8;
-      for (int s = 0; s < nks; ++s) {
-        const uint32_t ao = (uint32_t)s * 2u * BM * 16u, bo = (uint32_t)s * 2u * BN * 16u;
-        const uint64_t ah = kmajor_desc(pa + ao, BM * 16, 128), al = kmajor_desc(pa + C::PA + ao, BM * 16, 128);
-        const uint64_t bh = kmajor_desc(pb + bo, BN * 16, 128), bl = kmajor_desc(pb + C::PB + bo, BN * 16, 128);
-        umma_tf32(tmem, al, bh, idesc, (c > 0 || s > 0) ? 1u : 0u);
-        umma_tf32(tmem, ah, bl, idesc, 1u);
-        umma_tf32(tmem, ah, bh, idesc, 1u);
-      }
-      umma_commit(buf ? bar1 : bar0);
-    }
-    ++issued;
-  }
-  if (issued > 0) {
-    const int last = issued - 1;
-    if (!mbar_wait((last & 1) ? bar1 : bar0, (last >> 1) & 1)) {
-      failed = true;
-      atomicExch(&g_umma_status, 2);
-    }
-    // the slab before the last was waited for only if a later slab reused its buffer
-  }
-  failed = __syncthreads_or(failed);
-  fence_after();
-
-  if (!failed) {
-    const bool direct = it.slot < 0;
-    double* Cp = direct ? static_cast<double*>(bases.p[J.cbuf]) + J.coff : work + (long long)it.slot * BM * BN;
-    const bool accum = J.flags & JF_ACCUM;
-    const int quarter = warp & 3, half = warp >> 2;
-    const int r = 32 * quarter + lane;
-    constexpr int CW = BN / 2;
+      const int row0 = it.tm * BM, col0 = it.tn * BN;
+#pragma unroll 1
+      for (int cb = 0; cb < BN; cb += 32) {
+        uint32_t v[32];
+        if (it.nslab > 0) {
+          tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * BN + cb), v);
+        } else {
 #pragma unroll
-    for (int cc = 0; cc < CW; cc += 32) {
-      uint32_t v[32];
-      const int cb = half * CW + cc;
-      if (issued > 0) {
-        tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)cb, v);
-      } else {
+          for (int j = 0; j < 32; ++j) v[j] = 0u;
+        }
+        if (it.slot >= 0) {
+          float* S = ub.slots + (long long)it.slot * BM * BN;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = 0u;
-      }
-      if (direct) {
-        if (row0 + r < J.m) {
+          for (int j = 0; j < 32; ++j) S[r + (cb + j) * BM] = __uint_as_float(v[j]);
+        } else if (J.pack >= 0) {
+          const int s = (col0 + cb) / kPanelK;
+          if (s < J.pack_nslab) {
+            unsigned char* panel = ub.pvar + J.pack + ((long long)it.tm * J.pack_nslab + s) * (BM * 256);
+            const float al = (float)J.alpha;
+#pragma unroll
+            for (int kg = 0; kg < 8; ++kg) {
+              uint32_t h[4], l[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) split_hl_f(al * __uint_as_float(v[4 * kg + u]), h[u], l[u]);
+              st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
+              st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
+            }
+          }
+        } else if (row0 + r < J.m) {
+          double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
+          const bool accum = J.flags & JF_ACCUM;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            const int col = cb + j;
-            if (col0 + col < J.n) {
-              const long long idx = (row0 + r) + (long long)(col0 + col) * J.ldc;
+            const int col = col0 + cb + j;
+            if (col < J.n) {
+              const long long idx = (row0 + r) + (long long)col * J.ldc;
               const double x = (double)__uint_as_float(v[j]);
-              Cp[idx] = accum ? Cp[idx] + x : x;
+              C[idx] = accum ? C[idx] + x : x;
             }
           }
         }
-      } else {
+      }
+      fence_before();
+      mbar_arrive(saddr(&tempty[acc]));
+    }
+  }
+
+  fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(G::TCOLS) : "memory");
+  }
+}
+
+// Sum of the FP32 partial tiles of split items, in slot order, then the same
+// three outputs as the GEMM epilogue.  One thread per (row, 4 columns).
+template <int BN>
+__global__ void __launch_bounds__(256) umma_reduce(const UJob* __restrict__ jobs, const URed* __restrict__ red,
+                                                   Bases bases, UBufs ub) {
+  constexpr int BM = kUmmaTileM;
+  const URed R = red[blockIdx.x];
+  const UJob J = jobs[R.job];
+  const int row0 = R.tm * BM, col0 = R.tn * BN;
+  for (int e = threadIdx.x; e < BM * (BN / 4); e += blockDim.x) {
+    const int r = e % BM, c4 = (e / BM) * 4;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < R.nslot; ++k) {
+      const float* S = ub.slots + (long long)(R.slot0 + k) * BM * BN;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) Cp[r + (long long)(cb + j) * BM] = (double)__uint_as_float(v[j]);
+      for (int u = 0; u < 4; ++u) acc[u] += (double)S[r + (c4 + u) * BM];
+    }
+    if (J.pack >= 0) {
+      const int s = (col0 + c4) / kPanelK, kg = ((col0 + c4) % kPanelK) / 4;
+      if (s >= J.pack_nslab) continue;
+      unsigned char* panel = ub.pvar + J.pack + ((long long)R.tm * J.pack_nslab + s) * (BM * 256);
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) split_hl(J.alpha * acc[u], h[u], l[u]);
+      st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
+      st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
+    } else if (row0 + r < J.m) {
+      double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
+      const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int col = col0 + c4 + u;
+        if (col >= J.n) continue;
+        const long long idx = (row0 + r) + (long long)col * J.ldc;
+        C[idx] = accum ? C[idx] + acc[u] : acc[u];
       }
     }
   }
-  fence_before();
-  __syncthreads();
-  if (warp == 0) {
-    fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(C::TCOLS) : "memory");
+}
+
+template <int BN, int ST>
+void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
+                   const UBufs& u, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(umma_gemm<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG<BN, ST>::SMEM);
+    attr = true;
   }
+  const int grid = nitems < device_sm_count() ? nitems : device_sm_count();
+  umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, nitems, b, u);
 }
 
 }  // namespace
 
-int umma_tile_n() { return 64; }
-
-void launch_items_umma(const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems, const Bases& b,
-                       void* work, cudaStream_t s) {
-  if (nitems <= 0) return;
-  constexpr int BN = 64;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(items_umma_tf32x3<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UCfg<BN>::SMEM);
-    attr = true;
+int device_sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
+                                                  cudaSuccess && v > 0)
+      n = v;
+    else
+      return 148;
   }
-  items_umma_tf32x3<BN><<<nitems, kUThreads, UCfg<BN>::SMEM, s>>>(terms, jobs, items, b, static_cast<double*>(work));
+  return n;
+}
+
+void launch_pack(const PackJob* jobs, int njobs, long long nchunks, const Bases& b, unsigned char* dst,
+                 cudaStream_t s) {
+  if (njobs <= 0 || nchunks <= 0) return;
+  const long long blocks = (nchunks + 255) / 256;
+  pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(jobs, njobs, nchunks, b, dst);
+}
+
+void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
+                       const UBufs& u, cudaStream_t s) {
+  if (nitems <= 0) return;
+  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, nitems, b, u, s);
+  else launch_gemm_t<64, 4>(terms, jobs, items, nitems, b, u, s);
+}
+
+void launch_umma_reduce(int bn, const UJob* jobs, const URed* red, int nred, const Bases& b, const UBufs& u,
+                        cudaStream_t s) {
+  if (nred <= 0) return;
+  if (bn == 128) umma_reduce<128><<<nred, 256, 0, s>>>(jobs, red, b, u);
+  else umma_reduce<64><<<nred, 256, 0, s>>>(jobs, red, b, u);
 }
 
 int umma_status(bool reset) {
