@@ -1,25 +1,32 @@
 #!/usr/bin/env python
-"""bench.py -- H_eff*psi throughput of the two-site DMRG hot path on B200.
+"""bench.py -- H_eff*psi throughput and sweep time of the two-site DMRG hot path on B200.
 
 Workload (default): SU(2) spin-1/2 Heisenberg chain, open boundaries, L = 100,
 D = 512 kept multiplets.  The chain is grown on the GPU by the library's iDMRG
-(seeded like the reference, mt19937_64(42)) and the two-site problem at the
-centre bond is frozen; one benchmark step is one application of H_eff to psi on
-that problem (all sector products of one matvec, two grouped launches).
+(seeded like the reference, mt19937_64(42)) and checkpointed; one finite sweep
+runs in FP64 and one in the mixed precision form from that same checkpoint
+(sweep time and |dE|); then the two-site problem at the centre bond is frozen and
+one benchmark step is one application of H_eff to psi on it (all sector products
+of one matvec: psi -> TF32 panels, two grouped tcgen05 GEMM launches, split-K
+reductions where the plan has them).
 
 Arms
-  ours (default)      3xTF32 split-precision matvec (value), FP64 matvec, end to
-                      end through the C ABI with host buffers (e2e), Lanczos
-                      mixed vs FP64 energies, the reference CPU build on the same
-                      problem (cpu_baseline), roofline of the dominant launch.
+  ours (default)      3xTF32 split-precision matvec on tcgen05 (value), FP64
+                      matvec, end to end through the C ABI with host buffers
+                      (e2e), Lanczos mixed vs FP64 energies, the reference CPU
+                      build on the same problem (cpu_baseline), roofline of the
+                      dominant launch from per-launch CUDA events.
   --impl reference    the reference's own DMRG::hamiltonian_vector_multiplication_idmrg
                       (oracle/_ref, built from the reference sources) on the same
                       problem, all host threads.
 
-Timing: CUDA events on the library's stream, one event pair per launch, L2
-flushed (256 MiB write) between timed steps; the problem is ~20 MB, so without
-the flush it would sit in the 126 MB L2.  Multi-GPU runs are independent
-replicas (the path has no exchange step); time is the max over ranks.
+Timing: CUDA events on the library's stream, L2 flushed (256 MiB write) between
+timed steps; the problem is ~20 MB, so without the flush it would sit in the
+126 MB L2.  Multi-GPU runs are independent replicas (the path has no exchange
+step); time is the max over ranks.
+
+--export DIR writes the frozen problem (the reference's tensors and meta) to DIR;
+--problem DIR benchmarks a problem written that way instead of building the chain.
 """
 from __future__ import annotations
 
@@ -46,6 +53,11 @@ WORKLOADS = {
 }
 
 
+# Lanczos stop test of the timed sweeps (|<v|Hv>|/|Hv| within this of 1): tight
+# enough that the FP64 and the mixed sweep land on the same energy to ~1e-10.
+SWEEP_LANCZOS_TOL = 1e-12
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -55,6 +67,8 @@ def parse():
     ap.add_argument("--workload", default="su2_heisenberg_L100_D512", choices=sorted(WORKLOADS))
     ap.add_argument("--sweeps", type=int, default=1, help="timed finite sweeps before freezing")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--export", default=None, help="also write the frozen centre problem to this directory")
+    ap.add_argument("--problem", default=None, help="benchmark this exported problem instead of building the chain")
     return ap.parse_args()
 
 
@@ -165,22 +179,61 @@ def measured_peaks():
 
 
 def build_problem(wl: dict, device: int, sweeps: int, export_dir: str | None):
+    """iDMRG, checkpoint, `sweeps` FP64 sweeps and the same number of mixed sweeps
+    from the checkpoint, then freeze the centre of the FP64 chain."""
+    import sadmrg
+    ns = wl["lx"] * wl["ly"]
+
+    def new_chain():
+        h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=device)
+        h.chain_create(wl["lx"], wl["ly"], wl["D"], 1, 0, True, wl["J2"])
+        return h
+
+    h0 = new_chain()
+    t0 = time.perf_counter()
+    e_idmrg = h0.chain_idmrg()
+    t_idmrg = time.perf_counter() - t0
+    ck = tempfile.mkdtemp(prefix="sadmrg_ck_")
+    h0.chain_save_mps(ck)
+    h0.close()
+    runs = {}
+    keep = None
+    for name, prec in (("fp64", sadmrg.PREC_FP64), ("mixed", sadmrg.PREC_TF32X3)):
+        h = new_chain()
+        h.chain_read_mps(ck, wl["D"])
+        h.chain_prepare_sweep()
+        h.chain_set_precision(prec)
+        h.set_lanczos_tol(SWEEP_LANCZOS_TOL)
+        st0 = h.chain_stats()
+        times, es = [], []
+        for _ in range(sweeps):
+            t0 = time.perf_counter()
+            es.append(h.chain_sweep())
+            times.append(time.perf_counter() - t0)
+        st1 = h.chain_stats()
+        runs[name] = dict(sweep_s=[round(x, 3) for x in times], sweep_E=es,
+                          stats={k: st1[k] - st0[k] for k in st1 if k not in ("discarded", "near_ties")}
+                          | {"discarded": st1["discarded"], "near_ties": st1["near_ties"]})
+        if name == "fp64":
+            keep = h
+        else:
+            h.close()
+    import shutil
+    shutil.rmtree(ck, ignore_errors=True)
+    psi = keep.chain_freeze(ns // 2 - 1, export_dir)
+    dE = [abs(a - b) for a, b in zip(runs["mixed"]["sweep_E"], runs["fp64"]["sweep_E"])]
+    meta = dict(idmrg_s=round(t_idmrg, 3), idmrg_E=e_idmrg, sweep_lanczos_ov_tol=SWEEP_LANCZOS_TOL, sweeps=runs,
+                sweep_abs_dE=dE,
+                sweep_rel_dE=[d / abs(e) for d, e in zip(dE, runs["fp64"]["sweep_E"])],
+                sweep_speedup_mixed_over_fp64=[a / b for a, b in zip(runs["fp64"]["sweep_s"], runs["mixed"]["sweep_s"])])
+    return keep, psi, meta
+
+
+def load_problem(wl: dict, device: int, directory: str):
     import sadmrg
     h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=device)
-    h.chain_create(wl["lx"], wl["ly"], wl["D"], 1, 0, True, wl["J2"])
-    t0 = time.perf_counter()
-    e_idmrg = h.chain_idmrg()
-    t_idmrg = time.perf_counter() - t0
-    sweep_times, sweep_e = [], []
-    for _ in range(sweeps):
-        t0 = time.perf_counter()
-        sweep_e.append(h.chain_sweep())
-        sweep_times.append(time.perf_counter() - t0)
-    stats = h.chain_stats()
-    ns = wl["lx"] * wl["ly"]
-    psi = h.chain_freeze(ns // 2 - 1, export_dir)
-    return h, psi, dict(idmrg_s=round(t_idmrg, 3), idmrg_E=e_idmrg, sweep_s=[round(x, 3) for x in sweep_times],
-                        sweep_E=sweep_e, chain_stats=stats)
+    psi = sadmrg.load_exported_problem(h, directory)
+    return h, psi, {"source": "exported problem"}
 
 
 def run_reference_harness(export_dir: str, wl: dict, calls: int, threads: int):
@@ -213,11 +266,16 @@ def main():
         with tempfile.TemporaryDirectory() as td:
             # inputs: the same frozen problem (built on the GPU, written as files); the timed
             # path is the reference's own H_eff*psi on the host cores
-            h, psi, meta = build_problem(wl, local, a.sweeps, td)
+            if a.problem:
+                src = a.problem
+                h, psi, meta = load_problem(wl, local, src)
+            else:
+                src = td
+                h, psi, meta = build_problem(wl, local, a.sweeps, td)
             info = h.heff_info()
             h.close()
-            run_reference_harness(td, wl, max(1, a.warmup), cores)
-            secs = run_reference_harness(td, wl, a.steps, cores)
+            run_reference_harness(src, wl, max(1, a.warmup), cores)
+            secs = run_reference_harness(src, wl, a.steps, cores)
         v = info["flops"] * a.steps / secs / 1e12
         line = {"metric": "H_eff*psi TFLOP/s", "value": v, "unit": "TFLOP/s", "n_gpus": ws, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": secs / a.steps * 1e3, "higher_is_better": True,
@@ -235,8 +293,14 @@ def main():
     import torch
     import sadmrg
     torch.cuda.set_device(local)
-    export_dir = tempfile.mkdtemp(prefix="sadmrg_bench_") if rank == 0 else None
-    h, psi, meta = build_problem(wl, local, a.sweeps, export_dir)
+    if a.problem:
+        export_dir = a.problem
+        h, psi, meta = load_problem(wl, local, a.problem)
+    else:
+        export_dir = (a.export or tempfile.mkdtemp(prefix="sadmrg_bench_")) if rank == 0 else None
+        if export_dir:
+            os.makedirs(export_dir, exist_ok=True)
+        h, psi, meta = build_problem(wl, local, a.sweeps, export_dir)
     info = h.heff_info()
     n = info["n"]
     cplx = wl["cplx"]
@@ -247,39 +311,47 @@ def main():
     peaks = measured_peaks()
 
     def timed(prec, steps):
-        ms = np.zeros(2)
+        """mean per-launch device ms over `steps` matvecs, L2 flushed before each"""
+        acc, kinds = None, None
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
-            m, fl = h.heff_profile(prec, 1, x.data_ptr(), y.data_ptr())
-            ms += m
-        return ms / steps, fl
+            lp = h.heff_launch_profile(prec, 1, x.data_ptr(), y.data_ptr())
+            if acc is None:
+                kinds = [k for k, _ in lp]
+                acc = np.zeros(len(lp))
+            acc += np.array([m for _, m in lp])
+        return kinds, acc / max(steps, 1)
 
     for prec in (sadmrg.PREC_FP64, sadmrg.PREC_TF32X3):
         timed(prec, a.warmup)
+    _, stage_flops = h.heff_profile(sadmrg.PREC_FP64, 1, x.data_ptr(), y.data_ptr())
     barrier(ws)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         torch.cuda.nvtx.range_push("timed")
-        ms_mix, fl = timed(sadmrg.PREC_TF32X3, a.steps)
-        ms_64, _ = timed(sadmrg.PREC_FP64, a.steps)
+        k_mix, l_mix = timed(sadmrg.PREC_TF32X3, a.steps)
+        k_64, l_64 = timed(sadmrg.PREC_FP64, a.steps)
         torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(ws)
-    step_mix = reduce_max(float(ms_mix.sum()), ws)
-    step_64 = reduce_max(float(ms_64.sum()), ws)
+    step_mix = reduce_max(float(l_mix.sum()), ws)
+    step_64 = reduce_max(float(l_64.sum()), ws)
     flops = info["flops"]
     value = flops * ws / (step_mix / 1e3) / 1e12
     value64 = flops * ws / (step_64 / 1e3) / 1e12
-    # end to end through the C ABI with host buffers (H2D of psi, matvec, D2H of H psi)
+    # end to end through the C ABI with host buffers in pinned memory (H2D of psi, matvec, D2H of H psi)
     psi_host = np.ascontiguousarray(psi.data)
-    h.heff_apply(psi_host, sadmrg.PREC_TF32X3)
+    psi_pin = torch.from_numpy(psi_host.copy()).pin_memory()
+    out_pin = torch.empty_like(psi_pin).pin_memory()
+    h.heff_apply(psi_pin.numpy(), sadmrg.PREC_TF32X3, out=out_pin.numpy())
     barrier(ws)
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        out = h.heff_apply(psi_host, sadmrg.PREC_TF32X3)
+        h.heff_apply(psi_pin.numpy(), sadmrg.PREC_TF32X3, out=out_pin.numpy())
     e2e_s = reduce_max((time.perf_counter() - t0) / a.steps, ws)
     e2e = flops * ws / e2e_s / 1e12
+    out = out_pin.numpy().copy()
     # accuracy of the split-precision matvec and of the mixed Lanczos
     y64 = h.heff_apply(psi_host, sadmrg.PREC_FP64)
     mv_err = float(np.abs(out - y64).max() / np.abs(y64).max())
@@ -292,20 +364,26 @@ def main():
     emx, _, mvmx = h.heff_lanczos(psi_host, 100, sadmrg.PREC_TF32X3)
     t_lmx = time.perf_counter() - t0
     # dominant launch and its roofline (3xTF32: three TF32 products per useful product)
-    k = int(np.argmax(ms_mix))
-    achieved = fl[k] / (ms_mix[k] / 1e3) / 1e12
+    names = {0: "psi -> TF32 hi/lo panels", 1: "tcgen05 grouped GEMM, stage 0 (X = op1^T psi)",
+             2: "split-K reduction, stage 0", 3: "tcgen05 grouped GEMM, stage 1 (output lists)",
+             4: "split-K reduction, stage 1"}
+    gemm_idx = [i for i, kd in enumerate(k_mix) if kd in (1, 3)]
+    kd = max(gemm_idx, key=lambda i: l_mix[i])
+    stage = (k_mix[kd] - 1) // 2
+    achieved = stage_flops[stage] / (l_mix[kd] / 1e3) / 1e12
     peak = peaks["tf32_tflops"] / 3.0
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        traffic = tj.get(a.workload, {}).get(f"stage{k}")
+        traffic = tj.get(a.workload, {}).get(f"umma_gemm_stage{stage}")
     except Exception:
         pass
     line = {
         "metric": "H_eff*psi TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": step_mix, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "tf32x3 (f32 partial sums, f64 accumulation)", "data": "synthetic",
+        "vs_baseline": None, "dtype": "tf32x3 (tcgen05 kind::tf32 hi/lo products, f32 accumulation in tensor memory)",
+        "data": "synthetic",
         "config": {"workload": a.workload, "L": wl["lx"] * wl["ly"], "D": wl["D"],
                    "symmetry": "SU2" if wl["sym"] else "U1", "bond": f"centre ({n} psi elements)",
                    "flops_per_step": flops, "tasks": info["ntasks"], "l2": "flushed (256 MiB write) between steps",
@@ -318,11 +396,14 @@ def main():
         "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": int(n * (16 if cplx else 8)),
                 "d2h_bytes_per_step": int(n * (16 if cplx else 8))},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": f"grouped_gemm_tf32x3 stage {k}",
-                     "peak_source": "cuBLAS TF32 GEMM measured in this run / 3 (3xTF32)",
-                     "stage_ms": ms_mix.tolist(), "stage_flops": list(fl)},
+                     "frac": achieved / peak, "traffic": traffic, "kernel": f"umma_gemm stage {stage}",
+                     "peak_source": "of measured: cuBLAS TF32 GEMM (8192^3) timed in this run, / 3 for 3xTF32",
+                     "launches_mixed": [[names[k], round(m, 5)] for k, m in zip(k_mix, l_mix.tolist())],
+                     "launches_fp64": [[names[k].replace("tcgen05", "mma.sync f64"), round(m, 5)]
+                                       for k, m in zip(k_64, l_64.tolist())],
+                     "stage_flops": list(stage_flops)},
         "peaks_measured": peaks,
-        "gpu_launches": 2 * a.steps * 2,
+        "gpu_launches": a.steps * (len(k_mix) + len(k_64)),
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not a.no_cpu and os.path.exists(HARNESS):

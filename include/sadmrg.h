@@ -115,6 +115,14 @@ int sadmrg_heff_apply_noalloc(sadmrg_handle* h, const void* psi_dev, void* out_d
  * psi_dev / out_dev may be NULL (the handle's own buffers are used). */
 int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, double* ms,
                         double* flops);
+/* Per-launch device time of one H_eff*psi (no counterpart in the reference; for
+ * rooflines): an event after every kernel the matvec launches, averaged over
+ * reps.  On return *nlaunch is the number of launches of one matvec; for the
+ * first min(cap, *nlaunch) of them kind[i] says what ran (0 psi -> TF32 panels,
+ * 1 + 2*stage: the grouped GEMM of that stage, 2 + 2*stage: its split-K
+ * reduction) and ms[i] its mean time. */
+int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, int cap,
+                               int* nlaunch, int* kind, double* ms);
 /* Lanczos ground state (lanczos1) from psi; psi is overwritten by the Ritz vector.
  * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
  * FP64 restart from its result. */

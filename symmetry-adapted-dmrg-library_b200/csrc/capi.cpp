@@ -308,6 +308,63 @@ int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* p
   });
 }
 
+int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, int cap,
+                               int* nlaunch, int* kind, double* ms) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_launch_profile: no plan");
+    SADMRG_REQUIRE(reps >= 1 && nlaunch, SADMRG_ERR_ARG, "heff_launch_profile: arguments");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_launch_profile: precision");
+    const HeffPlan<S>& H = *S_.heff;
+    const S* in = psi_dev ? static_cast<const S*>(psi_dev) : S_.io.template as<S>();
+    S* out = out_dev ? static_cast<S*>(out_dev) : S_.io.template as<S>() + H.n;
+    Bases b{};
+    b.p[0] = const_cast<S*>(in);
+    b.p[1] = out;
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = H.scratch->get();
+    std::vector<double> acc;
+    std::vector<int> kinds;
+    for (int r = 0; r < reps; ++r) {
+      std::vector<std::pair<int, cudaEvent_t>> ev;
+      cudaEvent_t start;
+      SADMRG_CUDA(cudaEventCreate(&start));
+      SADMRG_CUDA(cudaEventRecord(start, c.stream));
+      c.prof = &ev;
+      try {
+        H.plan.run(c, ScalarInfo<S>::cplx, precision, b);
+      } catch (...) {
+        c.prof = nullptr;
+        throw;
+      }
+      c.prof = nullptr;
+      SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+      if (acc.empty()) {
+        acc.assign(ev.size(), 0.0);
+        for (auto& e : ev) kinds.push_back(e.first);
+      }
+      SADMRG_REQUIRE(acc.size() == ev.size(), SADMRG_ERR_STATE, "heff_launch_profile: launch count changed");
+      cudaEvent_t prev = start;
+      for (size_t i = 0; i < ev.size(); ++i) {
+        float t = 0.f;
+        SADMRG_CUDA(cudaEventElapsedTime(&t, prev, ev[i].second));
+        acc[i] += t;
+        prev = ev[i].second;
+      }
+      cudaEventDestroy(start);
+      for (auto& e : ev) cudaEventDestroy(e.second);
+    }
+    check_device_status();
+    *nlaunch = (int)acc.size();
+    for (int i = 0; i < (int)acc.size() && i < cap; ++i) {
+      if (kind) kind[i] = kinds[i];
+      if (ms) ms[i] = acc[i] / reps;
+    }
+  });
+}
+
 int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energy, int* matvecs) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;

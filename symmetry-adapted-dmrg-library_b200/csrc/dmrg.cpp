@@ -380,7 +380,20 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
 template <class S>
 LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
   if (prec == PREC_FP64) return lanczos1<S>(c, H, v, mlanc, PREC_FP64);
-  LanczosStats a = lanczos1<S>(c, H, v, mlanc, prec);
+  // Split-precision Krylov first.  Its stop test is held no tighter than 1e-10:
+  // |<v|Hv>|/|Hv| - 1 ~ |error of v|^2, and the 3xTF32 operator (relative error
+  // ~1e-7) leaves v accurate to ~1e-5 at best, so a tighter test only buys
+  // matvecs the FP64 restart makes up for anyway.
+  const double tol = c.lanczos_ov_tol;
+  c.lanczos_ov_tol = std::max(tol, 1e-10);
+  LanczosStats a;
+  try {
+    a = lanczos1<S>(c, H, v, mlanc, prec);
+  } catch (...) {
+    c.lanczos_ov_tol = tol;
+    throw;
+  }
+  c.lanczos_ov_tol = tol;
   LanczosStats b = lanczos1<S>(c, H, v, mlanc, PREC_FP64);  // FP64 defect-correction restart
   b.matvecs += a.matvecs;
   b.iters += a.iters;
@@ -422,7 +435,14 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
       jobs.push_back(J);
     }
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
-  const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream);
+  const double tj = now_s();
+  const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
+                                    &out.jacobi_kernel_ms);
+  out.jacobi_s = now_s() - tj;
+  for (auto& J : jobs) {
+    out.max_rows = std::max(out.max_rows, std::max(J.m, J.n));
+    out.max_cols = std::max(out.max_cols, std::min(J.m, J.n));
+  }
   c.launches += 1;
   SADMRG_REQUIRE(sweeps > 0 || jobs.empty(), SADMRG_ERR_NUMERIC, "svd: Jacobi sweeps did not converge");
   out.sweeps_max = sweeps;
@@ -848,7 +868,10 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   last_discarded = s.discarded_weight;
   if (s.near_tie) ++near_ties;
   if (std::getenv("SADMRG_VERBOSE")) {
-    std::fprintf(stderr, "svd (%d,%d) kept=%d dw=%.3e sectors:", il, ir, s.kept, s.discarded_weight);
+    std::fprintf(stderr, "svd (%d,%d) kept=%d dw=%.3e sweeps=%d jacobi=%.2fms kernel=%.2fms max=%dx%d total=%.2fms sectors:",
+                 il, ir, s.kept, s.discarded_weight, s.sweeps_max, s.jacobi_s * 1e3, s.jacobi_kernel_ms, s.max_rows,
+                 s.max_cols,
+                 (now_s() - t0) * 1e3);
     const Bond& b = uu[il].st.bonds[2];
     for (int k = 0; k < b.nmom(); ++k) std::fprintf(stderr, " %d:%d", b.q[k], b.d[k]);
     std::fprintf(stderr, "\n");

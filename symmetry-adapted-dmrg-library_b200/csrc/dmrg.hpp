@@ -60,6 +60,9 @@ struct SvdStats {
   int kept = 0;
   double discarded_weight = 0.0;
   int sweeps_max = 0;
+  double jacobi_s = 0.0;       // wall time of the Jacobi solve
+  double jacobi_kernel_ms = -1.0;
+  int max_rows = 0, max_cols = 0;
   bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative)
 };
 

@@ -64,7 +64,7 @@ constexpr int kUmmaTileM = 128;
 struct PackJob {              // FP64 matrix -> panels
   long long src;              // element offset in its source buffer
   long long dst;              // byte offset of panel (0, 0) in the packed buffer
-  long long chunk0;           // first 16-byte chunk of this job in the launch (prefix sum)
+  long long chunk0;           // first 16-byte chunk of this job in the launch (a multiple of 256)
   int srcbuf, ld, rows, K, trans, T;   // trans 0: (r, k) at src[r + k*ld]; 1: at src[k + r*ld]
 };
 struct UTerm {                // a term's operands as panel sets: A (T = 128), B (T = BN)
@@ -81,6 +81,7 @@ struct UJob {                 // output tile grid of one job
 };
 struct UItem {                // one output tile x a run of consecutive slabs
   int job, tm, tn, t0, s0, nslab, slot;   // t0: first term (absolute), s0: its first slab; slot < 0: direct
+  int red;                    // split items: their tile's URed
 };
 struct URed {                 // C tile = sum of FP32 partial slots [slot0, slot0 + nslot) in fixed order
   int job, tm, tn, slot0, nslot;
@@ -89,13 +90,13 @@ struct UBufs {
   const unsigned char* pconst;
   unsigned char* pvar;
   float* slots;
+  int* tile_cnt;              // per URed: items of the tile finished in this launch (reset by the last)
 };
-void launch_pack(const PackJob* jobs, int njobs, long long nchunks, const Bases& b, unsigned char* dst,
+// one 256-thread block per 256 chunks; blk_job[block] = its job
+void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,
                  cudaStream_t s);
-void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
-                       const UBufs& u, cudaStream_t s);
-void launch_umma_reduce(int bn, const UJob* jobs, const URed* red, int nred, const Bases& b, const UBufs& u,
-                        cudaStream_t s);
+void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
+                       const Bases& b, const UBufs& u, cudaStream_t s);
 // status word of the tcgen05 kernels: 0 = fine, otherwise a bounded wait ran out
 // (the tiles it guarded were not written); reset clears it.  -1 if unreadable.
 int umma_status(bool reset);
@@ -171,7 +172,8 @@ struct SvdJob {
 };
 // Host driver: one launch per round of block pairs, one sync per sweep to test
 // convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
+// kernel_ms (optional): device time of the sweep kernel when it ran as one launch.
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
-                   int max_sweeps, cudaStream_t s);
+                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr);
 
 }  // namespace sadmrg

@@ -280,10 +280,16 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     P.T = p.k.T;
     const long long nch = (long long)((P.rows + P.T - 1) / P.T) * P.T * nslab_of(P.K) * 8;
     long long& cc = p.cls == 0 ? U->cchunks : U->vchunks;
+    auto& blk = p.cls == 0 ? U->cblk : U->vblk;
+    auto& list = p.cls == 0 ? U->cpack : U->vpack;
     P.chunk0 = cc;
-    cc += nch;
-    (p.cls == 0 ? U->cpack : U->vpack).push_back(P);
+    const long long nb = (nch + 255) / 256;
+    for (long long i = 0; i < nb; ++i) blk.push_back((int)list.size());
+    cc += nb * 256;
+    list.push_back(P);
   }
+  SADMRG_REQUIRE(U->cchunks < (1LL << 31) && U->vchunks < (1LL << 31), SADMRG_ERR_LIMIT,
+                 "tcgen05 schedule: operand panels too large for one pack launch");
   U->terms.resize(flat_terms.size());
   for (size_t t = 0; t < flat_terms.size(); ++t) {
     UTerm u{};
@@ -366,15 +372,15 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
       for (int a = 0; a < tm; ++a)
         for (int b = 0; b < tn; ++b) {
           if (nch == 1) {
-            its.push_back({ns, UItem{(int)j, a, b, J.t0, 0, (int)ns, -1}});
+            its.push_back({ns, UItem{(int)j, a, b, J.t0, 0, (int)ns, -1, -1}});
             continue;
           }
-          const int slot0 = nslot;
+          const int slot0 = nslot, red = (int)U->reds.size();
           long long pos = 0;
           int t = J.t0, s0 = 0;
           for (long long ch = 0; ch < nch; ++ch) {
             const long long len = std::min(kc, ns - pos);
-            its.push_back({len, UItem{(int)j, a, b, t, s0, (int)len, nslot++}});
+            its.push_back({len, UItem{(int)j, a, b, t, s0, (int)len, nslot++, red}});
             long long left = len;
             while (left > 0) {
               const int avail = U->terms[t].nslab - s0;
@@ -401,13 +407,14 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   }
   U->nslot = nslot;
 
-  // device copies: [cpack | vpack | terms | jobs | items | reds]
+  // device copies: [cpack | vpack | terms | jobs | items | reds | cblk | vblk]
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t b0 = sizeof(PackJob) * U->cpack.size(), b1 = sizeof(PackJob) * U->vpack.size(),
                b2 = sizeof(UTerm) * U->terms.size(), b3 = sizeof(UJob) * U->jobs.size(),
-               b4 = sizeof(UItem) * U->items.size(), b5 = sizeof(URed) * U->reds.size();
+               b4 = sizeof(UItem) * U->items.size(), b5 = sizeof(URed) * U->reds.size(),
+               b6 = sizeof(int) * U->cblk.size(), b7 = sizeof(int) * U->vblk.size();
   const size_t o1 = al(b0), o2 = o1 + al(b1), o3 = o2 + al(b2), o4 = o3 + al(b3), o5 = o4 + al(b4),
-               total = o5 + al(b5) + 256;
+               o6 = o5 + al(b5), o7 = o6 + al(b6), total = o7 + al(b7) + 256;
   std::vector<unsigned char> h(total, 0);
   if (b0) std::memcpy(h.data(), U->cpack.data(), b0);
   if (b1) std::memcpy(h.data() + o1, U->vpack.data(), b1);
@@ -415,6 +422,8 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   if (b3) std::memcpy(h.data() + o3, U->jobs.data(), b3);
   if (b4) std::memcpy(h.data() + o4, U->items.data(), b4);
   if (b5) std::memcpy(h.data() + o5, U->reds.data(), b5);
+  if (b6) std::memcpy(h.data() + o6, U->cblk.data(), b6);
+  if (b7) std::memcpy(h.data() + o7, U->vblk.data(), b7);
   U->dev = std::make_shared<DevBuf>(total, c.stream);
   SADMRG_CUDA(cudaMemcpyAsync(U->dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
   unsigned char* base = U->dev->as<unsigned char>();
@@ -424,10 +433,14 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   U->d_jobs = reinterpret_cast<UJob*>(base + o3);
   U->d_items = reinterpret_cast<UItem*>(base + o4);
   U->d_reds = reinterpret_cast<URed*>(base + o5);
+  const int* d_cblk = reinterpret_cast<int*>(base + o6);
+  U->d_vblk = reinterpret_cast<int*>(base + o7);
   U->pconst = std::make_shared<DevBuf>((size_t)std::max<long long>(cbytes, 256), c.stream);
   U->pvar = std::make_shared<DevBuf>((size_t)std::max<long long>(vbytes, 256), c.stream);
   U->slots = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * kUmmaTileM * BN * sizeof(float), c.stream);
-  launch_pack(d_cpack, (int)U->cpack.size(), U->cchunks, cb, U->pconst->as<unsigned char>(), c.stream);
+  U->tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(U->reds.size(), 1), c.stream);
+  SADMRG_CUDA(cudaMemsetAsync(U->tile_cnt->get(), 0, U->tile_cnt->bytes(), c.stream));
+  launch_pack(d_cpack, d_cblk, (int)U->cblk.size(), cb, U->pconst->as<unsigned char>(), c.stream);
   ++c.launches;
   SADMRG_CUDA(cudaGetLastError());
   // the host image must outlive the async copy
@@ -441,10 +454,8 @@ int GemmPlan::launches_per_run(bool cplx, int prec) const {
   if (uses_umma(cplx, prec)) {
     const UmmaSchedule& U = *umma;
     if (!U.vpack.empty()) ++n;
-    for (int s = 0; s < nstage; ++s) {
+    for (int s = 0; s < nstage; ++s)
       if (U.stage_items[s + 1] > U.stage_items[s]) ++n;
-      if (U.stage_reds[s + 1] > U.stage_reds[s]) ++n;
-    }
     return n;
   }
   for (int s = 0; s < nstage; ++s) {
@@ -454,27 +465,32 @@ int GemmPlan::launches_per_run(bool cplx, int prec) const {
   return n;
 }
 
+static void mark(Ctx& c, int kind) {
+  if (!c.prof) return;
+  cudaEvent_t e;
+  SADMRG_CUDA(cudaEventCreate(&e));
+  SADMRG_CUDA(cudaEventRecord(e, c.stream));
+  c.prof->push_back({kind, e});
+}
+
 void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, int stage_hi,
                    void* work_override) const {
   if (stage_hi < 0) stage_hi = nstage;
   if (uses_umma(cplx, prec)) {
     const UmmaSchedule& U = *umma;
     UBufs ub{U.pconst->as<unsigned char>(), U.pvar->as<unsigned char>(),
-             work_override ? static_cast<float*>(work_override) : U.slots->as<float>()};
+             work_override ? static_cast<float*>(work_override) : U.slots->as<float>(), U.tile_cnt->as<int>()};
     if (stage_lo == 0 && !U.vpack.empty()) {
-      launch_pack(U.d_vpack, (int)U.vpack.size(), U.vchunks, b, ub.pvar, c.stream);
+      launch_pack(U.d_vpack, U.d_vblk, (int)U.vblk.size(), b, ub.pvar, c.stream);
       ++c.launches;
+      mark(c, 0);
     }
     for (int s = stage_lo; s < stage_hi; ++s) {
       const int ni = U.stage_items[s + 1] - U.stage_items[s];
       if (ni > 0) {
-        launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items + U.stage_items[s], ni, b, ub, c.stream);
+        launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items + U.stage_items[s], U.d_reds, ni, b, ub, c.stream);
         ++c.launches;
-      }
-      const int nr = U.stage_reds[s + 1] - U.stage_reds[s];
-      if (nr > 0) {
-        launch_umma_reduce(U.bn, U.d_jobs, U.d_reds + U.stage_reds[s], nr, b, ub, c.stream);
-        ++c.launches;
+        mark(c, 1 + 2 * s);
       }
     }
     SADMRG_CUDA(cudaGetLastError());
@@ -487,11 +503,13 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
     if (ni > 0) {
       launch_items(cplx, prec, d_terms, d_jobs, sched.d_items + sched.stage_items[s], ni, b, wk, c.stream);
       ++c.launches;
+      mark(c, 1 + 2 * s);
     }
     const int nr = sched.stage_reds[s + 1] - sched.stage_reds[s];
     if (nr > 0) {
       launch_reduce(cplx, d_jobs, sched.d_reds + sched.stage_reds[s], nr, b, wk, sched.bm, sched.bn, c.stream);
       ++c.launches;
+      mark(c, 2 + 2 * s);
     }
   }
   SADMRG_CUDA(cudaGetLastError());

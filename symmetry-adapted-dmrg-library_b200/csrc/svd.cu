@@ -39,14 +39,14 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
+// One visit of a column-block pair: load its 2b columns into shared memory, one
+// cyclic sweep of scalar rotations over all their column pairs, write back, and
+// apply the accumulated rotation to the same columns of V.  Adds the number of
+// rotations to *rotations.  Every thread of the block calls it.
 template <bool CPLX>
-__global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
-                                                                  const SvdPair* __restrict__ pairs, void* work,
-                                                                  void* vmat, double tol, int* rotations) {
+__device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, double tol,
+                                  unsigned char* smem_raw, int* rotations) {
   using T = typename SvdT<CPLX>::T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SvdPair P = pairs[blockIdx.x];
-  const SvdJob J = jobs[P.job];
   const int R = J.trans ? J.n : J.m;
   const int C = J.trans ? J.m : J.n;
   int cols[32];
@@ -147,6 +147,9 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* 
     }
     __syncthreads();
   }
+  const int nrot = local_rot;
+  __syncthreads();
+  if (nrot == 0) return;        // nothing moved: W and V stay as they are
   for (int e = tid; e < nc * R; e += kSvdThreads) {
     const int c = e / R, r = e % R;
     W[r + (long long)cols[c] * R] = Ws[e];
@@ -182,7 +185,110 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* 
     }
     __syncthreads();
   }
-  if (tid == 0 && local_rot > 0) atomicAdd(rotations, local_rot);
+  if (tid == 0) atomicAdd(rotations, nrot);
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
+                                                                  const SvdPair* __restrict__ pairs, void* work,
+                                                                  void* vmat, double tol, int* rotations) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SvdPair P = pairs[blockIdx.x];
+  const SvdJob J = jobs[P.job];
+  jacobi_pair_visit<CPLX>(J, P, work, vmat, tol, smem_raw, rotations);
+}
+
+// ---------------------------------------------------------------------------
+// All sweeps in one cooperative launch.  Rounds are separated by a grid barrier
+// (bounded); rotations are counted per sector in three rotating counter sets
+// (sweep s adds into set s % 3, the set of sweep s + 1 is cleared during sweep
+// s, when nobody reads it any more), and a sector whose sweep made no rotation
+// is skipped from then on.  Every block takes the same decisions from the same
+// counts, read after the barrier that ends the sweep.
+constexpr int kSvdMaxJobsCoop = 256;
+constexpr unsigned long long kSvdBarrierNs = 2000000000ull;
+
+struct SvdCtl {
+  unsigned count, gen;
+  int status;                 // 0, or 1 when a grid barrier ran out of time
+  int sweeps;                 // sweeps taken, -1 when max_sweeps was reached
+  unsigned long long t0, t1;  // device clock (ns) at the start and end of block 0
+};
+
+__device__ __forceinline__ unsigned long long svd_gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ bool svd_grid_sync(SvdCtl* ctl) {
+  __shared__ int ok_sh;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok_sh = 1;
+    volatile unsigned* gen = &ctl->gen;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(&ctl->count, 1u) == gridDim.x - 1) {
+      atomicExch(&ctl->count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->gen, 1u);
+    } else {
+      const unsigned long long t0 = svd_gtime();
+      for (long long it = 0; *gen == g; ++it) {
+        if (it > (1ll << 30) || ((it & 255) == 255 && svd_gtime() - t0 > kSvdBarrierNs)) {
+          ok_sh = 0;
+          atomicExch(&ctl->status, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok_sh != 0;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* __restrict__ jobs, int nj,
+                                                                  const SvdPair* __restrict__ pairs,
+                                                                  const int* __restrict__ roff, int max_rounds,
+                                                                  void* work, void* vmat, double tol, int* cnt,
+                                                                  SvdCtl* ctl, int max_sweeps) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned char done[kSvdMaxJobsCoop];
+  __shared__ int all_done;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->t0 = svd_gtime();
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) done[j] = 0;
+  __syncthreads();
+  int sweeps = -1;
+  for (int sw = 0; sw < max_sweeps; ++sw) {
+    int* cur = cnt + (sw % 3) * nj;
+    if (blockIdx.x == 0)
+      for (int j = threadIdx.x; j < nj; j += blockDim.x) cnt[((sw + 1) % 3) * nj + j] = 0;
+    for (int r = 0; r < max_rounds; ++r) {
+      for (int p = roff[r] + blockIdx.x; p < roff[r + 1]; p += gridDim.x) {
+        const SvdPair P = pairs[p];
+        if (done[P.job]) continue;
+        const SvdJob J = jobs[P.job];
+        jacobi_pair_visit<CPLX>(J, P, work, vmat, tol, smem_raw, cur + P.job);
+      }
+      if (!svd_grid_sync(ctl)) return;
+    }
+    if (threadIdx.x == 0) all_done = 1;
+    __syncthreads();
+    for (int j = threadIdx.x; j < nj; j += blockDim.x) {
+      if (!done[j] && *((volatile int*)(cur + j)) == 0) done[j] = 1;
+      if (!done[j]) all_done = 0;
+    }
+    __syncthreads();
+    if (all_done) { sweeps = sw + 1; break; }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->sweeps = sweeps;
+    ctl->t1 = svd_gtime();
+  }
 }
 
 // W = A (m >= n) or A^H (m < n); V = I
@@ -239,10 +345,13 @@ static int pick_block(bool cplx, int R) {
   return 0;
 }
 
-// Host driver: runs the sweeps, synchronising once per sweep to test convergence.
-// Returns the number of sweeps taken (or -1 when max_sweeps was reached).
+// Host driver.  Runs all sweeps in one cooperative launch when the device allows
+// it, otherwise one launch per round and one host synchronisation per sweep to
+// test convergence.  Returns the number of sweeps taken (or -1 when max_sweeps
+// was reached).
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s) {
+                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
+  if (kernel_ms) *kernel_ms = -1.0;
   const int nj = (int)hjobs.size();
   if (nj == 0) return 0;
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
@@ -296,6 +405,54 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   const double tol = std::sqrt((double)std::max(maxR, 1)) * 2.220446049250313e-16;
   int sweeps = -1;
   int h_rot = 0;
+  // preferred: every sweep in one cooperative launch (no host round trip per sweep)
+  int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+  SADMRG_CUDA(cudaGetDevice(&dev));
+  SADMRG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  SADMRG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (cplx) {
+    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_coop_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_coop_kernel<true>, kSvdThreads, smem));
+  } else {
+    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_coop_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_coop_kernel<false>, kSvdThreads, smem));
+  }
+  int max_pairs = 1;
+  for (int r = 0; r < max_rounds; ++r) max_pairs = std::max(max_pairs, roff[r + 1] - roff[r]);
+  if (coop && per_sm > 0 && nj <= kSvdMaxJobsCoop) {
+    const int grid = std::max(1, std::min(max_pairs, per_sm * nsm));
+    DevBuf droff(sizeof(int) * (max_rounds + 1), s), dcnt3(sizeof(int) * 3 * nj, s), dctl(sizeof(SvdCtl), s);
+    SADMRG_CUDA(cudaMemcpyAsync(droff.get(), roff.data(), sizeof(int) * (max_rounds + 1), cudaMemcpyHostToDevice, s));
+    SADMRG_CUDA(cudaMemsetAsync(dcnt3.get(), 0, sizeof(int) * 3 * nj, s));
+    SADMRG_CUDA(cudaMemsetAsync(dctl.get(), 0, sizeof(SvdCtl), s));
+    const SvdJob* pj = djobs.as<SvdJob>();
+    const SvdPair* pp = dpairs.as<SvdPair>();
+    const int* pr = droff.as<int>();
+    int* pc = dcnt3.as<int>();
+    SvdCtl* pctl = dctl.as<SvdCtl>();
+    int njv = nj, mr = max_rounds, ms = max_sweeps;
+    double tolv = tol;
+    void* a_work = work;
+    void* a_vmat = vmat;
+    void* args[] = {(void*)&pj, (void*)&njv, (void*)&pp, (void*)&pr, (void*)&mr, (void*)&a_work,
+                    (void*)&a_vmat, (void*)&tolv, (void*)&pc, (void*)&pctl, (void*)&ms};
+    if (cplx)
+      SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<true>, dim3(grid), dim3(kSvdThreads),
+                                              args, smem, s));
+    else
+      SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<false>, dim3(grid), dim3(kSvdThreads),
+                                              args, smem, s));
+    SvdCtl hctl{};
+    SADMRG_CUDA(cudaMemcpyAsync(&hctl, dctl.get(), sizeof(SvdCtl), cudaMemcpyDeviceToHost, s));
+    SADMRG_CUDA(cudaStreamSynchronize(s));
+    SADMRG_REQUIRE(hctl.status == 0, SADMRG_ERR_CUDA, "jacobi svd: a grid barrier ran out of time");
+    sweeps = hctl.sweeps;
+    if (kernel_ms) *kernel_ms = (double)(hctl.t1 - hctl.t0) * 1e-6;
+    if (cplx) jacobi_norms_kernel<true><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
+    else jacobi_norms_kernel<false><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
+    SADMRG_CUDA(cudaGetLastError());
+    return sweeps;
+  }
   for (int sw = 0; sw < max_sweeps; ++sw) {
     SADMRG_CUDA(cudaMemsetAsync(dcnt.get(), 0, sizeof(int), s));
     for (int r = 0; r < max_rounds; ++r) {

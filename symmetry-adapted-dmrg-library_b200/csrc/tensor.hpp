@@ -32,6 +32,8 @@ struct Ctx {
   double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
+  // when set, GemmPlan::run records an event after every launch (what ran, event)
+  std::vector<std::pair<int, cudaEvent_t>>* prof = nullptr;
   ~Ctx();
 };
 
@@ -85,14 +87,16 @@ struct GemmSchedule {
 struct UmmaSchedule {
   int bn = 64;
   std::vector<PackJob> cpack, vpack;       // constant panels (packed once), psi panels (every apply)
-  long long cchunks = 0, vchunks = 0;
+  long long cchunks = 0, vchunks = 0;      // multiples of 256 (one block per 256 chunks)
+  std::vector<int> cblk, vblk;             // block -> pack job
   std::vector<UTerm> terms;
   std::vector<UJob> jobs;
   std::vector<UItem> items;
   std::vector<URed> reds;
   std::vector<int> stage_items, stage_reds;
-  std::shared_ptr<DevBuf> dev, pconst, pvar, slots;
+  std::shared_ptr<DevBuf> dev, pconst, pvar, slots, tile_cnt;
   PackJob* d_vpack = nullptr;
+  int* d_vblk = nullptr;
   UTerm* d_terms = nullptr;
   UJob* d_jobs = nullptr;
   UItem* d_items = nullptr;

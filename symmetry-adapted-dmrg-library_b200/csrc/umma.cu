@@ -15,8 +15,10 @@
 //                      frees the stage, and after the item's last slab signals
 //                      the accumulator full;
 //   warps 2-5          epilogue: tcgen05.ld of the 128 x BN accumulator (each
-//                      warp its 32 lanes), then FP64 store (optionally adding),
-//                      FP32 split-K partial tile, or hi/lo panels of X.
+//                      warp its 32 lanes), then FP64 store (optionally adding)
+//                      or hi/lo panels of X; a split-K item writes an FP32
+//                      partial tile and the last item of its tile to finish
+//                      (atomic count per tile) sums all partials in slot order.
 // Two accumulators (2 x BN TMEM columns) let the epilogue of one item overlap
 // the MMAs of the next; the kernel is persistent (one CTA per SM, static
 // round-robin over the longest-first item list).
@@ -148,38 +150,33 @@ __device__ __forceinline__ void st_global_v4(void* p, uint32_t x, uint32_t y, ui
 // FP64 matrices -> TF32 hi/lo panels.  One thread per 16-byte chunk (4 k of one
 // row); consecutive threads take consecutive rows of one (slab, kg) column, so
 // the stores are contiguous and the loads coalesce along rows (trans 0) or read
-// one 32-byte sector per thread (trans 1).
-__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, int njobs, long long nchunks,
+// one 32-byte sector per thread (trans 1).  Every job starts on a multiple of
+// 256 chunks, so a block works for one job, looked up in blk_job.
+__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, const int* __restrict__ blk_job,
                                                    Bases bases, unsigned char* __restrict__ dst) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nchunks) return;
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].chunk0 <= c) lo = mid;
-    else hi = mid - 1;
-  }
-  const PackJob P = jobs[lo];
-  const long long local = c - P.chunk0;
-  const int nslab = (P.K + kPanelK - 1) / kPanelK;
-  const long long Rp = (long long)((P.rows + P.T - 1) / P.T) * P.T;
-  const int r = (int)(local % Rp);
-  const int kgs = (int)(local / Rp);
-  const int s = kgs >> 3, kg = kgs & 7;
-  const int p = r / P.T, rr = r % P.T;
+  const PackJob P = jobs[blk_job[blockIdx.x]];
+  const unsigned local = blockIdx.x * 256u + threadIdx.x - (unsigned)P.chunk0;
+  const unsigned T = (unsigned)P.T;
+  const unsigned nslab = ((unsigned)P.K + kPanelK - 1) / kPanelK;
+  const unsigned Rp = (((unsigned)P.rows + T - 1) / T) * T;
+  if (local >= Rp * nslab * 8u) return;
+  const unsigned r = local % Rp, kgs = local / Rp;
+  const unsigned s = kgs >> 3, kg = kgs & 7u;
+  const unsigned p = r / T, rr = r - p * T;
   const double* src = static_cast<const double*>(bases.p[P.srcbuf]) + P.src;
   uint32_t h[4], l[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
-    const int k = s * kPanelK + kg * 4 + u;
+    const unsigned k = s * kPanelK + kg * 4 + u;
     double v = 0.0;
-    if (r < P.rows && k < P.K) v = P.trans ? src[k + (long long)r * P.ld] : src[r + (long long)k * P.ld];
+    if (r < (unsigned)P.rows && k < (unsigned)P.K)
+      v = P.trans ? src[k + (long long)r * P.ld] : src[r + (long long)k * P.ld];
     split_hl(v, h[u], l[u]);
   }
-  unsigned char* panel = dst + P.dst + ((long long)p * nslab + s) * P.T * 256;
-  const long long off = ((long long)kg * P.T + rr) * 16;
+  unsigned char* panel = dst + P.dst + ((long long)p * nslab + s) * (T * 256u);
+  const unsigned off = (kg * T + rr) * 16u;
   st_global_v4(panel + off, h[0], h[1], h[2], h[3]);
-  st_global_v4(panel + (long long)P.T * 128 + off, l[0], l[1], l[2], l[3]);
+  st_global_v4(panel + T * 128u + off, l[0], l[1], l[2], l[3]);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,13 +194,15 @@ struct UG {
 template <int BN, int ST>
 __global__ void __launch_bounds__(kGThreads, 1)
     umma_gemm(const UTerm* __restrict__ terms, const UJob* __restrict__ jobs, const UItem* __restrict__ items,
-              int nitems, Bases bases, UBufs ub) {
+              const URed* __restrict__ reds, int nitems, Bases bases, UBufs ub) {
   using G = UG<BN, ST>;
   constexpr int BM = kUmmaTileM;
   extern __shared__ unsigned char usm_raw[];
   __shared__ __align__(8) unsigned long long full[ST], empty[ST], tfull[2], tempty[2];
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
+  __shared__ volatile int last_sh;
+  __shared__ volatile int ep_fail;
 
   unsigned char* usm =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm_raw) + 127) & ~uintptr_t(127));
@@ -227,6 +226,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     abort_sh = 0;
+    ep_fail = 0;
   }
   fence_before();
   __syncthreads();
@@ -335,21 +335,49 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const int quarter = warp & 3;           // TMEM lanes 32*quarter .. +31
     const int r = 32 * quarter + lane;      // tile row
     int il = 0;
+    // The four epilogue warps take every decision together: a failed wait is
+    // posted to ep_fail and read by all after the same named barrier (id 1).
     for (int ii = blockIdx.x; ii < nitems; ii += gridDim.x, ++il) {
-      if (__shfl_sync(0xffffffffu, abort_sh, 0)) break;
       const UItem it = items[ii];
       const UJob J = jobs[it.job];
       const int acc = il & 1;
-      const bool got = mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh);
-      if (!__all_sync(0xffffffffu, got)) {
-        if (lane == 0) {
-          if (!abort_sh) atomicExch(&g_umma_status, 8);
-          abort_sh = 1;
-        }
-        break;
+      if (!mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh)) {
+        if (!abort_sh) atomicExch(&g_umma_status, 8);
+        abort_sh = 1;
+        ep_fail = 1;
       }
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (ep_fail) break;
       fence_after();
       const int row0 = it.tm * BM, col0 = it.tn * BN;
+      // 32 columns [cb, cb + 32) of row r of the finished tile -> C, or -> A panels of X
+      auto emit = [&](int cb, const double (&x)[32]) {
+        if (J.pack >= 0) {
+          const int s = (col0 + cb) / kPanelK;
+          if (s < J.pack_nslab) {
+            unsigned char* panel = ub.pvar + J.pack + ((long long)it.tm * J.pack_nslab + s) * (BM * 256);
+#pragma unroll
+            for (int kg = 0; kg < 8; ++kg) {
+              uint32_t h[4], l[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) split_hl(J.alpha * x[4 * kg + u], h[u], l[u]);
+              st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
+              st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
+            }
+          }
+        } else if (row0 + r < J.m) {
+          double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
+          const bool accum = J.flags & JF_ACCUM;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = col0 + cb + j;
+            if (col < J.n) {
+              const long long idx = (row0 + r) + (long long)col * J.ldc;
+              C[idx] = accum ? C[idx] + x[j] : x[j];
+            }
+          }
+        }
+      };
 #pragma unroll 1
       for (int cb = 0; cb < BN; cb += 32) {
         uint32_t v[32];
@@ -363,36 +391,41 @@ __global__ void __launch_bounds__(kGThreads, 1)
           float* S = ub.slots + (long long)it.slot * BM * BN;
 #pragma unroll
           for (int j = 0; j < 32; ++j) S[r + (cb + j) * BM] = __uint_as_float(v[j]);
-        } else if (J.pack >= 0) {
-          const int s = (col0 + cb) / kPanelK;
-          if (s < J.pack_nslab) {
-            unsigned char* panel = ub.pvar + J.pack + ((long long)it.tm * J.pack_nslab + s) * (BM * 256);
-            const float al = (float)J.alpha;
+        } else {
+          double x[32];
 #pragma unroll
-            for (int kg = 0; kg < 8; ++kg) {
-              uint32_t h[4], l[4];
-#pragma unroll
-              for (int u = 0; u < 4; ++u) split_hl_f(al * __uint_as_float(v[4 * kg + u]), h[u], l[u]);
-              st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
-              st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
-            }
-          }
-        } else if (row0 + r < J.m) {
-          double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
-          const bool accum = J.flags & JF_ACCUM;
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = col0 + cb + j;
-            if (col < J.n) {
-              const long long idx = (row0 + r) + (long long)col * J.ldc;
-              const double x = (double)__uint_as_float(v[j]);
-              C[idx] = accum ? C[idx] + x : x;
-            }
-          }
+          for (int j = 0; j < 32; ++j) x[j] = (double)__uint_as_float(v[j]);
+          emit(cb, x);
         }
       }
       fence_before();
       mbar_arrive(saddr(&tempty[acc]));
+      if (it.slot >= 0) {
+        // split-K: the last of the tile's items to get here sums every slot in
+        // slot order (the same order whichever item is last) and emits the tile
+        const URed R = reds[it.red];
+        __threadfence();
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (tid == 64) last_sh = (atomicAdd(&ub.tile_cnt[it.red], 1) == R.nslot - 1) ? 1 : 0;
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (last_sh) {
+          __threadfence();
+#pragma unroll 1
+          for (int cb = 0; cb < BN; cb += 32) {
+            double x[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) x[j] = 0.0;
+            for (int k = 0; k < R.nslot; ++k) {
+              const float* S = ub.slots + (long long)(R.slot0 + k) * BM * BN;
+#pragma unroll
+              for (int j = 0; j < 32; ++j) x[j] += (double)__ldcg(S + r + (cb + j) * BM);
+            }
+            emit(cb, x);
+          }
+          if (tid == 64) ub.tile_cnt[it.red] = 0;   // ready for the next launch
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+      }
     }
   }
 
@@ -405,56 +438,16 @@ __global__ void __launch_bounds__(kGThreads, 1)
   }
 }
 
-// Sum of the FP32 partial tiles of split items, in slot order, then the same
-// three outputs as the GEMM epilogue.  One thread per (row, 4 columns).
-template <int BN>
-__global__ void __launch_bounds__(256) umma_reduce(const UJob* __restrict__ jobs, const URed* __restrict__ red,
-                                                   Bases bases, UBufs ub) {
-  constexpr int BM = kUmmaTileM;
-  const URed R = red[blockIdx.x];
-  const UJob J = jobs[R.job];
-  const int row0 = R.tm * BM, col0 = R.tn * BN;
-  for (int e = threadIdx.x; e < BM * (BN / 4); e += blockDim.x) {
-    const int r = e % BM, c4 = (e / BM) * 4;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = 0; k < R.nslot; ++k) {
-      const float* S = ub.slots + (long long)(R.slot0 + k) * BM * BN;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] += (double)S[r + (c4 + u) * BM];
-    }
-    if (J.pack >= 0) {
-      const int s = (col0 + c4) / kPanelK, kg = ((col0 + c4) % kPanelK) / 4;
-      if (s >= J.pack_nslab) continue;
-      unsigned char* panel = ub.pvar + J.pack + ((long long)R.tm * J.pack_nslab + s) * (BM * 256);
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) split_hl(J.alpha * acc[u], h[u], l[u]);
-      st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
-      st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
-    } else if (row0 + r < J.m) {
-      double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
-      const bool accum = J.flags & JF_ACCUM;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int col = col0 + c4 + u;
-        if (col >= J.n) continue;
-        const long long idx = (row0 + r) + (long long)col * J.ldc;
-        C[idx] = accum ? C[idx] + acc[u] : acc[u];
-      }
-    }
-  }
-}
-
 template <int BN, int ST>
-void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
-                   const UBufs& u, cudaStream_t s) {
+void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
+                   const Bases& b, const UBufs& u, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(umma_gemm<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG<BN, ST>::SMEM);
     attr = true;
   }
   const int grid = nitems < device_sm_count() ? nitems : device_sm_count();
-  umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, nitems, b, u);
+  umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, reds, nitems, b, u);
 }
 
 }  // namespace
@@ -472,25 +465,17 @@ int device_sm_count() {
   return n;
 }
 
-void launch_pack(const PackJob* jobs, int njobs, long long nchunks, const Bases& b, unsigned char* dst,
+void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,
                  cudaStream_t s) {
-  if (njobs <= 0 || nchunks <= 0) return;
-  const long long blocks = (nchunks + 255) / 256;
-  pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(jobs, njobs, nchunks, b, dst);
+  if (nblocks <= 0) return;
+  pack_kernel<<<nblocks, 256, 0, s>>>(jobs, blk_job, b, dst);
 }
 
-void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, int nitems, const Bases& b,
-                       const UBufs& u, cudaStream_t s) {
+void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
+                       const Bases& b, const UBufs& u, cudaStream_t s) {
   if (nitems <= 0) return;
-  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, nitems, b, u, s);
-  else launch_gemm_t<64, 4>(terms, jobs, items, nitems, b, u, s);
-}
-
-void launch_umma_reduce(int bn, const UJob* jobs, const URed* red, int nred, const Bases& b, const UBufs& u,
-                        cudaStream_t s) {
-  if (nred <= 0) return;
-  if (bn == 128) umma_reduce<128><<<nred, 256, 0, s>>>(jobs, red, b, u);
-  else umma_reduce<64><<<nred, 256, 0, s>>>(jobs, red, b, u);
+  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, reds, nitems, b, u, s);
+  else launch_gemm_t<64, 4>(terms, jobs, items, reds, nitems, b, u, s);
 }
 
 int umma_status(bool reset) {

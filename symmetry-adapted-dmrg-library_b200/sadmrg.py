@@ -19,7 +19,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsadmrg_b200.so")
+LIB_PATH = os.environ.get("SADMRG_LIB") or os.path.join(_HERE, "libsadmrg_b200.so")
 
 SYM_U1, SYM_SU2 = 0, 1
 PREC_FP64, PREC_TF32X3 = 0, 1
@@ -31,6 +31,7 @@ EXPORTED = [
     "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
+    "sadmrg_device_status", "sadmrg_heff_launch_profile",
 ]
 
 
@@ -71,6 +72,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
         "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
+        "sadmrg_heff_launch_profile": ([vp, C.c_int, C.c_int, vp, vp, C.c_int, ip, ip, dp], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -211,9 +213,11 @@ class Handle:
         self._check(self.lib.sadmrg_heff_info(self.h, C.byref(n), C.byref(fl), C.byref(by), C.byref(nt)), "heff_info")
         return {"n": n.value, "flops": fl.value, "bytes": by.value, "ntasks": nt.value}
 
-    def heff_apply(self, psi: np.ndarray, precision: int = PREC_FP64) -> np.ndarray:
+    def heff_apply(self, psi: np.ndarray, precision: int = PREC_FP64, out: Optional[np.ndarray] = None) -> np.ndarray:
         x = np.ascontiguousarray(psi, dtype=self.dtype)
-        out = np.empty_like(x)
+        if out is None:
+            out = np.empty_like(x)
+        assert out.dtype == x.dtype and out.shape == x.shape and out.flags.c_contiguous
         self._check(self.lib.sadmrg_heff_apply(self.h, x.ctypes.data, out.ctypes.data, int(precision)), "heff_apply")
         return out
 
@@ -239,6 +243,20 @@ class Handle:
         """H_eff*psi on device pointers without allocating (library's fixed device scratch)."""
         self._check(self.lib.sadmrg_heff_apply_noalloc(self.h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
                                                        int(precision)), "heff_apply_noalloc")
+
+    def heff_launch_profile(self, precision: int = PREC_FP64, reps: int = 10, psi_ptr: int = 0, out_ptr: int = 0):
+        """[(kind, mean ms)] for every kernel one matvec launches; kind 0: psi -> TF32 panels,
+        1 + 2*stage: grouped GEMM of that stage, 2 + 2*stage: its split-K reduction."""
+        cap = 64
+        n = C.c_int(0)
+        kinds = np.zeros(cap, dtype=np.int32)
+        ms = np.zeros(cap)
+        self._check(self.lib.sadmrg_heff_launch_profile(self.h, int(precision), int(reps), C.c_void_p(psi_ptr),
+                                                        C.c_void_p(out_ptr), cap, C.byref(n),
+                                                        kinds.ctypes.data_as(C.POINTER(C.c_int)),
+                                                        ms.ctypes.data_as(C.POINTER(C.c_double))),
+                    "heff_launch_profile")
+        return [(int(kinds[i]), float(ms[i])) for i in range(min(n.value, cap))]
 
     def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         x = np.array(psi, dtype=self.dtype, copy=True)
