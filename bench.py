@@ -50,6 +50,10 @@ WORKLOADS = {
     "su2_heisenberg_L100_D512": dict(sym=1, cplx=False, lx=1, ly=100, D=512, J2=0.0),
     "su2_ladder_2x32_D1024": dict(sym=1, cplx=False, lx=32, ly=2, D=1024, J2=0.0),
     "u1_heisenberg_L32_D64": dict(sym=0, cplx=False, lx=1, ly=32, D=64, J2=0.0),
+    # frozen centre of a 2 x 32 SU(2) ladder (snake mapping, open), 30 sectors per side
+    # with dims log-uniform in [8, 512] and N(0,1) entries from the seed
+    "su2_ladder_2x32_D2048_synth": dict(sym=1, cplx=False, lx=32, ly=2, D=2048, J2=0.0,
+                                        synthetic=dict(seed=2024, nsec=30, dmin=8, dmax=512)),
 }
 
 
@@ -229,6 +233,62 @@ def build_problem(wl: dict, device: int, sweeps: int, export_dir: str | None):
     return keep, psi, meta
 
 
+def make_synthetic(wl: dict, device: int, directory: str):
+    """Write a synthetic frozen two-site problem to `directory` in the export format.
+
+    The lattice, its couplings and the set of centre operators come from a small
+    chain of the same geometry frozen at its centre (meta.txt and the opr_* names);
+    every tensor is then replaced: both fused bonds get nsec SU(2) sectors 2J = 0, 2,
+    ... with dims drawn log-uniform in [dmin, dmax], psi holds the (J, J) blocks,
+    hh the (J, J) blocks (symmetrised), each operator the (J, 1, J') blocks with
+    |J - J'| <= 1, J + J' >= 1, all N(0,1) (operators scaled by 1/sqrt(rows))."""
+    import sadmrg
+    sp = wl["synthetic"]
+    ns = wl["lx"] * wl["ly"]
+    h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=device)
+    h.chain_create(wl["lx"], wl["ly"], 16, 1, 0, True, wl["J2"])
+    h.chain_idmrg()
+    h.chain_freeze(ns // 2 - 1, directory)
+    h.close()
+    rng = np.random.default_rng(sp["seed"])
+    n = sp["nsec"]
+    q = [2 * i for i in range(n)]
+
+    def dims():
+        return [int(round(np.exp(rng.uniform(np.log(sp["dmin"]), np.log(sp["dmax"]))))) for _ in range(n)]
+
+    dl, dr = dims(), dims()
+
+    def tensor(dirs, qs, ds, blocks, gen):
+        keys = sorted(blocks)
+        return sadmrg.BlockTensorData(dirs, qs, ds, 0, np.array(keys, np.int64),
+                                      np.concatenate([gen(k) for k in keys]))
+
+    def hh(d):
+        def g(k):
+            a = rng.standard_normal((d[k % n], d[k % n]))
+            return ((a + a.T) / 2).reshape(-1, order="F")
+        return tensor([-1, 1], [q, q], [d, d], [i + i * n for i in range(n)], g)
+
+    def op(d):
+        blocks = [i + j * n for i in range(n) for j in range(n) if abs(q[i] - q[j]) <= 2 and q[i] + q[j] >= 2]
+        return tensor([-1, -1, 1], [q, [2], q], [d, [1], d], blocks,
+                      lambda k: rng.standard_normal(d[k % n] * d[k // n]) / np.sqrt(d[k % n]))
+
+    psi = tensor([1, 1], [q, q], [dl, dr], [i + i * n for i in range(n)],
+                 lambda k: rng.standard_normal(dl[k % n] * dr[k % n]))
+    sadmrg.write_exported_tensor(directory, "psi", psi)
+    sadmrg.write_exported_tensor(directory, "hh_il", hh(dl))
+    sadmrg.write_exported_tensor(directory, "hh_ir", hh(dr))
+    for fn in sorted(os.listdir(directory)):
+        if fn.startswith("opr_il_") and fn.endswith(".txt"):
+            sadmrg.write_exported_tensor(directory, fn[:-4], op(dl))
+        elif fn.startswith("opr_ir_") and fn.endswith(".txt"):
+            sadmrg.write_exported_tensor(directory, fn[:-4], op(dr))
+    return dict(source="synthetic", sectors_per_side=n, dims_left=dl, dims_right=dr,
+                dims="log-uniform in [%d, %d], seed %d" % (sp["dmin"], sp["dmax"], sp["seed"]))
+
+
 def load_problem(wl: dict, device: int, directory: str):
     import sadmrg
     h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=device)
@@ -269,6 +329,10 @@ def main():
             if a.problem:
                 src = a.problem
                 h, psi, meta = load_problem(wl, local, src)
+            elif "synthetic" in wl:
+                src = td
+                make_synthetic(wl, local, td)
+                h, psi, meta = load_problem(wl, local, td)
             else:
                 src = td
                 h, psi, meta = build_problem(wl, local, a.sweeps, td)
@@ -296,6 +360,11 @@ def main():
     if a.problem:
         export_dir = a.problem
         h, psi, meta = load_problem(wl, local, a.problem)
+    elif "synthetic" in wl:
+        export_dir = (a.export or tempfile.mkdtemp(prefix="sadmrg_bench_"))
+        os.makedirs(export_dir, exist_ok=True)
+        meta = make_synthetic(wl, local, export_dir)
+        h, psi, _ = load_problem(wl, local, export_dir)
     else:
         export_dir = (a.export or tempfile.mkdtemp(prefix="sadmrg_bench_")) if rank == 0 else None
         if export_dir:
@@ -355,28 +424,39 @@ def main():
     # accuracy of the split-precision matvec and of the mixed Lanczos
     y64 = h.heff_apply(psi_host, sadmrg.PREC_FP64)
     mv_err = float(np.abs(out - y64).max() / np.abs(y64).max())
-    # Lanczos to a tight stop (|<v|Hv>|/|Hv| within 1e-14 of 1, <= 100 steps) from the frozen psi
-    h.set_lanczos_tol(1e-14)
-    t0 = time.perf_counter()
-    e64, _, mv64 = h.heff_lanczos(psi_host, 100, sadmrg.PREC_FP64)
-    t_l64 = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    emx, _, mvmx = h.heff_lanczos(psi_host, 100, sadmrg.PREC_TF32X3)
-    t_lmx = time.perf_counter() - t0
+    # Lanczos to a tight stop (|<v|Hv>|/|Hv| within 1e-14 of 1, <= 100 steps) from the frozen psi;
+    # the synthetic operators are not Hermitian, so that workload has no ground state to compare
+    e64 = emx = t_l64 = t_lmx = mv64 = mvmx = None
+    if "synthetic" not in wl:
+        h.set_lanczos_tol(1e-14)
+        t0 = time.perf_counter()
+        e64, _, mv64 = h.heff_lanczos(psi_host, 100, sadmrg.PREC_FP64)
+        t_l64 = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        emx, _, mvmx = h.heff_lanczos(psi_host, 100, sadmrg.PREC_TF32X3)
+        t_lmx = time.perf_counter() - t0
+    # the same matvecs replayed from a captured CUDA graph, 200 calls back to back (L2 warm)
+    graph = {"calls": 200,
+             "mixed_us": 1e3 * h.heff_graph_bench(sadmrg.PREC_TF32X3, 200, x.data_ptr(), y.data_ptr()),
+             "fp64_us": 1e3 * h.heff_graph_bench(sadmrg.PREC_FP64, 200, x.data_ptr(), y.data_ptr())}
+    graph["mixed_tflops"] = flops / (graph["mixed_us"] * 1e-6) / 1e12
+    graph["fp64_tflops"] = flops / (graph["fp64_us"] * 1e-6) / 1e12
     # dominant launch and its roofline (3xTF32: three TF32 products per useful product)
     names = {0: "psi -> TF32 hi/lo panels", 1: "tcgen05 grouped GEMM, stage 0 (X = op1^T psi)",
              2: "split-K reduction, stage 0", 3: "tcgen05 grouped GEMM, stage 1 (output lists)",
-             4: "split-K reduction, stage 1"}
-    gemm_idx = [i for i, kd in enumerate(k_mix) if kd in (1, 3)]
+             4: "split-K reduction, stage 1",
+             5: "tcgen05 grouped GEMM, whole matvec (psi panels + stage 0 + stage 1, one launch)"}
+    gemm_idx = [i for i, kd in enumerate(k_mix) if kd in (1, 3, 5)]
     kd = max(gemm_idx, key=lambda i: l_mix[i])
-    stage = (k_mix[kd] - 1) // 2
-    achieved = stage_flops[stage] / (l_mix[kd] / 1e3) / 1e12
+    stage = (k_mix[kd] - 1) // 2 if k_mix[kd] != 5 else None
+    kflops = sum(stage_flops) if stage is None else stage_flops[stage]
+    achieved = kflops / (l_mix[kd] / 1e3) / 1e12
     peak = peaks["tf32_tflops"] / 3.0
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        traffic = tj.get(a.workload, {}).get(f"umma_gemm_stage{stage}")
+        traffic = tj.get(a.workload, {}).get("umma_gemm_matvec" if stage is None else f"umma_gemm_stage{stage}")
     except Exception:
         pass
     line = {
@@ -390,13 +470,15 @@ def main():
                    "parallelism": f"replicas x{ws}"},
         "fp64": {"value": value64, "ms_per_step": step_64, "speedup_mixed_over_fp64": value / value64},
         "accuracy": {"matvec_rel_err_tf32x3": mv_err, "lanczos_E_fp64": e64, "lanczos_E_mixed": emx,
-                     "abs_dE": abs(emx - e64), "lanczos_s_fp64": t_l64, "lanczos_s_mixed": t_lmx,
-                     "matvecs_fp64": mv64, "matvecs_mixed": mvmx},
+                     "abs_dE": None if e64 is None else abs(emx - e64), "lanczos_s_fp64": t_l64,
+                     "lanczos_s_mixed": t_lmx, "matvecs_fp64": mv64, "matvecs_mixed": mvmx},
+        "cuda_graph": graph,
         "chain": meta,
         "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": int(n * (16 if cplx else 8)),
                 "d2h_bytes_per_step": int(n * (16 if cplx else 8))},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": f"umma_gemm stage {stage}",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "umma_gemm (whole matvec)" if stage is None else f"umma_gemm stage {stage}",
                      "peak_source": "of measured: cuBLAS TF32 GEMM (8192^3) timed in this run, / 3 for 3xTF32",
                      "launches_mixed": [[names[k], round(m, 5)] for k, m in zip(k_mix, l_mix.tolist())],
                      "launches_fp64": [[names[k].replace("tcgen05", "mma.sync f64"), round(m, 5)]

@@ -81,6 +81,12 @@ int sadmrg_device_status(sadmrg_handle* h, int* status);
  * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338). */
 int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol);
 
+/* How the split-precision matvec of real plans is launched (no counterpart in
+ * the reference): 0 (default) psi -> panels, then one tcgen05 launch per stage;
+ * 1 the whole matvec as one cooperative launch whose work items wait (bounded)
+ * for the panels they read. */
+int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused);
+
 /* ---- frozen two-site problem: H_eff * psi ---------------------------------
  * ops[] holds every block operator once; term i pairs ops[op1[i]] (left block,
  * legs (a, channel, a')) with ops[op2[i]] (right block, legs (b, channel, b')),
@@ -120,9 +126,14 @@ int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* p
  * reps.  On return *nlaunch is the number of launches of one matvec; for the
  * first min(cap, *nlaunch) of them kind[i] says what ran (0 psi -> TF32 panels,
  * 1 + 2*stage: the grouped GEMM of that stage, 2 + 2*stage: its split-K
- * reduction) and ms[i] its mean time. */
+ * reduction, 5: the whole matvec in one launch) and ms[i] its mean time. */
 int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev, int cap,
                                int* nlaunch, int* kind, double* ms);
+/* The same matvec replayed from a CUDA graph (no counterpart in the reference):
+ * one H_eff*psi on (psi_dev, out_dev) is captured once, the graph is launched
+ * reps times, and *ms is the mean device time per replay (CUDA events). */
+int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev,
+                            double* ms);
 /* Lanczos ground state (lanczos1) from psi; psi is overwritten by the Ritz vector.
  * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
  * FP64 restart from its result. */

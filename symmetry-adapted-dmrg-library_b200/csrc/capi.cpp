@@ -189,6 +189,13 @@ int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol) {
   });
 }
 
+int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(fused == 0 || fused == 1, SADMRG_ERR_ARG, "set_matvec_fusion: 0 or 1");
+    h->ctx.fused_matvec = fused != 0;
+  });
+}
+
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
@@ -362,6 +369,60 @@ int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const 
       if (kind) kind[i] = kinds[i];
       if (ms) ms[i] = acc[i] / reps;
     }
+  });
+}
+
+int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev,
+                            double* ms) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_graph_bench: no plan");
+    SADMRG_REQUIRE(reps >= 1 && ms, SADMRG_ERR_ARG, "heff_graph_bench: arguments");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_graph_bench: precision");
+    const HeffPlan<S>& H = *S_.heff;
+    Bases b{};
+    b.p[0] = const_cast<void*>(psi_dev ? psi_dev : S_.io.get());
+    b.p[1] = out_dev ? out_dev : static_cast<void*>(S_.io.template as<S>() + H.n);
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = H.scratch->get();
+    // one plain run first: lazy one-time setup (kernel attributes, device queries) stays out of the capture
+    H.plan.run(c, ScalarInfo<S>::cplx, precision, b);
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    SADMRG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      H.plan.run(c, ScalarInfo<S>::cplx, precision, b);
+    } catch (...) {
+      cudaStreamEndCapture(c.stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    SADMRG_CUDA(cudaStreamEndCapture(c.stream, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      SADMRG_CUDA(ie);
+    }
+    cudaEvent_t e0, e1;
+    SADMRG_CUDA(cudaEventCreate(&e0));
+    SADMRG_CUDA(cudaEventCreate(&e1));
+    SADMRG_CUDA(cudaGraphLaunch(ge, c.stream));   // warm
+    SADMRG_CUDA(cudaEventRecord(e0, c.stream));
+    for (int r = 0; r < reps; ++r) SADMRG_CUDA(cudaGraphLaunch(ge, c.stream));
+    SADMRG_CUDA(cudaEventRecord(e1, c.stream));
+    SADMRG_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    SADMRG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision, c.fused_matvec) * (reps + 1);
+    check_device_status();
   });
 }
 

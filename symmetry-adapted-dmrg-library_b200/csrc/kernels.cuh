@@ -71,6 +71,7 @@ struct UTerm {                // a term's operands as panel sets: A (T = 128), B
   long long a, b;             // byte offsets of panel (0, 0)
   int abuf, bbuf;             // 0: constant panels, 1: per-apply panels
   int nslab, klast;           // k slabs, k of the last slab (1..32)
+  int adep, bdep;             // dependency counter of the A / B panels written in the same launch, or -1
 };
 struct UJob {                 // output tile grid of one job
   long long coff;             // FP64 output: bases.p[cbuf] + coff, column-major, ldc
@@ -78,6 +79,7 @@ struct UJob {                 // output tile grid of one job
                               // per-apply buffer, scaled by alpha, with pack_nslab slabs per panel
   double alpha;
   int cbuf, m, n, ldc, flags, t0, nt, pack_nslab;
+  int dep;                    // counter bumped per finished tile (results read as panels later), or -1
 };
 struct UItem {                // one output tile x a run of consecutive slabs
   int job, tm, tn, t0, s0, nslab, slot;   // t0: first term (absolute), s0: its first slab; slot < 0: direct
@@ -91,12 +93,27 @@ struct UBufs {
   unsigned char* pvar;
   float* slots;
   int* tile_cnt;              // per URed: items of the tile finished in this launch (reset by the last)
+  int* deps;                  // dependency counters (psi pack jobs, then stage-0 results), zero between launches
+  const int* dep_target;      // value each counter reaches once its panels are complete
+  unsigned* fin;              // CTAs finished (the last one clears deps)
+};
+constexpr int kMaxPackJobs = 1024;   // psi pack jobs one fused launch can count
+struct UPhase {               // what one launch does besides its items
+  const PackJob* pk;          // psi -> panels jobs packed at the start of the launch
+  const int* pk_blk;          // pack block (256 chunks) -> job
+  int npk_blocks;             // 0: no packing in this launch
+  int npk_jobs;
+  int wait_deps;              // items wait for panels written in this launch (cooperative launch)
+  int ndeps;
 };
 // one 256-thread block per 256 chunks; blk_job[block] = its job
 void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,
                  cudaStream_t s);
+// One launch of the tcgen05 executor: optional psi packing, then the items.  With
+// ph.wait_deps the whole matvec (pack, stage 0, stage 1) runs as one cooperative
+// launch, every item waiting (bounded) for the panels it reads.
 void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
-                       const Bases& b, const UBufs& u, cudaStream_t s);
+                       const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s);
 // status word of the tcgen05 kernels: 0 = fine, otherwise a bounded wait ran out
 // (the tiles it guarded were not written); reset clears it.  -1 if unreadable.
 int umma_status(bool reset);

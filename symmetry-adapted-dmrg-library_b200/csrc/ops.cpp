@@ -267,8 +267,11 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     p.dst = tot;
     tot += (panel_bytes(p.k) + 255) & ~255LL;
   }
-  for (auto& p : packs) {
+  std::vector<int> vpack_of(packs.size(), -1);
+  for (size_t pi = 0; pi < packs.size(); ++pi) {
+    auto& p = packs[pi];
     if (p.cls == 2) continue;
+    if (p.cls == 1) vpack_of[pi] = (int)U->vpack.size();
     PackJob P{};
     P.src = p.k.src;
     P.dst = p.dst;
@@ -290,11 +293,27 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   }
   SADMRG_REQUIRE(U->cchunks < (1LL << 31) && U->vchunks < (1LL << 31), SADMRG_ERR_LIMIT,
                  "tcgen05 schedule: operand panels too large for one pack launch");
+  // dependency counters: [0, nv) psi pack jobs, then one per stage-0 result read as panels
+  const int nv = (int)U->vpack.size();
+  std::map<long long, int> xdep;   // stage-0 result offset -> its counter
+  for (size_t pi = 0; pi < packs.size(); ++pi)
+    if (packs[pi].cls == 2 && !xdep.count(packs[pi].k.src)) {
+      const int d = nv + (int)xdep.size();
+      xdep[packs[pi].k.src] = d;
+    }
+  auto dep_of = [&](int pi) -> int {
+    if (packs[pi].cls == 1) return vpack_of[pi];
+    if (packs[pi].cls == 2) return xdep[packs[pi].k.src];
+    return -1;
+  };
   U->terms.resize(flat_terms.size());
   for (size_t t = 0; t < flat_terms.size(); ++t) {
     UTerm u{};
+    u.adep = u.bdep = -1;
     const int K = flat_terms[t].k;
     if (K > 0) {
+      u.adep = dep_of(ta[t]);
+      u.bdep = dep_of(tb[t]);
       u.a = packs[ta[t]].dst;
       u.b = packs[tb[t]].dst;
       u.abuf = packs[ta[t]].cls ? 1 : 0;
@@ -326,6 +345,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     u.flags = J.flags;
     u.t0 = J.t0;
     u.nt = J.nt;
+    u.dep = -1;
     if (J.cbuf == 3) {
       auto it = xreader.find(J.coff);
       if (it == xreader.end() || job_stage[j] != 0 || (J.flags & JF_ACCUM)) return false;
@@ -334,6 +354,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
       u.pack = packs[it->second].dst;
       u.alpha = xalpha[J.coff];
       u.pack_nslab = nslab_of(J.n);
+      u.dep = xdep[J.coff];
       ++produced;
     } else if (J.cbuf != 1) {
       return false;
@@ -341,6 +362,12 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     U->jobs[j] = u;
   }
   if (produced != (int)xreader.size()) return false;
+  U->dep_target.assign(nv + xdep.size(), 0);
+  for (int b : U->vblk) U->dep_target[b] += 256;              // chunks (padded) per psi job
+  for (size_t j = 0; j < jobs.size(); ++j)
+    if (U->jobs[j].dep >= 0)
+      U->dep_target[U->jobs[j].dep] =
+          ((jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);   // tiles of the result
 
   // slab-granular items, longest first; split the reduction only when the
   // output tiles cannot keep every SM busy
@@ -412,9 +439,10 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   const size_t b0 = sizeof(PackJob) * U->cpack.size(), b1 = sizeof(PackJob) * U->vpack.size(),
                b2 = sizeof(UTerm) * U->terms.size(), b3 = sizeof(UJob) * U->jobs.size(),
                b4 = sizeof(UItem) * U->items.size(), b5 = sizeof(URed) * U->reds.size(),
-               b6 = sizeof(int) * U->cblk.size(), b7 = sizeof(int) * U->vblk.size();
+               b6 = sizeof(int) * U->cblk.size(), b7 = sizeof(int) * U->vblk.size(),
+               b8 = sizeof(int) * U->dep_target.size();
   const size_t o1 = al(b0), o2 = o1 + al(b1), o3 = o2 + al(b2), o4 = o3 + al(b3), o5 = o4 + al(b4),
-               o6 = o5 + al(b5), o7 = o6 + al(b6), total = o7 + al(b7) + 256;
+               o6 = o5 + al(b5), o7 = o6 + al(b6), o8 = o7 + al(b7), total = o8 + al(b8) + 256;
   std::vector<unsigned char> h(total, 0);
   if (b0) std::memcpy(h.data(), U->cpack.data(), b0);
   if (b1) std::memcpy(h.data() + o1, U->vpack.data(), b1);
@@ -424,6 +452,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   if (b5) std::memcpy(h.data() + o5, U->reds.data(), b5);
   if (b6) std::memcpy(h.data() + o6, U->cblk.data(), b6);
   if (b7) std::memcpy(h.data() + o7, U->vblk.data(), b7);
+  if (b8) std::memcpy(h.data() + o8, U->dep_target.data(), b8);
   U->dev = std::make_shared<DevBuf>(total, c.stream);
   SADMRG_CUDA(cudaMemcpyAsync(U->dev->get(), h.data(), total, cudaMemcpyHostToDevice, c.stream));
   unsigned char* base = U->dev->as<unsigned char>();
@@ -435,11 +464,14 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   U->d_reds = reinterpret_cast<URed*>(base + o5);
   const int* d_cblk = reinterpret_cast<int*>(base + o6);
   U->d_vblk = reinterpret_cast<int*>(base + o7);
+  U->d_dep_target = reinterpret_cast<int*>(base + o8);
   U->pconst = std::make_shared<DevBuf>((size_t)std::max<long long>(cbytes, 256), c.stream);
   U->pvar = std::make_shared<DevBuf>((size_t)std::max<long long>(vbytes, 256), c.stream);
   U->slots = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * kUmmaTileM * BN * sizeof(float), c.stream);
   U->tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(U->reds.size(), 1), c.stream);
   SADMRG_CUDA(cudaMemsetAsync(U->tile_cnt->get(), 0, U->tile_cnt->bytes(), c.stream));
+  U->deps = std::make_shared<DevBuf>(sizeof(int) * (U->dep_target.size() + 1), c.stream);   // + fin
+  SADMRG_CUDA(cudaMemsetAsync(U->deps->get(), 0, U->deps->bytes(), c.stream));
   launch_pack(d_cpack, d_cblk, (int)U->cblk.size(), cb, U->pconst->as<unsigned char>(), c.stream);
   ++c.launches;
   SADMRG_CUDA(cudaGetLastError());
@@ -449,11 +481,12 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   return true;
 }
 
-int GemmPlan::launches_per_run(bool cplx, int prec) const {
+int GemmPlan::launches_per_run(bool cplx, int prec, bool c_fused) const {
   int n = 0;
   if (uses_umma(cplx, prec)) {
     const UmmaSchedule& U = *umma;
-    if (!U.vpack.empty()) ++n;
+    if (c_fused) return 1;   // pack + both stages in one launch
+    int n = U.vblk.empty() ? 0 : 1;
     for (int s = 0; s < nstage; ++s)
       if (U.stage_items[s + 1] > U.stage_items[s]) ++n;
     return n;
@@ -478,19 +511,42 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
   if (stage_hi < 0) stage_hi = nstage;
   if (uses_umma(cplx, prec)) {
     const UmmaSchedule& U = *umma;
-    UBufs ub{U.pconst->as<unsigned char>(), U.pvar->as<unsigned char>(),
-             work_override ? static_cast<float*>(work_override) : U.slots->as<float>(), U.tile_cnt->as<int>()};
-    if (stage_lo == 0 && !U.vpack.empty()) {
-      launch_pack(U.d_vpack, U.d_vblk, (int)U.vblk.size(), b, ub.pvar, c.stream);
+    UBufs ub{};
+    ub.pconst = U.pconst->as<unsigned char>();
+    ub.pvar = U.pvar->as<unsigned char>();
+    ub.slots = work_override ? static_cast<float*>(work_override) : U.slots->as<float>();
+    ub.tile_cnt = U.tile_cnt->as<int>();
+    ub.deps = U.deps->as<int>();
+    ub.dep_target = U.d_dep_target;
+    ub.fin = reinterpret_cast<unsigned*>(U.deps->as<int>() + U.dep_target.size());
+    UPhase ph{};
+    ph.pk = U.d_vpack;
+    ph.pk_blk = U.d_vblk;
+    ph.npk_jobs = (int)U.vpack.size();
+    ph.ndeps = (int)U.dep_target.size();
+    const bool whole = stage_lo == 0 && stage_hi == nstage;
+    if (whole && c.fused_matvec && (int)U.vpack.size() <= kMaxPackJobs) {
+      // the whole matvec in one cooperative launch: psi packing, stage 0, stage 1
+      ph.npk_blocks = (int)U.vblk.size();
+      ph.wait_deps = 1;
+      const int ni = U.stage_items[nstage] - U.stage_items[0];
+      launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items, U.d_reds, ni, b, ub, ph, c.stream);
       ++c.launches;
-      mark(c, 0);
-    }
-    for (int s = stage_lo; s < stage_hi; ++s) {
-      const int ni = U.stage_items[s + 1] - U.stage_items[s];
-      if (ni > 0) {
-        launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items + U.stage_items[s], U.d_reds, ni, b, ub, c.stream);
+      mark(c, 5);
+    } else {
+      if (stage_lo == 0 && !U.vblk.empty()) {
+        launch_pack(U.d_vpack, U.d_vblk, (int)U.vblk.size(), b, ub.pvar, c.stream);
         ++c.launches;
-        mark(c, 1 + 2 * s);
+        mark(c, 0);
+      }
+      for (int s = stage_lo; s < stage_hi; ++s) {
+        const int ni = U.stage_items[s + 1] - U.stage_items[s];
+        if (ni > 0) {
+          launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items + U.stage_items[s], U.d_reds, ni, b, ub, ph,
+                            c.stream);
+          ++c.launches;
+          mark(c, 1 + 2 * s);
+        }
       }
     }
     SADMRG_CUDA(cudaGetLastError());

@@ -30,6 +30,7 @@ struct Ctx {
   double* d_partial = nullptr;
   int npart = 296;
   double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
+  bool fused_matvec = false;     // tcgen05 matvec as one cooperative launch instead of pack + two launches
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
   // when set, GemmPlan::run records an event after every launch (what ran, event)
@@ -94,7 +95,9 @@ struct UmmaSchedule {
   std::vector<UItem> items;
   std::vector<URed> reds;
   std::vector<int> stage_items, stage_reds;
-  std::shared_ptr<DevBuf> dev, pconst, pvar, slots, tile_cnt;
+  std::shared_ptr<DevBuf> dev, pconst, pvar, slots, tile_cnt, deps;
+  std::vector<int> dep_target;             // per dependency counter: its value when the panels are complete
+  int* d_dep_target = nullptr;
   PackJob* d_vpack = nullptr;
   int* d_vblk = nullptr;
   UTerm* d_terms = nullptr;
@@ -136,7 +139,7 @@ struct GemmPlan {
   size_t work_bytes(bool cplx, int prec) const {
     return uses_umma(cplx, prec) ? umma->slot_bytes() : sched.work_bytes();
   }
-  int launches_per_run(bool cplx, int prec) const;
+  int launches_per_run(bool cplx, int prec, bool fused) const;
   bool empty() const { return jobs.empty(); }
 
  private:

@@ -152,10 +152,8 @@ __device__ __forceinline__ void st_global_v4(void* p, uint32_t x, uint32_t y, ui
 // the stores are contiguous and the loads coalesce along rows (trans 0) or read
 // one 32-byte sector per thread (trans 1).  Every job starts on a multiple of
 // 256 chunks, so a block works for one job, looked up in blk_job.
-__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, const int* __restrict__ blk_job,
-                                                   Bases bases, unsigned char* __restrict__ dst) {
-  const PackJob P = jobs[blk_job[blockIdx.x]];
-  const unsigned local = blockIdx.x * 256u + threadIdx.x - (unsigned)P.chunk0;
+__device__ __forceinline__ void pack_chunk(const PackJob& P, unsigned local, const Bases& bases,
+                                           unsigned char* __restrict__ dst) {
   const unsigned T = (unsigned)P.T;
   const unsigned nslab = ((unsigned)P.K + kPanelK - 1) / kPanelK;
   const unsigned Rp = (((unsigned)P.rows + T - 1) / T) * T;
@@ -179,6 +177,22 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ j
   st_global_v4(panel + T * 128u + off, l[0], l[1], l[2], l[3]);
 }
 
+__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, const int* __restrict__ blk_job,
+                                                   Bases bases, unsigned char* __restrict__ dst) {
+  const PackJob P = jobs[blk_job[blockIdx.x]];
+  pack_chunk(P, blockIdx.x * 256u + threadIdx.x - (unsigned)P.chunk0, bases, dst);
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// generic-proxy global writes <-> async-proxy (bulk copy) global reads
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 template <int BN, int ST>
 struct UG {
@@ -194,7 +208,7 @@ struct UG {
 template <int BN, int ST>
 __global__ void __launch_bounds__(kGThreads, 1)
     umma_gemm(const UTerm* __restrict__ terms, const UJob* __restrict__ jobs, const UItem* __restrict__ items,
-              const URed* __restrict__ reds, int nitems, Bases bases, UBufs ub) {
+              const URed* __restrict__ reds, int nitems, Bases bases, UBufs ub, UPhase ph) {
   using G = UG<BN, ST>;
   constexpr int BM = kUmmaTileM;
   extern __shared__ unsigned char usm_raw[];
@@ -203,6 +217,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
   __shared__ volatile int abort_sh;
   __shared__ volatile int last_sh;
   __shared__ volatile int ep_fail;
+  __shared__ int pk_cnt[kMaxPackJobs];
 
   unsigned char* usm =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm_raw) + 127) & ~uintptr_t(127));
@@ -233,18 +248,61 @@ __global__ void __launch_bounds__(kGThreads, 1)
   fence_after();
   const uint32_t tmem = tmem_sh;
 
+  if (ph.npk_blocks > 0) {
+    // psi -> panels for this launch, by every thread: warps take 32-chunk groups
+    // (a group never straddles two jobs, whose chunk ranges are multiples of 256),
+    // count them per job in shared memory, then add each job's count once.
+    for (int j = tid; j < ph.npk_jobs; j += kGThreads) pk_cnt[j] = 0;
+    __syncthreads();
+    const unsigned ngroups = (unsigned)ph.npk_blocks * 8u;
+    for (unsigned gi = blockIdx.x * (kGThreads / 32) + warp; gi < ngroups; gi += gridDim.x * (kGThreads / 32)) {
+      const int job = ph.pk_blk[gi >> 3];
+      const PackJob P = ph.pk[job];
+      pack_chunk(P, gi * 32u + (unsigned)lane - (unsigned)P.chunk0, bases, ub.pvar);
+      if (lane == 0) atomicAdd(&pk_cnt[job], 32);
+    }
+    fence_proxy_async_global();
+    __threadfence();
+    __syncthreads();
+    for (int j = tid; j < ph.npk_jobs; j += kGThreads)
+      if (pk_cnt[j] > 0) atomicAdd(ub.deps + j, pk_cnt[j]);
+  }
+
   if (warp == 0) {
     // ---------------- producer ----------------
     if (lane == 0) {
       long long g = 0;
       uint32_t last_bar = 0, last_par = 0;
       bool issued_any = false;
+      int ready_term = -1;
+      // bounded wait until dependency counter d reaches its target
+      auto dep_wait = [&](int d) -> bool {
+        if (d < 0) return true;
+        const int target = ub.dep_target[d];
+        const unsigned long long t0 = gtime();
+        for (long long i = 0; i < kWaitIters; ++i) {
+          if (ld_acquire(ub.deps + d) >= target) return true;
+          if ((i & 63) == 63 && (abort_sh || gtime() - t0 > kWaitNs)) return false;
+          __nanosleep(64);
+        }
+        return false;
+      };
       for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x) {
         const UItem it = items[ii];
         int t = it.t0, s = it.s0;
         for (int q = 0; q < it.nslab; ++q) {
           while (s >= terms[t].nslab) { ++t; s = 0; }
           const UTerm T = terms[t];
+          if (ph.wait_deps && t != ready_term) {
+            // the panels this term reads are written in this launch: wait for them
+            if (!dep_wait(T.adep) || !dep_wait(T.bdep)) {
+              if (!abort_sh) atomicExch(&g_umma_status, 9);
+              abort_sh = 1;
+              break;
+            }
+            fence_proxy_async_global();
+            ready_term = t;
+          }
           const int st = (int)(g % ST);
           const uint32_t n = (uint32_t)(g / ST);
           if (!mbar_wait(saddr(&empty[st]), (n & 1u) ^ 1u, &abort_sh)) {
@@ -335,6 +393,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const int quarter = warp & 3;           // TMEM lanes 32*quarter .. +31
     const int r = 32 * quarter + lane;      // tile row
     int il = 0;
+    const int et = tid - 64;                // 0..127 within the epilogue warps
     // The four epilogue warps take every decision together: a failed wait is
     // posted to ep_fail and read by all after the same named barrier (id 1).
     for (int ii = blockIdx.x; ii < nitems; ii += gridDim.x, ++il) {
@@ -400,6 +459,15 @@ __global__ void __launch_bounds__(kGThreads, 1)
       }
       fence_before();
       mbar_arrive(saddr(&tempty[acc]));
+      // a finished tile of a result that later items read as panels: count it
+      auto signal_tile = [&]() {
+        if (J.dep < 0 || !ph.wait_deps) return;
+        fence_proxy_async_global();
+        __threadfence();
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (et == 0) atomicAdd(ub.deps + J.dep, 1);
+      };
+      if (it.slot < 0) signal_tile();
       if (it.slot >= 0) {
         // split-K: the last of the tile's items to get here sums every slot in
         // slot order (the same order whichever item is last) and emits the tile
@@ -425,6 +493,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
           if (tid == 64) ub.tile_cnt[it.red] = 0;   // ready for the next launch
         }
         asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (last_sh) signal_tile();
+        asm volatile("bar.sync 1, 128;" ::: "memory");
       }
     }
   }
@@ -436,18 +506,43 @@ __global__ void __launch_bounds__(kGThreads, 1)
     fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(G::TCOLS) : "memory");
   }
+  // the last CTA out clears the dependency counters for the next launch
+  if (tid == 0 && ph.ndeps > 0) {
+    __threadfence();
+    if (atomicAdd(ub.fin, 1u) == gridDim.x - 1) {
+      for (int d = 0; d < ph.ndeps; ++d) ub.deps[d] = 0;
+      *ub.fin = 0u;
+      __threadfence();
+    }
+  }
 }
 
 template <int BN, int ST>
 void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
-                   const Bases& b, const UBufs& u, cudaStream_t s) {
+                   const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(umma_gemm<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG<BN, ST>::SMEM);
     attr = true;
   }
-  const int grid = nitems < device_sm_count() ? nitems : device_sm_count();
-  umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, reds, nitems, b, u);
+  const int nsm = device_sm_count();
+  int grid = nitems > ph.npk_blocks ? nitems : ph.npk_blocks;
+  if (grid > nsm) grid = nsm;
+  if (grid < 1) grid = 1;
+  // CTAs wait on one another only when wait_deps is set: then every CTA must be
+  // resident at once, which a cooperative launch guarantees
+  if (ph.wait_deps) {
+    Bases bb = b;
+    UBufs uu = u;
+    UPhase pp = ph;
+    int ni = nitems;
+    void* args[] = {(void*)&terms, (void*)&jobs, (void*)&items, (void*)&reds, (void*)&ni, (void*)&bb, (void*)&uu,
+                    (void*)&pp};
+    cudaLaunchCooperativeKernel((const void*)umma_gemm<BN, ST>, dim3(grid), dim3(kGThreads), args,
+                                UG<BN, ST>::SMEM, s);
+  } else {
+    umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, reds, nitems, b, u, ph);
+  }
 }
 
 }  // namespace
@@ -472,10 +567,10 @@ void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bas
 }
 
 void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
-                       const Bases& b, const UBufs& u, cudaStream_t s) {
-  if (nitems <= 0) return;
-  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, reds, nitems, b, u, s);
-  else launch_gemm_t<64, 4>(terms, jobs, items, reds, nitems, b, u, s);
+                       const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
+  if (nitems <= 0 && ph.npk_blocks <= 0) return;
+  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, reds, nitems, b, u, ph, s);
+  else launch_gemm_t<64, 4>(terms, jobs, items, reds, nitems, b, u, ph, s);
 }
 
 int umma_status(bool reset) {

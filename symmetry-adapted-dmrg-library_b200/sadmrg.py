@@ -31,7 +31,7 @@ EXPORTED = [
     "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
-    "sadmrg_device_status", "sadmrg_heff_launch_profile",
+    "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
 ]
 
 
@@ -66,6 +66,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_device_status": ([vp, ip], C.c_int),
         "sadmrg_heff_plan": ([vp, td, td, td, C.c_int, td, C.c_int, ip, ip], C.c_int),
         "sadmrg_set_lanczos_tol": ([vp, C.c_double], C.c_int),
+        "sadmrg_set_matvec_fusion": ([vp, C.c_int], C.c_int),
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
@@ -73,6 +74,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
         "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
         "sadmrg_heff_launch_profile": ([vp, C.c_int, C.c_int, vp, vp, C.c_int, ip, ip, dp], C.c_int),
+        "sadmrg_heff_graph_bench": ([vp, C.c_int, C.c_int, vp, vp, dp], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -185,6 +187,10 @@ class Handle:
             msg = self.lib.sadmrg_last_error(self.h)
             raise SadmrgError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
 
+    def set_matvec_fusion(self, fused: bool):
+        """True: the split-precision matvec as one cooperative launch."""
+        self._check(self.lib.sadmrg_set_matvec_fusion(self.h, int(bool(fused))), "set_matvec_fusion")
+
     def set_lanczos_tol(self, ov_tol: float):
         self._check(self.lib.sadmrg_set_lanczos_tol(self.h, float(ov_tol)), "set_lanczos_tol")
 
@@ -246,7 +252,8 @@ class Handle:
 
     def heff_launch_profile(self, precision: int = PREC_FP64, reps: int = 10, psi_ptr: int = 0, out_ptr: int = 0):
         """[(kind, mean ms)] for every kernel one matvec launches; kind 0: psi -> TF32 panels,
-        1 + 2*stage: grouped GEMM of that stage, 2 + 2*stage: its split-K reduction."""
+        1 + 2*stage: grouped GEMM of that stage, 2 + 2*stage: its split-K reduction,
+        5: the whole matvec in one launch."""
         cap = 64
         n = C.c_int(0)
         kinds = np.zeros(cap, dtype=np.int32)
@@ -257,6 +264,13 @@ class Handle:
                                                         ms.ctypes.data_as(C.POINTER(C.c_double))),
                     "heff_launch_profile")
         return [(int(kinds[i]), float(ms[i])) for i in range(min(n.value, cap))]
+
+    def heff_graph_bench(self, precision: int = PREC_FP64, reps: int = 200, psi_ptr: int = 0, out_ptr: int = 0) -> float:
+        """Mean device ms of one matvec replayed `reps` times from a captured CUDA graph."""
+        ms = C.c_double()
+        self._check(self.lib.sadmrg_heff_graph_bench(self.h, int(precision), int(reps), C.c_void_p(psi_ptr),
+                                                     C.c_void_p(out_ptr), C.byref(ms)), "heff_graph_bench")
+        return ms.value
 
     def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         x = np.array(psi, dtype=self.dtype, copy=True)
@@ -386,6 +400,32 @@ def read_exported_tensor(directory: str, name: str, cplx: bool) -> Optional[Bloc
                 blocks.append(int(t[1]))
     data = np.fromfile(os.path.join(directory, name + ".bin"), dtype=np.complex128 if cplx else np.float64)
     return BlockTensorData(dirs, qs, ds, ls, np.array(blocks, np.int64), data)
+
+
+def write_exported_tensor(directory: str, name: str, t: BlockTensorData) -> None:
+    """Write t in the format of sadmrg_chain_freeze's export (<name>.txt + <name>.bin),
+    which read_exported_tensor and the reference harness's load mode read back."""
+    nb = t.nbond
+    sizes = []
+    lines = [f"nbond {nb} locspin {t.locspin} nten {int(np.prod([len(q) for q in t.qs]))}"]
+    for b in range(nb):
+        lines.append(f"bond {b} dir {t.dirs[b]} nmom {len(t.qs[b])} q " + " ".join(str(x) for x in t.qs[b]) +
+                     " d " + " ".join(str(x) for x in t.ds[b]))
+    off = 0
+    for bi in t.blocks:
+        lab = t.block_labels(int(bi))
+        q = [t.qs[b][lab[b]] for b in range(nb)]
+        d = [t.ds[b][lab[b]] for b in range(nb)]
+        n = int(np.prod(d))
+        lines.append(f"block {int(bi)} q " + " ".join(map(str, q)) + " d " + " ".join(map(str, d)) +
+                     f" off {off} n {n}")
+        off += n
+        sizes.append(n)
+    if off != t.data.size:
+        raise ValueError(f"{name}: blocks hold {off} elements, data has {t.data.size}")
+    with open(os.path.join(directory, name + ".txt"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    np.ascontiguousarray(t.data).tofile(os.path.join(directory, name + ".bin"))
 
 
 def load_exported_problem(h: "Handle", directory: str) -> BlockTensorData:

@@ -56,3 +56,17 @@ def test_umma_lanczos_energy():
     e32, _, _ = h.heff_lanczos(psi.data.copy(), 100, sadmrg.PREC_TF32X3)
     assert abs(e32 - e64) <= 1e-10 * abs(e64), (e32, e64)
     assert h.device_status() == 0
+
+
+def test_umma_fused_launch_matches():
+    """The whole matvec as one cooperative launch gives the same bits as pack + two launches."""
+    import sadmrg
+    for sym, L, D in ((1, 40, 192), (0, 32, 160)):
+        h, psi = _centre(sym, L, D)
+        a = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
+        h.set_matvec_fusion(True)
+        b = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
+        c = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
+        h.set_matvec_fusion(False)
+        assert np.array_equal(a, b) and np.array_equal(b, c)
+        assert h.device_status() == 0
