@@ -128,6 +128,7 @@ int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out) {
     SADMRG_CUDA(cudaStreamCreateWithFlags(&h->ctx.stream, cudaStreamNonBlocking));
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_scalars, 64 * sizeof(double)));
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_partial, sizeof(double) * 2 * 512 * (size_t)h->ctx.npart));
+    SADMRG_CUDA(cudaMallocHost(&h->ctx.h_pinned, sizeof(double) * Ctx::kPinnedDoubles));
     if (h->ctx.sym == Sym::SU2) h->ctx.cgc = std::make_unique<CGCFactors>(1);
   });
   if (rc != SADMRG_OK) {
@@ -570,10 +571,10 @@ int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     const Timers& t = S_.chain->timers;
-    const double v[10] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
+    const double v[12] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
                           (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded,
-                          (double)S_.chain->near_ties};
-    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
+                          (double)S_.chain->near_ties, t.svd_kernel, (double)t.svd_sweeps};
+    for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
   });
 }
 

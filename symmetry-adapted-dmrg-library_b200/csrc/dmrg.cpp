@@ -307,7 +307,16 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
     const double nor = std::sqrt(std::fabs(real_of(K.dot_host(K.F(0), K.F(0)))));
     if (nor > 1e-12) K.scale_host(K.F(0), 1.0 / nor);
   }
-  // one Lanczos step: F(m) = H F(m-1) - a F(m-1) - b F(m-2), reorthogonalised, normalised
+  // one Lanczos step: F(m) = H F(m-1) - a F(m-1) - b F(m-2), reorthogonalised, normalised.
+  // a and b go to page-locked host memory without a synchronisation; the host reads
+  // them at the next check point (every 4 steps, as the reference checks), so the
+  // steps in between queue back to back on the stream.
+  const int pin_stride = kCx<S> ? 2 : 1;
+  SADMRG_REQUIRE((mlanc + 2) * (pin_stride + 1) <= Ctx::kPinnedDoubles, SADMRG_ERR_LIMIT,
+                 "lanczos: mlanc too large for the pinned scalar buffer");
+  double* pin_a = c.h_pinned;                             // Re(a_m) at pin_a[(m-1)*stride]
+  double* pin_b = c.h_pinned + (mlanc + 2) * pin_stride;  // b_m
+  int synced = 0;                                          // steps whose a, b are on the host
   auto step = [&](int m, bool reorth) {
     matvec(K.F(m - 1), K.F(m));
     K.mdot(K.F(m - 1), 1, K.F(m), K.dots.get());
@@ -327,18 +336,30 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
     launch_lanczos_scalar(kCx<S>, 1, K.dots.get(), nullptr, K.beta.template as<double>() + m, c.stream);
     launch_scale_inv(kCx<S>, K.F(m), K.beta.template as<double>() + m, n, c.stream);
     c.launches += 2;
-    S co[2];
-    double bm;
-    SADMRG_CUDA(cudaMemcpyAsync(co, K.coef.get(), sizeof(S) * 2, cudaMemcpyDeviceToHost, c.stream));
-    SADMRG_CUDA(cudaMemcpyAsync(&bm, K.beta.template as<double>() + m, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    aal[m - 1] = real_of(co[1]);
-    nnl[m] = bm;
+    SADMRG_CUDA(cudaMemcpyAsync(pin_a + (m - 1) * pin_stride, K.coef.template as<S>() + 1, sizeof(S),
+                                cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaMemcpyAsync(pin_b + m, K.beta.template as<double>() + m, sizeof(double), cudaMemcpyDeviceToHost,
+                                c.stream));
     st.iters = m;
+  };
+  // bring a, b of steps (synced, m] to the host; returns the first step in that
+  // range whose b broke down (< tol), or 0.  Like the reference, the test starts
+  // at step 2 (step 1's b is never tested, src/dmrg_inst.cpp:1296-1326).
+  auto sync_to = [&](int m) -> int {
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    int brk = 0;
+    for (int j = synced + 1; j <= m; ++j) {
+      aal[j - 1] = pin_a[(j - 1) * pin_stride];
+      nnl[j] = pin_b[j];
+      if (!brk && j >= 2 && nnl[j] < tol) brk = j;
+    }
+    synced = m;
+    return brk;
   };
   double ee = 0.0, ov = 0.0;
   step(1, false);
   if (mlanc == 2) {
+    sync_to(1);
     if (nnl[1] < tol) {
       diatridiag(1);
       ritz_vec(1);
@@ -353,21 +374,31 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
     st.energy = eig[0];
     return st;
   }
+  // The reference tests b < tol after every step and checks the eigenvector every
+  // 4 steps (src/dmrg_inst.cpp:1313-1345); here both are evaluated at the check
+  // points, and a breakdown found there is handled as if it had been seen at its
+  // own step: the tridiagonal and the Ritz vector use the steps before it only,
+  // and the steps queued after it are discarded.
   for (int m = 2; m < mlanc; ++m) {
     step(m, true);
-    diatridiag(m);
-    if (nnl[m] < tol) {
-      ritz_vec(m);
+    if (m % 4 != 0 && m != mlanc - 1) continue;
+    const int brk = sync_to(m);
+    if (brk) {
+      st.iters = brk;
+      diatridiag(brk);
+      ritz_vec(brk);
       check(ee, ov);
       st.energy = eig[0];
       return st;
     }
+    diatridiag(m);
     if (m % 4 == 0) {
       ritz_vec(m);
       check(ee, ov);
       if (std::fabs(ov - 1.0) < c.lanczos_ov_tol) { st.energy = eig[0]; return st; }
     }
   }
+  sync_to(mlanc - 1);
   matvec(K.F(mlanc - 1), K.F(mlanc));
   aal[mlanc - 1] = real_of(K.dot_host(K.F(mlanc - 1), K.F(mlanc)));
   diatridiag(mlanc);
@@ -867,6 +898,8 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &ww);
   last_discarded = s.discarded_weight;
   if (s.near_tie) ++near_ties;
+  if (s.jacobi_kernel_ms > 0) timers.svd_kernel += s.jacobi_kernel_ms * 1e-3;
+  timers.svd_sweeps += s.sweeps_max > 0 ? s.sweeps_max : 0;
   if (std::getenv("SADMRG_VERBOSE")) {
     std::fprintf(stderr, "svd (%d,%d) kept=%d dw=%.3e sweeps=%d jacobi=%.2fms kernel=%.2fms max=%dx%d total=%.2fms sectors:",
                  il, ir, s.kept, s.discarded_weight, s.sweeps_max, s.jacobi_s * 1e3, s.jacobi_kernel_ms, s.max_rows,

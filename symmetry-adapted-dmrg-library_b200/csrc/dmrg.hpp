@@ -72,9 +72,11 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
                    int max_dcut, std::vector<double>* wout);
 
 struct Timers {
-  double lanczos = 0, env = 0, svd = 0, prep = 0;
+  double lanczos = 0, env = 0, svd = 0, prep = 0;   // host wall time of each phase
   long long matvecs = 0;
   double heff_flops = 0;
+  double svd_kernel = 0;        // device time of the Jacobi sweep kernels (s)
+  long long svd_sweeps = 0;     // Jacobi sweeps, summed over the truncations
 };
 
 template <class S>

@@ -5,8 +5,9 @@
 // contiguous range of the job's concatenated reduction dimension (the k of all
 // its terms laid end to end), so a matvec with a few large output blocks still
 // fills all 148 SMs.  An item that covers the whole range writes C directly;
-// otherwise it writes its partial tile to a workspace slot and a reduction
-// launch sums the slots in a fixed order -- results are bitwise reproducible.
+// otherwise it writes its partial tile to a workspace slot, and the last item of
+// the tile to finish sums the slots in a fixed order -- results are bitwise
+// reproducible and there is no separate reduction launch.
 //
 // Inner loop: operand slabs (BM x BK and BK x BN) are prefetched into registers
 // while the tensor cores work on the slab already in shared memory (two shared
@@ -121,88 +122,48 @@ struct Slab {
 };
 
 // ---------------------------------------------------------------------------
-// FP64, real
-template <int BM, int BN, int BK>
-__global__ void __launch_bounds__(kThreads) items_f64(const GemmTerm* __restrict__ terms, const GemmJob* __restrict__ jobs,
-                                                      const WorkItem* __restrict__ items, Bases bases,
-                                                      double* __restrict__ work) {
-  constexpr int PAD = 4;
-  __shared__ double As[2][BK][BM + PAD];
-  __shared__ double Bs[2][BK][BN + PAD];
-  using SL = Slab<double, BM, BN, BK>;
-  const WorkItem it = items[blockIdx.x];
-  const GemmJob J = jobs[it.job];
-  const int row0 = it.tm * BM, col0 = it.tn * BN;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  constexpr int WM = BM / 2, WN = BN / 2, MT = WM / 8, NT = WN / 8;
-  double acc[MT][NT][2];
-#pragma unroll
-  for (int i = 0; i < MT; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  SlabWalk w{J.t0 + it.t0, it.k0, it.kcount};
-  SL s;
-  int tt, kk, kt;
-  auto store = [&](int buf, const GemmTerm& T) {
-    const bool ta = T.flags & TF_TA, tb = T.flags & TF_TB;
-#pragma unroll
-    for (int q = 0; q < SL::EA; ++q) { int i, k; SL::a_pos(ta, q, i, k); As[buf][k][i] = s.a[q] * T.ar; }
-#pragma unroll
-    for (int q = 0; q < SL::EB; ++q) { int j, k; SL::b_pos(tb, q, j, k); Bs[buf][k][j] = s.b[q]; }
-  };
-  int buf = 0;
-  bool have = w.next(terms, BK, tt, kk, kt);
-  if (have) {
-    const GemmTerm T = terms[tt];
-    s.load(T, J, row0, col0, kk, kt, bases);
-    store(0, T);
-  }
+// Split-K fixup, run by every thread of an item that wrote a partial tile: the
+// last item of the tile to finish (per-tile atomic count) sums all its partial
+// tiles in slot order -- the same order whichever item is last -- adds C when
+// the job accumulates, writes C and clears the count for the next launch.
+template <bool CPLX>
+__device__ void split_fixup(const WorkItem& it, const GemmJob& J, const RedItem* __restrict__ reds,
+                            const Bases& bases, const void* work, int* tile_cnt, int BM, int BN) {
+  __shared__ int last;
+  __threadfence();
   __syncthreads();
-  while (have) {
-    int t2, k2, kt2;
-    const bool more = w.next(terms, BK, t2, k2, kt2);
-    GemmTerm T2;
-    if (more) { T2 = terms[t2]; s.load(T2, J, row0, col0, k2, kt2, bases); }
-#pragma unroll
-    for (int k4 = 0; k4 < BK; k4 += 4) {
-      double af[MT], bf[NT];
-#pragma unroll
-      for (int mi = 0; mi < MT; ++mi) af[mi] = As[buf][k4 + (lane & 3)][wm * WM + mi * 8 + (lane >> 2)];
-#pragma unroll
-      for (int ni = 0; ni < NT; ++ni) bf[ni] = Bs[buf][k4 + (lane & 3)][wn * WN + ni * 8 + (lane >> 2)];
-#pragma unroll
-      for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
-    }
-    if (more) store(buf ^ 1, T2);
-    __syncthreads();
-    buf ^= 1;
-    have = more;
-  }
-  const bool direct = it.slot < 0;
-  double* C = direct ? static_cast<double*>(bases.p[J.cbuf]) + J.coff : work + (long long)it.slot * BM * BN;
+  if (threadIdx.x == 0) last = atomicAdd(&tile_cnt[it.red], 1) == reds[it.red].nslot - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const RedItem R = reds[it.red];
+  const int row0 = R.tm * BM, col0 = R.tn * BN;
   const bool accum = J.flags & JF_ACCUM;
-#pragma unroll
-  for (int mi = 0; mi < MT; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < NT; ++ni)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = wm * WM + mi * 8 + (lane >> 2);
-        const int c = wn * WN + ni * 8 + 2 * (lane & 3) + e;
-        if (direct) {
-          if (row0 + r < J.m && col0 + c < J.n) {
-            const long long idx = (row0 + r) + (long long)(col0 + c) * J.ldc;
-            C[idx] = accum ? C[idx] + acc[mi][ni][e] : acc[mi][ni][e];
-          }
-        } else {
-          C[r + c * BM] = acc[mi][ni][e];
-        }
+  for (int e = threadIdx.x; e < BM * BN; e += blockDim.x) {
+    const int r = e % BM, c = e / BM;
+    if (row0 + r >= J.m || col0 + c >= J.n) continue;
+    const long long idx = (row0 + r) + (long long)(col0 + c) * J.ldc;
+    if (CPLX) {
+      const double2* W = static_cast<const double2*>(work);
+      double2 sum = make_double2(0.0, 0.0);
+      for (int k = 0; k < R.nslot; ++k) {
+        const double2 v = __ldcg(W + (long long)(R.slot0 + k) * BM * BN + e);
+        sum.x += v.x;
+        sum.y += v.y;
       }
+      double2* C = static_cast<double2*>(bases.p[J.cbuf]) + J.coff;
+      if (accum) { const double2 o = C[idx]; sum.x += o.x; sum.y += o.y; }
+      C[idx] = sum;
+    } else {
+      const double* W = static_cast<const double*>(work);
+      double sum = 0.0;
+      for (int k = 0; k < R.nslot; ++k) sum += __ldcg(W + (long long)(R.slot0 + k) * BM * BN + e);
+      double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
+      C[idx] = accum ? C[idx] + sum : sum;
+    }
+  }
+  if (threadIdx.x == 0) tile_cnt[it.red] = 0;
 }
-
 
 // ---------------------------------------------------------------------------
 // FP64, real, multistage: slabs are copied global -> shared with cp.async (8-byte,
@@ -224,7 +185,8 @@ template <int BM, int BN, int BK, int STAGES>
 __global__ void __launch_bounds__(kThreads, 3) items_f64_ms(const GemmTerm* __restrict__ terms,
                                                             const GemmJob* __restrict__ jobs,
                                                             const WorkItem* __restrict__ items, Bases bases,
-                                                            double* __restrict__ work) {
+                                                            double* __restrict__ work,
+                                                            const RedItem* __restrict__ reds, int* tile_cnt) {
   static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
   constexpr int SK = BM + 4;        // k-major row stride (rows of m or n)
   constexpr int SM = BK + 4;        // m/n-major row stride (rows of k)
@@ -339,6 +301,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_f64_ms(const GemmTerm* __re
           C[r + c * BM] = acc[mi][ni][e];
         }
       }
+  if (it.slot >= 0) split_fixup<false>(it, J, reds, bases, work, tile_cnt, BM, BN);
 }
 constexpr int kF64Stages = 3;
 constexpr size_t kF64MsSmem = (size_t)kF64Stages * 2 * (64 * 20) * sizeof(double);
@@ -350,7 +313,8 @@ template <int BM, int BN, int BK, int STAGES>
 __global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* __restrict__ terms,
                                                                const GemmJob* __restrict__ jobs,
                                                                const WorkItem* __restrict__ items, Bases bases,
-                                                               double* __restrict__ work) {
+                                                               double* __restrict__ work,
+                                                               const RedItem* __restrict__ reds, int* tile_cnt) {
   static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
   constexpr int SK = BM + 4, SM = BK + 4;
   constexpr int ABUF = (BM * SM > BK * SK) ? BM * SM : BK * SK;
@@ -489,6 +453,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* _
           C[r + c * BM] = accd[mi][ni][e];
         }
       }
+  if (it.slot >= 0) split_fixup<false>(it, J, reds, bases, work, tile_cnt, BM, BN);
 }
 
 // ---------------------------------------------------------------------------
@@ -496,7 +461,8 @@ __global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* _
 template <int BM, int BN, int BK>
 __global__ void __launch_bounds__(kThreads) items_z64(const GemmTerm* __restrict__ terms, const GemmJob* __restrict__ jobs,
                                                       const WorkItem* __restrict__ items, Bases bases,
-                                                      double2* __restrict__ work) {
+                                                      double2* __restrict__ work, const RedItem* __restrict__ reds,
+                                                      int* tile_cnt) {
   constexpr int PAD = 4;
   __shared__ double Ar[2][BK][BM + PAD], Ai[2][BK][BM + PAD];
   __shared__ double Br[2][BK][BN + PAD], Bi[2][BK][BN + PAD];
@@ -599,6 +565,7 @@ __global__ void __launch_bounds__(kThreads) items_z64(const GemmTerm* __restrict
           C[r + c * BM] = v;
         }
       }
+  if (it.slot >= 0) split_fixup<true>(it, J, reds, bases, work, tile_cnt, BM, BN);
 }
 
 // ---------------------------------------------------------------------------
@@ -607,7 +574,8 @@ template <bool CPLX, int BM, int BN, int BK>
 __global__ void __launch_bounds__(kThreads) items_tf32x3(const GemmTerm* __restrict__ terms,
                                                          const GemmJob* __restrict__ jobs,
                                                          const WorkItem* __restrict__ items, Bases bases,
-                                                         void* __restrict__ work) {
+                                                         void* __restrict__ work, const RedItem* __restrict__ reds,
+                                                         int* tile_cnt) {
   constexpr int PAD = 8;
   constexpr int NP = CPLX ? 2 : 1;
   using V = typename std::conditional<CPLX, double2, double>::type;
@@ -775,51 +743,18 @@ __global__ void __launch_bounds__(kThreads) items_tf32x3(const GemmTerm* __restr
           }
         }
       }
-}
-
-// ---------------------------------------------------------------------------
-// deterministic reduction of split-K partial tiles (fixed slot order)
-template <bool CPLX>
-__global__ void reduce_slots(const GemmJob* __restrict__ jobs, const RedItem* __restrict__ red, Bases bases,
-                             const void* __restrict__ work, int BM, int BN) {
-  const RedItem R = red[blockIdx.x];
-  const GemmJob J = jobs[R.job];
-  const int row0 = R.tm * BM, col0 = R.tn * BN;
-  const bool accum = J.flags & JF_ACCUM;
-  for (int e = threadIdx.x; e < BM * BN; e += blockDim.x) {
-    const int r = e % BM, c = e / BM;
-    if (row0 + r >= J.m || col0 + c >= J.n) continue;
-    const long long idx = (row0 + r) + (long long)(col0 + c) * J.ldc;
-    if (CPLX) {
-      const double2* W = static_cast<const double2*>(work);
-      double2 s = make_double2(0.0, 0.0);
-      for (int k = 0; k < R.nslot; ++k) {
-        const double2 v = W[(long long)(R.slot0 + k) * BM * BN + e];
-        s.x += v.x;
-        s.y += v.y;
-      }
-      double2* C = static_cast<double2*>(bases.p[J.cbuf]) + J.coff;
-      if (accum) { const double2 o = C[idx]; s.x += o.x; s.y += o.y; }
-      C[idx] = s;
-    } else {
-      const double* W = static_cast<const double*>(work);
-      double s = 0.0;
-      for (int k = 0; k < R.nslot; ++k) s += W[(long long)(R.slot0 + k) * BM * BN + e];
-      double* C = static_cast<double*>(bases.p[J.cbuf]) + J.coff;
-      C[idx] = accum ? C[idx] + s : s;
-    }
-  }
+  if (it.slot >= 0) split_fixup<CPLX>(it, J, reds, bases, work, tile_cnt, BM, BN);
 }
 
 int gemm_tile_m(bool cplx, int /*prec*/) { return cplx ? 32 : 64; }
 int gemm_tile_n(bool cplx, int /*prec*/) { return cplx ? 32 : 64; }
 
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
-                  const Bases& b, void* work, cudaStream_t s) {
+                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, cudaStream_t s) {
   if (nitems <= 0) return;
   if (prec == PREC_TF32X3) {
     if (cplx) {
-      items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work);
+      items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work, reds, tile_cnt);
     } else {
       static bool attr = false;
       if (!attr) {
@@ -828,11 +763,13 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
         attr = true;
       }
       items_tf32x3_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
-                                                                                 static_cast<double*>(work));
+                                                                                 static_cast<double*>(work), reds,
+                                                                                 tile_cnt);
     }
   } else {
     if (cplx) {
-      items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work));
+      items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work), reds,
+                                                          tile_cnt);
     } else {
       static bool attr = false;
       if (!attr) {
@@ -841,7 +778,8 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
         attr = true;
       }
       items_f64_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
-                                                                              static_cast<double*>(work));
+                                                                              static_cast<double*>(work), reds,
+                                                                              tile_cnt);
     }
   }
 }
@@ -871,11 +809,5 @@ int noalloc_scratch(void** ptr) {
   return 0;
 }
 
-void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
-                   int BM, int BN, cudaStream_t s) {
-  if (nred <= 0) return;
-  if (cplx) reduce_slots<true><<<nred, 256, 0, s>>>(jobs, red, b, work, BM, BN);
-  else reduce_slots<false><<<nred, 256, 0, s>>>(jobs, red, b, work, BM, BN);
-}
 
 }  // namespace sadmrg

@@ -35,6 +35,7 @@ struct WorkItem {             // one output tile x a contiguous range of the job
   int job, tm, tn;
   int t0, k0, kcount;         // first term (relative to the job's t0), offset in it, total k
   int slot;                   // < 0: write C directly; otherwise the partial-tile slot
+  int red;                    // split items: their tile's RedItem
 };
 struct RedItem {              // C tile = sum of slots [slot0, slot0 + nslot) (fixed order)
   int job, tm, tn, slot0, nslot;
@@ -49,8 +50,10 @@ struct Bases {
 enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
 
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).
+// Split items write partial tiles; the last of a tile's items sums them (tile_cnt
+// holds one zeroed counter per RedItem and is left zeroed).
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
-                  const Bases& b, void* work, cudaStream_t s);
+                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, cudaStream_t s);
 
 // ---- tcgen05 3xTF32 over TF32 hi/lo operand panels (umma.cu) --------------
 // An operand (rows x K after op) is stored as panels: panel (p, s) holds rows
@@ -118,8 +121,6 @@ void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem
 // (the tiles it guarded were not written); reset clears it.  -1 if unreadable.
 int umma_status(bool reset);
 int device_sm_count();
-void launch_reduce(bool cplx, const GemmJob* jobs, const RedItem* red, int nred, const Bases& b, const void* work,
-                   int bm, int bn, cudaStream_t s);
 // Fixed device scratch of the allocation-free H_eff*psi entry point (gemm.cu).
 constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 // Device address of that scratch on the current device (looked up once per

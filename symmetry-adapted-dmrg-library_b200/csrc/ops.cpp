@@ -12,6 +12,7 @@ namespace sadmrg {
 Ctx::~Ctx() {
   if (d_scalars) cudaFree(d_scalars);
   if (d_partial) cudaFree(d_partial);
+  if (h_pinned) cudaFreeHost(h_pinned);
 }
 
 // ---------------------------------------------------------------------------
@@ -120,15 +121,15 @@ void GemmPlan::build_schedule(GemmSchedule& sc, bool cplx) {
       for (int a = 0; a < tm; ++a)
         for (int b = 0; b < tn; ++b) {
           if (nch == 1) {
-            its.push_back({kt, WorkItem{(int)j, a, b, 0, 0, (int)kt, -1}});
+            its.push_back({kt, WorkItem{(int)j, a, b, 0, 0, (int)kt, -1, -1}});
             continue;
           }
-          const int slot0 = nslot;
+          const int slot0 = nslot, red = (int)sc.reds.size();
           long long pos = 0;
           int t = 0, k = 0;
           for (long long ch = 0; ch < nch; ++ch) {
             const long long len = std::min(kc, kt - pos);
-            its.push_back({len, WorkItem{(int)j, a, b, t, k, (int)len, nslot++}});
+            its.push_back({len, WorkItem{(int)j, a, b, t, k, (int)len, nslot++, red}});
             // advance (t, k) by len along the concatenated k
             long long left = len;
             while (left > 0) {
@@ -191,6 +192,8 @@ void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed, const Bases* const_bases)
   sched.d_reds = reinterpret_cast<RedItem*>(base + al(bt) + al(bj) + al(bi));
   sched.work = std::make_shared<DevBuf>((size_t)std::max(sched.nslot, 1) * sched.bm * sched.bn * (cplx ? 16 : 8),
                                         c.stream);
+  sched.tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(sched.reds.size(), 1), c.stream);
+  SADMRG_CUDA(cudaMemsetAsync(sched.tile_cnt->get(), 0, sched.tile_cnt->bytes(), c.stream));
   umma.reset();
   if (mixed && !cplx && const_bases) build_umma(c, *const_bases);
   // the host copies must stay alive until the async copies complete
@@ -491,10 +494,8 @@ int GemmPlan::launches_per_run(bool cplx, int prec, bool c_fused) const {
       if (U.stage_items[s + 1] > U.stage_items[s]) ++n;
     return n;
   }
-  for (int s = 0; s < nstage; ++s) {
+  for (int s = 0; s < nstage; ++s)
     if (sched.stage_items[s + 1] > sched.stage_items[s]) ++n;
-    if (sched.stage_reds[s + 1] > sched.stage_reds[s]) ++n;
-  }
   return n;
 }
 
@@ -557,15 +558,10 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
   for (int s = stage_lo; s < stage_hi; ++s) {
     const int ni = sched.stage_items[s + 1] - sched.stage_items[s];
     if (ni > 0) {
-      launch_items(cplx, prec, d_terms, d_jobs, sched.d_items + sched.stage_items[s], ni, b, wk, c.stream);
+      launch_items(cplx, prec, d_terms, d_jobs, sched.d_items + sched.stage_items[s], ni, b, wk, sched.d_reds,
+                   sched.tile_cnt->as<int>(), c.stream);
       ++c.launches;
       mark(c, 1 + 2 * s);
-    }
-    const int nr = sched.stage_reds[s + 1] - sched.stage_reds[s];
-    if (nr > 0) {
-      launch_reduce(cplx, d_jobs, sched.d_reds + sched.stage_reds[s], nr, b, wk, sched.bm, sched.bn, c.stream);
-      ++c.launches;
-      mark(c, 2 + 2 * s);
     }
   }
   SADMRG_CUDA(cudaGetLastError());

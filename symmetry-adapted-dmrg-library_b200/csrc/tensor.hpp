@@ -28,6 +28,8 @@ struct Ctx {
   std::unique_ptr<CGCFactors> cgc;
   double* d_scalars = nullptr;   // small device scratch for reductions
   double* d_partial = nullptr;
+  double* h_pinned = nullptr;    // page-locked host scratch (kPinnedDoubles) for async scalar reads
+  static constexpr int kPinnedDoubles = 4096;
   int npart = 296;
   double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
   bool fused_matvec = false;     // tcgen05 matvec as one cooperative launch instead of pack + two launches
@@ -77,6 +79,7 @@ struct GemmSchedule {
   WorkItem* d_items = nullptr;
   RedItem* d_reds = nullptr;
   std::shared_ptr<DevBuf> work;   // split-K partial tiles
+  std::shared_ptr<DevBuf> tile_cnt;   // per RedItem: items finished in the current launch
   int nslot = 0;
   size_t work_bytes() const { return work ? work->bytes() : 0; }
 };
