@@ -97,6 +97,14 @@ int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused);
 int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadmrg_tensor_desc* hh_left,
                      const sadmrg_tensor_desc* hh_right, int nops, const sadmrg_tensor_desc* ops, int nterms,
                      const int* op1, const int* op2);
+/* Excited-state penalty of the reference's H_eff (src/dmrg_inst.cpp:352-363):
+ * after this call every H_eff*psi (apply, apply_device, apply_noalloc, lanczos)
+ * also subtracts sum_k weights[k] <o_k|psi> o_k, with o_k the nvec vectors in
+ * vecs_host (psi's layout, one after another; the lower states projected on this
+ * two-site basis) and weights[k] their energies (the reference's gs_enr[k]).
+ * nvec = 0 removes the penalty.  The per-stage and per-launch profiles and the
+ * graph replay time the sector products only. */
+int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, const double* weights);
 /* psi elements, algorithmic flops and bytes of one matvec, number of sector products */
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks);
 /* out = H_eff psi with host buffers (copies in and out on the handle's stream) */

@@ -197,6 +197,35 @@ int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused) {
   });
 }
 
+int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, const double* weights) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_set_penalty: no plan");
+    SADMRG_REQUIRE(nvec >= 0 && nvec <= 512, SADMRG_ERR_ARG, "heff_set_penalty: 0 <= nvec <= 512");
+    SADMRG_REQUIRE(nvec == 0 || (vecs_host && weights), SADMRG_ERR_ARG, "heff_set_penalty: null vectors or weights");
+    HeffPlan<S>& H = *S_.heff;
+    H.npen = 0;
+    H.pen_o.reset();
+    H.pen_wo.reset();
+    H.pen_dot.reset();
+    if (nvec == 0) return;
+    const size_t bytes = sizeof(S) * (size_t)H.n * nvec;
+    H.pen_o = std::make_shared<DevBuf>(bytes, c.stream);
+    H.pen_wo = std::make_shared<DevBuf>(bytes, c.stream);
+    H.pen_dot = std::make_shared<DevBuf>(sizeof(S) * (nvec + 1), c.stream);
+    std::vector<S> wo((size_t)H.n * nvec);
+    const S* o = static_cast<const S*>(vecs_host);
+    for (int k = 0; k < nvec; ++k)
+      for (long long i = 0; i < H.n; ++i) wo[(size_t)k * H.n + i] = o[(size_t)k * H.n + i] * weights[k];
+    SADMRG_CUDA(cudaMemcpyAsync(H.pen_o->get(), vecs_host, bytes, cudaMemcpyHostToDevice, c.stream));
+    SADMRG_CUDA(cudaMemcpyAsync(H.pen_wo->get(), wo.data(), bytes, cudaMemcpyHostToDevice, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    H.npen = nvec;
+  });
+}
+
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
@@ -266,6 +295,7 @@ int sadmrg_heff_apply_noalloc(sadmrg_handle* h, const void* psi_dev, void* out_d
     b.p[2] = H.opsbuf->get();
     b.p[3] = scratch;
     H.plan.run(h->ctx, ScalarInfo<S>::cplx, precision, b, 0, -1, static_cast<unsigned char*>(scratch) + xbytes);
+    H.penalty(h->ctx, static_cast<const S*>(psi_dev), static_cast<S*>(out_dev));
   });
 }
 

@@ -158,6 +158,15 @@ void HeffPlan<S>::apply(Ctx& c, const S* psi, S* out, int prec) const {
   b.p[2] = opsbuf->get();
   b.p[3] = scratch->get();
   plan.run(c, kCx<S>, prec, b);
+  penalty(c, psi, out);
+}
+
+template <class S>
+void HeffPlan<S>::penalty(Ctx& c, const S* psi, S* out) const {
+  if (npen <= 0) return;
+  launch_multi_dot(kCx<S>, pen_o->get(), n, npen, psi, n, c.d_partial, c.npart, pen_dot->get(), c.stream);
+  launch_multi_axpy(kCx<S>, out, pen_wo->get(), n, npen, pen_dot->get(), n, c.stream);
+  c.launches += 3;
 }
 
 // ---------------------------------------------------------------------------

@@ -28,7 +28,14 @@ struct HeffPlan {
   long long flops = 0;               // algorithmic flops per matvec
   long long bytes = 0;               // psi in + out + operators, once
   int ntasks = 0;
+  // excited-state penalty (src/dmrg_inst.cpp:352-363): out -= sum_k w_k <o_k|psi> o_k,
+  // o_k the lower states in this two-site basis, w_k their energies
+  int npen = 0;
+  std::shared_ptr<DevBuf> pen_o;     // npen vectors o_k, psi layout
+  std::shared_ptr<DevBuf> pen_wo;    // w_k o_k
+  std::shared_ptr<DevBuf> pen_dot;   // <o_k|psi>
   void apply(Ctx& c, const S* psi, S* out, int prec) const;
+  void penalty(Ctx& c, const S* psi, S* out) const;
 };
 
 struct PairTerm {

@@ -32,6 +32,7 @@ EXPORTED = [
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
+    "sadmrg_heff_set_penalty",
 ]
 
 
@@ -68,6 +69,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_set_lanczos_tol": ([vp, C.c_double], C.c_int),
         "sadmrg_set_matvec_fusion": ([vp, C.c_int], C.c_int),
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
+        "sadmrg_heff_set_penalty": ([vp, C.c_int, vp, dp], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
@@ -211,6 +213,13 @@ class Handle:
         rc = self.lib.sadmrg_heff_plan(self.h, C.byref(d_psi), d_hl, d_hr, len(ops), arr, len(terms),
                                        op1.ctypes.data_as(ip), op2.ctypes.data_as(ip))
         self._check(rc, "heff_plan")
+
+    def heff_set_penalty(self, vecs, weights):
+        """Excited-state penalty: H_eff psi -= sum_k weights[k] <vecs[k]|psi> vecs[k]."""
+        v = np.ascontiguousarray(np.asarray(vecs, dtype=self.dtype).reshape(len(weights), -1)) if len(weights) else None
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        self._check(self.lib.sadmrg_heff_set_penalty(self.h, len(w), v.ctypes.data if v is not None else None,
+                                                     w.ctypes.data_as(C.POINTER(C.c_double))), "heff_set_penalty")
 
     def heff_info(self):
         n = C.c_longlong()
