@@ -147,6 +147,25 @@ int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const voi
  * FP64 restart from its result. */
 int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energy, int* matvecs);
 
+/* ---- many independent instances, one launch per stage ---------------------
+ * No counterpart in the reference (one DMRG per process).  sadmrg_batch_add
+ * appends the H_eff plan of another handle `inst` (same device, symmetry and
+ * scalar type) to h's batch; the instance handle may be destroyed once it has
+ * been added.  sadmrg_batch_finalize merges the plans: instance i's vectors are
+ * the segment [offsets[i], offsets[i+1]) of one long vector, and every batched
+ * matvec runs all instances' sector products in one launch per stage.
+ * sadmrg_batch_lanczos runs lanczos1 (or the mixed solver) on every instance at
+ * once from psi_host (all segments), leaves each instance's Ritz vector in its
+ * segment and its energy in energies[i]; matvecs[i] counts the matvecs instance i
+ * needed, *batched_matvecs the batched launches. */
+int sadmrg_batch_add(sadmrg_handle* h, sadmrg_handle* inst);
+int sadmrg_batch_finalize(sadmrg_handle* h);
+int sadmrg_batch_clear(sadmrg_handle* h);
+int sadmrg_batch_info(sadmrg_handle* h, int* ninst, long long* n, double* flops, int cap, long long* offsets);
+int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision);
+int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energies, int* matvecs,
+                         int* batched_matvecs);
+
 /* ---- block SVD truncation ---------------------------------------------------
  * psi: 2-leg two-site vector.  tu / tv: the current site tensors (only their
  * bonds 0 and 1 are read).  p1 / p2: powers of the singular values absorbed

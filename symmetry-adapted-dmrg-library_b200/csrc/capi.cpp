@@ -12,6 +12,7 @@ template <class S>
 struct State {
   std::unique_ptr<HeffPlan<S>> heff;
   std::unique_ptr<Chain<S>> chain;
+  std::unique_ptr<HeffBatch<S>> batch;
   BTensor<S> staged[2];
   DevBuf io;   // psi in / out for host-buffer calls
 };
@@ -473,6 +474,93 @@ int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precisi
     check_device_status();
     if (energy) *energy = st.energy;
     if (matvecs) *matvecs = st.matvecs;
+  });
+}
+
+// ---- many instances in one launch ------------------------------------------
+int sadmrg_batch_add(sadmrg_handle* h, sadmrg_handle* inst) {
+  if (!inst) return h ? fail(h, SADMRG_ERR_ARG, "batch_add: null instance") : SADMRG_ERR_ARG;
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    SADMRG_REQUIRE(inst->device == h->device && inst->ctx.sym == h->ctx.sym && inst->ctx.cplx == h->ctx.cplx,
+                   SADMRG_ERR_ARG, "batch_add: instance on another device or of another symmetry / scalar type");
+    auto& I = st_of<S>(inst);
+    SADMRG_REQUIRE(I.heff, SADMRG_ERR_STATE, "batch_add: the instance has no H_eff plan");
+    auto& S_ = st_of<S>(h);
+    if (!S_.batch) S_.batch = std::make_unique<HeffBatch<S>>();
+    S_.batch->add(h->ctx, *I.heff);
+  });
+}
+
+int sadmrg_batch_finalize(sadmrg_handle* h) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.batch, SADMRG_ERR_STATE, "batch_finalize: no instances added");
+    S_.batch->finalize(h->ctx);
+  });
+}
+
+int sadmrg_batch_clear(sadmrg_handle* h) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    st_of<S>(h).batch.reset();
+  });
+}
+
+int sadmrg_batch_info(sadmrg_handle* h, int* ninst, long long* n, double* flops, int cap, long long* offsets) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_info: not finalized");
+    const HeffBatch<S>& B = *S_.batch;
+    if (ninst) *ninst = B.nseg();
+    if (n) *n = B.merged.n;
+    if (flops) *flops = (double)B.merged.flops;
+    if (offsets)
+      for (int i = 0; i < cap && i < (int)B.seg.size(); ++i) offsets[i] = B.seg[i];
+  });
+}
+
+int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_apply: not finalized");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "batch_apply: precision");
+    const HeffPlan<S>& H = S_.batch->merged;
+    DevBuf io(sizeof(S) * 2 * std::max<long long>(H.n, 1), c.stream);
+    S* din = io.as<S>();
+    S* dout = din + H.n;
+    SADMRG_CUDA(cudaMemcpyAsync(din, psi_host, sizeof(S) * H.n, cudaMemcpyHostToDevice, c.stream));
+    H.apply(c, din, dout, precision);
+    SADMRG_CUDA(cudaMemcpyAsync(out_host, dout, sizeof(S) * H.n, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_status();
+  });
+}
+
+int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energies, int* matvecs,
+                         int* batched_matvecs) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_lanczos: not finalized");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "batch_lanczos: precision");
+    const HeffBatch<S>& B = *S_.batch;
+    DevBuf io(sizeof(S) * std::max<long long>(B.merged.n, 1), c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(io.get(), psi_host, sizeof(S) * B.merged.n, cudaMemcpyHostToDevice, c.stream));
+    BatchStats st = batch_lanczos_solve<S>(c, B, io.as<S>(), mlanc, precision);
+    SADMRG_CUDA(cudaMemcpyAsync(psi_host, io.get(), sizeof(S) * B.merged.n, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_status();
+    for (int i = 0; i < B.nseg(); ++i) {
+      if (energies) energies[i] = st.energy[i];
+      if (matvecs) matvecs[i] = st.matvecs[i];
+    }
+    if (batched_matvecs) *batched_matvecs = st.launches_matvec;
   });
 }
 

@@ -174,7 +174,7 @@ void HeffPlan<S>::penalty(Ctx& c, const S* psi, S* out) const {
 // implicit QL with Wilkinson-type shifts (the tql2 algorithm of Bowdler, Martin,
 // Reinsch and Wilkinson, 1968).  d: diagonal, e[i]: coupling of i and i+1.
 // On return d is ascending and z (column-major n x n) holds the eigenvectors.
-static void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
+void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
   z.assign((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) z[i + (size_t)i * n] = 1.0;
   e.resize(n, 0.0);

@@ -63,6 +63,44 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec);
 template <class S>
 LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec);
 
+// symmetric tridiagonal eigenproblem: d diagonal (ascending on return), e[i]
+// coupling of i and i+1, z column-major eigenvectors (dmrg.cpp)
+void tridiag_eig(int n, std::vector<double>& d, std::vector<double> e, std::vector<double>& z);
+
+// Many independent frozen two-site problems merged into one plan: their vectors
+// lie back to back (segment s = [seg[s], seg[s+1])) and one launch per stage
+// runs the sector products of all of them (batch.cpp).
+template <class S>
+struct HeffBatch {
+  struct Part {
+    std::vector<std::vector<GemmTerm>> job_terms;
+    std::vector<GemmJob> jobs;
+    std::vector<int> job_stage;
+    long long scratch = 0, n = 0, flops = 0;
+    std::shared_ptr<DevBuf> ops;     // the instance's packed operators (kept alive until finalize)
+  };
+  std::vector<Part> parts;
+  HeffPlan<S> merged;
+  std::vector<long long> seg;        // nseg + 1 offsets
+  std::shared_ptr<DevBuf> d_seg;
+  bool ready = false;
+  void add(Ctx& c, const HeffPlan<S>& H);
+  void finalize(Ctx& c);
+  int nseg() const { return (int)seg.size() - 1; }
+};
+
+struct BatchStats {
+  std::vector<double> energy;        // per instance
+  std::vector<int> matvecs;          // per instance (matvecs taken while it was not converged)
+  int launches_matvec = 0;           // batched matvecs (each one launch per stage for all instances)
+};
+
+// Lanczos::lanczos1 on every instance at once: the same recurrence and checks as
+// lanczos1 per segment; instances that converge keep their Ritz vector in v.
+// prec TF32X3: split-precision phase then an FP64 restart, as lanczos_solve.
+template <class S>
+BatchStats batch_lanczos_solve(Ctx& c, const HeffBatch<S>& B, S* v, int mlanc, int prec);
+
 struct SvdStats {
   int kept = 0;
   double discarded_weight = 0.0;

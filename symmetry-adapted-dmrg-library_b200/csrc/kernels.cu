@@ -308,3 +308,167 @@ void launch_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, co
 }
 
 }  // namespace sadmrg
+
+// ---------------------------------------------------------------------------
+// Segmented Krylov kernels for independent instances stored back to back:
+// segment s is [seg[s], seg[s + 1]).  One block per segment, so every
+// reduction runs in one fixed order (deterministic).
+namespace sadmrg {
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) seg_multi_dot_kernel(const void* V, long long ldv, int nv, const void* x,
+                                                            const long long* seg, void* out) {
+  __shared__ double red[2][8];
+  const int s = blockIdx.x;
+  const long long lo = seg[s], hi = seg[s + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j = 0; j < nv; ++j) {
+    double sr = 0.0, si = 0.0;
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      if (CPLX) {
+        const double2 a = static_cast<const double2*>(V)[j * ldv + i];
+        const double2 b = static_cast<const double2*>(x)[i];
+        sr += a.x * b.x + a.y * b.y;
+        si += a.x * b.y - a.y * b.x;
+      } else {
+        sr += static_cast<const double*>(V)[j * ldv + i] * static_cast<const double*>(x)[i];
+      }
+    }
+    sr = warp_sum(sr);
+    if (CPLX) si = warp_sum(si);
+    if (lane == 0) { red[0][warp] = sr; red[1][warp] = si; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += red[0][w]; b += red[1][w]; }
+      if (CPLX) static_cast<double2*>(out)[(long long)s * nv + j] = make_double2(a, b);
+      else static_cast<double*>(out)[(long long)s * nv + j] = a;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_seg_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, const long long* seg,
+                          int nseg, void* out, cudaStream_t s) {
+  if (nv <= 0 || nseg <= 0) return;
+  if (cplx) seg_multi_dot_kernel<true><<<nseg, 256, 0, s>>>(V, ldv, nv, x, seg, out);
+  else seg_multi_dot_kernel<false><<<nseg, 256, 0, s>>>(V, ldv, nv, x, seg, out);
+}
+
+// x -= sum_j c[s * cstride + j] V_j on segment s
+template <bool CPLX>
+__global__ void __launch_bounds__(256) seg_multi_axpy_kernel(void* x, const void* V, long long ldv, int nv,
+                                                             const void* c, int cstride, const long long* seg) {
+  const int s = blockIdx.x;
+  const long long lo = seg[s], hi = seg[s + 1];
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    if (CPLX) {
+      double2 acc = static_cast<double2*>(x)[i];
+      for (int j = 0; j < nv; ++j) {
+        const double2 cj = static_cast<const double2*>(c)[(long long)s * cstride + j];
+        const double2 v = static_cast<const double2*>(V)[j * ldv + i];
+        acc.x -= cj.x * v.x - cj.y * v.y;
+        acc.y -= cj.x * v.y + cj.y * v.x;
+      }
+      static_cast<double2*>(x)[i] = acc;
+    } else {
+      double acc = static_cast<double*>(x)[i];
+      for (int j = 0; j < nv; ++j)
+        acc -= static_cast<const double*>(c)[(long long)s * cstride + j] * static_cast<const double*>(V)[j * ldv + i];
+      static_cast<double*>(x)[i] = acc;
+    }
+  }
+}
+
+void launch_seg_multi_axpy(bool cplx, void* x, const void* V, long long ldv, int nv, const void* c, int cstride,
+                           const long long* seg, int nseg, cudaStream_t s) {
+  if (nv <= 0 || nseg <= 0) return;
+  if (cplx) seg_multi_axpy_kernel<true><<<nseg, 256, 0, s>>>(x, V, ldv, nv, c, cstride, seg);
+  else seg_multi_axpy_kernel<false><<<nseg, 256, 0, s>>>(x, V, ldv, nv, c, cstride, seg);
+}
+
+// x *= f(scal[s * sstride]) on segment s: f = 1/v (inv) or v
+template <bool CPLX>
+__global__ void __launch_bounds__(256) seg_scale_kernel(void* x, const double* scal, int sstride, int inv,
+                                                        const long long* seg) {
+  const int s = blockIdx.x;
+  const long long lo = seg[s], hi = seg[s + 1];
+  const double v = scal[(long long)s * sstride];
+  const double f = inv ? 1.0 / v : v;
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    if (CPLX) { double2 a = static_cast<double2*>(x)[i]; a.x *= f; a.y *= f; static_cast<double2*>(x)[i] = a; }
+    else static_cast<double*>(x)[i] *= f;
+  }
+}
+
+void launch_seg_scale(bool cplx, void* x, const double* scal, int sstride, int inv, const long long* seg, int nseg,
+                      cudaStream_t s) {
+  if (nseg <= 0) return;
+  if (cplx) seg_scale_kernel<true><<<nseg, 256, 0, s>>>(x, scal, sstride, inv, seg);
+  else seg_scale_kernel<false><<<nseg, 256, 0, s>>>(x, scal, sstride, inv, seg);
+}
+
+// y = sum_j c[s * cstride + j] V_j on the segments with mask[s] != 0
+template <bool CPLX>
+__global__ void __launch_bounds__(256) seg_lincomb_kernel(void* y, const void* V, long long ldv, int nv,
+                                                          const double* c, int cstride, const int* mask,
+                                                          const long long* seg) {
+  const int s = blockIdx.x;
+  if (!mask[s]) return;
+  const long long lo = seg[s], hi = seg[s + 1];
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    if (CPLX) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int j = 0; j < nv; ++j) {
+        const double cj = c[(long long)s * cstride + j];
+        const double2 v = static_cast<const double2*>(V)[j * ldv + i];
+        acc.x += cj * v.x;
+        acc.y += cj * v.y;
+      }
+      static_cast<double2*>(y)[i] = acc;
+    } else {
+      double acc = 0.0;
+      for (int j = 0; j < nv; ++j) acc += c[(long long)s * cstride + j] * static_cast<const double*>(V)[j * ldv + i];
+      static_cast<double*>(y)[i] = acc;
+    }
+  }
+}
+
+void launch_seg_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, const double* c, int cstride,
+                        const int* mask, const long long* seg, int nseg, cudaStream_t s) {
+  if (nseg <= 0) return;
+  if (cplx) seg_lincomb_kernel<true><<<nseg, 256, 0, s>>>(y, V, ldv, nv, c, cstride, mask, seg);
+  else seg_lincomb_kernel<false><<<nseg, 256, 0, s>>>(y, V, ldv, nv, c, cstride, mask, seg);
+}
+
+// per segment s: op 0: coef[2s] = beta_prev[s * bstride], coef[2s + 1] = Re(dot[s])
+//                op 1: out[s * ostride] = sqrt(|Re(dot[s])|)
+template <bool CPLX>
+__global__ void seg_lanczos_scalar_kernel(int op, const void* dot, const double* beta_prev, int bstride, void* out,
+                                          int ostride, int nseg) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  const double re = CPLX ? static_cast<const double2*>(dot)[s].x : static_cast<const double*>(dot)[s];
+  if (op == 0) {
+    const double b = beta_prev[(long long)s * bstride];
+    if (CPLX) {
+      static_cast<double2*>(out)[2 * s] = make_double2(b, 0.0);
+      static_cast<double2*>(out)[2 * s + 1] = make_double2(re, 0.0);
+    } else {
+      static_cast<double*>(out)[2 * s] = b;
+      static_cast<double*>(out)[2 * s + 1] = re;
+    }
+  } else {
+    static_cast<double*>(out)[(long long)s * ostride] = sqrt(fabs(re));
+  }
+}
+
+void launch_seg_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, int bstride, void* out,
+                               int ostride, int nseg, cudaStream_t s) {
+  if (nseg <= 0) return;
+  const int blocks = (nseg + 127) / 128;
+  if (cplx) seg_lanczos_scalar_kernel<true><<<blocks, 128, 0, s>>>(op, dot, beta_prev, bstride, out, ostride, nseg);
+  else seg_lanczos_scalar_kernel<false><<<blocks, 128, 0, s>>>(op, dot, beta_prev, bstride, out, ostride, nseg);
+}
+
+}  // namespace sadmrg

@@ -180,6 +180,25 @@ void launch_scale_inv(bool cplx, void* x, const double* scal, long long n, cudaS
 void launch_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, const double* c_dev, long long n,
                     cudaStream_t s);
 
+// ---- segmented Krylov operations (independent instances back to back) -----
+// segment s covers [seg[s], seg[s + 1]) of every vector; one block per segment
+// out[s * nv + j] = <V_j | x> on segment s
+void launch_seg_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, const long long* seg,
+                          int nseg, void* out, cudaStream_t s);
+// x -= sum_j c[s * cstride + j] V_j on segment s
+void launch_seg_multi_axpy(bool cplx, void* x, const void* V, long long ldv, int nv, const void* c, int cstride,
+                           const long long* seg, int nseg, cudaStream_t s);
+// x *= scal[s * sstride] (inv = 0) or 1 / scal[s * sstride] (inv = 1) on segment s
+void launch_seg_scale(bool cplx, void* x, const double* scal, int sstride, int inv, const long long* seg, int nseg,
+                      cudaStream_t s);
+// y = sum_j c[s * cstride + j] V_j (real c) on the segments with mask[s] != 0
+void launch_seg_lincomb(bool cplx, void* y, const void* V, long long ldv, int nv, const double* c, int cstride,
+                        const int* mask, const long long* seg, int nseg, cudaStream_t s);
+// per segment: op 0: coef[2s] = beta_prev[s * bstride], coef[2s + 1] = Re(dot[s]); op 1: out[s * ostride] =
+// sqrt(|Re dot[s]|)
+void launch_seg_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, int bstride, void* out,
+                               int ostride, int nseg, cudaStream_t s);
+
 // ---- one-sided Jacobi SVD of sector blocks --------------------------------
 struct SvdJob {
   long long aoff;             // input block (m x n, lda = m) in the input buffer

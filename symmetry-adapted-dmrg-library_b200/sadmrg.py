@@ -32,7 +32,8 @@ EXPORTED = [
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
-    "sadmrg_heff_set_penalty",
+    "sadmrg_heff_set_penalty", "sadmrg_batch_add", "sadmrg_batch_finalize", "sadmrg_batch_clear",
+    "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos",
 ]
 
 
@@ -70,6 +71,12 @@ def load(path: str = LIB_PATH):
         "sadmrg_set_matvec_fusion": ([vp, C.c_int], C.c_int),
         "sadmrg_heff_info": ([vp, lp, dp, dp, ip], C.c_int),
         "sadmrg_heff_set_penalty": ([vp, C.c_int, vp, dp], C.c_int),
+        "sadmrg_batch_add": ([vp, vp], C.c_int),
+        "sadmrg_batch_finalize": ([vp], C.c_int),
+        "sadmrg_batch_clear": ([vp], C.c_int),
+        "sadmrg_batch_info": ([vp, ip, lp, dp, C.c_int, lp], C.c_int),
+        "sadmrg_batch_apply": ([vp, vp, vp, C.c_int], C.c_int),
+        "sadmrg_batch_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip, ip], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
@@ -220,6 +227,44 @@ class Handle:
         w = np.ascontiguousarray(weights, dtype=np.float64)
         self._check(self.lib.sadmrg_heff_set_penalty(self.h, len(w), v.ctypes.data if v is not None else None,
                                                      w.ctypes.data_as(C.POINTER(C.c_double))), "heff_set_penalty")
+
+    # -- many instances ---------------------------------------------------------
+    def batch_add(self, inst: "Handle"):
+        """Append inst's H_eff plan to this handle's batch (inst may be closed afterwards)."""
+        self._check(self.lib.sadmrg_batch_add(self.h, inst.h), "batch_add")
+
+    def batch_finalize(self):
+        self._check(self.lib.sadmrg_batch_finalize(self.h), "batch_finalize")
+        return self.batch_info()
+
+    def batch_clear(self):
+        self._check(self.lib.sadmrg_batch_clear(self.h), "batch_clear")
+
+    def batch_info(self):
+        ni, n, fl = C.c_int(), C.c_longlong(), C.c_double()
+        self._check(self.lib.sadmrg_batch_info(self.h, C.byref(ni), C.byref(n), C.byref(fl), 0, None), "batch_info")
+        off = np.zeros(ni.value + 1, dtype=np.int64)
+        self._check(self.lib.sadmrg_batch_info(self.h, C.byref(ni), C.byref(n), C.byref(fl), len(off),
+                                               off.ctypes.data_as(C.POINTER(C.c_longlong))), "batch_info")
+        return {"ninst": ni.value, "n": n.value, "flops": fl.value, "offsets": off}
+
+    def batch_apply(self, psi: np.ndarray, precision: int = PREC_FP64) -> np.ndarray:
+        x = np.ascontiguousarray(psi, dtype=self.dtype)
+        out = np.empty_like(x)
+        self._check(self.lib.sadmrg_batch_apply(self.h, x.ctypes.data, out.ctypes.data, int(precision)), "batch_apply")
+        return out
+
+    def batch_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
+        """(energies, Ritz vectors (all segments), matvecs per instance, batched matvec launches)."""
+        info = self.batch_info()
+        x = np.array(psi, dtype=self.dtype, copy=True)
+        e = np.zeros(info["ninst"])
+        mv = np.zeros(info["ninst"], dtype=np.int32)
+        bm = C.c_int()
+        self._check(self.lib.sadmrg_batch_lanczos(self.h, x.ctypes.data, int(mlanc), int(precision),
+                                                  e.ctypes.data_as(C.POINTER(C.c_double)),
+                                                  mv.ctypes.data_as(C.POINTER(C.c_int)), C.byref(bm)), "batch_lanczos")
+        return e, x, mv, bm.value
 
     def heff_info(self):
         n = C.c_longlong()
