@@ -54,6 +54,11 @@ WORKLOADS = {
     # with dims log-uniform in [8, 512] and N(0,1) entries from the seed
     "su2_ladder_2x32_D2048_synth": dict(sym=1, cplx=False, lx=32, ly=2, D=2048, J2=0.0,
                                         synthetic=dict(seed=2024, nsec=30, dmin=8, dmax=512)),
+    # 256 independent U(1) J1-J2 chains (L uniform in 16..64, J2 in [0, 0.6], D in 32..256, from the
+    # seed, L even); each instance's centre Lanczos solve, all instances batched into one launch per stage
+    "u1_j1j2_batch256": dict(sym=0, cplx=False, lx=1, ly=0, D=0, J2=0.0,
+                             batch=dict(n=256, seed=5, L=(16, 64), J2=(0.0, 0.6), D=(32, 256), mlanc=100,
+                                        tol=1e-12, cpu_sample=8)),
 }
 
 
@@ -312,16 +317,170 @@ def run_reference_harness(export_dir: str, wl: dict, calls: int, threads: int):
     raise RuntimeError("reference harness printed no timing")
 
 
+def batch_instances(sp: dict):
+    """(L, J2, D) of every instance, from the seed: L even (the chain needs an even
+    number of sites) and uniform in [L0, L1], J2 uniform, D uniform."""
+    rng = np.random.default_rng(sp["seed"])
+    n = sp["n"]
+    Ls = 2 * rng.integers(sp["L"][0] // 2, sp["L"][1] // 2 + 1, size=n)
+    J2s = rng.uniform(sp["J2"][0], sp["J2"][1], size=n)
+    Ds = rng.integers(sp["D"][0], sp["D"][1] + 1, size=n)
+    return Ls, J2s, Ds
+
+
+def run_batch(a, wl: dict, ws: int, rank: int, local: int, cores: int):
+    """Many-instance workload: every instance's centre solve, batched vs one at a time."""
+    import torch
+    import sadmrg
+    torch.cuda.set_device(local)
+    sp = wl["batch"]
+    rng = np.random.default_rng(sp["seed"])
+    n = sp["n"]
+    Ls, J2s, Ds = batch_instances(sp)
+    tol, mlanc = sp["tol"], sp["mlanc"]
+    b = sadmrg.Handle(sym=0, cplx=False, device=local)
+    b.set_lanczos_tol(tol)
+    psis, e_one, mv_one = [], [], []
+    t_one = 0.0
+    t0b = time.perf_counter()
+    sample_dirs = []
+    for i in range(n):
+        h = sadmrg.Handle(sym=0, cplx=False, device=local)
+        h.chain_create(1, int(Ls[i]), int(Ds[i]), 1, 0, True, float(J2s[i]))
+        h.chain_idmrg()
+        d = None
+        if rank == 0 and i < sp["cpu_sample"] and not a.no_cpu and os.path.exists(HARNESS):
+            d = tempfile.mkdtemp(prefix="sadmrg_inst_")
+            sample_dirs.append(d)
+        psi = h.chain_freeze(int(Ls[i]) // 2 - 1, d)
+        psis.append(np.ascontiguousarray(psi.data))
+        h.set_lanczos_tol(tol)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, _, mv = h.heff_lanczos(psis[-1], mlanc, sadmrg.PREC_FP64)
+        t_one += time.perf_counter() - t0
+        e_one.append(e)
+        mv_one.append(mv)
+        b.batch_add(h)
+        h.close()
+    t_build = time.perf_counter() - t0b - t_one
+    info = b.batch_finalize()
+    x = np.concatenate(psis)
+    flops = info["flops"]
+    # batched matvec throughput, L2 warm (back-to-back batched matvecs)
+    peaks = measured_peaks()
+    for prec in (sadmrg.PREC_FP64, sadmrg.PREC_TF32X3):
+        b.batch_profile(prec, max(1, a.warmup))
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        ms_mx = b.batch_profile(sadmrg.PREC_TF32X3, a.steps)
+        ms_64 = b.batch_profile(sadmrg.PREC_FP64, a.steps)
+    ms_mx, ms_64 = reduce_max(ms_mx, ws), reduce_max(ms_64, ws)
+    value = flops * ws / (ms_mx * 1e-3) / 1e12
+    # batched solves (host psi in, Ritz vectors out)
+    b.batch_lanczos(x, mlanc, sadmrg.PREC_FP64)   # warm
+    t0 = time.perf_counter()
+    e64, _, mv64, nb64 = b.batch_lanczos(x, mlanc, sadmrg.PREC_FP64)
+    t64 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    emx, _, mvmx, nbmx = b.batch_lanczos(x, mlanc, sadmrg.PREC_TF32X3)
+    tmx = time.perf_counter() - t0
+    e_one = np.array(e_one)
+    # end to end: batched matvec with host buffers
+    b.batch_apply(x, sadmrg.PREC_TF32X3)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        b.batch_apply(x, sadmrg.PREC_TF32X3)
+    e2e_s = (time.perf_counter() - t0) / a.steps
+    line = {
+        "metric": "H_eff*psi TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_mx, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "tf32x3 (tcgen05 kind::tf32 hi/lo products, f32 accumulation in tensor memory)", "data": "synthetic",
+        "config": {"workload": a.workload, "instances": n, "L": [int(Ls.min()), int(Ls.max())],
+                   "D": [int(Ds.min()), int(Ds.max())], "J2": [float(J2s.min()), float(J2s.max())],
+                   "symmetry": "U1", "psi_elems": int(info["n"]), "flops_per_step": flops,
+                   "l2": "warm (back-to-back batched matvecs)", "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": flops / (ms_64 * 1e-3) / 1e12, "ms_per_step": ms_64,
+                 "speedup_mixed_over_fp64": ms_64 / ms_mx},
+        "solves": {"lanczos_ov_tol": tol, "one_at_a_time_fp64_s": t_one, "one_at_a_time_fp64_per_s": n / t_one,
+                   "batched_fp64_s": t64, "batched_fp64_per_s": n / t64, "batched_mixed_s": tmx,
+                   "batched_mixed_per_s": n / tmx, "speedup_batched_mixed_over_one_at_a_time": t_one / tmx,
+                   "max_rel_dE_batched_fp64_vs_single": float(np.max(np.abs(e64 - e_one) / np.abs(e_one))),
+                   "max_rel_dE_batched_mixed_vs_single_fp64": float(np.max(np.abs(emx - e_one) / np.abs(e_one))),
+                   "matvecs_single_total": int(np.sum(mv_one)), "batched_launches_fp64": nb64,
+                   "batched_launches_mixed": nbmx},
+        "build_s": round(t_build, 2),
+        "e2e": {"value": flops / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": int(x.nbytes),
+                "d2h_bytes_per_step": int(x.nbytes)},
+        "roofline": {"bound": "tensor", "achieved": value / ws, "peak": peaks["tf32_tflops"] / 3.0, "unit": "TFLOP/s",
+                     "frac": value / ws / (peaks["tf32_tflops"] / 3.0), "traffic": None,
+                     "kernel": "batched matvec (psi panels + two tcgen05 launches for all instances)",
+                     "peak_source": "of measured: cuBLAS TF32 GEMM (8192^3) timed in this run, / 3 for 3xTF32"},
+        "peaks_measured": peaks,
+        "gpu_launches": 2 * a.steps * 3,
+        "clocks": clk.summary(),
+    }
+    if sample_dirs:
+        try:
+            sec, fl = 0.0, 0.0
+            for d in sample_dirs:
+                wl1 = dict(sym=0, cplx=False)
+                sec += run_reference_harness(d, wl1, 20, cores)
+                hh = sadmrg.Handle(sym=0, cplx=False, device=local)
+                sadmrg.load_exported_problem(hh, d)
+                fl += 20 * hh.heff_info()["flops"]
+                hh.close()
+            line["cpu_baseline"] = {"value": fl / sec / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                    "sample": f"20 H_eff*psi calls on each of the first {len(sample_dirs)} instances"}
+        except Exception as ex:
+            line["cpu_baseline"] = {"value": None, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                    "sample": f"failed: {ex}"}
+    if rank == 0:
+        print(json.dumps(line))
+    b.close()
+
+
 def main():
     a = parse()
     wl = WORKLOADS[a.workload]
     ws, rank, local = dist_init()
     cores = os.cpu_count() or 1
+    if "batch" in wl and a.impl != "reference":
+        run_batch(a, wl, ws, rank, local, cores)
+        return
     if a.impl == "reference":
         if rank != 0:
             return
         if not os.path.exists(HARNESS):
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
+            return
+        if "batch" in wl:
+            # the reference solves one instance at a time: its H_eff*psi on the first instances
+            import sadmrg
+            sp = wl["batch"]
+            Ls, J2s, Ds = batch_instances(sp)
+            sec = fl = 0.0
+            k = sp["cpu_sample"]
+            for i in range(k):
+                with tempfile.TemporaryDirectory() as td:
+                    h = sadmrg.Handle(sym=0, cplx=False, device=local)
+                    h.chain_create(1, int(Ls[i]), int(Ds[i]), 1, 0, True, float(J2s[i]))
+                    h.chain_idmrg()
+                    h.chain_freeze(int(Ls[i]) // 2 - 1, td)
+                    f1 = h.heff_info()["flops"]
+                    h.close()
+                    run_reference_harness(td, wl, 1, cores)
+                    sec += run_reference_harness(td, wl, a.steps, cores)
+                    fl += a.steps * f1
+            v = fl / sec / 1e12
+            print(json.dumps({"metric": "H_eff*psi TFLOP/s", "value": v, "unit": "TFLOP/s", "n_gpus": ws,
+                              "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec / (a.steps * k) * 1e3,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic", "impl": "reference",
+                              "config": {"workload": a.workload, "instances_sampled": k, "l2": "host run"},
+                              "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                               "sample": f"{a.steps} H_eff*psi calls on each of the first {k} instances"},
+                              "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
             return
         with tempfile.TemporaryDirectory() as td:
             # inputs: the same frozen problem (built on the GPU, written as files); the timed
@@ -511,4 +670,13 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    try:
+        main()
+    except BaseException:
+        # report and leave without interpreter teardown: device handles still open
+        # on an error path are released by the process exit
+        import traceback
+        traceback.print_exc()
+        sys.stdout.flush()
+        sys.stderr.flush()
+        os._exit(1)

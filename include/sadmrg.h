@@ -165,6 +165,8 @@ int sadmrg_batch_info(sadmrg_handle* h, int* ninst, long long* n, double* flops,
 int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, int precision);
 int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energies, int* matvecs,
                          int* batched_matvecs);
+/* mean device time (ms, CUDA events, back to back) of one batched matvec over reps */
+int sadmrg_batch_profile(sadmrg_handle* h, int precision, int reps, double* ms);
 
 /* ---- block SVD truncation ---------------------------------------------------
  * psi: 2-leg two-site vector.  tu / tv: the current site tensors (only their

@@ -23,7 +23,6 @@ template <class S> constexpr bool kCxB = ScalarInfo<S>::cplx;
 
 template <class S>
 void HeffBatch<S>::add(Ctx& c, const HeffPlan<S>& H) {
-  (void)c;
   SADMRG_REQUIRE(!ready, SADMRG_ERR_STATE, "batch: already finalized");
   Part p;
   p.job_terms = H.plan.job_terms;
@@ -32,7 +31,15 @@ void HeffBatch<S>::add(Ctx& c, const HeffPlan<S>& H) {
   p.scratch = H.plan.scratch_elems;
   p.n = H.n;
   p.flops = H.flops;
-  p.ops = H.opsbuf;
+  // The operators are copied on the batch's stream and the copy is awaited here:
+  // the instance's buffers belong to its own handle (and stream), which the
+  // caller may destroy as soon as this returns.
+  const size_t bytes = H.opsbuf ? H.opsbuf->bytes() : 0;
+  if (bytes) {
+    p.ops = std::make_shared<DevBuf>(bytes, c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(p.ops->get(), H.opsbuf->get(), bytes, cudaMemcpyDeviceToDevice, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
   parts.push_back(std::move(p));
 }
 

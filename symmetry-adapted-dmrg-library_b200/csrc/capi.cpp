@@ -541,6 +541,35 @@ int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, i
   });
 }
 
+int sadmrg_batch_profile(sadmrg_handle* h, int precision, int reps, double* ms) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_profile: not finalized");
+    SADMRG_REQUIRE(reps >= 1 && ms, SADMRG_ERR_ARG, "batch_profile: arguments");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "batch_profile: precision");
+    const HeffPlan<S>& H = S_.batch->merged;
+    DevBuf io(sizeof(S) * 2 * std::max<long long>(H.n, 1), c.stream);
+    SADMRG_CUDA(cudaMemsetAsync(io.get(), 0, sizeof(S) * 2 * std::max<long long>(H.n, 1), c.stream));
+    S* din = io.as<S>();
+    H.apply(c, din, din + H.n, precision);   // warm
+    cudaEvent_t e0, e1;
+    SADMRG_CUDA(cudaEventCreate(&e0));
+    SADMRG_CUDA(cudaEventCreate(&e1));
+    SADMRG_CUDA(cudaEventRecord(e0, c.stream));
+    for (int r = 0; r < reps; ++r) H.apply(c, din, din + H.n, precision);
+    SADMRG_CUDA(cudaEventRecord(e1, c.stream));
+    SADMRG_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    SADMRG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_device_status();
+  });
+}
+
 int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energies, int* matvecs,
                          int* batched_matvecs) {
   return dispatch(h, [&](auto* tag) {

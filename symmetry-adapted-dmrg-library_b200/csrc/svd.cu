@@ -102,9 +102,14 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
       const double g = CPLX ? sqrt(gr * gr + gi * gi) : fabs(gr);
       const double nrm = sqrt(a) * sqrt(b);
       if (!(nrm > 1e-300) || g <= tol * nrm) continue;
-      // rotation zeroing the (p,q) entry of the 2x2 Gram matrix [[a, g],[g*, b]]
+      // rotation zeroing the (p,q) entry of the 2x2 Gram matrix [[a, g],[g*, b]];
+      // for |zeta| > 1e150, zeta^2 would overflow: t = 1 / (2 zeta) to double
+      // precision there, and a t that underflows to 0 means the pair is already
+      // orthogonal to working precision (no rotation, none counted)
       const double zeta = (b - a) / (2.0 * g);
-      const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
+                                          : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      if (!(t != 0.0)) continue;
       const double c = 1.0 / sqrt(1.0 + t * t);
       const double s = c * t;
       // phase e^{i phi} = gamma / |gamma|

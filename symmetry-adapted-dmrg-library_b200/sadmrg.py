@@ -12,7 +12,9 @@ blocks by block index, and their column-major data concatenated in block order).
 from __future__ import annotations
 
 import ctypes as C
+import atexit
 import os
+import weakref
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -33,7 +35,7 @@ EXPORTED = [
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
     "sadmrg_heff_set_penalty", "sadmrg_batch_add", "sadmrg_batch_finalize", "sadmrg_batch_clear",
-    "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos",
+    "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos", "sadmrg_batch_profile",
 ]
 
 
@@ -77,6 +79,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_batch_info": ([vp, ip, lp, dp, C.c_int, lp], C.c_int),
         "sadmrg_batch_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_batch_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip, ip], C.c_int),
+        "sadmrg_batch_profile": ([vp, C.c_int, C.c_int, dp], C.c_int),
         "sadmrg_heff_apply": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
@@ -167,6 +170,18 @@ class BlockTensorData:
                           blocks.ctypes.data_as(C.POINTER(C.c_longlong)), data.ctypes.data)
 
 
+_live = weakref.WeakSet()
+_atexit_registered = False
+
+
+def _close_all():
+    for h in list(_live):
+        try:
+            h.close()
+        except Exception:
+            pass
+
+
 class Handle:
     """One device + one stream (sadmrg_create)."""
 
@@ -179,6 +194,15 @@ class Handle:
         if rc != 0:
             raise SadmrgError(f"sadmrg_create failed with status {rc}")
         self.h = h
+        # Handles still open at interpreter exit are destroyed by an exit hook that
+        # is registered after the first handle (and so after the CUDA runtime's own
+        # exit hook, which then runs later): destroying one after the runtime has
+        # shut down would touch freed runtime state.
+        global _atexit_registered
+        _live.add(self)
+        if not _atexit_registered:
+            atexit.register(_close_all)
+            _atexit_registered = True
 
     def close(self):
         if getattr(self, "h", None):
@@ -253,6 +277,11 @@ class Handle:
         out = np.empty_like(x)
         self._check(self.lib.sadmrg_batch_apply(self.h, x.ctypes.data, out.ctypes.data, int(precision)), "batch_apply")
         return out
+
+    def batch_profile(self, precision: int = PREC_FP64, reps: int = 20) -> float:
+        ms = C.c_double()
+        self._check(self.lib.sadmrg_batch_profile(self.h, int(precision), int(reps), C.byref(ms)), "batch_profile")
+        return ms.value
 
     def batch_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         """(energies, Ritz vectors (all segments), matvecs per instance, batched matvec launches)."""

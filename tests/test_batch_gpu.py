@@ -59,3 +59,19 @@ def test_batch_matvec_and_lanczos():
             assert abs(np.linalg.norm(vi) - 1.0) < 1e-10
         assert nb <= mv.max() + 8 and mv.min() > 0
     assert b.device_status() == 0
+
+
+def test_batch_outlives_instances():
+    """Instances may be closed once added: the batch keeps its own copy of their operators."""
+    import sadmrg
+    inst = _instances()
+    ref = [h.heff_apply(p.data, sadmrg.PREC_FP64) for h, p in inst]
+    xs = [p.data for _, p in inst]
+    b = sadmrg.Handle(sym=0, cplx=False)
+    for h, _ in inst:
+        b.batch_add(h)
+        h.close()
+    off = b.batch_finalize()["offsets"]
+    y = b.batch_apply(np.concatenate(xs), sadmrg.PREC_FP64)
+    for i, r in enumerate(ref):
+        assert np.abs(y[off[i]:off[i + 1]] - r).max() <= 1e-12 * np.abs(r).max()
