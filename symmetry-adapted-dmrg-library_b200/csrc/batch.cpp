@@ -69,6 +69,7 @@ void HeffBatch<S>::finalize(Ctx& c) {
     for (size_t j = 0; j < q.jobs.size(); ++j) {
       const GemmJob& J = q.jobs[j];
       const int nj = P.add_job(q.job_stage[j], J.cbuf, J.coff + base(J.cbuf), J.m, J.n, J.ldc, J.flags);
+      P.jobs[nj].tag = i;   // a masked matvec skips the jobs of converged instances
       for (const GemmTerm& t : q.job_terms[j])
         P.add_term(nj, t.abuf, t.aoff + base(t.abuf), t.lda, t.bbuf, t.boff + base(t.bbuf), t.ldb, t.k, t.flags,
                    t.ar, t.ai);
@@ -97,12 +98,13 @@ struct BatchKrylov {
   Ctx& c;
   long long N;
   int ns, mlanc, bs;            // segments, Krylov size, beta row stride
-  DevBuf ff, vh, dots, coef, beta, cdev, mask, norm;
+  DevBuf ff, vh, dots, coef, beta, cdev, mask, norm, active;
   S* h_coef = nullptr;          // per step: coef (2 per segment) copied as it is made
   double* h_beta = nullptr;     // beta rows (ns x bs)
   S* h_dots = nullptr;          // 2 per segment
   double* h_cdev = nullptr;     // Ritz coefficients (ns x (mlanc + 1))
   int* h_mask = nullptr;
+  int* h_active = nullptr;      // instances whose matvec work still runs (written only after a stream sync)
   BatchKrylov(Ctx& cc, long long n, int nseg, int ml) : c(cc), N(n), ns(nseg), mlanc(ml), bs(ml + 2) {
     ff.alloc(sizeof(S) * N * (mlanc + 1), c.stream);
     vh.alloc(sizeof(S) * N * 2, c.stream);
@@ -112,12 +114,16 @@ struct BatchKrylov {
     cdev.alloc(sizeof(double) * (size_t)ns * (mlanc + 1), c.stream);
     mask.alloc(sizeof(int) * ns, c.stream);
     norm.alloc(sizeof(double) * ns, c.stream);
+    active.alloc(sizeof(int) * ns, c.stream);
     SADMRG_CUDA(cudaMemsetAsync(beta.get(), 0, sizeof(double) * (size_t)ns * bs, c.stream));
     SADMRG_CUDA(cudaMallocHost(&h_coef, sizeof(S) * (size_t)ns * 2 * (mlanc + 1)));
     SADMRG_CUDA(cudaMallocHost(&h_beta, sizeof(double) * (size_t)ns * bs));
     SADMRG_CUDA(cudaMallocHost(&h_dots, sizeof(S) * (size_t)ns * 2));
     SADMRG_CUDA(cudaMallocHost(&h_cdev, sizeof(double) * (size_t)ns * (mlanc + 1)));
     SADMRG_CUDA(cudaMallocHost(&h_mask, sizeof(int) * ns));
+    SADMRG_CUDA(cudaMallocHost(&h_active, sizeof(int) * ns));
+    std::fill(h_active, h_active + ns, 1);
+    SADMRG_CUDA(cudaMemcpyAsync(active.get(), h_active, sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
   }
   ~BatchKrylov() {
     cudaStreamSynchronize(c.stream);
@@ -126,6 +132,7 @@ struct BatchKrylov {
     cudaFreeHost(h_dots);
     cudaFreeHost(h_cdev);
     cudaFreeHost(h_mask);
+    cudaFreeHost(h_active);
   }
   S* F(int i) { return ff.as<S>() + (size_t)i * N; }
 };
@@ -144,8 +151,17 @@ BatchStats batch_lanczos1(Ctx& c, const HeffBatch<S>& B, S* v, int mlanc, int pr
   st.matvecs.assign(ns, 0);
   std::vector<char> done(ns, 0);
   std::vector<std::vector<double>> aal(ns, std::vector<double>(mlanc, 0.0)), nnl(ns, std::vector<double>(mlanc + 1, 0.0));
+  // Converged instances are switched off in the matvec (their jobs skip all
+  // work; their segments of the output keep stale values that nothing reads).
   auto matvec = [&](const S* in, S* out) {
-    H.apply(c, in, out, prec);
+    c.job_mask = K.active.template as<int>();
+    try {
+      H.apply(c, in, out, prec);
+    } catch (...) {
+      c.job_mask = nullptr;
+      throw;
+    }
+    c.job_mask = nullptr;
     ++st.launches_matvec;
     for (int s = 0; s < ns; ++s)
       if (!done[s]) ++st.matvecs[s];
@@ -266,15 +282,19 @@ BatchStats batch_lanczos1(Ctx& c, const HeffBatch<S>& B, S* v, int mlanc, int pr
       if (!any) continue;
       ritz(m + 1);
       check();
-      bool all = true;
+      bool all = true, changed = false;
       for (int s = 0; s < ns; ++s) {
         if (K.h_mask[s] && (finishing[s] || std::fabs(ov[s] - 1.0) < c.lanczos_ov_tol)) {
           done[s] = 1;
           st.energy[s] = e0[s];
+          K.h_active[s] = 0;
+          changed = true;
         }
         if (!done[s]) all = false;
       }
       if (all) return st;
+      if (changed)   // check() synchronised the stream, so h_active is not being read by an earlier copy
+        SADMRG_CUDA(cudaMemcpyAsync(K.active.get(), K.h_active, sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
     }
   }
   // instances still open after mlanc - 1 steps: one more matvec, then the Ritz vector

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_f64_ms(const GemmTerm* __re
                                                             const GemmJob* __restrict__ jobs,
                                                             const WorkItem* __restrict__ items, Bases bases,
                                                             double* __restrict__ work,
-                                                            const RedItem* __restrict__ reds, int* tile_cnt) {
+                                                            const RedItem* __restrict__ reds, int* tile_cnt, const int* mask) {
   static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
   constexpr int SK = BM + 4;        // k-major row stride (rows of m or n)
   constexpr int SM = BK + 4;        // m/n-major row stride (rows of k)
@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_f64_ms(const GemmTerm* __re
   __shared__ int sh_flags[STAGES];
   const WorkItem it = items[blockIdx.x];
   const GemmJob J = jobs[it.job];
+  if (mask && !mask[J.tag]) return;   // instance switched off for this launch
   const int row0 = it.tm * BM, col0 = it.tn * BN;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* _
                                                                const GemmJob* __restrict__ jobs,
                                                                const WorkItem* __restrict__ items, Bases bases,
                                                                double* __restrict__ work,
-                                                               const RedItem* __restrict__ reds, int* tile_cnt) {
+                                                               const RedItem* __restrict__ reds, int* tile_cnt, const int* mask) {
   static_assert(BM == 64 && BN == 64 && BK == 16, "layout strides assume 64 x 64 x 16");
   constexpr int SK = BM + 4, SM = BK + 4;
   constexpr int ABUF = (BM * SM > BK * SK) ? BM * SM : BK * SK;
@@ -326,6 +327,7 @@ __global__ void __launch_bounds__(kThreads, 3) items_tf32x3_ms(const GemmTerm* _
   __shared__ int sh_flags[STAGES];
   const WorkItem it = items[blockIdx.x];
   const GemmJob J = jobs[it.job];
+  if (mask && !mask[J.tag]) return;   // instance switched off for this launch
   const int row0 = it.tm * BM, col0 = it.tn * BN;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -462,13 +464,14 @@ template <int BM, int BN, int BK>
 __global__ void __launch_bounds__(kThreads) items_z64(const GemmTerm* __restrict__ terms, const GemmJob* __restrict__ jobs,
                                                       const WorkItem* __restrict__ items, Bases bases,
                                                       double2* __restrict__ work, const RedItem* __restrict__ reds,
-                                                      int* tile_cnt) {
+                                                      int* tile_cnt, const int* mask) {
   constexpr int PAD = 4;
   __shared__ double Ar[2][BK][BM + PAD], Ai[2][BK][BM + PAD];
   __shared__ double Br[2][BK][BN + PAD], Bi[2][BK][BN + PAD];
   using SL = Slab<double2, BM, BN, BK>;
   const WorkItem it = items[blockIdx.x];
   const GemmJob J = jobs[it.job];
+  if (mask && !mask[J.tag]) return;   // instance switched off for this launch
   const int row0 = it.tm * BM, col0 = it.tn * BN;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -575,7 +578,7 @@ __global__ void __launch_bounds__(kThreads) items_tf32x3(const GemmTerm* __restr
                                                          const GemmJob* __restrict__ jobs,
                                                          const WorkItem* __restrict__ items, Bases bases,
                                                          void* __restrict__ work, const RedItem* __restrict__ reds,
-                                                         int* tile_cnt) {
+                                                         int* tile_cnt, const int* mask) {
   constexpr int PAD = 8;
   constexpr int NP = CPLX ? 2 : 1;
   using V = typename std::conditional<CPLX, double2, double>::type;
@@ -584,6 +587,7 @@ __global__ void __launch_bounds__(kThreads) items_tf32x3(const GemmTerm* __restr
   __shared__ uint32_t Bh[2][NP][BK][BN + PAD], Bl[2][NP][BK][BN + PAD];
   const WorkItem it = items[blockIdx.x];
   const GemmJob J = jobs[it.job];
+  if (mask && !mask[J.tag]) return;   // instance switched off for this launch
   const int row0 = it.tm * BM, col0 = it.tn * BN;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -750,11 +754,12 @@ int gemm_tile_m(bool cplx, int /*prec*/) { return cplx ? 32 : 64; }
 int gemm_tile_n(bool cplx, int /*prec*/) { return cplx ? 32 : 64; }
 
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
-                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, cudaStream_t s) {
+                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, const int* mask,
+                  cudaStream_t s) {
   if (nitems <= 0) return;
   if (prec == PREC_TF32X3) {
     if (cplx) {
-      items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work, reds, tile_cnt);
+      items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work, reds, tile_cnt, mask);
     } else {
       static bool attr = false;
       if (!attr) {
@@ -764,12 +769,12 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
       }
       items_tf32x3_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
                                                                                  static_cast<double*>(work), reds,
-                                                                                 tile_cnt);
+                                                                                 tile_cnt, mask);
     }
   } else {
     if (cplx) {
       items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work), reds,
-                                                          tile_cnt);
+                                                          tile_cnt, mask);
     } else {
       static bool attr = false;
       if (!attr) {
@@ -779,7 +784,7 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
       }
       items_f64_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
                                                                               static_cast<double*>(work), reds,
-                                                                              tile_cnt);
+                                                                              tile_cnt, mask);
     }
   }
 }

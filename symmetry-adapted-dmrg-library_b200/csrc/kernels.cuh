@@ -27,6 +27,8 @@ struct GemmJob {              // C (m x n, column-major, ldc) receives its terms
   long long coff;
   int cbuf, m, n, ldc;
   int t0, nt, flags;
+  int tag;                    // instance of a merged batch plan (0 otherwise): a launch given a mask
+                              // skips every item of a job whose mask[tag] is 0
 };
 struct GemmTile {
   int job, tm, tn;
@@ -52,8 +54,9 @@ enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).
 // Split items write partial tiles; the last of a tile's items sums them (tile_cnt
 // holds one zeroed counter per RedItem and is left zeroed).
+// mask: null, or per job tag; items of a job with mask[tag] == 0 do nothing.
 void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* jobs, const WorkItem* items, int nitems,
-                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, cudaStream_t s);
+                  const Bases& b, void* work, const RedItem* reds, int* tile_cnt, const int* mask, cudaStream_t s);
 
 // ---- tcgen05 3xTF32 over TF32 hi/lo operand panels (umma.cu) --------------
 // An operand (rows x K after op) is stored as panels: panel (p, s) holds rows
@@ -83,6 +86,7 @@ struct UJob {                 // output tile grid of one job
   double alpha;
   int cbuf, m, n, ldc, flags, t0, nt, pack_nslab;
   int dep;                    // counter bumped per finished tile (results read as panels later), or -1
+  int tag;                    // as GemmJob::tag
 };
 struct UItem {                // one output tile x a run of consecutive slabs
   int job, tm, tn, t0, s0, nslab, slot;   // t0: first term (absolute), s0: its first slab; slot < 0: direct
@@ -99,6 +103,7 @@ struct UBufs {
   int* deps;                  // dependency counters (psi pack jobs, then stage-0 results), zero between launches
   const int* dep_target;      // value each counter reaches once its panels are complete
   unsigned* fin;              // CTAs finished (the last one clears deps)
+  const int* mask;            // null, or per job tag: 0 skips the job's items (not with wait_deps)
 };
 constexpr int kMaxPackJobs = 1024;   // psi pack jobs one fused launch can count
 struct UPhase {               // what one launch does besides its items

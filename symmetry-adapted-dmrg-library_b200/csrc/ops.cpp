@@ -348,6 +348,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     u.flags = J.flags;
     u.t0 = J.t0;
     u.nt = J.nt;
+    u.tag = J.tag;
     u.dep = -1;
     if (J.cbuf == 3) {
       auto it = xreader.find(J.coff);
@@ -520,13 +521,14 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
     ub.deps = U.deps->as<int>();
     ub.dep_target = U.d_dep_target;
     ub.fin = reinterpret_cast<unsigned*>(U.deps->as<int>() + U.dep_target.size());
+    ub.mask = c.job_mask;
     UPhase ph{};
     ph.pk = U.d_vpack;
     ph.pk_blk = U.d_vblk;
     ph.npk_jobs = (int)U.vpack.size();
     ph.ndeps = (int)U.dep_target.size();
     const bool whole = stage_lo == 0 && stage_hi == nstage;
-    if (whole && c.fused_matvec && (int)U.vpack.size() <= kMaxPackJobs) {
+    if (whole && c.fused_matvec && !c.job_mask && (int)U.vpack.size() <= kMaxPackJobs) {
       // the whole matvec in one cooperative launch: psi packing, stage 0, stage 1
       ph.npk_blocks = (int)U.vblk.size();
       ph.wait_deps = 1;
@@ -559,7 +561,7 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
     const int ni = sched.stage_items[s + 1] - sched.stage_items[s];
     if (ni > 0) {
       launch_items(cplx, prec, d_terms, d_jobs, sched.d_items + sched.stage_items[s], ni, b, wk, sched.d_reds,
-                   sched.tile_cnt->as<int>(), c.stream);
+                   sched.tile_cnt->as<int>(), c.job_mask, c.stream);
       ++c.launches;
       mark(c, 1 + 2 * s);
     }

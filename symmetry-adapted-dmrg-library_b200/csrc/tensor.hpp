@@ -33,6 +33,7 @@ struct Ctx {
   int npart = 296;
   double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
   bool fused_matvec = false;     // tcgen05 matvec as one cooperative launch instead of pack + two launches
+  const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
   // when set, GemmPlan::run records an event after every launch (what ran, event)

@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
       };
       for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x) {
         const UItem it = items[ii];
+        if (ub.mask && !ub.mask[jobs[it.job].tag]) continue;   // instance switched off for this launch
         int t = it.t0, s = it.s0;
         for (int q = 0; q < it.nslab; ++q) {
           while (s >= terms[t].nslab) { ++t; s = 0; }
@@ -335,8 +336,9 @@ __global__ void __launch_bounds__(kGThreads, 1)
       int il = 0;
       uint32_t last_bar = 0, last_par = 0;
       bool committed = false;
-      for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x, ++il) {
+      for (int ii = blockIdx.x; ii < nitems && !abort_sh; ii += gridDim.x) {
         const UItem it = items[ii];
+        if (ub.mask && !ub.mask[jobs[it.job].tag]) continue;
         const int acc = il & 1;
         if (!mbar_wait(saddr(&tempty[acc]), (((uint32_t)il >> 1) & 1u) ^ 1u, &abort_sh)) {
           if (!abort_sh) atomicExch(&g_umma_status, 5);
@@ -384,6 +386,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         last_bar = saddr(&tfull[acc]);
         last_par = ((uint32_t)il >> 1) & 1u;
         committed = true;
+        ++il;
       }
       // every MMA this thread issued has finished before tensor memory is freed
       if (committed && !mbar_wait(last_bar, last_par, nullptr)) atomicExch(&g_umma_status, 7);
@@ -396,9 +399,10 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const int et = tid - 64;                // 0..127 within the epilogue warps
     // The four epilogue warps take every decision together: a failed wait is
     // posted to ep_fail and read by all after the same named barrier (id 1).
-    for (int ii = blockIdx.x; ii < nitems; ii += gridDim.x, ++il) {
+    for (int ii = blockIdx.x; ii < nitems; ii += gridDim.x) {
       const UItem it = items[ii];
       const UJob J = jobs[it.job];
+      if (ub.mask && !ub.mask[J.tag]) continue;
       const int acc = il & 1;
       if (!mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh)) {
         if (!abort_sh) atomicExch(&g_umma_status, 8);
@@ -496,6 +500,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         if (last_sh) signal_tile();
         asm volatile("bar.sync 1, 128;" ::: "memory");
       }
+      ++il;
     }
   }
 
