@@ -182,6 +182,12 @@ int sadmrg_svd_truncate(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const s
  * L sites is lx = 1, ly = L); open = 1 drops the periodic wrap; J2 adds
  * next-nearest-neighbour couplings along the site order. */
 int sadmrg_chain_create(sadmrg_handle* h, int lx, int ly, int bondd, int physpn, int totspin, int open, double J2);
+/* Adds Dz (S_a x S_b)_z on every J1 bond a < b (chain order) of a U(1) complex
+ * chain: the bond's S+_a S-_b and S-_a S+_b parts get (J + i Dz)/2 and
+ * (J - i Dz)/2.  Call before sadmrg_chain_idmrg / sadmrg_chain_read_mps.  No
+ * counterpart in the reference (one real coupling per pair, coup[] in
+ * src/dmrg_inst.cpp:146-160); SADMRG_ERR_ARG for SU(2) or real scalars. */
+int sadmrg_chain_set_dm(sadmrg_handle* h, double dz);
 int sadmrg_chain_set_precision(sadmrg_handle* h, int precision);
 int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy);
 int sadmrg_chain_prepare_sweep(sadmrg_handle* h);

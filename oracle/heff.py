@@ -55,8 +55,18 @@ def contract2(t1: BT, i1: int, t2: BT, i2: int) -> BT:
     return out
 
 
-def heff_apply(vec: BT, hh_l, hh_r, opr_l: dict, opr_r: dict, hmap: dict, coup, il: int, ir: int, ns: int) -> BT:
-    """H_eff * psi for the ground state (no excited-state penalty)."""
+def channel_scaled(src: BT, J: float, dz: float) -> BT:
+    """src with each block scaled by J - i dz q / 2, q its channel (leg 1) charge: the U(1)
+    pair coupling of a J1 bond with a DM term Dz (S_a x S_b)_z, a < b (charge -2 pairs
+    S+_a S-_b, +2 pairs S-_a S+_b).  Not in the reference (one real coupling per pair)."""
+    out = src.zeros_like()
+    out.blocks = {k: (J - 0.5j * dz * k[1]) * v for k, v in src.blocks.items()}
+    return out
+
+
+def heff_apply(vec: BT, hh_l, hh_r, opr_l: dict, opr_r: dict, hmap: dict, coup, il: int, ir: int, ns: int,
+               dz: float = 0.0) -> BT:
+    """H_eff * psi for the ground state (no excited-state penalty); dz: DM term on J1 bonds (U(1))."""
     if hh_l is None and hh_r is None:
         vec2 = vec.zeros_like()
         vec2.blocks = {k: np.zeros_like(v) for k, v in vec.blocks.items()}
@@ -79,7 +89,10 @@ def heff_apply(vec: BT, hh_l, hh_r, opr_l: dict, opr_r: dict, hmap: dict, coup, 
             if h > 0:
                 src = opr_r.get(k) if il < ns // 2 else opr_l.get(j)
                 if src is not None:
-                    op = add_into(op, src, coup[h])
+                    if h == 1 and dz != 0.0:
+                        op = add_into(op, channel_scaled(src, coup[h], dz))
+                    else:
+                        op = add_into(op, src, coup[h])
         if op is None:
             continue
         j, k = (m0, None) if il < ns // 2 else (None, ir + m0)

@@ -719,6 +719,37 @@ void Chain<S>::init_local_operators() {
   }
 }
 
+// op += (coupling of the pair a < b) * src.  On J1 bonds with a DM term,
+// J S_a.S_b + Dz (S_a x S_b)_z = J Sz Sz + (J + i Dz)/2 S+_a S-_b + (J - i Dz)/2 S-_a S+_b,
+// and the U(1) channel leg labels these parts: charge -2 pairs S+_a with S-_b
+// (sigma[0] holds S+/sqrt2 at channel -2), 0 pairs Sz with Sz, +2 pairs S-_a
+// with S+_b; both operators of a pair carry the same label, so weighting the
+// summed side's channels by (J + i Dz, J, J - i Dz) adds the term.  Not in the
+// reference, whose couplings are one real scalar per pair.
+template <class S>
+void Chain<S>::add_coupled(BTensor<S>& op, const BTensor<S>& src, int a, int b) {
+  const int h = hmap[a][b];
+  const double J = coup[h];
+  if constexpr (kCx<S>) {
+    if (h == 1 && dz != 0.0) {
+      const S w[3] = {S(J, dz), S(J, 0.0), S(J, -dz)};
+      ops::add_into_channels<S>(c, op, src, w);
+      return;
+    }
+  }
+  ops::add_into<S>(c, op, src, S(J));
+}
+
+template <class S>
+void Chain<S>::set_dm(double d) {
+  SADMRG_REQUIRE(d == 0.0 || (c.sym == Sym::U1 && kCx<S>), SADMRG_ERR_ARG,
+                 "chain: the DM term needs U(1) symmetry and complex scalars");
+  for (int i = 0; i < ns; ++i)
+    SADMRG_REQUIRE(uu[i].null() && hh[i].null(), SADMRG_ERR_STATE,
+                   "chain: set the DM term before iDMRG or loading a checkpoint");
+  dz = d;
+}
+
 template <class S>
 void Chain<S>::random_init(BTensor<S>& t) {
   std::vector<S> h(t.nelem);
@@ -751,7 +782,7 @@ void Chain<S>::prepare_site_operator_from_left(int i, bool real_env) {
     if (fll[i][k] == 1) newopr[k] = ops::operator_transformation<S>(c, U, U, opr[i - 1][k], 0);
   BTensor<S> op;
   for (int m = 0; m < i; ++m)
-    if (hmap[i][m] > 0) ops::add_into<S>(c, op, opr[i - 1][m], S(coup[hmap[i][m]]));
+    if (hmap[i][m] > 0) add_coupled(op, opr[i - 1][m], m, i);
   if (!op.null()) {
     BTensor<S> ht = ops::operator_pairup<S>(c, U, U, op, sigma[1], 0);
     ops::add_into<S>(c, hnew, ht, S(1.0));
@@ -786,7 +817,7 @@ void Chain<S>::prepare_site_operator_from_right(int i, bool real_env) {
   BTensor<S> op;
   for (int m = 0; m < ns - 1 - i; ++m) {
     const int k = i + 1 + m;
-    if (hmap[i][k] > 0) ops::add_into<S>(c, op, opr[i + 1][k], S(coup[hmap[i][k]]));
+    if (hmap[i][k] > 0) add_coupled(op, opr[i + 1][k], i, k);
   }
   if (!op.null()) {
     BTensor<S> ht = ops::operator_pairup<S>(c, U, U, op, sigma[0], 1);
@@ -851,7 +882,7 @@ HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec) {
     for (int m = 0; m < m4; ++m) {
       if (il < ns / 2) k = ir + m;
       else j = m;
-      if (hmap[j][k] > 0) ops::add_into<S>(c, op, il < ns / 2 ? opr[ir][k] : opr[il][j], S(coup[hmap[j][k]]));
+      if (hmap[j][k] > 0) add_coupled(op, il < ns / 2 ? opr[ir][k] : opr[il][j], j, k);
     }
     if (op.null()) continue;
     sums.push_back(std::move(op));
@@ -1120,7 +1151,7 @@ static void write_tensor(Ctx& c, const BTensor<S>& t, const std::string& base) {
     for (int b = 0; b < t.st.nbond(); ++b) std::fprintf(f, " %d", q[b]);
     std::fprintf(f, " d");
     for (int b = 0; b < t.st.nbond(); ++b) std::fprintf(f, " %d", d[b]);
-    std::fprintf(f, " off %lld n %lld\n", t.off[i], t.st.block_elems(i));
+    std::fprintf(f, " off %lld n %lld\n", (long long)t.off[i], (long long)t.st.block_elems(i));
   }
   std::fclose(f);
   std::vector<S> h = ops::to_host<S>(c, t);
@@ -1142,8 +1173,8 @@ void Chain<S>::export_problem(int il, const BTensor<S>& psi, const std::string& 
   }
   FILE* f = std::fopen((dir + "/meta.txt").c_str(), "w");
   SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "export: cannot write meta");
-  std::fprintf(f, "sym %d cplx %d ns %d lx %d ly %d D %d sec %d il %d ir %d J2 %.17g open 1 maxangm 0\n",
-               c.sym == Sym::SU2 ? 1 : 0, kCx<S> ? 1 : 0, ns, lx, ly, bondd, totspin, il, ir, coup[2]);
+  std::fprintf(f, "sym %d cplx %d ns %d lx %d ly %d D %d sec %d il %d ir %d J2 %.17g open 1 maxangm 0 dz %.17g\n",
+               c.sym == Sym::SU2 ? 1 : 0, kCx<S> ? 1 : 0, ns, lx, ly, bondd, totspin, il, ir, coup[2], dz);
   std::fprintf(f, "coup");
   for (int k = 0; k <= ns / 2; ++k) std::fprintf(f, " %.17g", coup[k]);
   std::fprintf(f, "\n");

@@ -132,6 +132,8 @@ class Chain {
   void prepare_sweep();
   void sweep();
   double energy() const { return gs_enr; }
+  // Dz (S_a x S_b)_z on every J1 bond a < b (U(1), complex only; before iDMRG)
+  void set_dm(double d);
 
   // building blocks (public for the frozen-problem API and tests)
   void prepare_site_operator_from_left(int i, bool real_env);
@@ -155,6 +157,7 @@ class Chain {
   int max_dcut;
   std::vector<std::vector<int>> hmap, fll, frr;
   std::vector<double> coup;
+  double dz = 0.0;            // DM coupling on J1 bonds (set_dm)
   std::vector<BTensor<S>> uu, hh;
   std::vector<std::vector<BTensor<S>>> opr;
   std::array<BTensor<S>, 2> sigma;
@@ -174,6 +177,7 @@ class Chain {
   void random_init(BTensor<S>& t);
   void init_local_operators();
   void svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2);
+  void add_coupled(BTensor<S>& op, const BTensor<S>& src, int a, int b);
 };
 
 }  // namespace sadmrg

@@ -991,13 +991,21 @@ BTensor<S> contract(Ctx& c, const BTensor<S>& t1, int i1, const BTensor<S>& t2, 
   return out;
 }
 
+// dst += alpha_b * src block by block (BlockTensor::operator+= presence rules,
+// src/block_tensor_inst.cpp:225-252); alpha_b = alpha, or alpha * chan_w[(q + 2) / 2]
+// with q the U(1) charge of the block's channel leg (bond 1) when chan_w is given.
 template <class S>
-void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha) {
+static void add_into_impl(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha, const S* chan_w) {
   if (src.null()) return;
   if (dst.null()) {
-    dst = clone(c, src);
-    if (alpha != S(1)) scale(c, dst, alpha);
-    return;
+    if (!chan_w) {
+      dst = clone(c, src);
+      if (alpha != S(1)) scale(c, dst, alpha);
+      return;
+    }
+    std::vector<char> pres(src.nten(), 0);
+    for (long i = 0; i < src.nten(); ++i) pres[i] = src.present(i);
+    dst = alloc_tensor<S>(c, src.st, pres);   // zero-filled
   }
   SADMRG_REQUIRE(dst.st == src.st, SADMRG_ERR_ARG, "add_into: different structures");
   bool same = true;
@@ -1013,8 +1021,18 @@ void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha) {
       if (dst.present(i)) sd.push_back(Seg{target.off[i], dst.off[i], dst.st.block_elems(i), 1.0, 0.0});
   }
   BTensor<S>& T = same ? dst : target;
-  for (long i = 0; i < src.nten(); ++i)
-    if (src.present(i)) ss.push_back(Seg{T.off[i], src.off[i], src.st.block_elems(i), re_of(alpha), im_of(alpha)});
+  int q[8], d[8];
+  for (long i = 0; i < src.nten(); ++i) {
+    if (!src.present(i)) continue;
+    S a = alpha;
+    if (chan_w) {
+      src.st.block(i, q, d);
+      const int ci = (q[1] + 2) / 2;
+      SADMRG_REQUIRE(ci >= 0 && ci < 3 && q[1] % 2 == 0, SADMRG_ERR_ARG, "add_into: channel charge outside {-2,0,2}");
+      a = alpha * chan_w[ci];
+    }
+    ss.push_back(Seg{T.off[i], src.off[i], src.st.block_elems(i), re_of(a), im_of(a)});
+  }
   DevBuf dsegs(sizeof(Seg) * (sd.size() + ss.size()) + 16, c.stream);
   std::vector<Seg> all = sd;
   all.insert(all.end(), ss.begin(), ss.end());
@@ -1026,6 +1044,17 @@ void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha) {
   }
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
   if (!same) dst = std::move(target);
+}
+
+template <class S>
+void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha) {
+  add_into_impl<S>(c, dst, src, alpha, nullptr);
+}
+
+template <class S>
+void add_into_channels(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, const S chan_w[3]) {
+  SADMRG_REQUIRE(c.sym == Sym::U1, SADMRG_ERR_ARG, "add_into_channels: U(1) operators only");
+  add_into_impl<S>(c, dst, src, S(1), chan_w);
 }
 
 template <class S>
@@ -1143,6 +1172,7 @@ std::vector<S> to_host(Ctx& c, const BTensor<S>& t) {
                                          const BTensor<S>&, int);                                                \
   template BTensor<S> contract<S>(Ctx&, const BTensor<S>&, int, const BTensor<S>&, int);                         \
   template void add_into<S>(Ctx&, BTensor<S>&, const BTensor<S>&, S);                                            \
+  template void add_into_channels<S>(Ctx&, BTensor<S>&, const BTensor<S>&, const S*);                            \
   template void scale<S>(Ctx&, BTensor<S>&, S);                                                                  \
   template void take_conjugate<S>(BTensor<S>&, int);                                                             \
   template void makeup_input_vector<S>(Ctx&, BTensor<S>&);                                                       \

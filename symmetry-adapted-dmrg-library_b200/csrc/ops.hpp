@@ -27,6 +27,8 @@ template <class S> BTensor<S> contract(Ctx& c, const BTensor<S>& t1, int i1, con
 
 // dst = dst (+) alpha * src with the reference's operator+= presence rules
 template <class S> void add_into(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, S alpha);
+// U(1) only: dst += chan_w[(q + 2) / 2] * (the blocks of src whose channel leg, bond 1, has charge q)
+template <class S> void add_into_channels(Ctx& c, BTensor<S>& dst, const BTensor<S>& src, const S chan_w[3]);
 template <class S> void scale(Ctx& c, BTensor<S>& t, S alpha);
 template <class S> void take_conjugate(BTensor<S>& t, int bond);
 template <class S> void makeup_input_vector(Ctx& c, BTensor<S>& t);

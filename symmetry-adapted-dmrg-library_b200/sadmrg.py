@@ -30,7 +30,7 @@ EXPORTED = [
     "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
     "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device", "sadmrg_heff_apply_noalloc",
     "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
-    "sadmrg_chain_create", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
+    "sadmrg_chain_create", "sadmrg_chain_set_dm", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
@@ -90,6 +90,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
+        "sadmrg_chain_set_dm": ([vp, C.c_double], C.c_int),
         "sadmrg_chain_idmrg": ([vp, dp], C.c_int),
         "sadmrg_chain_prepare_sweep": ([vp], C.c_int),
         "sadmrg_chain_sweep": ([vp, dp], C.c_int),
@@ -404,6 +405,10 @@ class Handle:
         self._check(self.lib.sadmrg_chain_create(self.h, lx, ly, bondd, physpn, totspin, int(bool(open_bc)),
                                                  float(J2)), "chain_create")
 
+    def chain_set_dm(self, dz: float):
+        """Dz (S_a x S_b)_z on every J1 bond (U(1) complex chains, before iDMRG)."""
+        self._check(self.lib.sadmrg_chain_set_dm(self.h, float(dz)), "chain_set_dm")
+
     def chain_set_precision(self, prec: int):
         self._check(self.lib.sadmrg_chain_set_precision(self.h, int(prec)), "chain_set_precision")
 
@@ -511,6 +516,19 @@ def write_exported_tensor(directory: str, name: str, t: BlockTensorData) -> None
     np.ascontiguousarray(t.data).tofile(os.path.join(directory, name + ".bin"))
 
 
+def channel_weights(t: BlockTensorData, J: float, dz: float) -> np.ndarray:
+    """Per-element coupling of a U(1) operator on a J1 bond with a DM term: J - i dz q / 2,
+    q the charge of the block's channel leg (bond 1), as sadmrg_chain_set_dm defines it."""
+    w = np.empty(t.data.size, np.complex128)
+    off = 0
+    for bi in t.blocks:
+        lab = t.block_labels(int(bi))
+        n = int(np.prod([t.ds[b][lab[b]] for b in range(t.nbond)]))
+        w[off:off + n] = J - 0.5j * dz * t.qs[1][lab[1]]
+        off += n
+    return w
+
+
 def load_exported_problem(h: "Handle", directory: str) -> BlockTensorData:
     """Plan H_eff*psi on a problem exported by sadmrg_chain_freeze (the reference's operator set)."""
     meta = open(os.path.join(directory, "meta.txt")).read().split("\n")
@@ -518,6 +536,7 @@ def load_exported_problem(h: "Handle", directory: str) -> BlockTensorData:
     m = {kv[i]: kv[i + 1] for i in range(0, len(kv) - 1, 2)}
     il, ir, ns = int(m["il"]), int(m["ir"]), int(m["ns"])
     coup = [float(x) for x in meta[1].split()[1:]]
+    dz = float(m.get("dz", 0.0))
     hmap = {}
     for line in meta[2:]:
         t = line.split()
@@ -540,12 +559,15 @@ def load_exported_problem(h: "Handle", directory: str) -> BlockTensorData:
             t = read_exported_tensor(directory, f"opr_ir_{k}" if left else f"opr_il_{j}", cplx)
             if t is None:
                 continue
+            w = coup[hv]
+            if hv == 1 and dz != 0.0:
+                w = channel_weights(t, coup[hv], dz)
             if acc is None:
-                acc = BlockTensorData(t.dirs, t.qs, t.ds, t.locspin, t.blocks.copy(), coup[hv] * t.data)
+                acc = BlockTensorData(t.dirs, t.qs, t.ds, t.locspin, t.blocks.copy(), w * t.data)
             else:
                 if list(acc.blocks) != list(t.blocks):
                     raise ValueError("summed operators with different block sets are not supported here")
-                acc.data = acc.data + coup[hv] * t.data
+                acc.data = acc.data + w * t.data
         if acc is None:
             continue
         fixed = read_exported_tensor(directory, f"opr_il_{m0}" if left else f"opr_ir_{ir + m0}", cplx)
