@@ -65,6 +65,13 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
 // zero padded; it starts at dst + (p * nslab + s) * T * 256 bytes.  This is the
 // K-major, no-swizzle core-matrix layout tcgen05.mma reads, so a panel moves
 // into shared memory as one contiguous bulk copy.
+// Complex products run as real ones of twice the size: C = A B (complex m x n,
+// k) is Ch = Ah Bh with Ch (2m x n) and Bh (2k x n) the interleaved storage of
+// C and B read as real column-major matrices (no copy), and Ah (2m x 2k) the
+// real form of A, Ah(2i+p, 2j+q) = Re A(i,j) for p == q, -Im A(i,j) for
+// (p, q) = (0, 1), Im A(i,j) for (1, 0).  The real flop count is the complex
+// one (8 per complex multiply-add), and the pack kernel writes Ah / Bh panels
+// straight from the complex operands (cmode 1 / 2).
 constexpr int kPanelK = 32;
 constexpr int kUmmaTileM = 128;
 struct PackJob {              // FP64 matrix -> panels
@@ -72,6 +79,9 @@ struct PackJob {              // FP64 matrix -> panels
   long long dst;              // byte offset of panel (0, 0) in the packed buffer
   long long chunk0;           // first 16-byte chunk of this job in the launch (a multiple of 256)
   int srcbuf, ld, rows, K, trans, T;   // trans 0: (r, k) at src[r + k*ld]; 1: at src[k + r*ld]
+  int cmode;                  // 0 real; complex source (src, ld in complex elements, rows / K of the real
+                              // form): 1 Ah (rows 2m, K 2k), 2 Bh read as rows n x K 2k
+  int conj;                   // complex: conjugate the source elements first
 };
 struct UTerm {                // a term's operands as panel sets: A (T = 128), B (T = BN)
   long long a, b;             // byte offsets of panel (0, 0)
@@ -87,6 +97,8 @@ struct UJob {                 // output tile grid of one job
   int cbuf, m, n, ldc, flags, t0, nt, pack_nslab;
   int dep;                    // counter bumped per finished tile (results read as panels later), or -1
   int tag;                    // as GemmJob::tag
+  int cx;                     // complex plan: the tile is a real-form block (rows 2i, 2i+1 = Re, Im of
+                              // row i); panels of the result are written in the real form Xh (cmode 1)
 };
 struct UItem {                // one output tile x a run of consecutive slabs
   int job, tm, tn, t0, s0, nslab, slot;   // t0: first term (absolute), s0: its first slab; slot < 0: direct

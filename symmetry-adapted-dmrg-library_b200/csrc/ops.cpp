@@ -195,7 +195,7 @@ void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed, const Bases* const_bases)
   sched.tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(sched.reds.size(), 1), c.stream);
   SADMRG_CUDA(cudaMemsetAsync(sched.tile_cnt->get(), 0, sched.tile_cnt->bytes(), c.stream));
   umma.reset();
-  if (mixed && !cplx && const_bases) build_umma(c, *const_bases);
+  if (mixed && const_bases) build_umma(c, *const_bases, cplx);
   // the host copies must stay alive until the async copies complete
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -203,13 +203,13 @@ void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed, const Bases* const_bases)
 // tcgen05 schedule (see UmmaSchedule).  Returns false, leaving umma empty, when
 // some term does not fit the panel scheme; the plan then runs 3xTF32 on the
 // mma.sync kernels.
-bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
+bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   auto U = std::make_shared<UmmaSchedule>();
   const int nsm = device_sm_count();
   // tile width: 128 when the 128-wide output tiles alone fill the GPU twice per stage
   long long t128 = 0;
   for (size_t j = 0; j < jobs.size(); ++j)
-    t128 += (long long)((jobs[j].m + 127) / 128) * ((jobs[j].n + 127) / 128);
+    t128 += (long long)(((cplx ? 2 : 1) * jobs[j].m + 127) / 128) * ((jobs[j].n + 127) / 128);
   U->bn = (t128 >= 2LL * nsm * std::max(nstage, 1)) ? 128 : 64;
   const int BN = U->bn;
 
@@ -217,8 +217,10 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     int buf;
     long long src;
     int ld, rows, K, trans, T;
+    int cm;          // 2 * cmode + conj (PackJob)
     bool operator<(const Key& o) const {
-      return std::tie(buf, src, ld, rows, K, trans, T) < std::tie(o.buf, o.src, o.ld, o.rows, o.K, o.trans, o.T);
+      return std::tie(buf, src, ld, rows, K, trans, T, cm) <
+             std::tie(o.buf, o.src, o.ld, o.rows, o.K, o.trans, o.T, o.cm);
     }
   };
   struct Pk {
@@ -228,8 +230,8 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   };
   std::map<Key, int> index;
   std::vector<Pk> packs;
-  auto get = [&](int buf, long long src, int ld, int rows, int K, int trans, int T) -> int {
-    const Key k{buf, src, ld, rows, K, trans, T};
+  auto get = [&](int buf, long long src, int ld, int rows, int K, int trans, int T, int cm) -> int {
+    const Key k{buf, src, ld, rows, K, trans, T, cm};
     auto it = index.find(k);
     if (it != index.end()) return it->second;
     const int cls = buf == 2 ? 0 : buf == 0 ? 1 : buf == 3 ? 2 : -1;
@@ -249,11 +251,16 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     for (int t = J.t0; t < J.t0 + J.nt; ++t) {
       const GemmTerm& T = flat_terms[t];
       if (T.k == 0) continue;
-      const int a = get(T.abuf, T.aoff, T.lda, J.m, T.k, (T.flags & TF_TA) ? 1 : 0, kUmmaTileM);
-      const int b = get(T.bbuf, T.boff, T.ldb, J.n, T.k, (T.flags & TF_TB) ? 0 : 1, BN);
+      if (T.ai != 0.0) return false;
+      // complex: Ah (2m x 2k, cmode 1) times Bh (2k x n, cmode 2)
+      const int xm = cplx ? 2 : 1;
+      const int cma = cplx ? 2 + ((T.flags & TF_CA) ? 1 : 0) : 0;
+      const int cmb = cplx ? 4 + ((T.flags & TF_CB) ? 1 : 0) : 0;
+      const int a = get(T.abuf, T.aoff, T.lda, xm * J.m, xm * T.k, (T.flags & TF_TA) ? 1 : 0, kUmmaTileM, cma);
+      const int b = get(T.bbuf, T.boff, T.ldb, J.n, xm * T.k, (T.flags & TF_TB) ? 0 : 1, BN, cmb);
       if (a < 0 || b < 0 || packs[b].cls == 2) return false;
       if (packs[a].cls == 2) {
-        if (T.flags & TF_TA) return false;
+        if (T.flags & (TF_TA | TF_CA)) return false;
         auto it = xalpha.find(T.aoff);
         if (it == xalpha.end()) xalpha[T.aoff] = T.ar;
         else if (it->second != T.ar) return false;
@@ -284,6 +291,8 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
     P.K = p.k.K;
     P.trans = p.k.trans;
     P.T = p.k.T;
+    P.cmode = p.k.cm >> 1;
+    P.conj = p.k.cm & 1;
     const long long nch = (long long)((P.rows + P.T - 1) / P.T) * P.T * nslab_of(P.K) * 8;
     long long& cc = p.cls == 0 ? U->cchunks : U->vchunks;
     auto& blk = p.cls == 0 ? U->cblk : U->vblk;
@@ -313,7 +322,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   for (size_t t = 0; t < flat_terms.size(); ++t) {
     UTerm u{};
     u.adep = u.bdep = -1;
-    const int K = flat_terms[t].k;
+    const int K = (cplx ? 2 : 1) * flat_terms[t].k;
     if (K > 0) {
       u.adep = dep_of(ta[t]);
       u.bdep = dep_of(tb[t]);
@@ -337,14 +346,16 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   U->jobs.resize(jobs.size());
   for (size_t j = 0; j < jobs.size(); ++j) {
     const GemmJob& J = jobs[j];
+    const int xm = cplx ? 2 : 1;   // complex: the real form of C (interleaved storage read as real)
     UJob u{};
-    u.coff = J.coff;
+    u.coff = xm * J.coff;
     u.pack = -1;
     u.alpha = 1.0;
     u.cbuf = J.cbuf;
-    u.m = J.m;
+    u.m = xm * J.m;
     u.n = J.n;
-    u.ldc = J.ldc;
+    u.ldc = xm * J.ldc;
+    u.cx = cplx ? 1 : 0;
     u.flags = J.flags;
     u.t0 = J.t0;
     u.nt = J.nt;
@@ -354,10 +365,12 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
       auto it = xreader.find(J.coff);
       if (it == xreader.end() || job_stage[j] != 0 || (J.flags & JF_ACCUM)) return false;
       const Key& k = packs[it->second].k;
-      if (k.rows != J.m || k.K != J.n || k.ld != J.ldc || k.trans != 0 || k.T != kUmmaTileM) return false;
+      if (k.rows != xm * J.m || k.K != xm * J.n || k.ld != J.ldc || k.trans != 0 || k.T != kUmmaTileM ||
+          k.cm != (cplx ? 2 : 0))
+        return false;
       u.pack = packs[it->second].dst;
       u.alpha = xalpha[J.coff];
-      u.pack_nslab = nslab_of(J.n);
+      u.pack_nslab = nslab_of(xm * J.n);
       u.dep = xdep[J.coff];
       ++produced;
     } else if (J.cbuf != 1) {
@@ -371,7 +384,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
   for (size_t j = 0; j < jobs.size(); ++j)
     if (U->jobs[j].dep >= 0)
       U->dep_target[U->jobs[j].dep] =
-          ((jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);   // tiles of the result
+          ((U->jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);   // tiles of the result
 
   // slab-granular items, longest first; split the reduction only when the
   // output tiles cannot keep every SM busy
@@ -385,7 +398,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
       if (job_stage[j] != s) continue;
       long long ns = 0;
       for (int t = jobs[j].t0; t < jobs[j].t0 + jobs[j].nt; ++t) ns += U->terms[t].nslab;
-      const long long tiles = (long long)((jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);
+      const long long tiles = (long long)((U->jobs[j].m + kUmmaTileM - 1) / kUmmaTileM) * ((jobs[j].n + BN - 1) / BN);
       ntile += tiles;
       total += tiles * std::max<long long>(ns, 1);
     }
@@ -398,7 +411,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb) {
       long long ns = 0;
       for (int t = J.t0; t < J.t0 + J.nt; ++t) ns += U->terms[t].nslab;
       if (ns == 0 && (J.flags & JF_ACCUM)) continue;
-      const int tm = (J.m + kUmmaTileM - 1) / kUmmaTileM, tn = (J.n + BN - 1) / BN;
+      const int tm = (U->jobs[j].m + kUmmaTileM - 1) / kUmmaTileM, tn = (J.n + BN - 1) / BN;
       const long long nch = std::max<long long>(1, (ns + kc - 1) / kc);
       for (int a = 0; a < tm; ++a)
         for (int b = 0; b < tn; ++b) {

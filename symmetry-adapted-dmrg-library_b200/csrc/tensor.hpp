@@ -85,10 +85,12 @@ struct GemmSchedule {
   size_t work_bytes() const { return work ? work->bytes() : 0; }
 };
 
-// The tcgen05 schedule of a real plan: operand panels, panel-addressed terms,
-// jobs, slab-granular items (umma.cu).  Built only when every term fits the
-// panel scheme (constant operands in buffer 2, psi in buffer 0, stage-0 results
-// in buffer 3 consumed only as untransposed A operands with one alpha each).
+// The tcgen05 schedule of a plan: operand panels, panel-addressed terms, jobs,
+// slab-granular items (umma.cu); complex plans run in the real form of every
+// product (kernels.cuh).  Built only when every term fits the panel scheme
+// (constant operands in buffer 2, psi in buffer 0, stage-0 results in buffer 3
+// consumed only as untransposed A operands with one real alpha each, other
+// terms with coefficient 1).
 struct UmmaSchedule {
   int bn = 64;
   std::vector<PackJob> cpack, vpack;       // constant panels (packed once), psi panels (every apply)
@@ -136,7 +138,7 @@ struct GemmPlan {
   // mixed: also build the tcgen05 schedule; its constant panels are packed from
   // const_bases (buffer 2) on the context's stream.
   void finalize(Ctx& c, bool cplx, bool mixed = false, const Bases* const_bases = nullptr);
-  bool uses_umma(bool cplx, int prec) const { return prec == PREC_TF32X3 && !cplx && umma != nullptr; }
+  bool uses_umma(bool /*cplx*/, int prec) const { return prec == PREC_TF32X3 && umma != nullptr; }
   void run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo = 0, int stage_hi = -1,
            void* work_override = nullptr) const;
   // bytes of split-K workspace a run at this precision uses
@@ -148,7 +150,7 @@ struct GemmPlan {
 
  private:
   void build_schedule(GemmSchedule& s, bool cplx);
-  bool build_umma(Ctx& c, const Bases& cb);
+  bool build_umma(Ctx& c, const Bases& cb, bool cplx);
 };
 
 }  // namespace sadmrg

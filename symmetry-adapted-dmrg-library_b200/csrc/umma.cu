@@ -161,15 +161,37 @@ __device__ __forceinline__ void pack_chunk(const PackJob& P, unsigned local, con
   const unsigned r = local % Rp, kgs = local / Rp;
   const unsigned s = kgs >> 3, kg = kgs & 7u;
   const unsigned p = r / T, rr = r - p * T;
-  const double* src = static_cast<const double*>(bases.p[P.srcbuf]) + P.src;
   uint32_t h[4], l[4];
+  if (P.cmode == 0) {
+    const double* src = static_cast<const double*>(bases.p[P.srcbuf]) + P.src;
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    const unsigned k = s * kPanelK + kg * 4 + u;
-    double v = 0.0;
-    if (r < (unsigned)P.rows && k < (unsigned)P.K)
-      v = P.trans ? src[k + (long long)r * P.ld] : src[r + (long long)k * P.ld];
-    split_hl(v, h[u], l[u]);
+    for (int u = 0; u < 4; ++u) {
+      const unsigned k = s * kPanelK + kg * 4 + u;
+      double v = 0.0;
+      if (r < (unsigned)P.rows && k < (unsigned)P.K)
+        v = P.trans ? src[k + (long long)r * P.ld] : src[r + (long long)k * P.ld];
+      split_hl(v, h[u], l[u]);
+    }
+  } else {
+    // real form of a complex operand: element (i, j) of op(src) feeds k = 2j, 2j + 1
+    const double2* src = static_cast<const double2*>(bases.p[P.srcbuf]) + P.src;
+    const unsigned i = P.cmode == 1 ? (r >> 1) : r, p1 = r & 1u;
+#pragma unroll
+    for (int u = 0; u < 4; u += 2) {
+      const unsigned k = s * kPanelK + kg * 4 + u;   // even
+      double2 z = make_double2(0.0, 0.0);
+      if (r < (unsigned)P.rows && k < (unsigned)P.K) {
+        const unsigned j = k >> 1;
+        z = P.trans ? src[j + (long long)i * P.ld] : src[i + (long long)j * P.ld];
+        if (P.conj) z.y = -z.y;
+      }
+      double v0, v1;
+      if (P.cmode == 2) { v0 = z.x; v1 = z.y; }            // Bh(2j, l), Bh(2j + 1, l)
+      else if (p1 == 0) { v0 = z.x; v1 = -z.y; }           // Ah(2i, 2j), Ah(2i, 2j + 1)
+      else { v0 = z.y; v1 = z.x; }                         // Ah(2i + 1, 2j), Ah(2i + 1, 2j + 1)
+      split_hl(v0, h[u], l[u]);
+      split_hl(v1, h[u + 1], l[u + 1]);
+    }
   }
   unsigned char* panel = dst + P.dst + ((long long)p * nslab + s) * (T * 256u);
   const unsigned off = (kg * T + rr) * 16u;
@@ -415,7 +437,36 @@ __global__ void __launch_bounds__(kGThreads, 1)
       const int row0 = it.tm * BM, col0 = it.tn * BN;
       // 32 columns [cb, cb + 32) of row r of the finished tile -> C, or -> A panels of X
       auto emit = [&](int cb, const double (&x)[32]) {
-        if (J.pack >= 0) {
+        if (J.pack >= 0 && J.cx) {
+          // real form Xh of the complex result: this thread holds Re (r even) or Im (r odd)
+          // of row r/2, its lane neighbour the other part; columns [cb, cb + 32) feed
+          // k = 2 (col0 + cb) .. + 63 of Xh, two slabs
+          const bool odd = r & 1;
+          const int s0 = 2 * (col0 + cb) / kPanelK;
+#pragma unroll
+          for (int hs = 0; hs < 2; ++hs) {
+            const int s = s0 + hs;
+            unsigned char* panel = ub.pvar + J.pack + ((long long)it.tm * J.pack_nslab + s) * (BM * 256);
+            const bool live = s < J.pack_nslab;   // the same for every lane
+#pragma unroll
+            for (int kg = 0; kg < 8; ++kg) {
+              uint32_t h[4], l[4];
+#pragma unroll
+              for (int w = 0; w < 2; ++w) {
+                const int j = 16 * hs + 2 * kg + w;
+                const double own = x[j];
+                const double nb = __shfl_xor_sync(0xffffffffu, own, 1);
+                const double v0 = own, v1 = odd ? nb : -nb;   // (Re, -Im) on row 2i, (Im, Re) on 2i + 1
+                split_hl(J.alpha * v0, h[2 * w], l[2 * w]);
+                split_hl(J.alpha * v1, h[2 * w + 1], l[2 * w + 1]);
+              }
+              if (live) {
+                st_global_v4(panel + (kg * BM + r) * 16, h[0], h[1], h[2], h[3]);
+                st_global_v4(panel + BM * 128 + (kg * BM + r) * 16, l[0], l[1], l[2], l[3]);
+              }
+            }
+          }
+        } else if (J.pack >= 0) {
           const int s = (col0 + cb) / kPanelK;
           if (s < J.pack_nslab) {
             unsigned char* panel = ub.pvar + J.pack + ((long long)it.tm * J.pack_nslab + s) * (BM * 256);

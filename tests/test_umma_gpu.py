@@ -70,3 +70,32 @@ def test_umma_fused_launch_matches():
         h.set_matvec_fusion(False)
         assert np.array_equal(a, b) and np.array_equal(b, c)
         assert h.device_status() == 0
+
+
+@pytest.mark.parametrize("sym,L,D,J2,dz", [(0, 24, 128, 0.5, 0.3), (1, 32, 128, 0.0, 0.0)])
+def test_umma_complex_matvec_matches_fp64(sym, L, D, J2, dz):
+    """Complex plans on tcgen05 in the real form (interleaved C and B read as real,
+    A expanded to its 2 x 2 real blocks, X written as real-form panels)."""
+    import sadmrg
+    h = sadmrg.Handle(sym=sym, cplx=True)
+    h.chain_create(1, L, D, 1, 0, True, J2)
+    if dz:
+        h.chain_set_dm(dz)
+    h.chain_idmrg()
+    psi = h.chain_freeze(L // 2 - 1)
+    kinds = {k for k, _ in h.heff_launch_profile(sadmrg.PREC_TF32X3, 2)}
+    assert 0 in kinds, kinds            # psi -> panels: the tcgen05 schedule ran
+    rng = np.random.default_rng(5)
+    n = psi.data.size
+    for x in (psi.data, rng.standard_normal(n) + 1j * rng.standard_normal(n)):
+        y64 = h.heff_apply(x, sadmrg.PREC_FP64)
+        y32 = h.heff_apply(x, sadmrg.PREC_TF32X3)
+        scale = np.abs(y64).max()
+        err = np.abs(y32 - y64).max() / scale
+        assert err < 1e-5, err
+        assert np.any(y32 != y64)
+    h.set_lanczos_tol(1e-14)
+    e64, _, _ = h.heff_lanczos(psi.data.copy(), 100, sadmrg.PREC_FP64)
+    e32, _, _ = h.heff_lanczos(psi.data.copy(), 100, sadmrg.PREC_TF32X3)
+    assert abs(e32 - e64) <= 1e-10 * abs(e64), (e32, e64)
+    assert h.device_status() == 0
