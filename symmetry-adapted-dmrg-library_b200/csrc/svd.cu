@@ -3,15 +3,17 @@
 // Replaces the per-sector LAPACK gesvd of the reference
 // (src/dense_inst.cpp:447-541, called from src/block_tensor_inst.cpp:535-557).
 // Method: Hestenes one-sided Jacobi (Hestenes 1958; Demmel & Veselic 1992,
-// with the parallel block ordering of Brent & Luk).  The C = min(m,n) columns
-// of W (A, or A^H when m < n) are split into column blocks of b <= 16.  Every
-// round of a sweep pairs the blocks by the circle method; one CTA loads the
-// 2b columns of its pair into shared memory, runs one cyclic sweep of scalar
-// rotations over all of their column pairs (one warp per pair), writes them
-// back, and applies the accumulated 2b x 2b rotation to the matching columns
-// of V.  Sweeps repeat until a full sweep performs no rotation, so the result
-// keeps the high relative accuracy of one-sided Jacobi on small singular
-// values, which the reference's 1e-10 relative cut-off depends on.
+// with the parallel block ordering of Brent & Luk and the norm-sorted column
+// order of de Rijk 1989).  The C = min(m,n) columns of W (A, or A^H when m < n)
+// are ordered by decreasing norm at the start of every sweep and split into
+// column blocks of b = 16.  Every round of a sweep pairs the blocks by the
+// circle method; one CTA forms the 32 x 32 Gram matrix of its pair on the FP64
+// tensor cores (DMMA, W streamed in row chunks), runs a cyclic sweep of the
+// one-sided rotations on it, and applies the accumulated 32 x 32 rotation to
+// the pair's columns of W and V (DMMA again).  Sweeps repeat until a full sweep
+// performs no rotation, so the result keeps the columnwise relative accuracy of
+// one-sided Jacobi on small singular values, which the reference's 1e-10
+// relative cut-off depends on.
 #include <cuda_runtime.h>
 #include <cmath>
 #include <vector>
@@ -23,7 +25,7 @@ namespace sadmrg {
 
 constexpr int kSvdThreads = 512;
 constexpr int kSvdWarps = kSvdThreads / 32;
-constexpr size_t kSvdSmemBudget = 200 * 1024;
+constexpr int kSvdB = 16;              // columns per block; a visit takes two blocks
 
 struct SvdPair {
   int job, bi, bj, b;   // column blocks bi, bj (bj < 0: bi alone); b = block width
@@ -39,156 +41,272 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
-// One visit of a column-block pair: load its 2b columns into shared memory, one
-// cyclic sweep of scalar rotations over all their column pairs, write back, and
-// apply the accumulated rotation to the same columns of V.  Adds the number of
-// rotations to *rotations.  Every thread of the block calls it.
+// scalar helpers for T = double / double2 (complex)
+__device__ __forceinline__ double cj_mul(double a, double b) { return a * b; }   // conj(a) b
+__device__ __forceinline__ double2 cj_mul(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double cmul(double a, double b) { return a * b; }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double cadd(double a, double b) { return a + b; }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double cconj(double a) { return a; }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double cre(double a) { return a; }
+__device__ __forceinline__ double cre(double2 a) { return a.x; }
+template <class T> __device__ __forceinline__ T czero();
+template <> __device__ __forceinline__ double czero<double>() { return 0.0; }
+template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
+
+// D (8 x 8) += A (8 x 4, row-major) B (4 x 8, col-major) on the FP64 tensor cores.
+// Lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and D(l / 4, 2 (l % 4) + i), i = 0, 1.
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kNc = 2 * kSvdB;         // columns of one visit
+constexpr int kLdG = kNc + 1;          // row stride of G, Q and the row chunk (padding against bank conflicts)
+constexpr int kChunk = 64;             // rows per streamed chunk of W or V
+constexpr int kInnerMax = 1;           // inner sweeps of one visit (more cut outer sweeps by less than they cost)
+
 template <bool CPLX>
-__device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, double tol,
-                                  unsigned char* smem_raw, int* rotations) {
+constexpr size_t svd_smem_bytes() {
+  return (size_t)(2 * kNc + kChunk) * kLdG * (CPLX ? 16 : 8);
+}
+
+// One visit of a column-block pair (Hestenes one-sided Jacobi in Gram form):
+//   1. G = Wp^H Wp for the pair's nc <= 32 columns Wp, streamed from W in row chunks;
+//   2. cyclic one-sided Jacobi on G: rotation (p, q) from a = G_pp, b = G_qq,
+//      g = G_pq exactly as on the columns themselves, G <- J^H G J, Q <- Q J,
+//      with the rotated diagonal set to a - t|g|, b + t|g| and G_pq to 0; up to
+//      kInnerMax sweeps, stopping after a sweep that rotates nothing;
+//   3. Wp <- Wp Q and Vp <- Vp Q, streamed in row chunks.
+// Only G, Q and one row chunk live in shared memory, so the visit width does not
+// depend on the height of the block.  The rotations rotate the Gram entries of
+// the columns exactly as the column updates would (a rotation that mixes a small
+// column with a large one has |s| <= sqrt(a_small / a_large)), so the entries
+// keep the columnwise relative accuracy of the direct method; W itself changes
+// only by the orthogonal Q.  Adds the number of rotations to *rotations.  Every
+// thread of the block calls it; 16 warps, warp k owns pair k of each round.
+template <bool CPLX>
+__device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
+                                  double tol, unsigned char* smem_raw, int* rotations) {
   using T = typename SvdT<CPLX>::T;
+  static_assert(kSvdWarps * 2 >= kNc, "one warp per column pair of a round");
   const int R = J.trans ? J.n : J.m;
   const int C = J.trans ? J.m : J.n;
-  int cols[32];
-  int nc = 0;
-  for (int c = P.bi * P.b; c < min((P.bi + 1) * P.b, C); ++c) cols[nc++] = c;
-  if (P.bj >= 0)
-    for (int c = P.bj * P.b; c < min((P.bj + 1) * P.b, C); ++c) cols[nc++] = c;
-  T* Ws = reinterpret_cast<T*>(smem_raw);                 // nc columns of R
-  T* Q = Ws + (size_t)nc * R;                              // nc x nc
-  __shared__ int local_rot;
+  __shared__ int cols[kNc];
+  __shared__ int nrot_sh, sweep_rot_sh;
+  T* G = reinterpret_cast<T*>(smem_raw);   // kNc x kLdG, row-major
+  T* Q = G + kNc * kLdG;
+  T* Ck = Q + kNc * kLdG;                  // kChunk x kLdG: rows of W or V, row-major
   T* W = static_cast<T*>(work) + J.woff;
   T* V = static_cast<T*>(vmat) + J.voff;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) local_rot = 0;
-  for (int e = tid; e < nc * R; e += kSvdThreads) {
-    const int c = e / R, r = e % R;
-    Ws[e] = W[r + (long long)cols[c] * R];
-  }
-  for (int e = tid; e < nc * nc; e += kSvdThreads) {
-    if (CPLX) reinterpret_cast<double2*>(Q)[e] = make_double2((e % nc) == (e / nc) ? 1.0 : 0.0, 0.0);
-    else reinterpret_cast<double*>(Q)[e] = (e % nc) == (e / nc) ? 1.0 : 0.0;
+  int nc = 0;
+  {
+    const int n0 = min(P.b, C - P.bi * P.b);
+    const int n1 = P.bj >= 0 ? min(P.b, C - P.bj * P.b) : 0;
+    nc = n0 + n1;
+    // block position -> column through the job's current order (columns by decreasing norm)
+    const int* pj = perm + J.soff;
+    if (tid < n0) cols[tid] = pj[P.bi * P.b + tid];
+    else if (tid < nc) cols[tid] = pj[P.bj * P.b + (tid - n0)];
+    if (tid == 0) nrot_sh = 0;
   }
   __syncthreads();
-  const int N = nc + (nc & 1);
-  for (int rnd = 0; rnd < N - 1; ++rnd) {
-    for (int pi = warp; pi < N / 2; pi += kSvdWarps) {
-      int p, q;
-      if (pi == 0) { p = N - 1; q = rnd; }
-      else { p = (rnd + pi) % (N - 1); q = (rnd - pi + (N - 1)) % (N - 1); }
-      if (p >= nc || q >= nc) continue;
-      if (p > q) { const int tmp = p; p = q; q = tmp; }
-      T* wp = Ws + (size_t)p * R;
-      T* wq = Ws + (size_t)q * R;
-      double a = 0.0, b = 0.0, gr = 0.0, gi = 0.0;
-      for (int r = lane; r < R; r += 32) {
-        if (CPLX) {
-          const double2 x = reinterpret_cast<double2*>(wp)[r], y = reinterpret_cast<double2*>(wq)[r];
-          a += x.x * x.x + x.y * x.y;
-          b += y.x * y.x + y.y * y.y;
-          gr += x.x * y.x + x.y * y.y;
-          gi += x.x * y.y - x.y * y.x;
-        } else {
-          const double x = reinterpret_cast<double*>(wp)[r], y = reinterpret_cast<double*>(wq)[r];
-          a += x * x;
-          b += y * y;
-          gr += x * y;
-        }
-      }
-      a = wsum(a);
-      b = wsum(b);
-      gr = wsum(gr);
-      if (CPLX) gi = wsum(gi);
-      const double g = CPLX ? sqrt(gr * gr + gi * gi) : fabs(gr);
-      const double nrm = sqrt(a) * sqrt(b);
-      if (!(nrm > 1e-300) || g <= tol * nrm) continue;
-      // rotation zeroing the (p,q) entry of the 2x2 Gram matrix [[a, g],[g*, b]];
-      // for |zeta| > 1e150, zeta^2 would overflow: t = 1 / (2 zeta) to double
-      // precision there, and a t that underflows to 0 means the pair is already
-      // orthogonal to working precision (no rotation, none counted)
-      const double zeta = (b - a) / (2.0 * g);
-      const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
-                                          : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-      if (!(t != 0.0)) continue;
-      const double c = 1.0 / sqrt(1.0 + t * t);
-      const double s = c * t;
-      // phase e^{i phi} = gamma / |gamma|
-      const double er = CPLX ? gr / g : (gr >= 0.0 ? 1.0 : -1.0);
-      const double ei = CPLX ? gi / g : 0.0;
-      // [wp wq] <- [wp wq] [[c, s e^{i phi}], [-s e^{-i phi}, c]]
-      for (int r = lane; r < R; r += 32) {
-        if (CPLX) {
-          const double2 x = reinterpret_cast<double2*>(wp)[r], y = reinterpret_cast<double2*>(wq)[r];
-          // -s e^{-i phi} * y
-          const double2 yp = make_double2(-s * (er * y.x + ei * y.y), -s * (er * y.y - ei * y.x));
-          // s e^{i phi} * x
-          const double2 xp = make_double2(s * (er * x.x - ei * x.y), s * (er * x.y + ei * x.x));
-          reinterpret_cast<double2*>(wp)[r] = make_double2(c * x.x + yp.x, c * x.y + yp.y);
-          reinterpret_cast<double2*>(wq)[r] = make_double2(xp.x + c * y.x, xp.y + c * y.y);
-        } else {
-          const double x = reinterpret_cast<double*>(wp)[r], y = reinterpret_cast<double*>(wq)[r];
-          const double sg = s * er;
-          reinterpret_cast<double*>(wp)[r] = c * x - sg * y;
-          reinterpret_cast<double*>(wq)[r] = sg * x + c * y;
-        }
-      }
-      for (int r = lane; r < nc; r += 32) {
-        T* qp = Q + (size_t)p * nc;
-        T* qq = Q + (size_t)q * nc;
-        if (CPLX) {
-          const double2 x = reinterpret_cast<double2*>(qp)[r], y = reinterpret_cast<double2*>(qq)[r];
-          const double2 yp = make_double2(-s * (er * y.x + ei * y.y), -s * (er * y.y - ei * y.x));
-          const double2 xp = make_double2(s * (er * x.x - ei * x.y), s * (er * x.y + ei * x.x));
-          reinterpret_cast<double2*>(qp)[r] = make_double2(c * x.x + yp.x, c * x.y + yp.y);
-          reinterpret_cast<double2*>(qq)[r] = make_double2(xp.x + c * y.x, xp.y + c * y.y);
-        } else {
-          const double x = reinterpret_cast<double*>(qp)[r], y = reinterpret_cast<double*>(qq)[r];
-          const double sg = s * er;
-          reinterpret_cast<double*>(qp)[r] = c * x - sg * y;
-          reinterpret_cast<double*>(qq)[r] = sg * x + c * y;
-        }
-      }
-      if (lane == 0) atomicAdd(&local_rot, 1);
+
+  // 1. Gram matrix on the FP64 tensor cores: warp w owns the 8 x 8 tile (w / 4, w % 4)
+  //    of G = Wp^H Wp; k runs over the rows of the chunk (zero-filled past the block)
+  const int pt = warp >> 2, qt = warp & 3;
+  const int fr = lane >> 2, fk = lane & 3;
+  double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;   // Re (and Im) of D(fr, 2 fk + i)
+  for (int r0 = 0; r0 < R; r0 += kChunk) {
+    const int rows = min(kChunk, R - r0);
+    for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
+      const int r = e % kChunk, c = e / kChunk;
+      Ck[r * kLdG + c] = (r < rows && c < nc) ? W[(r0 + r) + (long long)cols[c] * R] : czero<T>();
     }
     __syncthreads();
-  }
-  const int nrot = local_rot;
-  __syncthreads();
-  if (nrot == 0) return;        // nothing moved: W and V stay as they are
-  for (int e = tid; e < nc * R; e += kSvdThreads) {
-    const int c = e / R, r = e % R;
-    W[r + (long long)cols[c] * R] = Ws[e];
-  }
-  __syncthreads();
-  // V[:, cols] <- V[:, cols] * Q, staged through the (now free) column area in row chunks
-  const int chunk = max(1, min(C, (int)(((size_t)nc * R) / (size_t)max(nc, 1))));
-  T* Vs = Ws;
-  for (int r0 = 0; r0 < C; r0 += chunk) {
-    const int rows = min(chunk, C - r0);
-    for (int e = tid; e < rows * nc; e += kSvdThreads) {
-      const int c = e / rows, r = e % rows;
-      Vs[e] = V[(r0 + r) + (long long)cols[c] * C];
-    }
-    __syncthreads();
-    for (int e = tid; e < rows * nc; e += kSvdThreads) {
-      const int c = e / rows, r = e % rows;
-      if (CPLX) {
-        double sr = 0.0, si = 0.0;
-        for (int k = 0; k < nc; ++k) {
-          const double2 v = reinterpret_cast<double2*>(Vs)[r + k * rows];
-          const double2 q = reinterpret_cast<double2*>(Q)[k + c * nc];
-          sr += v.x * q.x - v.y * q.y;
-          si += v.x * q.y + v.y * q.x;
-        }
-        reinterpret_cast<double2*>(V)[(r0 + r) + (long long)cols[c] * C] = make_double2(sr, si);
+#pragma unroll 4
+    for (int k0 = 0; k0 < kChunk; k0 += 4) {
+      const T x = Ck[(k0 + fk) * kLdG + pt * 8 + fr];   // A(p, r) = conj(W(r, p))
+      const T y = Ck[(k0 + fk) * kLdG + qt * 8 + fr];   // B(r, q) = W(r, q)
+      if constexpr (CPLX) {
+        dmma(g0, g1, x.x, y.x);
+        dmma(g0, g1, x.y, y.y);
+        dmma(h0, h1, x.x, y.y);
+        dmma(h0, h1, -x.y, y.x);
       } else {
-        double sr = 0.0;
-        for (int k = 0; k < nc; ++k)
-          sr += reinterpret_cast<double*>(Vs)[r + k * rows] * reinterpret_cast<double*>(Q)[k + c * nc];
-        reinterpret_cast<double*>(V)[(r0 + r) + (long long)cols[c] * C] = sr;
+        dmma(g0, g1, x, y);
       }
     }
     __syncthreads();
+  }
+  // stored from the tiles on and above the diagonal, mirrored, so that G is exactly Hermitian
+  for (int i = 0; i < 2; ++i) {
+    const int p = pt * 8 + fr, q = qt * 8 + 2 * fk + i;
+    if (p > q) continue;
+    T v;
+    if constexpr (CPLX) v = make_double2(i ? g1 : g0, i ? h1 : h0);
+    else v = i ? g1 : g0;
+    G[p * kLdG + q] = v;
+    G[q * kLdG + p] = cconj(v);
+  }
+  for (int e = tid; e < kNc * kNc; e += kSvdThreads) {
+    const int r = e / kNc, c = e % kNc;
+    Q[r * kLdG + c] = czero<T>();
+    if (r == c) reinterpret_cast<double*>(Q + r * kLdG + c)[0] = 1.0;
+  }
+  __syncthreads();
+
+  // 2. inner sweeps on G
+  const int N = nc + (nc & 1);
+  for (int isw = 0; isw < kInnerMax && N > 1; ++isw) {
+    if (tid == 0) sweep_rot_sh = 0;
+    __syncthreads();
+    for (int rnd = 0; rnd < N - 1; ++rnd) {
+      bool act = false;
+      int p = 0, q = 0;
+      double c = 1.0, s = 0.0, er = 1.0, ei = 0.0, tg = 0.0, a = 0.0, b = 0.0;
+      if (warp < N / 2) {
+        if (warp == 0) { p = N - 1; q = rnd; }
+        else { p = (rnd + warp) % (N - 1); q = (rnd - warp + (N - 1)) % (N - 1); }
+        if (p > q) { const int t = p; p = q; q = t; }
+        if (q < nc) {
+          a = cre(G[p * kLdG + p]);
+          b = cre(G[q * kLdG + q]);
+          const T gpq = G[p * kLdG + q];
+          double gr, gi = 0.0;
+          if constexpr (CPLX) { gr = gpq.x; gi = gpq.y; } else { gr = gpq; }
+          const double g = CPLX ? sqrt(gr * gr + gi * gi) : fabs(gr);
+          const double nrm = sqrt(fmax(a, 0.0)) * sqrt(fmax(b, 0.0));
+          if (nrm > 1e-300 && g > tol * nrm) {
+            // same rotation as on the columns; for |zeta| > 1e150 zeta^2 would overflow
+            const double zeta = (b - a) / (2.0 * g);
+            const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
+                                                : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            if (t != 0.0) {
+              act = true;
+              c = 1.0 / sqrt(1.0 + t * t);
+              s = c * t;
+              er = CPLX ? gr / g : (gr >= 0.0 ? 1.0 : -1.0);
+              ei = CPLX ? gi / g : 0.0;
+              tg = t * g;
+            }
+          }
+        }
+      }
+      __syncwarp();
+      // columns p, q of G and Q: [x y] <- [x y] [[c, s e^{i phi}], [-s e^{-i phi}, c]]
+      if (act && lane < nc) {
+        T* gpr = G + lane * kLdG;
+        T* qr = Q + lane * kLdG;
+        if constexpr (CPLX) {
+          const double2 ep = make_double2(s * er, s * ei), em = make_double2(-s * er, s * ei);   // s e^{i phi}, -s e^{-i phi}
+          double2 x = gpr[p], y = gpr[q];
+          gpr[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
+          gpr[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
+          x = qr[p]; y = qr[q];
+          qr[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
+          qr[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
+        } else {
+          const double sg = s * er;
+          double x = gpr[p], y = gpr[q];
+          gpr[p] = c * x - sg * y;
+          gpr[q] = sg * x + c * y;
+          x = qr[p]; y = qr[q];
+          qr[p] = c * x - sg * y;
+          qr[q] = sg * x + c * y;
+        }
+      }
+      __syncthreads();
+      // rows p, q of G: G <- J^H G; the rotated 2 x 2 block is set to its exact values
+      if (act && lane < nc) {
+        T* rp = G + p * kLdG;
+        T* rq = G + q * kLdG;
+        if constexpr (CPLX) {
+          const double2 x = rp[lane], y = rq[lane];
+          const double2 mp = make_double2(-s * er, -s * ei), pm = make_double2(s * er, -s * ei);   // -s e^{i phi}, s e^{-i phi}
+          rp[lane] = cadd(make_double2(c * x.x, c * x.y), cmul(mp, y));
+          rq[lane] = cadd(cmul(pm, x), make_double2(c * y.x, c * y.y));
+        } else {
+          const double sg = s * er;
+          const double x = rp[lane], y = rq[lane];
+          rp[lane] = c * x - sg * y;
+          rq[lane] = sg * x + c * y;
+        }
+        if (lane == p) { rp[p] = czero<T>(); reinterpret_cast<double*>(rp + p)[0] = a - tg; }
+        if (lane == q) { rq[q] = czero<T>(); reinterpret_cast<double*>(rq + q)[0] = b + tg; }
+        if (lane == q) rp[q] = czero<T>();
+        if (lane == p) rq[p] = czero<T>();
+        if (lane == 0) atomicAdd(&sweep_rot_sh, 1);
+      }
+      __syncthreads();
+    }
+    const int sr = sweep_rot_sh;
+    if (tid == 0) nrot_sh += sr;
+    __syncthreads();
+    if (sr == 0) break;
+  }
+  const int nrot = nrot_sh;
+  if (nrot == 0) return;        // nothing moved: W and V stay as they are
+
+  // 3. W_pair <- W_pair Q and V_pair <- V_pair Q, in row chunks: each chunk (64 x 32,
+  //    zero-filled) times Q on the FP64 tensor cores (warp w: output tiles w and w + 16 of
+  //    the 8 x 4 tile grid), the product written back over the chunk and stored coalesced
+  for (int pass = 0; pass < 2; ++pass) {
+    T* M = pass == 0 ? W : V;
+    const int rows_all = pass == 0 ? R : C;
+    for (int r0 = 0; r0 < rows_all; r0 += kChunk) {
+      const int rows = min(kChunk, rows_all - r0);
+      for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
+        const int r = e % kChunk, c = e / kChunk;
+        Ck[r * kLdG + c] = (r < rows && c < nc) ? M[(r0 + r) + (long long)cols[c] * rows_all] : czero<T>();
+      }
+      __syncthreads();
+      double d[2][4];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int t = warp + 16 * u, rt = t >> 2, jt = t & 3;
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+        for (int k0 = 0; k0 < kNc; k0 += 4) {
+          const T x = Ck[(rt * 8 + fr) * kLdG + k0 + fk];
+          const T y = Q[(k0 + fk) * kLdG + jt * 8 + fr];
+          if constexpr (CPLX) {
+            dmma(a0, a1, x.x, y.x);
+            dmma(a0, a1, -x.y, y.y);
+            dmma(b0, b1, x.x, y.y);
+            dmma(b0, b1, x.y, y.x);
+          } else {
+            dmma(a0, a1, x, y);
+          }
+        }
+        d[u][0] = a0; d[u][1] = a1; d[u][2] = b0; d[u][3] = b1;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int t = warp + 16 * u, rt = t >> 2, jt = t & 3;
+        for (int i = 0; i < 2; ++i) {
+          T v;
+          if constexpr (CPLX) v = make_double2(d[u][i], d[u][2 + i]);
+          else v = d[u][i];
+          Ck[(rt * 8 + fr) * kLdG + jt * 8 + 2 * fk + i] = v;
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
+        const int r = e % kChunk, j = e / kChunk;
+        if (r < rows && j < nc) M[(r0 + r) + (long long)cols[j] * rows_all] = Ck[r * kLdG + j];
+      }
+      __syncthreads();
+    }
   }
   if (tid == 0) atomicAdd(rotations, nrot);
 }
@@ -196,11 +314,12 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
 template <bool CPLX>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
                                                                   const SvdPair* __restrict__ pairs, void* work,
-                                                                  void* vmat, double tol, int* rotations) {
+                                                                  void* vmat, const int* perm, double tol,
+                                                                  int* rotations) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SvdPair P = pairs[blockIdx.x];
   const SvdJob J = jobs[P.job];
-  jacobi_pair_visit<CPLX>(J, P, work, vmat, tol, smem_raw, rotations);
+  jacobi_pair_visit<CPLX>(J, P, work, vmat, perm, tol, smem_raw, rotations);
 }
 
 // ---------------------------------------------------------------------------
@@ -259,8 +378,8 @@ template <bool CPLX>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* __restrict__ jobs, int nj,
                                                                   const SvdPair* __restrict__ pairs,
                                                                   const int* __restrict__ roff, int max_rounds,
-                                                                  void* work, void* vmat, double tol, int* cnt,
-                                                                  SvdCtl* ctl, int max_sweeps) {
+                                                                  void* work, void* vmat, double* nrm, int* perm,
+                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned char done[kSvdMaxJobsCoop];
   __shared__ int all_done;
@@ -272,12 +391,53 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
     int* cur = cnt + (sw % 3) * nj;
     if (blockIdx.x == 0)
       for (int j = threadIdx.x; j < nj; j += blockDim.x) cnt[((sw + 1) % 3) * nj + j] = 0;
+    // column order of this sweep: decreasing norm (de Rijk), ties by index.  Norms
+    // one warp per column, then every column's rank counted over its sector.
+    {
+      using T = typename SvdT<CPLX>::T;
+      const int lane = threadIdx.x & 31;
+      const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+      for (int j = 0; j < nj; ++j) {
+        if (done[j]) continue;
+        const SvdJob J = jobs[j];
+        const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
+        const T* W = static_cast<const T*>(work) + J.woff;
+        for (int c = gw; c < C; c += nw) {
+          double a = 0.0;
+          for (int r = lane; r < R; r += 32) {
+            const T x = W[r + (long long)c * R];
+            if constexpr (CPLX) a += x.x * x.x + x.y * x.y;
+            else a += x * x;
+          }
+          a = wsum(a);
+          if (lane == 0) nrm[J.soff + c] = a;
+        }
+      }
+      if (!svd_grid_sync(ctl)) return;
+      const int gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+      for (int j = 0; j < nj; ++j) {
+        if (done[j]) continue;
+        const SvdJob J = jobs[j];
+        const int C = J.trans ? J.m : J.n;
+        const double* nj_ = nrm + J.soff;
+        for (int c = gt; c < C; c += nt) {
+          const double v = nj_[c];
+          int rank = 0;
+          for (int k = 0; k < C; ++k) {
+            const double u = nj_[k];
+            rank += (u > v || (u == v && k < c)) ? 1 : 0;
+          }
+          perm[J.soff + rank] = c;
+        }
+      }
+      if (!svd_grid_sync(ctl)) return;
+    }
     for (int r = 0; r < max_rounds; ++r) {
       for (int p = roff[r] + blockIdx.x; p < roff[r + 1]; p += gridDim.x) {
         const SvdPair P = pairs[p];
         if (done[P.job]) continue;
         const SvdJob J = jobs[P.job];
-        jacobi_pair_visit<CPLX>(J, P, work, vmat, tol, smem_raw, cur + P.job);
+        jacobi_pair_visit<CPLX>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
       }
       if (!svd_grid_sync(ctl)) return;
     }
@@ -298,13 +458,15 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
 
 // W = A (m >= n) or A^H (m < n); V = I
 template <bool CPLX>
-__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat) {
+__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm) {
   using T = typename SvdT<CPLX>::T;
   const SvdJob J = jobs[blockIdx.x];
   const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
   const T* A = static_cast<const T*>(a) + J.aoff;
   T* W = static_cast<T*>(work) + J.woff;
   T* V = static_cast<T*>(vmat) + J.voff;
+  if (blockIdx.y == 0)
+    for (int c = threadIdx.x; c < C; c += blockDim.x) perm[J.soff + c] = c;
   for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)R * C;
        e += (long long)blockDim.x * gridDim.y) {
     const int r = (int)(e % R), c = (int)(e / R);
@@ -341,15 +503,6 @@ __global__ void jacobi_norms_kernel(const SvdJob* jobs, const void* work, double
   }
 }
 
-static int pick_block(bool cplx, int R) {
-  const size_t es = cplx ? 16 : 8;
-  for (int b = 16; b >= 1; b /= 2) {
-    const size_t need = ((size_t)2 * b * R + (size_t)4 * b * b) * es;
-    if (need <= kSvdSmemBudget) return b;
-  }
-  return 0;
-}
-
 // Host driver.  Runs all sweeps in one cooperative launch when the device allows
 // it, otherwise one launch per round and one host synchronisation per sweep to
 // test convergence.  Returns the number of sweeps taken (or -1 when max_sweeps
@@ -366,14 +519,12 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     const int R = hjobs[j].trans ? hjobs[j].n : hjobs[j].m;
     const int C = hjobs[j].trans ? hjobs[j].m : hjobs[j].n;
     maxR = std::max(maxR, R);
-    bsz[j] = pick_block(cplx, R);
-    SADMRG_REQUIRE(bsz[j] > 0, SADMRG_ERR_LIMIT, "jacobi svd: sector block too tall for shared memory");
+    bsz[j] = kSvdB;
     nblk[j] = (C + bsz[j] - 1) / bsz[j];
     const int N = nblk[j] + (nblk[j] & 1);
     nrounds[j] = nblk[j] <= 1 ? 1 : N - 1;
     max_rounds = std::max(max_rounds, nrounds[j]);
-    const int nc = std::min(C, 2 * bsz[j]);
-    smem = std::max(smem, ((size_t)nc * R + (size_t)nc * nc) * (cplx ? 16 : 8));
+    smem = cplx ? svd_smem_bytes<true>() : svd_smem_bytes<false>();
   }
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
@@ -396,12 +547,16 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     flat.insert(flat.end(), rounds[r].begin(), rounds[r].end());
   }
   roff[max_rounds] = (int)flat.size();
-  DevBuf djobs(sizeof(SvdJob) * nj, s), dpairs(sizeof(SvdPair) * flat.size(), s), dcnt(sizeof(int), s);
+  long long nsv = 1;   // singular-value slots (the column order lives at the same offsets)
+  for (int j = 0; j < nj; ++j)
+    nsv = std::max<long long>(nsv, hjobs[j].soff + (hjobs[j].trans ? hjobs[j].m : hjobs[j].n));
+  DevBuf djobs(sizeof(SvdJob) * nj, s), dpairs(sizeof(SvdPair) * flat.size(), s), dcnt(sizeof(int), s),
+      dperm(sizeof(int) * nsv, s);
   SADMRG_CUDA(cudaMemcpyAsync(djobs.get(), hjobs.data(), sizeof(SvdJob) * nj, cudaMemcpyHostToDevice, s));
   SADMRG_CUDA(cudaMemcpyAsync(dpairs.get(), flat.data(), sizeof(SvdPair) * flat.size(), cudaMemcpyHostToDevice, s));
   dim3 ig(nj, 16);
-  if (cplx) jacobi_init_kernel<true><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat);
-  else jacobi_init_kernel<false><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat);
+  if (cplx) jacobi_init_kernel<true><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
+  else jacobi_init_kernel<false><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
   SADMRG_CUDA(cudaGetLastError());
   if (cplx)
     SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -439,8 +594,11 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     double tolv = tol;
     void* a_work = work;
     void* a_vmat = vmat;
-    void* args[] = {(void*)&pj, (void*)&njv, (void*)&pp, (void*)&pr, (void*)&mr, (void*)&a_work,
-                    (void*)&a_vmat, (void*)&tolv, (void*)&pc, (void*)&pctl, (void*)&ms};
+    double* a_nrm = sv;   // column norms of each sweep; the final singular values overwrite them
+    int* a_perm = dperm.as<int>();
+    void* args[] = {(void*)&pj,     (void*)&njv,    (void*)&pp,   (void*)&pr, (void*)&mr,   (void*)&a_work,
+                    (void*)&a_vmat, (void*)&a_nrm, (void*)&a_perm, (void*)&tolv, (void*)&pc, (void*)&pctl,
+                    (void*)&ms};
     if (cplx)
       SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<true>, dim3(grid), dim3(kSvdThreads),
                                               args, smem, s));
@@ -465,10 +623,10 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
       if (np == 0) continue;
       if (cplx)
         jacobi_pair_kernel<true><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                               work, vmat, tol, dcnt.as<int>());
+                                                               work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
       else
         jacobi_pair_kernel<false><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                                work, vmat, tol, dcnt.as<int>());
+                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
     }
     SADMRG_CUDA(cudaGetLastError());
     SADMRG_CUDA(cudaMemcpyAsync(&h_rot, dcnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
