@@ -70,7 +70,8 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 
 constexpr int kNc = 2 * kSvdB;         // columns of one visit
 constexpr int kLdG = kNc + 1;          // row stride of G, Q and the row chunk (padding against bank conflicts)
-constexpr int kChunk = 64;             // rows per streamed chunk of W or V
+constexpr int kChunk = 128;            // rows per streamed chunk of W or V
+constexpr int kChunkPer = kChunk * kNc / kSvdThreads;   // chunk elements per thread
 constexpr int kInnerMax = 1;           // inner sweeps of one visit (more cut outer sweeps by less than they cost)
 
 template <bool CPLX>
@@ -125,13 +126,28 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   const int pt = warp >> 2, qt = warp & 3;
   const int fr = lane >> 2, fk = lane & 3;
   double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;   // Re (and Im) of D(fr, 2 fk + i)
-  for (int r0 = 0; r0 < R; r0 += kChunk) {
-    const int rows = min(kChunk, R - r0);
-    for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
-      const int r = e % kChunk, c = e / kChunk;
-      Ck[r * kLdG + c] = (r < rows && c < nc) ? W[(r0 + r) + (long long)cols[c] * R] : czero<T>();
+  // Row chunks of a column set (W or V), read into registers one chunk ahead of
+  // the one in shared memory so that the global loads overlap the products.
+  T pre[kChunkPer];
+  auto fetch = [&](const T* M, int ld, int r0, int rows) {
+#pragma unroll
+    for (int u = 0; u < kChunkPer; ++u) {
+      const int e = tid + u * kSvdThreads, r = e % kChunk, c = e / kChunk;
+      pre[u] = (r < rows && c < nc) ? M[(r0 + r) + (long long)cols[c] * ld] : czero<T>();
     }
+  };
+  auto stage = [&]() {
+#pragma unroll
+    for (int u = 0; u < kChunkPer; ++u) {
+      const int e = tid + u * kSvdThreads, r = e % kChunk, c = e / kChunk;
+      Ck[r * kLdG + c] = pre[u];
+    }
+  };
+  fetch(W, R, 0, min(kChunk, R));
+  for (int r0 = 0; r0 < R; r0 += kChunk) {
+    stage();
     __syncthreads();
+    if (r0 + kChunk < R) fetch(W, R, r0 + kChunk, min(kChunk, R - r0 - kChunk));
 #pragma unroll 4
     for (int k0 = 0; k0 < kChunk; k0 += 4) {
       const T x = Ck[(k0 + fk) * kLdG + pt * 8 + fr];   // A(p, r) = conj(W(r, p))
@@ -256,57 +272,69 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   const int nrot = nrot_sh;
   if (nrot == 0) return;        // nothing moved: W and V stay as they are
 
-  // 3. W_pair <- W_pair Q and V_pair <- V_pair Q, in row chunks: each chunk (64 x 32,
-  //    zero-filled) times Q on the FP64 tensor cores (warp w: output tiles w and w + 16 of
-  //    the 8 x 4 tile grid), the product written back over the chunk and stored coalesced
-  for (int pass = 0; pass < 2; ++pass) {
-    T* M = pass == 0 ? W : V;
-    const int rows_all = pass == 0 ? R : C;
-    for (int r0 = 0; r0 < rows_all; r0 += kChunk) {
-      const int rows = min(kChunk, rows_all - r0);
-      for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
-        const int r = e % kChunk, c = e / kChunk;
-        Ck[r * kLdG + c] = (r < rows && c < nc) ? M[(r0 + r) + (long long)cols[c] * rows_all] : czero<T>();
-      }
-      __syncthreads();
-      double d[2][4];
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int t = warp + 16 * u, rt = t >> 2, jt = t & 3;
-        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-#pragma unroll
-        for (int k0 = 0; k0 < kNc; k0 += 4) {
-          const T x = Ck[(rt * 8 + fr) * kLdG + k0 + fk];
-          const T y = Q[(k0 + fk) * kLdG + jt * 8 + fr];
-          if constexpr (CPLX) {
-            dmma(a0, a1, x.x, y.x);
-            dmma(a0, a1, -x.y, y.y);
-            dmma(b0, b1, x.x, y.y);
-            dmma(b0, b1, x.y, y.x);
-          } else {
-            dmma(a0, a1, x, y);
-          }
-        }
-        d[u][0] = a0; d[u][1] = a1; d[u][2] = b0; d[u][3] = b1;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int t = warp + 16 * u, rt = t >> 2, jt = t & 3;
-        for (int i = 0; i < 2; ++i) {
-          T v;
-          if constexpr (CPLX) v = make_double2(d[u][i], d[u][2 + i]);
-          else v = d[u][i];
-          Ck[(rt * 8 + fr) * kLdG + jt * 8 + 2 * fk + i] = v;
-        }
-      }
-      __syncthreads();
-      for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
-        const int r = e % kChunk, j = e / kChunk;
-        if (r < rows && j < nc) M[(r0 + r) + (long long)cols[j] * rows_all] = Ck[r * kLdG + j];
-      }
-      __syncthreads();
+  // 3. W_pair <- W_pair Q and V_pair <- V_pair Q, in row chunks (W's, then V's): each
+  //    chunk (128 x 32, zero-filled) times Q on the FP64 tensor cores (warp w: output
+  //    tiles w, w + 16, ... of the 16 x 4 tile grid), the product written back over the
+  //    chunk and stored coalesced; the next chunk is read while this one is multiplied
+  const int nw_chunks = (R + kChunk - 1) / kChunk, nv_chunks = (C + kChunk - 1) / kChunk;
+  auto chunk_of = [&](int k, T*& M, int& ld, int& r0, int& rows) {
+    if (k < nw_chunks) { M = W; ld = R; r0 = k * kChunk; }
+    else { M = V; ld = C; r0 = (k - nw_chunks) * kChunk; }
+    rows = min(kChunk, ld - r0);
+  };
+  {
+    T* M; int ld, r0, rows;
+    chunk_of(0, M, ld, r0, rows);
+    fetch(M, ld, r0, rows);
+  }
+  for (int k = 0; k < nw_chunks + nv_chunks; ++k) {
+    T* M; int ld, r0, rows;
+    chunk_of(k, M, ld, r0, rows);
+    stage();
+    __syncthreads();
+    if (k + 1 < nw_chunks + nv_chunks) {
+      T* M2; int ld2, r2, rows2;
+      chunk_of(k + 1, M2, ld2, r2, rows2);
+      fetch(M2, ld2, r2, rows2);
     }
+    constexpr int kTiles = (kChunk / 8) * (kNc / 8) / kSvdWarps;   // output tiles per warp
+    double d[kTiles][4];
+#pragma unroll
+    for (int u = 0; u < kTiles; ++u) {
+      const int t = warp + kSvdWarps * u, rt = t >> 2, jt = t & 3;
+      double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+      for (int k0 = 0; k0 < kNc; k0 += 4) {
+        const T x = Ck[(rt * 8 + fr) * kLdG + k0 + fk];
+        const T y = Q[(k0 + fk) * kLdG + jt * 8 + fr];
+        if constexpr (CPLX) {
+          dmma(a0, a1, x.x, y.x);
+          dmma(a0, a1, -x.y, y.y);
+          dmma(b0, b1, x.x, y.y);
+          dmma(b0, b1, x.y, y.x);
+        } else {
+          dmma(a0, a1, x, y);
+        }
+      }
+      d[u][0] = a0; d[u][1] = a1; d[u][2] = b0; d[u][3] = b1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kTiles; ++u) {
+      const int t = warp + kSvdWarps * u, rt = t >> 2, jt = t & 3;
+      for (int i = 0; i < 2; ++i) {
+        T v;
+        if constexpr (CPLX) v = make_double2(d[u][i], d[u][2 + i]);
+        else v = d[u][i];
+        Ck[(rt * 8 + fr) * kLdG + jt * 8 + 2 * fk + i] = v;
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
+      const int r = e % kChunk, j = e / kChunk;
+      if (r < rows && j < nc) M[(r0 + r) + (long long)cols[j] * ld] = Ck[r * kLdG + j];
+    }
+    __syncthreads();
   }
   if (tid == 0) atomicAdd(rotations, nrot);
 }

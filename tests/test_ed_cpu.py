@@ -42,3 +42,12 @@ def test_ed_dm_gauge_identity():
     e0 = ed.ground_energy(L, False, J2=0.5, dz=0.0)
     e1 = ed.ground_energy(L, False, J2=0.5, dz=dz)
     assert abs(e1 - e0) > 1e-3
+
+
+def test_ed_known_answers():
+    """Known answers for the reference build (periodic, its own runs) and ED (open chains)."""
+    assert abs(ed.ground_energy(8, periodic=True) - (-3.6510934089372)) < 1e-11
+    assert abs(ed.ground_energy(12, periodic=True) - (-5.3873909174452)) < 1e-11
+    assert abs(ed.ground_energy(12, periodic=True, two_sz=2) - (-5.0315434037424)) < 1e-11
+    assert abs(ed.ground_energy(8, periodic=False) - (-3.3749325986879)) < 1e-11
+    assert abs(ed.ground_energy(12, periodic=False) - (-5.1420906328405)) < 1e-11
