@@ -127,6 +127,17 @@ int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out) {
   h->ctx.cplx = cplx != 0;
   const int rc = guard(h, [&]() {
     SADMRG_CUDA(cudaStreamCreateWithFlags(&h->ctx.stream, cudaStreamNonBlocking));
+    // Plans, Krylov spaces and SVD work buffers are allocated and freed once per
+    // bond (stream-ordered).  With the pool's default release threshold (0) every
+    // synchronisation hands the freed memory back to the driver and the next bond
+    // maps it again, which costs milliseconds per bond; keep it cached in this
+    // process instead (sadmrg_destroy trims the pool).
+    {
+      cudaMemPool_t pool;
+      SADMRG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+      uint64_t keep = UINT64_MAX;
+      SADMRG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_scalars, 64 * sizeof(double)));
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_partial, sizeof(double) * 2 * 512 * (size_t)h->ctx.npart));
     SADMRG_CUDA(cudaMallocHost(&h->ctx.h_pinned, sizeof(double) * Ctx::kPinnedDoubles));
@@ -150,6 +161,9 @@ int sadmrg_destroy(sadmrg_handle* h) {
     cudaStreamSynchronize(h->ctx.stream);
     cudaStreamDestroy(h->ctx.stream);
   }
+  // hand the pool's cached, now unused memory back (memory of other live handles stays)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   delete h;
   return SADMRG_OK;
 }
