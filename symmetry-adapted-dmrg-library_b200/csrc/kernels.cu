@@ -212,16 +212,22 @@ __global__ void multi_dot_partial(const void* V, long long ldv, int nv, const vo
 }
 
 template <bool CPLX>
+// one warp per dot: lane l sums partials l, l + 32, ... and the warp adds the
+// 32 sums in a fixed tree (the same order every call)
 __global__ void multi_dot_final(const double* partial, int npart, int nv, void* out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), l = threadIdx.x & 31;
   if (j >= nv) return;
   double a = 0.0, b = 0.0;
-  for (int p = 0; p < npart; ++p) {
+  for (int p = l; p < npart; p += 32) {
     a += partial[(p * (long long)nv + j) * 2 + 0];
-    b += partial[(p * (long long)nv + j) * 2 + 1];
+    if (CPLX) b += partial[(p * (long long)nv + j) * 2 + 1];
   }
-  if (CPLX) static_cast<double2*>(out)[j] = make_double2(a, b);
-  else static_cast<double*>(out)[j] = a;
+  a = warp_sum(a);
+  if (CPLX) b = warp_sum(b);
+  if (l == 0) {
+    if (CPLX) static_cast<double2*>(out)[j] = make_double2(a, b);
+    else static_cast<double*>(out)[j] = a;
+  }
 }
 
 void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n, double* partial,
@@ -229,10 +235,10 @@ void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const voi
   if (nv <= 0) return;
   if (cplx) {
     multi_dot_partial<true><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
-    multi_dot_final<true><<<(nv + 127) / 128, 128, 0, s>>>(partial, npart, nv, out);
+    multi_dot_final<true><<<(nv + 3) / 4, 128, 0, s>>>(partial, npart, nv, out);
   } else {
     multi_dot_partial<false><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
-    multi_dot_final<false><<<(nv + 127) / 128, 128, 0, s>>>(partial, npart, nv, out);
+    multi_dot_final<false><<<(nv + 3) / 4, 128, 0, s>>>(partial, npart, nv, out);
   }
 }
 
