@@ -207,7 +207,8 @@ int sadmrg_chain_freeze(sadmrg_handle* h, int il, const char* export_dir);
 int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d);
 /* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded,
  *          near_ties (truncations whose cut split a pair of singular values equal to 1e-8),
- *          svd_kernel_s (device time of the Jacobi sweeps), svd_sweeps]; the first n are written */
+ *          svd_kernel_s (device time of the Jacobi sweeps), svd_sweeps,
+ *          plan_s (host time of building H_eff plans, part of lanczos_s)]; the first n are written */
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
 /* kind: 0 = uu[site], 1 = hh[site], 2 = opr[site][k] */
 int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t);

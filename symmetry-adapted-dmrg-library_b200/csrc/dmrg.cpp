@@ -913,7 +913,9 @@ void Chain<S>::lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec) {
   }
   if (mlanc > ndata) mlanc = (int)ndata + 1;
   if (mlanc < 2) mlanc = 2;
+  const double tp = now_s();
   HeffPlan<S> H = heff_plan(il, ir, vec);
+  timers.plan += now_s() - tp;
   LanczosStats st = lanczos_solve<S>(c, H, vec.data(), mlanc, prec);
   gs_enr = st.energy;
   if (std::getenv("SADMRG_VERBOSE"))

@@ -122,6 +122,7 @@ struct Timers {
   double heff_flops = 0;
   double svd_kernel = 0;        // device time of the Jacobi sweep kernels (s)
   long long svd_sweeps = 0;     // Jacobi sweeps, summed over the truncations
+  double plan = 0;              // host wall time of building H_eff plans (part of lanczos)
 };
 
 template <class S>
