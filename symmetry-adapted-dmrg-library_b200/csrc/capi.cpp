@@ -140,6 +140,8 @@ int sadmrg_create(int sym, int cplx, int device, sadmrg_handle** out) {
     }
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_scalars, 64 * sizeof(double)));
     SADMRG_CUDA(cudaMalloc(&h->ctx.d_partial, sizeof(double) * 2 * 512 * (size_t)h->ctx.npart));
+    SADMRG_CUDA(cudaMalloc(&h->ctx.d_counter, sizeof(unsigned)));
+    SADMRG_CUDA(cudaMemset(h->ctx.d_counter, 0, sizeof(unsigned)));
     SADMRG_CUDA(cudaMallocHost(&h->ctx.h_pinned, sizeof(double) * Ctx::kPinnedDoubles));
     if (h->ctx.sym == Sym::SU2) h->ctx.cgc = std::make_unique<CGCFactors>(1);
   });

@@ -164,7 +164,8 @@ void HeffPlan<S>::apply(Ctx& c, const S* psi, S* out, int prec) const {
 template <class S>
 void HeffPlan<S>::penalty(Ctx& c, const S* psi, S* out) const {
   if (npen <= 0) return;
-  launch_multi_dot(kCx<S>, pen_o->get(), n, npen, psi, n, c.d_partial, c.npart, pen_dot->get(), c.stream);
+  launch_multi_dot(kCx<S>, pen_o->get(), n, npen, psi, n, c.d_partial, c.npart, pen_dot->get(), c.d_counter,
+                   c.stream);
   launch_multi_axpy(kCx<S>, out, pen_wo->get(), n, npen, pen_dot->get(), n, c.stream);
   c.launches += 3;
 }
@@ -247,9 +248,11 @@ struct Krylov {
     SADMRG_CUDA(cudaMemsetAsync(beta.get(), 0, sizeof(double) * (mlanc + 4), c.stream));
   }
   S* F(int i) { return ff.as<S>() + (size_t)i * n; }
-  void mdot(const S* V, int nv, const S* x, void* out) {
-    launch_multi_dot(kCx<S>, V, n, nv, x, n, c.d_partial, c.npart, out, c.stream);
-    c.launches += 2;
+  void mdot(const S* V, int nv, const S* x, void* out, int scalar_op = -1, const double* beta_prev = nullptr,
+            void* scalar_out = nullptr) {
+    launch_multi_dot(kCx<S>, V, n, nv, x, n, c.d_partial, c.npart, out, c.d_counter, c.stream, scalar_op, beta_prev,
+                     scalar_out);
+    ++c.launches;
   }
   S dot_host(const S* a, const S* b) {  // <a|b>
     mdot(a, 1, b, dots.get());
@@ -328,9 +331,7 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
   int synced = 0;                                          // steps whose a, b are on the host
   auto step = [&](int m, bool reorth) {
     matvec(K.F(m - 1), K.F(m));
-    K.mdot(K.F(m - 1), 1, K.F(m), K.dots.get());
-    launch_lanczos_scalar(kCx<S>, 0, K.dots.get(), K.beta.template as<double>() + (m - 1), K.coef.get(), c.stream);
-    ++c.launches;
+    K.mdot(K.F(m - 1), 1, K.F(m), K.dots.get(), 0, K.beta.template as<double>() + (m - 1), K.coef.get());
     if (m >= 2)
       launch_multi_axpy(kCx<S>, K.F(m), K.F(m - 2), n, 2, K.coef.get(), n, c.stream);
     else
@@ -341,10 +342,9 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
       launch_multi_axpy(kCx<S>, K.F(m), K.F(0), n, m, K.dots.get(), n, c.stream);
       ++c.launches;
     }
-    K.mdot(K.F(m), 1, K.F(m), K.dots.get());
-    launch_lanczos_scalar(kCx<S>, 1, K.dots.get(), nullptr, K.beta.template as<double>() + m, c.stream);
+    K.mdot(K.F(m), 1, K.F(m), K.dots.get(), 1, nullptr, K.beta.template as<double>() + m);
     launch_scale_inv(kCx<S>, K.F(m), K.beta.template as<double>() + m, n, c.stream);
-    c.launches += 2;
+    ++c.launches;
     SADMRG_CUDA(cudaMemcpyAsync(pin_a + (m - 1) * pin_stride, K.coef.template as<S>() + 1, sizeof(S),
                                 cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaMemcpyAsync(pin_b + m, K.beta.template as<double>() + m, sizeof(double), cudaMemcpyDeviceToHost,

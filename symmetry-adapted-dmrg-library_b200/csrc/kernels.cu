@@ -147,7 +147,7 @@ void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStre
 }
 
 template <bool CPLX>
-__global__ void lanczos_scalar_kernel(int op, const void* dot, const double* beta_prev, void* out) {
+__device__ __forceinline__ void lanczos_scalar_op(int op, const void* dot, const double* beta_prev, void* out) {
   const double re = CPLX ? static_cast<const double2*>(dot)[0].x : static_cast<const double*>(dot)[0];
   if (op == 0) {
     if (CPLX) {
@@ -160,6 +160,11 @@ __global__ void lanczos_scalar_kernel(int op, const void* dot, const double* bet
   } else {
     static_cast<double*>(out)[0] = sqrt(fabs(re));
   }
+}
+
+template <bool CPLX>
+__global__ void lanczos_scalar_kernel(int op, const void* dot, const double* beta_prev, void* out) {
+  lanczos_scalar_op<CPLX>(op, dot, beta_prev, out);
 }
 
 void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s) {
@@ -175,71 +180,97 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// <V_j|x> in one launch: every block writes its partial sums, and the last block
+// to finish (atomic count) adds them up -- one warp per dot, lane l taking
+// partials l, l + 32, ... and the warp summing in a fixed tree, so the result
+// does not depend on which block is last -- and, if op >= 0, applies the Krylov
+// scalar step of lanczos_scalar_kernel to out[0].  counter is zero between launches.
 template <bool CPLX>
-__global__ void multi_dot_partial(const void* V, long long ldv, int nv, const void* x, long long n, double* partial) {
-  __shared__ double red[2][32];
+__global__ void multi_dot_fused(const void* V, long long ldv, int nv, const void* x, long long n, double* partial,
+                                void* out, unsigned* counter, int op, const double* beta_prev, void* sout) {
+  constexpr int kG = 8;                 // dots per pass over the block's range
+  __shared__ double red[2][kG][32];
+  __shared__ int last;
   const long long per = (n + gridDim.x - 1) / gridDim.x;
   const long long lo = per * blockIdx.x, hi = min(n, lo + per);
-  for (int j = 0; j < nv; ++j) {
-    double sr = 0.0, si = 0.0;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < nv; j0 += kG) {
+    const int g = min(kG, nv - j0);
+    double sr[kG], si[kG];
+#pragma unroll
+    for (int u = 0; u < kG; ++u) { sr[u] = 0.0; si[u] = 0.0; }
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
       if (CPLX) {
-        const double2 a = static_cast<const double2*>(V)[j * ldv + i];
         const double2 b = static_cast<const double2*>(x)[i];
-        sr += a.x * b.x + a.y * b.y;  // conj(a) * b
-        si += a.x * b.y - a.y * b.x;
+#pragma unroll
+        for (int u = 0; u < kG; ++u)
+          if (u < g) {
+            const double2 a = static_cast<const double2*>(V)[(j0 + u) * ldv + i];
+            sr[u] += a.x * b.x + a.y * b.y;  // conj(a) * b
+            si[u] += a.x * b.y - a.y * b.x;
+          }
       } else {
-        sr += static_cast<const double*>(V)[j * ldv + i] * static_cast<const double*>(x)[i];
+        const double b = static_cast<const double*>(x)[i];
+#pragma unroll
+        for (int u = 0; u < kG; ++u)
+          if (u < g) sr[u] += static_cast<const double*>(V)[(j0 + u) * ldv + i] * b;
       }
     }
-    sr = warp_sum(sr);
-    if (CPLX) si = warp_sum(si);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+#pragma unroll
+    for (int u = 0; u < kG; ++u) {
+      if (u >= g) break;
+      const double a = warp_sum(sr[u]);
+      const double b = CPLX ? warp_sum(si[u]) : 0.0;
+      if (l == 0) { red[0][u][w] = a; red[1][u][w] = b; }
+    }
     __syncthreads();
-    if (threadIdx.x < 32) {
-      const int nw = blockDim.x >> 5;
-      double a = (l < nw) ? red[0][l] : 0.0, b = (l < nw) ? red[1][l] : 0.0;
+    if (w < g) {   // warp u adds up dot j0 + u over the block's warps
+      double a = (l < nw) ? red[0][w][l] : 0.0, b = (l < nw) ? red[1][w][l] : 0.0;
       a = warp_sum(a);
       if (CPLX) b = warp_sum(b);
       if (l == 0) {
-        partial[(blockIdx.x * (long long)nv + j) * 2 + 0] = a;
-        partial[(blockIdx.x * (long long)nv + j) * 2 + 1] = b;
+        partial[(blockIdx.x * (long long)nv + j0 + w) * 2 + 0] = a;
+        partial[(blockIdx.x * (long long)nv + j0 + w) * 2 + 1] = b;
       }
     }
     __syncthreads();
   }
-}
-
-template <bool CPLX>
-// one warp per dot: lane l sums partials l, l + 32, ... and the warp adds the
-// 32 sums in a fixed tree (the same order every call)
-__global__ void multi_dot_final(const double* partial, int npart, int nv, void* out) {
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), l = threadIdx.x & 31;
-  if (j >= nv) return;
-  double a = 0.0, b = 0.0;
-  for (int p = l; p < npart; p += 32) {
-    a += partial[(p * (long long)nv + j) * 2 + 0];
-    if (CPLX) b += partial[(p * (long long)nv + j) * 2 + 1];
+  __threadfence();   // every writer's partials before the count
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int j = w; j < nv; j += nw) {
+    double a = 0.0, b = 0.0;
+    for (int p = l; p < (int)gridDim.x; p += 32) {
+      a += __ldcg(partial + (p * (long long)nv + j) * 2 + 0);
+      if (CPLX) b += __ldcg(partial + (p * (long long)nv + j) * 2 + 1);
+    }
+    a = warp_sum(a);
+    if (CPLX) b = warp_sum(b);
+    if (l == 0) {
+      if (CPLX) static_cast<double2*>(out)[j] = make_double2(a, b);
+      else static_cast<double*>(out)[j] = a;
+    }
   }
-  a = warp_sum(a);
-  if (CPLX) b = warp_sum(b);
-  if (l == 0) {
-    if (CPLX) static_cast<double2*>(out)[j] = make_double2(a, b);
-    else static_cast<double*>(out)[j] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (op >= 0) lanczos_scalar_op<CPLX>(op, out, beta_prev, sout);
+    *counter = 0u;
   }
 }
 
 void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n, double* partial,
-                      int npart, void* out, cudaStream_t s) {
+                      int npart, void* out, unsigned* counter, cudaStream_t s, int scalar_op, const double* beta_prev,
+                      void* scalar_out) {
   if (nv <= 0) return;
-  if (cplx) {
-    multi_dot_partial<true><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
-    multi_dot_final<true><<<(nv + 3) / 4, 128, 0, s>>>(partial, npart, nv, out);
-  } else {
-    multi_dot_partial<false><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial);
-    multi_dot_final<false><<<(nv + 3) / 4, 128, 0, s>>>(partial, npart, nv, out);
-  }
+  if (cplx)
+    multi_dot_fused<true><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial, out, counter, scalar_op, beta_prev,
+                                               scalar_out);
+  else
+    multi_dot_fused<false><<<npart, 256, 0, s>>>(V, ldv, nv, x, n, partial, out, counter, scalar_op, beta_prev,
+                                                scalar_out);
 }
 
 template <bool CPLX>

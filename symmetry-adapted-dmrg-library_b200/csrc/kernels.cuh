@@ -185,9 +185,12 @@ void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStre
 void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s);
 
 // ---- Krylov vector operations ---------------------------------------------
-// out[j] = <V_j | x> (conjugated first argument), j < nv, deterministic
+// out[j] = <V_j | x> (conjugated first argument), j < nv, deterministic, one launch
+// (counter: a device word, zero between launches).  scalar_op >= 0 also applies
+// the lanczos_scalar step `scalar_op` to out[0] (into scalar_out) in the same launch.
 void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n,
-                      double* partial, int npart, void* out, cudaStream_t s);
+                      double* partial, int npart, void* out, unsigned* counter, cudaStream_t s, int scalar_op = -1,
+                      const double* beta_prev = nullptr, void* scalar_out = nullptr);
 // x -= sum_j c[j] V_j   (c read from device memory)
 void launch_multi_axpy(bool cplx, void* x, const void* V, long long ldv, int nv, const void* c, long long n,
                        cudaStream_t s);

@@ -12,6 +12,7 @@ namespace sadmrg {
 Ctx::~Ctx() {
   if (d_scalars) cudaFree(d_scalars);
   if (d_partial) cudaFree(d_partial);
+  if (d_counter) cudaFree(d_counter);
   if (h_pinned) cudaFreeHost(h_pinned);
 }
 

@@ -28,6 +28,7 @@ struct Ctx {
   std::unique_ptr<CGCFactors> cgc;
   double* d_scalars = nullptr;   // small device scratch for reductions
   double* d_partial = nullptr;
+  unsigned* d_counter = nullptr; // last-block counter of the one-launch reductions (zero between launches)
   double* h_pinned = nullptr;    // page-locked host scratch (kPinnedDoubles) for async scalar reads
   static constexpr int kPinnedDoubles = 4096;
   int npart = 296;
