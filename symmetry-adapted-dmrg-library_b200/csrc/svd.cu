@@ -180,6 +180,23 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   }
   __syncthreads();
 
+  // a pair that needs no rotation on the fresh G keeps the inner sweep from
+  // rotating at all: skip the visit when no pair of it does
+  {
+    int need = 0;
+    for (int e = tid; e < nc * nc; e += kSvdThreads) {
+      const int p = e / nc, q = e % nc;
+      if (p >= q) continue;
+      const double a = cre(G[p * kLdG + p]), b = cre(G[q * kLdG + q]);
+      const T gpq = G[p * kLdG + q];
+      double g;
+      if constexpr (CPLX) g = sqrt(gpq.x * gpq.x + gpq.y * gpq.y); else g = fabs(gpq);
+      const double nrm = sqrt(fmax(a, 0.0)) * sqrt(fmax(b, 0.0));
+      if (nrm > 1e-300 && g > tol * nrm) need = 1;
+    }
+    if (!__syncthreads_or(need)) return;
+  }
+
   // 2. inner sweeps on G
   const int N = nc + (nc & 1);
   for (int isw = 0; isw < kInnerMax && N > 1; ++isw) {
