@@ -275,7 +275,7 @@ struct Krylov {
 };
 
 template <class S>
-LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
+LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test) {
   LanczosStats st;
   const long long n = H.n;
   Krylov<S> K(c, n, mlanc);
@@ -402,6 +402,18 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec) {
     }
     diatridiag(m);
     if (m % 4 == 0) {
+      if (residual_test) {
+        // |H y - theta y| = b_m |z_m| for the Ritz pair (theta, y) of the m steps; the
+        // overlap test |<y|Hy>|/|Hy| - 1 ~ r^2 / (2 theta^2) without the check matvec
+        const double r = nnl[m] * std::fabs(z[m - 1]);
+        if (r * r < 2.0 * c.lanczos_ov_tol * eig[0] * eig[0]) {
+          ritz_vec(m);
+          st.energy = eig[0];
+          st.overlap = 1.0 - r * r / (2.0 * eig[0] * eig[0]);
+          return st;
+        }
+        continue;
+      }
       ritz_vec(m);
       check(ee, ov);
       if (std::fabs(ov - 1.0) < c.lanczos_ov_tol) { st.energy = eig[0]; return st; }
@@ -424,11 +436,13 @@ LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int pr
   // |<v|Hv>|/|Hv| - 1 ~ |error of v|^2, and the 3xTF32 operator (relative error
   // ~1e-7) leaves v accurate to ~1e-5 at best, so a tighter test only buys
   // matvecs the FP64 restart makes up for anyway.
+  // It stops on the Lanczos residual estimate b_m |z_m| (no check matvecs); the
+  // FP64 restart below is the reference's lanczos1 with its own checks.
   const double tol = c.lanczos_ov_tol;
   c.lanczos_ov_tol = std::max(tol, 1e-10);
   LanczosStats a;
   try {
-    a = lanczos1<S>(c, H, v, mlanc, prec);
+    a = lanczos1<S>(c, H, v, mlanc, prec, /*residual_test=*/true);
   } catch (...) {
     c.lanczos_ov_tol = tol;
     throw;
@@ -1194,8 +1208,8 @@ template HeffPlan<double> build_heff<double>(Ctx&, const BTensor<double>&, const
 template HeffPlan<dcmplex> build_heff<dcmplex>(Ctx&, const BTensor<dcmplex>&, const BTensor<dcmplex>*,
                                                const BTensor<dcmplex>*, const std::vector<const BTensor<dcmplex>*>&,
                                                const std::vector<PairTerm>&);
-template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
-template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
+template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool);
+template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool);
 template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
 template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
 template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,
