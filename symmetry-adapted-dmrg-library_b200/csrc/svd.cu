@@ -187,12 +187,11 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     for (int e = tid; e < nc * nc; e += kSvdThreads) {
       const int p = e / nc, q = e % nc;
       if (p >= q) continue;
-      const double a = cre(G[p * kLdG + p]), b = cre(G[q * kLdG + q]);
+      const double ab = cre(G[p * kLdG + p]) * cre(G[q * kLdG + q]);
       const T gpq = G[p * kLdG + q];
-      double g;
-      if constexpr (CPLX) g = sqrt(gpq.x * gpq.x + gpq.y * gpq.y); else g = fabs(gpq);
-      const double nrm = sqrt(fmax(a, 0.0)) * sqrt(fmax(b, 0.0));
-      if (nrm > 1e-300 && g > tol * nrm) need = 1;
+      double g2;
+      if constexpr (CPLX) g2 = gpq.x * gpq.x + gpq.y * gpq.y; else g2 = gpq * gpq;
+      if (ab > 0.0 && g2 > tol * tol * ab) need = 1;
     }
     if (!__syncthreads_or(need)) return;
   }
@@ -216,19 +215,22 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
           const T gpq = G[p * kLdG + q];
           double gr, gi = 0.0;
           if constexpr (CPLX) { gr = gpq.x; gi = gpq.y; } else { gr = gpq; }
-          const double g = CPLX ? sqrt(gr * gr + gi * gi) : fabs(gr);
-          const double nrm = sqrt(fmax(a, 0.0)) * sqrt(fmax(b, 0.0));
-          if (nrm > 1e-300 && g > tol * nrm) {
+          const double g2 = gr * gr + gi * gi;
+          // rotate when |g| > tol sqrt(ab), compared squared; the parameters keep the
+          // dependent chain of square roots and divisions short (it sets the round time)
+          if (a * b > 0.0 && g2 > tol * tol * (a * b)) {
+            const double g = CPLX ? sqrt(g2) : fabs(gr);
+            const double ig = 1.0 / g;
             // same rotation as on the columns; for |zeta| > 1e150 zeta^2 would overflow
-            const double zeta = (b - a) / (2.0 * g);
+            const double zeta = 0.5 * (b - a) * ig;
             const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
-                                                : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                                                : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
             if (t != 0.0) {
               act = true;
-              c = 1.0 / sqrt(1.0 + t * t);
+              c = rsqrt(1.0 + t * t);
               s = c * t;
-              er = CPLX ? gr / g : (gr >= 0.0 ? 1.0 : -1.0);
-              ei = CPLX ? gi / g : 0.0;
+              er = CPLX ? gr * ig : (gr >= 0.0 ? 1.0 : -1.0);
+              ei = CPLX ? gi * ig : 0.0;
               tg = t * g;
             }
           }
