@@ -403,7 +403,10 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
       ntile += tiles;
       total += tiles * std::max<long long>(ns, 1);
     }
-    long long kc = std::max<long long>(4, (total + target - 1) / target);
+    // slabs per chunk: about one SM's share of the stage and never below 16 --
+    // every split item pays for an FP32 partial tile and the fix-up, which at
+    // 4 slabs per chunk cost more than the balance won (D=512: 99 -> 60 us)
+    long long kc = std::max<long long>(16, (total + nsm - 1) / nsm);
     if (ntile >= target / 2) kc = (long long)1 << 40;
     std::vector<std::pair<long long, UItem>> its;
     for (size_t j = 0; j < jobs.size(); ++j) {
