@@ -81,10 +81,11 @@ int sadmrg_device_status(sadmrg_handle* h, int* status);
  * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338). */
 int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol);
 
-/* How the split-precision matvec of real plans is launched (no counterpart in
- * the reference): 0 (default) psi -> panels, then one tcgen05 launch per stage;
- * 1 the whole matvec as one cooperative launch whose work items wait (bounded)
- * for the panels they read. */
+/* How the split-precision matvec is launched (no counterpart in the reference):
+ * 0 psi -> panels, then one tcgen05 launch per stage; 1 the whole matvec as one
+ * cooperative launch whose work items wait (bounded) for the panels they read;
+ * -1 (default) one launch for plans below 4 GFLOP per matvec (latency bound),
+ * one per stage above.  All three give the same bits. */
 int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused);
 
 /* ---- frozen two-site problem: H_eff * psi ---------------------------------

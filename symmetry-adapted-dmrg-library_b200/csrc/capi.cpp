@@ -209,8 +209,8 @@ int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol) {
 
 int sadmrg_set_matvec_fusion(sadmrg_handle* h, int fused) {
   return guard(h, [&]() {
-    SADMRG_REQUIRE(fused == 0 || fused == 1, SADMRG_ERR_ARG, "set_matvec_fusion: 0 or 1");
-    h->ctx.fused_matvec = fused != 0;
+    SADMRG_REQUIRE(fused >= -1 && fused <= 1, SADMRG_ERR_ARG, "set_matvec_fusion: -1, 0 or 1");
+    h->ctx.fused_matvec = fused;
   });
 }
 
@@ -469,7 +469,8 @@ int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const voi
     cudaEventDestroy(e1);
     cudaGraphExecDestroy(ge);
     cudaGraphDestroy(g);
-    c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision, c.fused_matvec) * (reps + 1);
+    c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision,
+                                                   H.plan.runs_fused(c, ScalarInfo<S>::cplx, precision)) * (reps + 1);
     check_device_status();
   });
 }

@@ -502,6 +502,13 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   return true;
 }
 
+bool GemmPlan::runs_fused(const Ctx& c, bool cplx, int prec) const {
+  if (!uses_umma(cplx, prec) || c.job_mask || (int)umma->vpack.size() > kMaxPackJobs) return false;
+  // small plans are latency bound and gain from one launch (D=512: 57 -> 46 us);
+  // large ones lose to the dependency waits (D=2048: 494 -> 583 us)
+  return c.fused_matvec > 0 || (c.fused_matvec < 0 && (double)flops < Ctx::kAutoFuseFlops);
+}
+
 int GemmPlan::launches_per_run(bool cplx, int prec, bool c_fused) const {
   int n = 0;
   if (uses_umma(cplx, prec)) {
@@ -545,7 +552,7 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
     ph.npk_jobs = (int)U.vpack.size();
     ph.ndeps = (int)U.dep_target.size();
     const bool whole = stage_lo == 0 && stage_hi == nstage;
-    if (whole && c.fused_matvec && !c.job_mask && (int)U.vpack.size() <= kMaxPackJobs) {
+    if (whole && runs_fused(c, cplx, prec)) {
       // the whole matvec in one cooperative launch: psi packing, stage 0, stage 1
       ph.npk_blocks = (int)U.vblk.size();
       ph.wait_deps = 1;

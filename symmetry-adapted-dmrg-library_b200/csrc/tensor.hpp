@@ -33,7 +33,10 @@ struct Ctx {
   static constexpr int kPinnedDoubles = 4096;
   int npart = 296;
   double lanczos_ov_tol = 1e-8;  // stop when |<v|Hv>|/|Hv| is this close to 1 (src/dmrg_inst.cpp:1338)
-  bool fused_matvec = false;     // tcgen05 matvec as one cooperative launch instead of pack + two launches
+  // tcgen05 matvec as one cooperative launch instead of pack + one launch per
+  // stage: 1 always, 0 never, -1 (default) for plans below kAutoFuseFlops
+  int fused_matvec = -1;
+  static constexpr double kAutoFuseFlops = 4e9;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
@@ -147,6 +150,8 @@ struct GemmPlan {
     return uses_umma(cplx, prec) ? umma->slot_bytes() : sched.work_bytes();
   }
   int launches_per_run(bool cplx, int prec, bool fused) const;
+  // whether run() takes the single-launch path for a whole matvec under c's setting
+  bool runs_fused(const Ctx& c, bool cplx, int prec) const;
   bool empty() const { return jobs.empty(); }
 
  private:

@@ -221,9 +221,11 @@ class Handle:
             msg = self.lib.sadmrg_last_error(self.h)
             raise SadmrgError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
 
-    def set_matvec_fusion(self, fused: bool):
-        """True: the split-precision matvec as one cooperative launch."""
-        self._check(self.lib.sadmrg_set_matvec_fusion(self.h, int(bool(fused))), "set_matvec_fusion")
+    def set_matvec_fusion(self, fused: Optional[bool]):
+        """True: the split-precision matvec as one cooperative launch; False: pack + one
+        launch per stage; None (the default): one launch for small plans only."""
+        self._check(self.lib.sadmrg_set_matvec_fusion(self.h, -1 if fused is None else int(bool(fused))),
+                    "set_matvec_fusion")
 
     def set_lanczos_tol(self, ov_tol: float):
         self._check(self.lib.sadmrg_set_lanczos_tol(self.h, float(ov_tol)), "set_lanczos_tol")

@@ -63,12 +63,18 @@ def test_umma_fused_launch_matches():
     import sadmrg
     for sym, L, D in ((1, 40, 192), (0, 32, 160)):
         h, psi = _centre(sym, L, D)
+        h.set_matvec_fusion(False)
         a = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
+        kinds = {k for k, _ in h.heff_launch_profile(sadmrg.PREC_TF32X3, 1)}
+        assert 5 not in kinds and 0 in kinds
         h.set_matvec_fusion(True)
         b = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
         c = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
-        h.set_matvec_fusion(False)
-        assert np.array_equal(a, b) and np.array_equal(b, c)
+        assert {k for k, _ in h.heff_launch_profile(sadmrg.PREC_TF32X3, 1)} == {5}
+        h.set_matvec_fusion(None)   # the default: these plans are small, so one launch
+        d = h.heff_apply(psi.data, sadmrg.PREC_TF32X3)
+        assert {k for k, _ in h.heff_launch_profile(sadmrg.PREC_TF32X3, 1)} == {5}
+        assert np.array_equal(a, b) and np.array_equal(b, c) and np.array_equal(c, d)
         assert h.device_status() == 0
 
 
