@@ -48,7 +48,7 @@ struct Bases {
 
 // Item kernel families.  GEMM_MMA_SYNC: FP64 DMMA and the mma.sync 3xTF32
 // (gemm.cu); GEMM_UMMA: tcgen05 3xTF32 over pre-split operand panels with the
-// accumulator in tensor memory, real data only (umma.cu).
+// accumulator in tensor memory, complex plans in real form (umma.cu).
 enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
 
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).

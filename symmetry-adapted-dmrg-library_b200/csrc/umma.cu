@@ -1,5 +1,6 @@
 // umma.cu -- 3xTF32 grouped block-GEMM on the fifth-generation tensor cores
-// (tcgen05.mma .kind::tf32, FP32 accumulators in tensor memory), real data.
+// (tcgen05.mma .kind::tf32, FP32 accumulators in tensor memory); complex plans
+// run in the real form described in kernels.cuh.
 //
 // Operands are pre-split into TF32 hi/lo panels (layout in kernels.cuh): the
 // constant operators once per plan, psi once per matvec (pack_kernel), and the
