@@ -275,7 +275,9 @@ struct Krylov {
 };
 
 template <class S>
-LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test) {
+LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test,
+                      int check_every) {
+  if (!residual_test || check_every < 1) check_every = 4;
   LanczosStats st;
   const long long n = H.n;
   Krylov<S> K(c, n, mlanc);
@@ -390,7 +392,7 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, b
   // and the steps queued after it are discarded.
   for (int m = 2; m < mlanc; ++m) {
     step(m, true);
-    if (m % 4 != 0 && m != mlanc - 1) continue;
+    if (m % check_every != 0 && m != mlanc - 1) continue;
     const int brk = sync_to(m);
     if (brk) {
       st.iters = brk;
@@ -401,7 +403,7 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, b
       return st;
     }
     diatridiag(m);
-    if (m % 4 == 0) {
+    if (m % check_every == 0) {
       if (residual_test) {
         // |H y - theta y| = b_m |z_m| for the Ritz pair (theta, y) of the m steps; the
         // overlap test |<y|Hy>|/|Hy| - 1 ~ r^2 / (2 theta^2) without the check matvec
@@ -436,8 +438,9 @@ LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int pr
   // |<v|Hv>|/|Hv| - 1 ~ |error of v|^2, and the 3xTF32 operator (relative error
   // ~1e-7) leaves v accurate to ~1e-5 at best, so a tighter test only buys
   // matvecs the FP64 restart makes up for anyway.
-  // It stops on the Lanczos residual estimate b_m |z_m| (no check matvecs); the
-  // FP64 restart below is the reference's lanczos1 with its own checks.
+  // It stops on the Lanczos residual estimate b_m |z_m| (no check matvecs); so
+  // does the FP64 restart below (the reference's lanczos1 with FP64 matvecs,
+  // tested after every step).  prec == PREC_FP64 alone keeps the reference's checks.
   const double tol = c.lanczos_ov_tol;
   c.lanczos_ov_tol = std::max(tol, 1e-10);
   LanczosStats a;
@@ -448,7 +451,10 @@ LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int pr
     throw;
   }
   c.lanczos_ov_tol = tol;
-  LanczosStats b = lanczos1<S>(c, H, v, mlanc, PREC_FP64);  // FP64 defect-correction restart
+  // FP64 defect-correction restart: from a vector already near the TF32 floor it
+  // converges within a few steps, so it tests the (free) residual estimate after
+  // every step rather than spending a check matvec every 4 steps
+  LanczosStats b = lanczos1<S>(c, H, v, mlanc, PREC_FP64, /*residual_test=*/true, /*check_every=*/1);
   b.matvecs += a.matvecs;
   b.iters += a.iters;
   return b;
@@ -1208,8 +1214,8 @@ template HeffPlan<double> build_heff<double>(Ctx&, const BTensor<double>&, const
 template HeffPlan<dcmplex> build_heff<dcmplex>(Ctx&, const BTensor<dcmplex>&, const BTensor<dcmplex>*,
                                                const BTensor<dcmplex>*, const std::vector<const BTensor<dcmplex>*>&,
                                                const std::vector<PairTerm>&);
-template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool);
-template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool);
+template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool, int);
+template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool, int);
 template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
 template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
 template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,

@@ -57,10 +57,11 @@ struct LanczosStats {
 // Lanczos::lanczos1 (src/dmrg_inst.cpp:1286-1348) on device vectors.
 // v (length n) holds the start vector on entry and the Ritz vector on exit.
 // residual_test: at the check points stop on the Lanczos residual estimate
-// b_m |z_m| instead of the reference's check matvec (used by the split-precision
-// phase of the mixed solver only).
+// b_m |z_m| instead of the reference's check matvec, with check points every
+// check_every steps (the reference: 4); used by the mixed solver only.
 template <class S>
-LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test = false);
+LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test = false,
+                      int check_every = 4);
 // Mixed precision: lanczos1 with 3xTF32 matvecs, then an FP64 restart from
 // its Ritz vector (defect correction) so the energy is an FP64 Lanczos result.
 template <class S>
