@@ -147,6 +147,11 @@ int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const voi
  * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
  * FP64 restart from its result. */
 int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precision, double* energy, int* matvecs);
+/* Lanczos::lanczos2 (src/dmrg_inst.cpp:1352-1397), FP64: the same recurrence
+ * without convergence checks -- all mlanc steps; at a breakdown (b < 1e-6 from
+ * step 2) the Ritz pair of the steps before it.  psi is overwritten by the Ritz
+ * vector. */
+int sadmrg_heff_lanczos2(sadmrg_handle* h, void* psi_host, int mlanc, double* energy, int* matvecs);
 
 /* ---- many independent instances, one launch per stage ---------------------
  * No counterpart in the reference (one DMRG per process).  sadmrg_batch_add

@@ -494,6 +494,25 @@ int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precisi
   });
 }
 
+int sadmrg_heff_lanczos2(sadmrg_handle* h, void* psi_host, int mlanc, double* energy, int* matvecs) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_lanczos2: no plan");
+    SADMRG_REQUIRE(mlanc >= 2, SADMRG_ERR_ARG, "heff_lanczos2: mlanc < 2");
+    const long long n = S_.heff->n;
+    S* dv = S_.io.template as<S>();
+    SADMRG_CUDA(cudaMemcpyAsync(dv, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
+    LanczosStats st = lanczos2<S>(c, *S_.heff, dv, mlanc);
+    SADMRG_CUDA(cudaMemcpyAsync(psi_host, dv, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    check_device_status();
+    if (energy) *energy = st.energy;
+    if (matvecs) *matvecs = st.matvecs;
+  });
+}
+
 // ---- many instances in one launch ------------------------------------------
 int sadmrg_batch_add(sadmrg_handle* h, sadmrg_handle* inst) {
   if (!inst) return h ? fail(h, SADMRG_ERR_ARG, "batch_add: null instance") : SADMRG_ERR_ARG;

@@ -276,8 +276,9 @@ struct Krylov {
 
 template <class S>
 LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test,
-                      int check_every) {
+                      int check_every, bool variant2) {
   if (!residual_test || check_every < 1) check_every = 4;
+  if (variant2) check_every = mlanc + 1;   // lanczos2: no check points before the last step
   LanczosStats st;
   const long long n = H.n;
   Krylov<S> K(c, n, mlanc);
@@ -394,6 +395,16 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, b
     step(m, true);
     if (m % check_every != 0 && m != mlanc - 1) continue;
     const int brk = sync_to(m);
+    if (brk && variant2) {
+      // Lanczos::lanczos2 returns at a breakdown with the Ritz pair of the steps
+      // before it (computed in its previous iteration; at step 2 that is T_1)
+      st.iters = brk;
+      diatridiag(brk - 1);
+      ritz_vec(brk - 1);
+      K.scale_host(v, 1.0 / std::sqrt(std::fabs(real_of(K.dot_host(v, v)))));
+      st.energy = eig[0];
+      return st;
+    }
     if (brk) {
       st.iters = brk;
       diatridiag(brk);
@@ -426,9 +437,14 @@ LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, b
   aal[mlanc - 1] = real_of(K.dot_host(K.F(mlanc - 1), K.F(mlanc)));
   diatridiag(mlanc);
   ritz_vec(mlanc);
-  check(ee, ov);
+  if (!variant2) check(ee, ov);
   st.energy = eig[0];
   return st;
+}
+
+template <class S>
+LanczosStats lanczos2(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc) {
+  return lanczos1<S>(c, H, v, mlanc, PREC_FP64, false, 4, /*variant2=*/true);
 }
 
 template <class S>
@@ -1214,8 +1230,10 @@ template HeffPlan<double> build_heff<double>(Ctx&, const BTensor<double>&, const
 template HeffPlan<dcmplex> build_heff<dcmplex>(Ctx&, const BTensor<dcmplex>&, const BTensor<dcmplex>*,
                                                const BTensor<dcmplex>*, const std::vector<const BTensor<dcmplex>*>&,
                                                const std::vector<PairTerm>&);
-template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool, int);
-template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool, int);
+template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool, int, bool);
+template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool, int, bool);
+template LanczosStats lanczos2<double>(Ctx&, const HeffPlan<double>&, double*, int);
+template LanczosStats lanczos2<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int);
 template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
 template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
 template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,

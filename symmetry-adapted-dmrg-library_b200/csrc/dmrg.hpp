@@ -61,7 +61,13 @@ struct LanczosStats {
 // check_every steps (the reference: 4); used by the mixed solver only.
 template <class S>
 LanczosStats lanczos1(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int prec, bool residual_test = false,
-                      int check_every = 4);
+                      int check_every = 4, bool variant2 = false);
+// Lanczos::lanczos2 (src/dmrg_inst.cpp:1352-1397), FP64: the same recurrence with
+// full reorthogonalisation but no convergence checks -- all mlanc steps, the
+// energy and Ritz vector of the full tridiagonal; a breakdown (b < 1e-6, from
+// step 2) returns the Ritz pair of the steps before it.
+template <class S>
+LanczosStats lanczos2(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc);
 // Mixed precision: lanczos1 with 3xTF32 matvecs, then an FP64 restart from
 // its Ritz vector (defect correction) so the energy is an FP64 Lanczos result.
 template <class S>

@@ -29,7 +29,7 @@ PREC_FP64, PREC_TF32X3 = 0, 1
 EXPORTED = [
     "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
     "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device", "sadmrg_heff_apply_noalloc",
-    "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_svd_truncate",
+    "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_heff_lanczos2", "sadmrg_svd_truncate",
     "sadmrg_chain_create", "sadmrg_chain_set_dm", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
@@ -84,6 +84,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_apply_device": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_apply_noalloc": ([vp, vp, vp, C.c_int], C.c_int),
         "sadmrg_heff_lanczos": ([vp, vp, C.c_int, C.c_int, dp, ip], C.c_int),
+        "sadmrg_heff_lanczos2": ([vp, vp, C.c_int, dp, ip], C.c_int),
         "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
         "sadmrg_heff_launch_profile": ([vp, C.c_int, C.c_int, vp, vp, C.c_int, ip, ip, dp], C.c_int),
         "sadmrg_heff_graph_bench": ([vp, C.c_int, C.c_int, vp, vp, dp], C.c_int),
@@ -364,6 +365,15 @@ class Handle:
         mv = C.c_int()
         self._check(self.lib.sadmrg_heff_lanczos(self.h, x.ctypes.data, int(mlanc), int(precision), C.byref(e),
                                                  C.byref(mv)), "heff_lanczos")
+        return e.value, x, mv.value
+
+    def heff_lanczos2(self, psi: np.ndarray, mlanc: int = 40):
+        """Lanczos::lanczos2 (FP64, no convergence checks): (energy, Ritz vector, matvecs)."""
+        x = np.array(psi, dtype=self.dtype, copy=True)
+        e = C.c_double()
+        mv = C.c_int()
+        self._check(self.lib.sadmrg_heff_lanczos2(self.h, x.ctypes.data, int(mlanc), C.byref(e), C.byref(mv)),
+                    "heff_lanczos2")
         return e.value, x, mv.value
 
     # -- SVD -------------------------------------------------------------------
