@@ -653,7 +653,9 @@ def main():
                    "symmetry": "SU2" if wl["sym"] else "U1", "bond": f"centre ({n} psi elements)",
                    "flops_per_step": flops, "tasks": info["ntasks"], "l2": "flushed (256 MiB write) between steps",
                    "parallelism": f"replicas x{ws}"},
-        "fp64": {"value": value64, "ms_per_step": step_64, "speedup_mixed_over_fp64": value / value64},
+        "matvecs_per_s": ws * 1e3 / step_mix,
+        "fp64": {"value": value64, "ms_per_step": step_64, "matvecs_per_s": ws * 1e3 / step_64,
+                 "speedup_mixed_over_fp64": value / value64},
         "accuracy": {"matvec_rel_err_tf32x3": mv_err, "lanczos_E_fp64": e64, "lanczos_E_mixed": emx,
                      "abs_dE": None if e64 is None else abs(emx - e64), "lanczos_s_fp64": t_l64,
                      "lanczos_s_mixed": t_lmx, "matvecs_fp64": mv64, "matvecs_mixed": mvmx},
