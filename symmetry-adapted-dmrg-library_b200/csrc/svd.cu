@@ -69,6 +69,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 }
 
 constexpr int kNc = 2 * kSvdB;         // columns of one visit
+constexpr int kTD = kNc / 8;           // 8 x 8 DMMA tiles along one side of G
 constexpr int kLdG = kNc + 1;          // row stride of G, Q and the row chunk (padding against bank conflicts)
 constexpr int kChunk = 128;            // rows per streamed chunk of W or V
 constexpr int kChunkPer = kChunk * kNc / kSvdThreads;   // chunk elements per thread
@@ -121,9 +122,12 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   }
   __syncthreads();
 
-  // 1. Gram matrix on the FP64 tensor cores: warp w owns the 8 x 8 tile (w / 4, w % 4)
-  //    of G = Wp^H Wp; k runs over the rows of the chunk (zero-filled past the block)
-  const int pt = warp >> 2, qt = warp & 3;
+  // 1. Gram matrix on the FP64 tensor cores: warp w < kTD^2 owns the 8 x 8 tile
+  //    (w / kTD, w % kTD) of G = Wp^H Wp; k runs over the rows of the chunk
+  //    (zero-filled past the block)
+  static_assert(kNc % 8 == 0 && kTD * kTD <= kSvdWarps, "one warp per Gram tile");
+  const bool gram_warp = warp < kTD * kTD;
+  const int pt = warp / kTD, qt = warp % kTD;
   const int fr = lane >> 2, fk = lane & 3;
   double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;   // Re (and Im) of D(fr, 2 fk + i)
   // Row chunks of a column set (W or V), read into registers one chunk ahead of
@@ -149,7 +153,7 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     __syncthreads();
     if (r0 + kChunk < R) fetch(W, R, r0 + kChunk, min(kChunk, R - r0 - kChunk));
 #pragma unroll 4
-    for (int k0 = 0; k0 < kChunk; k0 += 4) {
+    for (int k0 = 0; k0 < kChunk && gram_warp; k0 += 4) {
       const T x = Ck[(k0 + fk) * kLdG + pt * 8 + fr];   // A(p, r) = conj(W(r, p))
       const T y = Ck[(k0 + fk) * kLdG + qt * 8 + fr];   // B(r, q) = W(r, q)
       if constexpr (CPLX) {
@@ -164,7 +168,7 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     __syncthreads();
   }
   // stored from the tiles on and above the diagonal, mirrored, so that G is exactly Hermitian
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < 2 && gram_warp; ++i) {
     const int p = pt * 8 + fr, q = qt * 8 + 2 * fk + i;
     if (p > q) continue;
     T v;
@@ -320,7 +324,7 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     double d[kTiles][4];
 #pragma unroll
     for (int u = 0; u < kTiles; ++u) {
-      const int t = warp + kSvdWarps * u, rt = t >> 2, jt = t & 3;
+      const int t = warp + kSvdWarps * u, rt = t / kTD, jt = t % kTD;
       double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
 #pragma unroll
       for (int k0 = 0; k0 < kNc; k0 += 4) {
@@ -340,7 +344,7 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < kTiles; ++u) {
-      const int t = warp + kSvdWarps * u, rt = t >> 2, jt = t & 3;
+      const int t = warp + kSvdWarps * u, rt = t / kTD, jt = t % kTD;
       for (int i = 0; i < 2; ++i) {
         T v;
         if constexpr (CPLX) v = make_double2(d[u][i], d[u][2 + i]);
