@@ -6,10 +6,11 @@
 // with the parallel block ordering of Brent & Luk and the norm-sorted column
 // order of de Rijk 1989).  The C = min(m,n) columns of W (A, or A^H when m < n)
 // are ordered by decreasing norm at the start of every sweep and split into
-// column blocks of b = 16.  Every round of a sweep pairs the blocks by the
-// circle method; one CTA forms the 32 x 32 Gram matrix of its pair on the FP64
+// column blocks of b = 8 or 16 (chosen per call).  Every round of a sweep
+// pairs the blocks by the circle method; one CTA forms the 2b x 2b Gram matrix
+// of its pair on the FP64
 // tensor cores (DMMA, W streamed in row chunks), runs a cyclic sweep of the
-// one-sided rotations on it, and applies the accumulated 32 x 32 rotation to
+// one-sided rotations on it, and applies the accumulated 2b x 2b rotation to
 // the pair's columns of W and V (DMMA again).  Sweeps repeat until a full sweep
 // performs no rotation, so the result keeps the columnwise relative accuracy of
 // one-sided Jacobi on small singular values, which the reference's 1e-10
@@ -25,7 +26,7 @@ namespace sadmrg {
 
 constexpr int kSvdThreads = 512;
 constexpr int kSvdWarps = kSvdThreads / 32;
-constexpr int kSvdB = 16;              // columns per block; a visit takes two blocks
+// columns per block (a visit takes two blocks): 8 or 16, chosen per call by run_jacobi_svd
 
 struct SvdPair {
   int job, bi, bj, b;   // column blocks bi, bj (bj < 0: bi alone); b = block width
@@ -68,20 +69,24 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-constexpr int kNc = 2 * kSvdB;         // columns of one visit
-constexpr int kTD = kNc / 8;           // 8 x 8 DMMA tiles along one side of G
-constexpr int kLdG = kNc + 1;          // row stride of G, Q and the row chunk (padding against bank conflicts)
 constexpr int kChunk = 128;            // rows per streamed chunk of W or V
-constexpr int kChunkPer = kChunk * kNc / kSvdThreads;   // chunk elements per thread
 constexpr int kInnerMax = 1;           // inner sweeps of one visit (more cut outer sweeps by less than they cost)
 
-template <bool CPLX>
+template <int B>                       // B: columns per block
+struct SvdGeom {
+  static constexpr int Nc = 2 * B;                          // columns of one visit
+  static constexpr int TD = Nc / 8;                         // 8 x 8 DMMA tiles along one side of G
+  static constexpr int Ld = Nc + 1;                         // row stride of G, Q and the row chunk
+  static constexpr int ChunkPer = kChunk * Nc / kSvdThreads;   // chunk elements per thread
+};
+
+template <bool CPLX, int B>
 constexpr size_t svd_smem_bytes() {
-  return (size_t)(2 * kNc + kChunk) * kLdG * (CPLX ? 16 : 8);
+  return (size_t)(2 * SvdGeom<B>::Nc + kChunk) * SvdGeom<B>::Ld * (CPLX ? 16 : 8);
 }
 
 // One visit of a column-block pair (Hestenes one-sided Jacobi in Gram form):
-//   1. G = Wp^H Wp for the pair's nc <= 32 columns Wp, streamed from W in row chunks;
+//   1. G = Wp^H Wp for the pair's nc <= 2B columns Wp, streamed from W in row chunks;
 //   2. cyclic one-sided Jacobi on G: rotation (p, q) from a = G_pp, b = G_qq,
 //      g = G_pq exactly as on the columns themselves, G <- J^H G J, Q <- Q J,
 //      with the rotated diagonal set to a - t|g|, b + t|g| and G_pq to 0; up to
@@ -94,10 +99,12 @@ constexpr size_t svd_smem_bytes() {
 // keep the columnwise relative accuracy of the direct method; W itself changes
 // only by the orthogonal Q.  Adds the number of rotations to *rotations.  Every
 // thread of the block calls it; 16 warps, warp k owns pair k of each round.
-template <bool CPLX>
+template <bool CPLX, int B>
 __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
                                   double tol, unsigned char* smem_raw, int* rotations) {
   using T = typename SvdT<CPLX>::T;
+  constexpr int kNc = SvdGeom<B>::Nc, kTD = SvdGeom<B>::TD, kLdG = SvdGeom<B>::Ld;
+  constexpr int kChunkPer = SvdGeom<B>::ChunkPer;
   static_assert(kSvdWarps * 2 >= kNc, "one warp per column pair of a round");
   const int R = J.trans ? J.n : J.m;
   const int C = J.trans ? J.m : J.n;
@@ -362,7 +369,7 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   if (tid == 0) atomicAdd(rotations, nrot);
 }
 
-template <bool CPLX>
+template <bool CPLX, int B>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
                                                                   const SvdPair* __restrict__ pairs, void* work,
                                                                   void* vmat, const int* perm, double tol,
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SvdPair P = pairs[blockIdx.x];
   const SvdJob J = jobs[P.job];
-  jacobi_pair_visit<CPLX>(J, P, work, vmat, perm, tol, smem_raw, rotations);
+  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
 }
 
 // ---------------------------------------------------------------------------
@@ -425,7 +432,7 @@ __device__ bool svd_grid_sync(SvdCtl* ctl) {
   return ok_sh != 0;
 }
 
-template <bool CPLX>
+template <bool CPLX, int B>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* __restrict__ jobs, int nj,
                                                                   const SvdPair* __restrict__ pairs,
                                                                   const int* __restrict__ roff, int max_rounds,
@@ -488,7 +495,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
         const SvdPair P = pairs[p];
         if (done[P.job]) continue;
         const SvdJob J = jobs[P.job];
-        jacobi_pair_visit<CPLX>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
+        jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
       }
       if (!svd_grid_sync(ctl)) return;
     }
@@ -558,11 +565,10 @@ __global__ void jacobi_norms_kernel(const SvdJob* jobs, const void* work, double
 // it, otherwise one launch per round and one host synchronisation per sweep to
 // test convergence.  Returns the number of sweeps taken (or -1 when max_sweeps
 // was reached).
-int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
-  if (kernel_ms) *kernel_ms = -1.0;
+template <bool CPLX, int B>
+static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
+                      int max_sweeps, cudaStream_t s, double* kernel_ms) {
   const int nj = (int)hjobs.size();
-  if (nj == 0) return 0;
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
   size_t smem = 0;
@@ -570,12 +576,12 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     const int R = hjobs[j].trans ? hjobs[j].n : hjobs[j].m;
     const int C = hjobs[j].trans ? hjobs[j].m : hjobs[j].n;
     maxR = std::max(maxR, R);
-    bsz[j] = kSvdB;
+    bsz[j] = B;
     nblk[j] = (C + bsz[j] - 1) / bsz[j];
     const int N = nblk[j] + (nblk[j] & 1);
     nrounds[j] = nblk[j] <= 1 ? 1 : N - 1;
     max_rounds = std::max(max_rounds, nrounds[j]);
-    smem = cplx ? svd_smem_bytes<true>() : svd_smem_bytes<false>();
+    smem = svd_smem_bytes<CPLX, B>();
   }
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
@@ -606,13 +612,9 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   SADMRG_CUDA(cudaMemcpyAsync(djobs.get(), hjobs.data(), sizeof(SvdJob) * nj, cudaMemcpyHostToDevice, s));
   SADMRG_CUDA(cudaMemcpyAsync(dpairs.get(), flat.data(), sizeof(SvdPair) * flat.size(), cudaMemcpyHostToDevice, s));
   dim3 ig(nj, 16);
-  if (cplx) jacobi_init_kernel<true><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
-  else jacobi_init_kernel<false><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
+  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
   SADMRG_CUDA(cudaGetLastError());
-  if (cplx)
-    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  else
-    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<CPLX, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const double tol = std::sqrt((double)std::max(maxR, 1)) * 2.220446049250313e-16;
   int sweeps = -1;
   int h_rot = 0;
@@ -621,13 +623,8 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   SADMRG_CUDA(cudaGetDevice(&dev));
   SADMRG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   SADMRG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  if (cplx) {
-    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_coop_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_coop_kernel<true>, kSvdThreads, smem));
-  } else {
-    SADMRG_CUDA(cudaFuncSetAttribute(jacobi_coop_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_coop_kernel<false>, kSvdThreads, smem));
-  }
+  SADMRG_CUDA(cudaFuncSetAttribute(jacobi_coop_kernel<CPLX, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_coop_kernel<CPLX, B>, kSvdThreads, smem));
   int max_pairs = 1;
   for (int r = 0; r < max_rounds; ++r) max_pairs = std::max(max_pairs, roff[r + 1] - roff[r]);
   if (coop && per_sm > 0 && nj <= kSvdMaxJobsCoop) {
@@ -650,20 +647,15 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     void* args[] = {(void*)&pj,     (void*)&njv,    (void*)&pp,   (void*)&pr, (void*)&mr,   (void*)&a_work,
                     (void*)&a_vmat, (void*)&a_nrm, (void*)&a_perm, (void*)&tolv, (void*)&pc, (void*)&pctl,
                     (void*)&ms};
-    if (cplx)
-      SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<true>, dim3(grid), dim3(kSvdThreads),
-                                              args, smem, s));
-    else
-      SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<false>, dim3(grid), dim3(kSvdThreads),
-                                              args, smem, s));
+    SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<CPLX, B>, dim3(grid), dim3(kSvdThreads),
+                                            args, smem, s));
     SvdCtl hctl{};
     SADMRG_CUDA(cudaMemcpyAsync(&hctl, dctl.get(), sizeof(SvdCtl), cudaMemcpyDeviceToHost, s));
     SADMRG_CUDA(cudaStreamSynchronize(s));
     SADMRG_REQUIRE(hctl.status == 0, SADMRG_ERR_CUDA, "jacobi svd: a grid barrier ran out of time");
     sweeps = hctl.sweeps;
     if (kernel_ms) *kernel_ms = (double)(hctl.t1 - hctl.t0) * 1e-6;
-    if (cplx) jacobi_norms_kernel<true><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
-    else jacobi_norms_kernel<false><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
+    jacobi_norms_kernel<CPLX><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
     SADMRG_CUDA(cudaGetLastError());
     return sweeps;
   }
@@ -672,11 +664,7 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     for (int r = 0; r < max_rounds; ++r) {
       const int np = roff[r + 1] - roff[r];
       if (np == 0) continue;
-      if (cplx)
-        jacobi_pair_kernel<true><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                               work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
-      else
-        jacobi_pair_kernel<false><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
+      jacobi_pair_kernel<CPLX, B><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
                                                                 work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
     }
     SADMRG_CUDA(cudaGetLastError());
@@ -684,10 +672,35 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     SADMRG_CUDA(cudaStreamSynchronize(s));
     if (h_rot == 0) { sweeps = sw + 1; break; }
   }
-  if (cplx) jacobi_norms_kernel<true><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
-  else jacobi_norms_kernel<false><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
+  jacobi_norms_kernel<CPLX><<<nj, 256, 0, s>>>(djobs.as<SvdJob>(), work, sv);
   SADMRG_CUDA(cudaGetLastError());
   return sweeps;
+}
+
+int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
+                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
+  if (kernel_ms) *kernel_ms = -1.0;
+  if (hjobs.empty()) return 0;
+  // column blocks of 16, or of 8 when the widest round of 16-column pairs would
+  // keep fewer than half the SMs busy: narrower pairs double the CTAs per round
+  // and cut each visit's work to a quarter, which wins while SMs are idle (D=512:
+  // 1.87 -> 1.65 s of SVD per sweep) and loses once they are not (complex D=2048:
+  // 4.8 -> 5.5 s per iDMRG)
+  int dev = 0, nsm = 0;
+  SADMRG_CUDA(cudaGetDevice(&dev));
+  SADMRG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  long long pairs16 = 0;
+  for (const SvdJob& J : hjobs) {
+    const int C = J.trans ? J.m : J.n;
+    const int nb = (C + 15) / 16;
+    pairs16 += nb <= 1 ? 1 : nb / 2;
+  }
+  const bool narrow = 2 * pairs16 < nsm;
+  if (cplx)
+    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
+                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
+  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
+                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
 }
 
 }  // namespace sadmrg
