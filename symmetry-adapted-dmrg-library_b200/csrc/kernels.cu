@@ -162,16 +162,6 @@ __device__ __forceinline__ void lanczos_scalar_op(int op, const void* dot, const
   }
 }
 
-template <bool CPLX>
-__global__ void lanczos_scalar_kernel(int op, const void* dot, const double* beta_prev, void* out) {
-  lanczos_scalar_op<CPLX>(op, dot, beta_prev, out);
-}
-
-void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s) {
-  if (cplx) lanczos_scalar_kernel<true><<<1, 1, 0, s>>>(op, dot, beta_prev, out);
-  else lanczos_scalar_kernel<false><<<1, 1, 0, s>>>(op, dot, beta_prev, out);
-}
-
 // --------------------------------------------------------------------------
 // Krylov vector kernels
 __device__ __forceinline__ double warp_sum(double v) {

@@ -46,10 +46,6 @@ struct Bases {
   void* p[kMaxBases];
 };
 
-// Item kernel families.  GEMM_MMA_SYNC: FP64 DMMA and the mma.sync 3xTF32
-// (gemm.cu); GEMM_UMMA: tcgen05 3xTF32 over pre-split operand panels with the
-// accumulator in tensor memory, complex plans in real form (umma.cu).
-enum GemmKind : int { GEMM_MMA_SYNC = 0, GEMM_UMMA = 1 };
 
 // Grouped GEMM over work items (deterministic split-K; see gemm.cu).
 // Split items write partial tiles; the last of a tile's items sums them (tile_cnt
@@ -179,15 +175,13 @@ void launch_gather(bool cplx, void* dst, const void* src, const double* w, const
 void launch_scale(bool cplx, void* x, double ar, double ai, long long n, cudaStream_t s);
 // fill with a constant
 void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStream_t s);
-// tiny scalar helpers for the Krylov recurrence (single thread)
-//   op 0: coef[0] = beta_prev[0]; coef[1] = Re(dot[0])     (three-term recurrence)
-//   op 1: out[0] = sqrt(|Re(dot[0])|)                       (norm)
-void launch_lanczos_scalar(bool cplx, int op, const void* dot, const double* beta_prev, void* out, cudaStream_t s);
 
 // ---- Krylov vector operations ---------------------------------------------
 // out[j] = <V_j | x> (conjugated first argument), j < nv, deterministic, one launch
-// (counter: a device word, zero between launches).  scalar_op >= 0 also applies
-// the lanczos_scalar step `scalar_op` to out[0] (into scalar_out) in the same launch.
+// (counter: a device word, zero between launches).  scalar_op >= 0 also applies a
+// Krylov scalar step to out[0] in the same launch: 0 -> scalar_out[0] =
+// beta_prev[0], scalar_out[1] = Re out[0] (three-term recurrence coefficients);
+// 1 -> scalar_out[0] = sqrt(|Re out[0]|) (a norm).
 void launch_multi_dot(bool cplx, const void* V, long long ldv, int nv, const void* x, long long n,
                       double* partial, int npart, void* out, unsigned* counter, cudaStream_t s, int scalar_op = -1,
                       const double* beta_prev = nullptr, void* scalar_out = nullptr);
