@@ -78,7 +78,10 @@ const char* sadmrg_last_error(const sadmrg_handle* h);
 int sadmrg_device_status(sadmrg_handle* h, int* status);
 
 /* Lanczos convergence: stop at a check (every 4 steps) once |<v|Hv>|/|Hv| is
- * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338). */
+ * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338).
+ * The split-precision solver (SADMRG_PREC_TF32X3) applies the same tolerance
+ * through the Lanczos residual estimate r = b_m |z_m| (|<v|Hv>|/|Hv| - 1 ~
+ * r^2 / (2 E^2)), without check matvecs. */
 int sadmrg_set_lanczos_tol(sadmrg_handle* h, double ov_tol);
 
 /* How the split-precision matvec is launched (no counterpart in the reference):
