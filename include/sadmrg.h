@@ -146,6 +146,15 @@ int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const 
  * reps times, and *ms is the mean device time per replay (CUDA events). */
 int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev,
                             double* ms);
+/* Timed steps of the same captured matvec (no counterpart in the reference):
+ * the graph of one H_eff*psi on (psi_dev, out_dev) is captured once; then per
+ * step, on the handle's stream, flush_bytes of flush_dev are overwritten (to
+ * evict the operands from L2; 0 for none) and the graph is launched between two
+ * CUDA events.  ms[i] is the device time of step i (steps values). */
+int sadmrg_heff_graph_steps(sadmrg_handle* h, int precision, int steps, const void* psi_dev, void* out_dev,
+                            void* flush_dev, long long flush_bytes, double* ms);
+/* kernels one H_eff*psi launches at this precision (the penalty's included) */
+int sadmrg_heff_launches_per_matvec(sadmrg_handle* h, int precision, int* n);
 /* Lanczos ground state (lanczos1) from psi; psi is overwritten by the Ritz vector.
  * precision SADMRG_PREC_TF32X3 runs the split-precision Lanczos followed by an
  * FP64 restart from its result. */
@@ -206,6 +215,28 @@ int sadmrg_chain_sweep(sadmrg_handle* h, double* energy);
  * SU(2) CGC blocks) in directory dir.  read_mps is followed by prepare_sweep. */
 int sadmrg_chain_read_mps(sadmrg_handle* h, const char* dir, int bond_read);
 int sadmrg_chain_save_mps(sadmrg_handle* h, const char* dir);
+/* DMRG::save_ww / read_ww (src/dmrg_inst.cpp:1145-1165): the singular values of
+ * the truncations.  The chain keeps them as the reference's ww array: every
+ * truncation overwrites its first n entries (the kept values sector by sector,
+ * then from position kept the discarded ones) and the return pass of a sweep
+ * clears the first bondd entries before each truncation (src/dmrg_inst.cpp:934).
+ * save_ww writes bondd * (physpn + 1) doubles to ww-<ns>-<D>-<2S>-0.bin in dir;
+ * read_ww reads the first bond_read doubles of ww-<ns>-<bond_read>-<2S>-0.bin,
+ * or sets them to 1 when that file is absent. */
+int sadmrg_chain_save_ww(sadmrg_handle* h, const char* dir);
+int sadmrg_chain_read_ww(sadmrg_handle* h, const char* dir, int bond_read);
+/* DMRG::save_enr / read_enr (src/dmrg_inst.cpp:993-1016): save_enr appends the
+ * chain's energy (16 significant digits) to enr-<ns>-<D>-<2S>-0.dat in dir;
+ * read_enr sets it to the last value of enr-<ns>-<bond_read>-<2S>-0.dat (unchanged
+ * when the file is absent). */
+int sadmrg_chain_save_enr(sadmrg_handle* h, const char* dir);
+int sadmrg_chain_read_enr(sadmrg_handle* h, const char* dir, int bond_read);
+/* the chain's ww array: *n its length, the first min(cap, *n) values to out */
+int sadmrg_chain_ww(sadmrg_handle* h, int cap, int* n, double* out);
+/* Lanczos length of the chain's solves: the reference's constant mlanc = 40
+ * (src/dmrg_inst.cpp:267), capped like it at the vector length + 1.  The stop
+ * test is sadmrg_set_lanczos_tol. */
+int sadmrg_chain_set_mlanc(sadmrg_handle* h, int mlanc);
 /* Freeze the two-site problem at bond (il, il+1): psi = the current site tensors'
  * product (DMRG::prepare_input_vector), the fused environments and the H_eff plan
  * become the handle's heff plan (sadmrg_heff_*), psi is staged (which = 0).  If

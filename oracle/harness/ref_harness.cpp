@@ -18,6 +18,12 @@
 //     array (src/block_tensor_inst.cpp:579-602 vs src/dmrg_inst.cpp:84); we give
 //     it room for all of them.
 //   * fixed sweep count, no early stop.
+//   * Lanczos settings: -mlanc / -lanc_check set the two constants the
+//     reference hard-codes (src/dmrg_inst.cpp:267 mlanc = 40, :1338 stop at
+//     |<v|Hv>|/|Hv| within 1e-8 of 1); oracle/Makefile compiles dmrg_inst.cpp
+//     with those constants read from the globals below, defaults unchanged.
+//   * -sweepdir: the directory sweep() writes its checkpoint files to
+//     (save_mps2 / save_ww / save_enr, src/dmrg_inst.cpp:940-942).
 // Private members are reached with the usual access-specifier override.
 #include <omp.h>
 #include <chrono>
@@ -40,11 +46,14 @@
 #include "cgc_tables.hpp"
 #undef private
 #undef protected
+#include "../shims/lanczos_knobs.h"
 
 int max_dcut = 64;
 int psize = 1;
 int myrank = 0;
 CGCTables* g_cgc_tables = nullptr;
+int ref_lanczos_mlanc = 40;        // src/dmrg_inst.cpp:267
+double ref_lanczos_check = 1e-8;   // src/dmrg_inst.cpp:1338
 void makeup_clebsch_gordan_coefficient_tensors(int physpn, int max_angm, CGCTables& t);
 
 struct Opts;
@@ -62,6 +71,9 @@ struct Opts {
   int bench_heff = 0;  // time this many H*v calls on the centre problem
   std::string load;    // directory with an exported two-site problem (time / check H*v on it)
   int quiet = 1;
+  int mlanc = 40;           // Lanczos length (reference: 40)
+  double lanc_check = 1e-8; // Lanczos stop test (reference: 1e-8)
+  std::string sweepdir = "/tmp";
 };
 
 template <class S, class Sym>
@@ -195,7 +207,9 @@ static int run(const Opts& o) {
   for (int s = 0; s < o.sweeps; ++s) {
     auto a = std::chrono::steady_clock::now();
     mute();
-    if (chdir("/tmp") != 0) return 3;  // sweep() writes its checkpoint files to the working directory
+    // sweep() writes its checkpoint files to the working directory
+    mkdir(o.sweepdir.c_str(), 0755);
+    if (chdir(o.sweepdir.c_str()) != 0) return 3;
     chain.sweep();
     if (chdir(cwd) != 0) return 3;
     unmute();
@@ -387,9 +401,20 @@ static int run_load(const Opts& o) {
   if constexpr (Sym::has_cgc) {
     // fac_hamilt_vec for 2J beyond the constructor's max_angm = 20, computed with the
     // reference's own Dense / CGCTable code by the formula of src/cgc_tables.cpp:153-164
-    const int M = 64;
+    // table size: past the largest sector label of the problem's psi (+ the channel 2J = 2)
+    int M = 64;
+    {
+      std::ifstream fp(o.load + "/psi.txt");
+      std::string w;
+      while (fp >> w)
+        if (w == "q") {
+          std::string x;
+          while (fp >> x && x != "d") M = std::max(M, std::atoi(x.c_str()) + 8);
+        }
+    }
     double*** f = new double**[M];
-    Dense<double> sg[M], c, t1, t2;
+    std::vector<Dense<double>> sg(M);
+    Dense<double> c, t1, t2;
     for (int i = 0; i < M; ++i) sg[i].make_singlet(i);
     for (int i = 0; i < M; ++i) {
       f[i] = new double*[M];
@@ -468,8 +493,13 @@ int main(int argc, char** argv) {
     else if (a == "-load") o.load = nxt();
     else if (a == "-bench_heff") o.bench_heff = std::stoi(nxt());
     else if (a == "-verbose") o.quiet = 0;
+    else if (a == "-mlanc") o.mlanc = std::stoi(nxt());
+    else if (a == "-lanc_check") o.lanc_check = std::stod(nxt());
+    else if (a == "-sweepdir") o.sweepdir = nxt();
     else { std::cerr << "unknown option " << a << "\n"; return 2; }
   }
+  ref_lanczos_mlanc = o.mlanc;
+  ref_lanczos_check = o.lanc_check;
   if (!o.load.empty()) {
     if (o.sym == 0 && o.cplx == 0) return run_load<double, U1Symmetry>(o);
     if (o.sym == 0 && o.cplx == 1) return run_load<dcmplex, U1Symmetry>(o);

@@ -420,6 +420,86 @@ int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const 
   });
 }
 
+int sadmrg_heff_graph_steps(sadmrg_handle* h, int precision, int steps, const void* psi_dev, void* out_dev,
+                            void* flush_dev, long long flush_bytes, double* ms) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_graph_steps: no plan");
+    SADMRG_REQUIRE(steps >= 1 && ms && flush_bytes >= 0 && (flush_dev || flush_bytes == 0), SADMRG_ERR_ARG,
+                   "heff_graph_steps: arguments");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_graph_steps: precision");
+    const HeffPlan<S>& H = *S_.heff;
+    Bases b{};
+    b.p[0] = const_cast<void*>(psi_dev ? psi_dev : S_.io.get());
+    b.p[1] = out_dev ? out_dev : static_cast<void*>(S_.io.template as<S>() + H.n);
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = H.scratch->get();
+    // one plain run first: lazy one-time setup (kernel attributes, device queries) stays out of the capture
+    H.plan.run(c, ScalarInfo<S>::cplx, precision, b);
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    SADMRG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      H.plan.run(c, ScalarInfo<S>::cplx, precision, b);
+    } catch (...) {
+      cudaStreamEndCapture(c.stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    SADMRG_CUDA(cudaStreamEndCapture(c.stream, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      SADMRG_CUDA(ie);
+    }
+    std::vector<cudaEvent_t> ev(2 * (size_t)steps, nullptr);
+    auto cleanup = [&]() {
+      for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+      cudaGraphExecDestroy(ge);
+      cudaGraphDestroy(g);
+    };
+    try {
+      for (auto& e : ev) SADMRG_CUDA(cudaEventCreate(&e));
+      for (int r = 0; r < steps; ++r) {
+        // evict the operands from L2 before the step (a write larger than L2), outside the events
+        if (flush_bytes > 0) SADMRG_CUDA(cudaMemsetAsync(flush_dev, r & 0xff, (size_t)flush_bytes, c.stream));
+        SADMRG_CUDA(cudaEventRecord(ev[2 * r], c.stream));
+        SADMRG_CUDA(cudaGraphLaunch(ge, c.stream));
+        SADMRG_CUDA(cudaEventRecord(ev[2 * r + 1], c.stream));
+      }
+      SADMRG_CUDA(cudaEventSynchronize(ev[2 * steps - 1]));
+      for (int r = 0; r < steps; ++r) {
+        float t = 0.f;
+        SADMRG_CUDA(cudaEventElapsedTime(&t, ev[2 * r], ev[2 * r + 1]));
+        ms[r] = t;
+      }
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+    c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision,
+                                                   H.plan.runs_fused(c, ScalarInfo<S>::cplx, precision)) * (steps + 1);
+    check_device_status();
+  });
+}
+
+int sadmrg_heff_launches_per_matvec(sadmrg_handle* h, int precision, int* n) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.heff && n, SADMRG_ERR_ARG, "heff_launches_per_matvec: no plan");
+    const HeffPlan<S>& H = *S_.heff;
+    *n = H.plan.launches_per_run(ScalarInfo<S>::cplx, precision,
+                                 H.plan.runs_fused(h->ctx, ScalarInfo<S>::cplx, precision)) +
+         (H.npen > 0 ? 3 : 0);
+  });
+}
+
 int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const void* psi_dev, void* out_dev,
                             double* ms) {
   return dispatch(h, [&](auto* tag) {
@@ -724,6 +804,58 @@ int sadmrg_chain_save_mps(sadmrg_handle* h, const char* dir) {
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     SADMRG_REQUIRE(dir, SADMRG_ERR_ARG, "save_mps: null path");
     S_.chain->save_mps(dir);
+  });
+}
+
+int sadmrg_chain_set_mlanc(sadmrg_handle* h, int mlanc) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(mlanc >= 2 && mlanc <= 1000, SADMRG_ERR_ARG, "chain_set_mlanc: mlanc outside [2, 1000]");
+    S_.chain->mlanc_max = mlanc;
+  });
+}
+
+}  // extern "C"
+
+// checkpoint files of the singular values and the energy: fn(chain, dir)
+template <class F>
+static int chain_file_op(sadmrg_handle* h, const char* dir, const char* what, F&& fn) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(dir, SADMRG_ERR_ARG, std::string(what) + ": null path");
+    fn(*S_.chain, std::string(dir));
+  });
+}
+
+extern "C" {
+
+int sadmrg_chain_save_ww(sadmrg_handle* h, const char* dir) {
+  return chain_file_op(h, dir, "save_ww", [](auto& ch, const std::string& d) { ch.save_ww(d); });
+}
+int sadmrg_chain_read_ww(sadmrg_handle* h, const char* dir, int bond_read) {
+  if (bond_read < 1) return fail(h, SADMRG_ERR_ARG, "read_ww: bond_read < 1");
+  return chain_file_op(h, dir, "read_ww", [&](auto& ch, const std::string& d) { ch.read_ww(d, bond_read); });
+}
+int sadmrg_chain_save_enr(sadmrg_handle* h, const char* dir) {
+  return chain_file_op(h, dir, "save_enr", [](auto& ch, const std::string& d) { ch.save_enr(d); });
+}
+int sadmrg_chain_read_enr(sadmrg_handle* h, const char* dir, int bond_read) {
+  return chain_file_op(h, dir, "read_enr", [&](auto& ch, const std::string& d) { ch.read_enr(d, bond_read); });
+}
+
+int sadmrg_chain_ww(sadmrg_handle* h, int cap, int* n, double* out) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(n, SADMRG_ERR_ARG, "chain_ww: null count");
+    const auto& w = S_.chain->ww;
+    *n = (int)w.size();
+    for (int i = 0; i < cap && i < (int)w.size(); ++i) out[i] = w[i];
   });
 }
 

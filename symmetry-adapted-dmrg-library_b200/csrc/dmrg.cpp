@@ -566,16 +566,24 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   for (int k = 0; k < dcut; ++k) dim[isort[k]]++;
   std::vector<int> amom, bdim;
   double kept_w = 0.0;
-  if (wout) wout->clear();
-  for (int i = 0; i < nm1; ++i)
+  // the singular values in the reference's output order (src/block_tensor_inst.cpp:576-600):
+  // the kept ones sector by sector from position 0, then from position dcut the
+  // discarded ones of every sector, sector by sector
+  if (wout) wout->assign(wsort.size(), 0.0);
+  int wm = 0, wm1 = dcut;
+  for (int i = 0; i < nm1; ++i) {
+    if (job_of[i] < 0) continue;
+    const std::vector<double>& ws = ssort[job_of[i]];
     if (dim[i] > 0) {
       amom.push_back(bb0.q[i]);
       bdim.push_back(dim[i]);
-      for (int k = 0; k < dim[i]; ++k) {
-        kept_w += ssort[job_of[i]][k] * ssort[job_of[i]][k];
-        if (wout) wout->push_back(ssort[job_of[i]][k]);
-      }
+      for (int k = 0; k < dim[i]; ++k) kept_w += ws[k] * ws[k];
     }
+    if (wout) {
+      for (int k = 0; k < dim[i]; ++k) (*wout)[wm++] = ws[k];
+      for (int k = dim[i]; k < dc[i]; ++k) (*wout)[wm1++] = ws[k];
+    }
+  }
   out.kept = dcut;
   out.discarded_weight = wtotal > 0 ? std::max(0.0, 1.0 - kept_w / wtotal) : 0.0;
   Bond nb(bb0.dir, amom, bdim);
@@ -973,7 +981,12 @@ void Chain<S>::wavefunc_transformation(int i, int dir) {
 template <class S>
 void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   const double t0 = now_s();
-  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &ww);
+  std::vector<double> w;
+  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w);
+  // BlockTensor::svd overwrites the first n values of the chain's ww array and
+  // leaves the rest as it was (src/block_tensor_inst.cpp:576-600)
+  if (ww.size() < w.size()) ww.resize(w.size(), 0.0);
+  std::copy(w.begin(), w.end(), ww.begin());
   last_discarded = s.discarded_weight;
   if (s.near_tie) ++near_ties;
   if (s.jacobi_kernel_ms > 0) timers.svd_kernel += s.jacobi_kernel_ms * 1e-3;
@@ -1078,6 +1091,7 @@ void Chain<S>::sweep() {
     prepare_site_operator_from_left(i - 2, false);
     prepare_site_operator_from_right(i - 1, false);
     lanczos_solve_eigenvector(i - 2, i - 1, vec);
+    std::fill(ww.begin(), ww.begin() + std::min<size_t>(ww.size(), bondd), 0.0);   // src/dmrg_inst.cpp:934
     svd_step(vec, i - 2, i - 1, 1.0, 0.0);
   }
 }
@@ -1156,6 +1170,64 @@ void Chain<S>::save_mps(const std::string& dir) const {
     if (!cg.empty()) std::fwrite(cg.data(), sizeof(double), cg.size(), fb);
     std::fclose(fb);
   }
+}
+
+// DMRG::save_ww (src/dmrg_inst.cpp:1145-1153): bondd * phdim doubles of the ww
+// array, ww-<ns>-<bondd>-<2S>-0.bin (the array is kept at least that long here,
+// zero beyond what the truncations wrote)
+template <class S>
+void Chain<S>::save_ww(const std::string& dir) const {
+  const std::string name = dir + "/ww-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
+                           std::to_string(totspin) + "-0.bin";
+  std::vector<double> w((size_t)bondd * (physpn + 1), 0.0);
+  std::copy(ww.begin(), ww.begin() + std::min(ww.size(), w.size()), w.begin());
+  FILE* f = std::fopen(name.c_str(), "wb");
+  SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "save_ww: cannot write " + name);
+  const size_t put = std::fwrite(w.data(), sizeof(double), w.size(), f);
+  std::fclose(f);
+  SADMRG_REQUIRE(put == w.size(), SADMRG_ERR_ARG, "save_ww: short write " + name);
+}
+
+// DMRG::read_ww (src/dmrg_inst.cpp:1156-1165): the first read1 doubles of
+// ww-<ns>-<read1>-<2S>-0.bin, or read1 ones when the file is absent
+template <class S>
+void Chain<S>::read_ww(const std::string& dir, int read1) {
+  const std::string name = dir + "/ww-" + std::to_string(ns) + "-" + std::to_string(read1) + "-" +
+                           std::to_string(totspin) + "-0.bin";
+  if (ww.size() < (size_t)read1) ww.resize(read1, 0.0);
+  FILE* f = std::fopen(name.c_str(), "rb");
+  if (!f) {
+    std::fill(ww.begin(), ww.begin() + read1, 1.0);
+    return;
+  }
+  const size_t got = std::fread(ww.data(), sizeof(double), read1, f);
+  std::fclose(f);
+  SADMRG_REQUIRE(got == (size_t)read1, SADMRG_ERR_ARG, "read_ww: short " + name);
+}
+
+// DMRG::save_enr (src/dmrg_inst.cpp:996-1003): appends gs_enr to
+// enr-<ns>-<bondd>-<2S>-0.dat, 16 significant digits
+template <class S>
+void Chain<S>::save_enr(const std::string& dir) const {
+  const std::string name = dir + "/enr-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
+                           std::to_string(totspin) + "-0.dat";
+  FILE* f = std::fopen(name.c_str(), "a");
+  SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "save_enr: cannot write " + name);
+  std::fprintf(f, "%.16g\n", gs_enr);
+  std::fclose(f);
+}
+
+// DMRG::read_enr (src/dmrg_inst.cpp:1008-1016): gs_enr = the last value of
+// enr-<ns>-<read1>-<2S>-0.dat; unchanged when the file is absent
+template <class S>
+void Chain<S>::read_enr(const std::string& dir, int read1) {
+  const std::string name = dir + "/enr-" + std::to_string(ns) + "-" + std::to_string(read1) + "-" +
+                           std::to_string(totspin) + "-0.dat";
+  FILE* f = std::fopen(name.c_str(), "r");
+  if (!f) return;
+  double e;
+  while (std::fscanf(f, "%lf", &e) == 1) gs_enr = e;
+  std::fclose(f);
 }
 
 template <class S>

@@ -157,6 +157,11 @@ class Chain {
   // DMRG::read_mps / save_mps2 checkpoint format (src/dmrg_inst.cpp:947-1079)
   bool read_mps(const std::string& dir, int bond_read);
   void save_mps(const std::string& dir) const;
+  // DMRG::save_ww / read_ww / save_enr / read_enr (src/dmrg_inst.cpp:993-1030, 1145-1177)
+  void save_ww(const std::string& dir) const;
+  void read_ww(const std::string& dir, int read1);
+  void save_enr(const std::string& dir) const;
+  void read_enr(const std::string& dir, int read1);
   // the two-site problem at bond (il, il+1): psi from the current site tensors and
   // the H_eff plan of DMRG::hamiltonian_vector_multiplication_idmrg
   HeffPlan<S> freeze(int il, BTensor<S>& psi);
@@ -173,6 +178,8 @@ class Chain {
   std::vector<std::vector<BTensor<S>>> opr;
   std::array<BTensor<S>, 2> sigma;
   double gs_enr = 0.0;
+  // singular values of the truncations, laid out as the reference's ww array:
+  // each truncation overwrites its first n values (kept, then discarded)
   std::vector<double> ww;
   double last_discarded = 0.0;
   int near_ties = 0;          // truncations whose cut fell inside a near-degenerate pair

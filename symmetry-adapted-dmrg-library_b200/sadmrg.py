@@ -36,6 +36,8 @@ EXPORTED = [
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
     "sadmrg_heff_set_penalty", "sadmrg_batch_add", "sadmrg_batch_finalize", "sadmrg_batch_clear",
     "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos", "sadmrg_batch_profile",
+    "sadmrg_chain_set_mlanc", "sadmrg_chain_save_ww", "sadmrg_chain_read_ww", "sadmrg_chain_save_enr",
+    "sadmrg_chain_read_enr", "sadmrg_chain_ww", "sadmrg_heff_graph_steps", "sadmrg_heff_launches_per_matvec",
 ]
 
 
@@ -88,6 +90,8 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_profile": ([vp, C.c_int, C.c_int, vp, vp, dp, dp], C.c_int),
         "sadmrg_heff_launch_profile": ([vp, C.c_int, C.c_int, vp, vp, C.c_int, ip, ip, dp], C.c_int),
         "sadmrg_heff_graph_bench": ([vp, C.c_int, C.c_int, vp, vp, dp], C.c_int),
+        "sadmrg_heff_graph_steps": ([vp, C.c_int, C.c_int, vp, vp, vp, C.c_longlong, dp], C.c_int),
+        "sadmrg_heff_launches_per_matvec": ([vp, C.c_int, ip], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -98,6 +102,12 @@ def load(path: str = LIB_PATH):
         "sadmrg_chain_bond": ([vp, C.c_int, C.c_int, ip, ip, ip], C.c_int),
         "sadmrg_chain_read_mps": ([vp, C.c_char_p, C.c_int], C.c_int),
         "sadmrg_chain_save_mps": ([vp, C.c_char_p], C.c_int),
+        "sadmrg_chain_set_mlanc": ([vp, C.c_int], C.c_int),
+        "sadmrg_chain_save_ww": ([vp, C.c_char_p], C.c_int),
+        "sadmrg_chain_read_ww": ([vp, C.c_char_p, C.c_int], C.c_int),
+        "sadmrg_chain_save_enr": ([vp, C.c_char_p], C.c_int),
+        "sadmrg_chain_read_enr": ([vp, C.c_char_p, C.c_int], C.c_int),
+        "sadmrg_chain_ww": ([vp, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_freeze": ([vp, C.c_int, C.c_char_p], C.c_int),
         "sadmrg_chain_stats": ([vp, dp, C.c_int], C.c_int),
         "sadmrg_chain_set_tensor": ([vp, C.c_int, C.c_int, C.c_int, td], C.c_int),
@@ -359,6 +369,21 @@ class Handle:
                                                      C.c_void_p(out_ptr), C.byref(ms)), "heff_graph_bench")
         return ms.value
 
+    def heff_graph_steps(self, precision: int, steps: int, psi_ptr: int = 0, out_ptr: int = 0, flush_ptr: int = 0,
+                         flush_bytes: int = 0) -> np.ndarray:
+        """Device ms of `steps` replays of one captured matvec, L2 flushed (flush_bytes written) before each."""
+        ms = np.zeros(int(steps))
+        self._check(self.lib.sadmrg_heff_graph_steps(self.h, int(precision), int(steps), psi_ptr or None,
+                                                     out_ptr or None, flush_ptr or None, int(flush_bytes),
+                                                     ms.ctypes.data_as(C.POINTER(C.c_double))), "heff_graph_steps")
+        return ms
+
+    def heff_launches_per_matvec(self, precision: int) -> int:
+        n = C.c_int()
+        self._check(self.lib.sadmrg_heff_launches_per_matvec(self.h, int(precision), C.byref(n)),
+                    "heff_launches_per_matvec")
+        return n.value
+
     def heff_lanczos(self, psi: np.ndarray, mlanc: int = 40, precision: int = PREC_FP64):
         x = np.array(psi, dtype=self.dtype, copy=True)
         e = C.c_double()
@@ -442,6 +467,31 @@ class Handle:
 
     def chain_save_mps(self, directory: str):
         self._check(self.lib.sadmrg_chain_save_mps(self.h, directory.encode()), "chain_save_mps")
+
+    def chain_set_mlanc(self, mlanc: int):
+        """Lanczos length of the chain's solves (the reference's mlanc = 40)."""
+        self._check(self.lib.sadmrg_chain_set_mlanc(self.h, int(mlanc)), "chain_set_mlanc")
+
+    def chain_save_ww(self, directory: str):
+        self._check(self.lib.sadmrg_chain_save_ww(self.h, directory.encode()), "chain_save_ww")
+
+    def chain_read_ww(self, directory: str, bond_read: int):
+        self._check(self.lib.sadmrg_chain_read_ww(self.h, directory.encode(), int(bond_read)), "chain_read_ww")
+
+    def chain_save_enr(self, directory: str):
+        self._check(self.lib.sadmrg_chain_save_enr(self.h, directory.encode()), "chain_save_enr")
+
+    def chain_read_enr(self, directory: str, bond_read: int):
+        self._check(self.lib.sadmrg_chain_read_enr(self.h, directory.encode(), int(bond_read)), "chain_read_enr")
+
+    def chain_ww(self) -> np.ndarray:
+        """The chain's ww array (singular values of the truncations, the reference's layout)."""
+        n = C.c_int()
+        self._check(self.lib.sadmrg_chain_ww(self.h, 0, C.byref(n), None), "chain_ww")
+        out = np.zeros(max(n.value, 1))
+        self._check(self.lib.sadmrg_chain_ww(self.h, n.value, C.byref(n), out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "chain_ww")
+        return out[:n.value]
 
     def chain_freeze(self, il: int, export_dir: Optional[str] = None) -> BlockTensorData:
         """Freeze the two-site problem at (il, il+1) as the handle's H_eff plan; returns psi."""

@@ -9,6 +9,11 @@ Run in a container that has the reference sources (the harness is built by
   energy and the SVD factors / singular values that follow.
 * ``sweeps_<case>.npz``   -- energies after iDMRG and after every sweep, and the
   sector dimensions of every bond after every sweep.
+* ``baseline_<case>.npz`` -- the same for the benchmark configurations, run with
+  the benchmark's Lanczos settings (at most 100 steps, stop at |<v|Hv>|/|Hv|
+  within 1e-10 of 1; the reference's constants are 40 and 1e-8), with the
+  reference's iDMRG checkpoint (both sides sweep from it) and the checkpoint
+  files of singular values and energies its sweeps wrote (ww-*.bin, enr-*.dat).
 
     python tests/golden/make_golden.py
 """
@@ -47,6 +52,12 @@ SWEEP_CASES = {
     "su2_L12_periodic": ["-sym", "su2", "-L", "12", "-d", "64", "-sweeps", "2", "-open", "0"],
     "u1_L32_D64": ["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "2"],
 }
+
+# configuration 1 of the benchmark: U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps
+BASELINE_CASES = {
+    "u1_L32_D64": ["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"],
+}
+BASELINE_LANCZOS = ["-mlanc", "100", "-lanc_check", "1e-10"]
 
 
 def read_tensor(dirpath: str, name: str, cplx: bool) -> dict:
@@ -102,7 +113,8 @@ def parse_sweeps(stdout: str):
 def main():
     if not os.path.exists(HARNESS):
         sys.exit("build the reference harness first: make -C oracle")
-    for name, args in CENTRE_CASES.items():
+    only_baseline = "--baseline-only" in sys.argv
+    for name, args in ({} if only_baseline else CENTRE_CASES).items():
         cplx = args[args.index("-cplx") + 1] == "1"
         with tempfile.TemporaryDirectory() as wd:
             dd = os.path.join(wd, "dump")
@@ -119,7 +131,7 @@ def main():
             arrays["sweep_energies"] = np.array(energies)
             np.savez_compressed(os.path.join(HERE, f"centre_{name}.npz"), **arrays)
             print("wrote", name, len(arrays))
-    for name, args in SWEEP_CASES.items():
+    for name, args in ({} if only_baseline else SWEEP_CASES).items():
         ck = {}
         with tempfile.TemporaryDirectory() as wd:
             # the MPS after the reference's iDMRG, in its save_mps2 format: both sides sweep from it
@@ -138,6 +150,25 @@ def main():
                             e_idmrg=np.float64(e_idmrg), energies=np.array(energies),
                             bonds=np.array(per_sweep[-1]), bonds_per_sweep=np.array(per_sweep), **ck)
         print("wrote", name, e_idmrg, energies, len(ck))
+
+    for name, args in BASELINE_CASES.items():
+        arrays = {}
+        with tempfile.TemporaryDirectory() as wd:
+            ckd, swd = os.path.join(wd, "ck"), os.path.join(wd, "sw")
+            stdout = run(args + BASELINE_LANCZOS + ["-save", ckd, "-sweepdir", swd, "-threads", "8"], wd)
+            for fn in sorted(os.listdir(ckd)):
+                arrays["ck__" + fn] = np.frombuffer(open(os.path.join(ckd, fn), "rb").read(), dtype=np.uint8)
+            for fn in sorted(os.listdir(swd)):
+                if fn.startswith(("ww-", "enr-")):
+                    arrays["sw__" + fn] = np.frombuffer(open(os.path.join(swd, fn), "rb").read(), dtype=np.uint8)
+        e_idmrg, energies, bonds = parse_sweeps(stdout)
+        per_sweep = []
+        for s_ in sorted(k for k in bonds if k >= 0):
+            per_sweep.append([f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])])
+        np.savez_compressed(os.path.join(HERE, f"baseline_{name}.npz"), args=np.array(" ".join(args)),
+                            lanczos=np.array(" ".join(BASELINE_LANCZOS)), e_idmrg=np.float64(e_idmrg),
+                            energies=np.array(energies), bonds_per_sweep=np.array(per_sweep), **arrays)
+        print("wrote baseline", name, e_idmrg, energies)
 
 
 if __name__ == "__main__":

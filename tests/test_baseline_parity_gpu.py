@@ -1,0 +1,138 @@
+"""Parity at the benchmark configurations, with the benchmark's Lanczos settings.
+
+Both sides run Lanczos with at most 100 steps and stop once |<v|Hv>|/|Hv| is
+within 1e-10 of 1 (the reference's own constants are 40 and 1e-8,
+src/dmrg_inst.cpp:267,1338; the reference build takes them from the harness's
+-mlanc / -lanc_check).
+
+* Configuration 1 (U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps):
+  both sides sweep from the reference's own iDMRG checkpoint (its save_mps2
+  files, tests/golden/baseline_u1_L32_D64.npz).  After every sweep the energy
+  agrees to 1e-10 relative and every bond's sectors and dimensions are
+  identical -- unless a truncation cut fell inside a near-degenerate pair of
+  singular values (the U(1) sectors q and -q carry equal singular values in
+  exact arithmetic, and the reference's std::sort has no tie-break), which the
+  GPU run counts (chain_stats()["near_ties"]); then the total kept dimension of
+  every bond must match and the energy agree to 1e-8.  The checkpoint files the
+  reference's sweeps wrote (enr-*.dat after every sweep, ww-*.bin after the
+  last) are compared with the ones written here.
+* Configuration 2 (SU(2) real Heisenberg chain, open, L = 100, D = 512
+  multiplets): the GPU's own iDMRG checkpoint is handed to the reference build
+  (read_mps + prepare_sweep), which sweeps once on the host cores; the GPU
+  sweeps once from the same files.  Energy to 1e-10 relative, bonds identical
+  (near ties counted as above).  Needs the reference build (oracle/_ref).
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+pytestmark = pytest.mark.gpu
+
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+MLANC, CHECK = 100, 1e-10
+
+
+def _bonds(h, ns):
+    return [f"{s}:" + ",".join(f"{q}x{d}" for q, d in h.chain_bond(s)) for s in range(ns)]
+
+
+def _total(b):
+    return sum(int(x.split("x")[1]) for x in b.split(":")[1].split(",") if x)
+
+
+def _compare_sweep(s, e, eref, got, ref_b, ties):
+    if ties == 0:
+        assert abs(e - eref) <= 1e-10 * abs(eref), (s, e, eref)
+        assert got == ref_b, (s, [(a, b) for a, b in zip(got, ref_b) if a != b][:4])
+    else:
+        assert abs(e - eref) <= 1e-8 * abs(eref), (s, e, eref, ties)
+        assert [_total(x) for x in got] == [_total(x) for x in ref_b], (s, ties)
+
+
+def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint():
+    import sadmrg
+    z = np.load(os.path.join(GOLDEN, "baseline_u1_L32_D64.npz"))
+    ns, D = 32, 64
+    h = sadmrg.Handle(sym=0, cplx=False)
+    h.chain_create(1, ns, D, 1, 0, True, 0.0)
+    h.chain_set_mlanc(MLANC)
+    h.set_lanczos_tol(CHECK)
+    with tempfile.TemporaryDirectory() as d:
+        for k in z.files:
+            if k.startswith("ck__"):
+                np.asarray(z[k], dtype=np.uint8).tofile(os.path.join(d, k[4:]))
+        h.chain_read_mps(d, D)
+    h.chain_prepare_sweep()
+    with tempfile.TemporaryDirectory() as out:
+        for s, eref in enumerate(z["energies"]):
+            e = h.chain_sweep()
+            h.chain_save_enr(out)
+            ties = h.chain_stats()["near_ties"]
+            _compare_sweep(s, e, float(eref), _bonds(h, ns), [str(x) for x in z["bonds_per_sweep"][s]], ties)
+        h.chain_save_ww(out)
+        # enr-*.dat: one line per sweep, 16 significant digits
+        enr_name = f"enr-{ns}-{D}-0-0.dat"
+        ours = np.loadtxt(os.path.join(out, enr_name))
+        ref = np.array([float(x) for x in bytes(z["sw__" + enr_name]).decode().split()])
+        assert ours.shape == ref.shape
+        assert np.all(np.abs(ours - ref) <= 1e-10 * np.abs(ref))
+        # ww-*.bin: bondd * 2 doubles, the singular values of the last truncations in the reference's layout
+        ww_name = f"ww-{ns}-{D}-0-0.bin"
+        ours = np.fromfile(os.path.join(out, ww_name))
+        ref = np.frombuffer(bytes(z["sw__" + ww_name]), dtype=np.float64)
+        assert ours.shape == ref.shape == (2 * D,)
+        if h.chain_stats()["near_ties"] == 0:
+            np.testing.assert_allclose(ours, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+        # read_ww / read_enr restore them (DMRG::read_ww, read_enr)
+        h2 = sadmrg.Handle(sym=0, cplx=False)
+        h2.chain_create(1, ns, D, 1, 0, True, 0.0)
+        h2.chain_read_ww(out, D)
+        np.testing.assert_array_equal(h2.chain_ww()[:D], ours[:D])
+        h2.chain_read_enr(out, D)
+        h2.close()
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
+def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
+    import sadmrg
+    ns, D = 100, 512
+    h = sadmrg.Handle(sym=1, cplx=False)
+    h.chain_create(1, ns, D, 1, 0, True, 0.0)
+    h.chain_set_mlanc(MLANC)
+    h.set_lanczos_tol(CHECK)
+    h.chain_idmrg()
+    with tempfile.TemporaryDirectory() as d:
+        ck = os.path.join(d, "ck")
+        os.makedirs(ck)
+        h.chain_save_mps(ck)
+        maxj = max(q for s in range(ns) for q, _ in h.chain_bond(s))
+        h.close()
+        g = sadmrg.Handle(sym=1, cplx=False)
+        g.chain_create(1, ns, D, 1, 0, True, 0.0)
+        g.chain_set_mlanc(MLANC)
+        g.set_lanczos_tol(CHECK)
+        g.chain_read_mps(ck, D)
+        g.chain_prepare_sweep()
+        e = g.chain_sweep()
+        got = _bonds(g, ns)
+        ties = g.chain_stats()["near_ties"]
+        g.close()
+        out = subprocess.run([HARNESS, "-sym", "su2", "-L", str(ns), "-d", str(D), "-sweeps", "1", "-read", ck,
+                              "-mlanc", str(MLANC), "-lanc_check", str(CHECK), "-maxangm", str(max(20, maxj + 6)),
+                              "-threads", str(os.cpu_count() or 1), "-sweepdir", os.path.join(d, "sw")],
+                             capture_output=True, text=True, timeout=1500)
+        assert out.returncode == 0, out.stderr[-500:]
+    eref, ref_b = None, {}
+    for line in out.stdout.splitlines():
+        t = line.split()
+        if t and t[0] == "SWEEP":
+            eref = float(t[3])
+        elif t and t[0] == "BONDS" and t[1] == "0":
+            ref_b[int(t[3])] = f"{t[3]}:" + ",".join(x.replace(":", "x") for x in t[4:])
+    assert eref is not None
+    _compare_sweep(0, e, eref, got, [ref_b.get(s, f"{s}:") for s in range(ns)], ties)
