@@ -76,6 +76,18 @@ const char* sadmrg_last_error(const sadmrg_handle* h);
  * heff_profile, chain_idmrg, chain_sweep) check it themselves and fail with
  * SADMRG_ERR_CUDA. */
 int sadmrg_device_status(sadmrg_handle* h, int* status);
+/* Failure-path check of those bounded waits (no counterpart in the reference).
+ * Runs one split-precision H_eff*psi of the current plan (on the handle's own
+ * zeroed psi buffer) as a single cooperative launch in which the first psi panel
+ * set is never reported complete -- its completion target is raised by one for
+ * this launch only, a flag nothing sets -- with every wait limited to wait_ns
+ * (1 ms .. 2 s).  The items that read those panels give up, their CTAs wait for
+ * the copies and MMAs they issued, free their tensor memory and return.  *status
+ * is the status word the launch left (nonzero: a wait ran out), which this call
+ * clears together with the plan's split-K and dependency counters, so the next
+ * call computes normally.  SADMRG_ERR_STATE when the plan has no tcgen05
+ * schedule with psi panels. */
+int sadmrg_heff_wait_fault_test(sadmrg_handle* h, long long wait_ns, int* status);
 
 /* Lanczos convergence: stop at a check (every 4 steps) once |<v|Hv>|/|Hv| is
  * within ov_tol of 1.  Default 1e-8, the reference's constant (src/dmrg_inst.cpp:1338).

@@ -82,14 +82,28 @@ static State<S>& st_of(sadmrg_handle* h);
 template <> State<double>& st_of<double>(sadmrg_handle* h) { return h->sd; }
 template <> State<dcmplex>& st_of<dcmplex>(sadmrg_handle* h) { return h->sz; }
 
+// After a bounded wait ran out, the persistent plans' split-K and dependency
+// counters are part-way: zero them so the next call computes normally.
+static void reset_plan_counters(sadmrg_handle* h) {
+  auto reset = [&](auto& S_) {
+    if (S_.heff) S_.heff->plan.reset_counters(h->ctx);
+    if (S_.batch) S_.batch->merged.plan.reset_counters(h->ctx);
+  };
+  reset(h->sd);
+  reset(h->sz);
+  SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
+}
+
 // A tcgen05 item kernel whose bounded wait ran out leaves its tile unwritten and
 // raises a device status word; calls that synchronise anyway check it.
-static void check_device_status() {
+static void check_device_status(sadmrg_handle* h) {
   const int v = umma_status(true);
   if (v < 0) throw Error(SADMRG_ERR_CUDA, "cannot read the tcgen05 status word");
-  if (v != 0)
+  if (v != 0) {
+    reset_plan_counters(h);
     throw Error(SADMRG_ERR_CUDA, "tcgen05 GEMM: a bounded wait ran out (status " + std::to_string(v) +
                                      "); the results of this call are invalid");
+  }
 }
 
 template <class F>
@@ -110,6 +124,32 @@ int sadmrg_device_status(sadmrg_handle* h, int* status) {
     SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
     const int v = umma_status(true);
     SADMRG_REQUIRE(v >= 0, SADMRG_ERR_CUDA, "device_status: cannot read the status word");
+    if (v != 0) reset_plan_counters(h);
+    *status = v;
+  });
+}
+
+int sadmrg_heff_wait_fault_test(sadmrg_handle* h, long long wait_ns, int* status) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    Ctx& c = h->ctx;
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "wait_fault_test: no plan");
+    SADMRG_REQUIRE(status && wait_ns >= 1000000 && wait_ns <= 2000000000LL, SADMRG_ERR_ARG,
+                   "wait_fault_test: wait_ns outside [1 ms, 2 s]");
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+    SADMRG_REQUIRE(umma_status(true) == 0, SADMRG_ERR_STATE, "wait_fault_test: status word already set");
+    const HeffPlan<S>& H = *S_.heff;
+    Bases b{};
+    b.p[0] = S_.io.get();
+    b.p[1] = S_.io.template as<S>() + H.n;
+    b.p[2] = H.opsbuf->get();
+    b.p[3] = H.scratch->get();
+    SADMRG_CUDA(cudaMemsetAsync(S_.io.get(), 0, sizeof(S) * H.n, c.stream));
+    H.plan.run_starved(c, ScalarInfo<S>::cplx, b, 0, wait_ns);
+    const int v = umma_status(true);
+    SADMRG_REQUIRE(v >= 0, SADMRG_ERR_CUDA, "wait_fault_test: cannot read the status word");
+    reset_plan_counters(h);
     *status = v;
   });
 }
@@ -269,7 +309,7 @@ int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, in
     S_.heff->apply(c, din, dout, precision);
     SADMRG_CUDA(cudaMemcpyAsync(out_host, dout, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    check_device_status();
+    check_device_status(h);
   });
 }
 
@@ -349,7 +389,7 @@ int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* p
       acc[1] += t1;
     }
     for (auto& e : ev) cudaEventDestroy(e);
-    check_device_status();
+    check_device_status(h);
     ms[0] = acc[0] / reps;
     ms[1] = acc[1] / reps;
     // algorithmic flops per stage
@@ -411,7 +451,7 @@ int sadmrg_heff_launch_profile(sadmrg_handle* h, int precision, int reps, const 
       cudaEventDestroy(start);
       for (auto& e : ev) cudaEventDestroy(e.second);
     }
-    check_device_status();
+    check_device_status(h);
     *nlaunch = (int)acc.size();
     for (int i = 0; i < (int)acc.size() && i < cap; ++i) {
       if (kind) kind[i] = kinds[i];
@@ -484,7 +524,7 @@ int sadmrg_heff_graph_steps(sadmrg_handle* h, int precision, int steps, const vo
     cleanup();
     c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision,
                                                    H.plan.runs_fused(c, ScalarInfo<S>::cplx, precision)) * (steps + 1);
-    check_device_status();
+    check_device_status(h);
   });
 }
 
@@ -551,7 +591,7 @@ int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const voi
     cudaGraphDestroy(g);
     c.launches += (long long)H.plan.launches_per_run(ScalarInfo<S>::cplx, precision,
                                                    H.plan.runs_fused(c, ScalarInfo<S>::cplx, precision)) * (reps + 1);
-    check_device_status();
+    check_device_status(h);
   });
 }
 
@@ -568,7 +608,7 @@ int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precisi
     LanczosStats st = lanczos_solve<S>(c, *S_.heff, dv, mlanc, precision);
     SADMRG_CUDA(cudaMemcpyAsync(psi_host, dv, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    check_device_status();
+    check_device_status(h);
     if (energy) *energy = st.energy;
     if (matvecs) *matvecs = st.matvecs;
   });
@@ -587,7 +627,7 @@ int sadmrg_heff_lanczos2(sadmrg_handle* h, void* psi_host, int mlanc, double* en
     LanczosStats st = lanczos2<S>(c, *S_.heff, dv, mlanc);
     SADMRG_CUDA(cudaMemcpyAsync(psi_host, dv, sizeof(S) * n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    check_device_status();
+    check_device_status(h);
     if (energy) *energy = st.energy;
     if (matvecs) *matvecs = st.matvecs;
   });
@@ -653,7 +693,7 @@ int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, i
     H.apply(c, din, dout, precision);
     SADMRG_CUDA(cudaMemcpyAsync(out_host, dout, sizeof(S) * H.n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    check_device_status();
+    check_device_status(h);
   });
 }
 
@@ -682,7 +722,7 @@ int sadmrg_batch_profile(sadmrg_handle* h, int precision, int reps, double* ms) 
     *ms = t / reps;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    check_device_status();
+    check_device_status(h);
   });
 }
 
@@ -700,7 +740,7 @@ int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precis
     BatchStats st = batch_lanczos_solve<S>(c, B, io.as<S>(), mlanc, precision);
     SADMRG_CUDA(cudaMemcpyAsync(psi_host, io.get(), sizeof(S) * B.merged.n, cudaMemcpyDeviceToHost, c.stream));
     SADMRG_CUDA(cudaStreamSynchronize(c.stream));
-    check_device_status();
+    check_device_status(h);
     for (int i = 0; i < B.nseg(); ++i) {
       if (energies) energies[i] = st.energy[i];
       if (matvecs) matvecs[i] = st.matvecs[i];
@@ -760,7 +800,7 @@ int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy) {
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     S_.chain->do_idmrg();
     SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
-    check_device_status();
+    check_device_status(h);
     if (energy) *energy = S_.chain->energy();
   });
 }
@@ -782,7 +822,7 @@ int sadmrg_chain_sweep(sadmrg_handle* h, double* energy) {
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     S_.chain->sweep();
     SADMRG_CUDA(cudaStreamSynchronize(h->ctx.stream));
-    check_device_status();
+    check_device_status(h);
     if (energy) *energy = S_.chain->energy();
   });
 }

@@ -761,12 +761,8 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
     if (cplx) {
       items_tf32x3<true, 32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, work, reds, tile_cnt, mask);
     } else {
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(items_tf32x3_ms<64, 64, 16, kF64Stages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kF64MsSmem);
-        attr = true;
-      }
+      static unsigned char attr[kMaxDevices] = {0};
+      ensure_smem_attr((const void*)items_tf32x3_ms<64, 64, 16, kF64Stages>, (int)kF64MsSmem, attr);
       items_tf32x3_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
                                                                                  static_cast<double*>(work), reds,
                                                                                  tile_cnt, mask);
@@ -776,12 +772,8 @@ void launch_items(bool cplx, int prec, const GemmTerm* terms, const GemmJob* job
       items_z64<32, 32, 16><<<nitems, kThreads, 0, s>>>(terms, jobs, items, b, static_cast<double2*>(work), reds,
                                                           tile_cnt, mask);
     } else {
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(items_f64_ms<64, 64, 16, kF64Stages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kF64MsSmem);
-        attr = true;
-      }
+      static unsigned char attr[kMaxDevices] = {0};
+      ensure_smem_attr((const void*)items_f64_ms<64, 64, 16, kF64Stages>, (int)kF64MsSmem, attr);
       items_f64_ms<64, 64, 16, kF64Stages><<<nitems, kThreads, kF64MsSmem, s>>>(terms, jobs, items, b,
                                                                               static_cast<double*>(work), reds,
                                                                               tile_cnt, mask);
@@ -798,11 +790,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 int noalloc_scratch(void** ptr) {
   static std::mutex mu;
-  static void* cache[64] = {nullptr};
+  static void* cache[kMaxDevices] = {nullptr};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
-  if (dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+  if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> g(mu);
   if (!cache[dev]) {
     void* p = nullptr;

@@ -121,6 +121,7 @@ struct UPhase {               // what one launch does besides its items
   int npk_jobs;
   int wait_deps;              // items wait for panels written in this launch (cooperative launch)
   int ndeps;
+  long long wait_ns;          // limit of every bounded wait; 0: the default (2 s)
 };
 // one 256-thread block per 256 chunks; blk_job[block] = its job
 void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,
@@ -134,6 +135,10 @@ void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem
 // (the tiles it guarded were not written); reset clears it.  -1 if unreadable.
 int umma_status(bool reset);
 int device_sm_count();
+constexpr int kMaxDevices = 64;
+// cudaFuncSetAttribute(fn, MaxDynamicSharedMemorySize, bytes) once per device
+// (the attribute is per device); done[] holds one flag per device ordinal
+void ensure_smem_attr(const void* fn, int bytes, unsigned char* done);
 // Fixed device scratch of the allocation-free H_eff*psi entry point (gemm.cu).
 constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 // Device address of that scratch on the current device (looked up once per

@@ -524,6 +524,51 @@ int GemmPlan::launches_per_run(bool cplx, int prec, bool c_fused) const {
   return n;
 }
 
+void GemmPlan::reset_counters(Ctx& c) const {
+  if (sched.tile_cnt && sched.tile_cnt->bytes())
+    SADMRG_CUDA(cudaMemsetAsync(sched.tile_cnt->get(), 0, sched.tile_cnt->bytes(), c.stream));
+  if (umma) {
+    if (umma->tile_cnt && umma->tile_cnt->bytes())
+      SADMRG_CUDA(cudaMemsetAsync(umma->tile_cnt->get(), 0, umma->tile_cnt->bytes(), c.stream));
+    if (umma->deps && umma->deps->bytes())   // the dependency counters and the finished-CTA count
+      SADMRG_CUDA(cudaMemsetAsync(umma->deps->get(), 0, umma->deps->bytes(), c.stream));
+  }
+}
+
+void GemmPlan::run_starved(Ctx& c, bool cplx, const Bases& b, int starve, long long wait_ns) const {
+  SADMRG_REQUIRE(umma && !umma->vblk.empty() && starve >= 0 && starve < (int)umma->dep_target.size(),
+                 SADMRG_ERR_STATE, "starved run: the plan has no tcgen05 schedule with psi panels");
+  SADMRG_REQUIRE((int)umma->vpack.size() <= kMaxPackJobs, SADMRG_ERR_STATE, "starved run: too many pack jobs");
+  const UmmaSchedule& U = *umma;
+  std::vector<int> tgt = U.dep_target;
+  tgt[starve] += 1;   // one more than the launch will ever count: nothing completes it
+  DevBuf dt(sizeof(int) * tgt.size(), c.stream);
+  SADMRG_CUDA(cudaMemcpyAsync(dt.get(), tgt.data(), sizeof(int) * tgt.size(), cudaMemcpyHostToDevice, c.stream));
+  UBufs ub{};
+  ub.pconst = U.pconst->as<unsigned char>();
+  ub.pvar = U.pvar->as<unsigned char>();
+  ub.slots = U.slots->as<float>();
+  ub.tile_cnt = U.tile_cnt->as<int>();
+  ub.deps = U.deps->as<int>();
+  ub.dep_target = dt.as<int>();
+  ub.fin = reinterpret_cast<unsigned*>(U.deps->as<int>() + U.dep_target.size());
+  ub.mask = nullptr;
+  UPhase ph{};
+  ph.pk = U.d_vpack;
+  ph.pk_blk = U.d_vblk;
+  ph.npk_jobs = (int)U.vpack.size();
+  ph.ndeps = (int)U.dep_target.size();
+  ph.npk_blocks = (int)U.vblk.size();
+  ph.wait_deps = 1;
+  ph.wait_ns = wait_ns;
+  const int ni = U.stage_items[nstage] - U.stage_items[0];
+  launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items, U.d_reds, ni, b, ub, ph, c.stream);
+  ++c.launches;
+  SADMRG_CUDA(cudaGetLastError());
+  SADMRG_CUDA(cudaStreamSynchronize(c.stream));   // dt must outlive the launch
+  (void)cplx;
+}
+
 static void mark(Ctx& c, int kind) {
   if (!c.prof) return;
   cudaEvent_t e;

@@ -150,6 +150,15 @@ struct GemmPlan {
     return uses_umma(cplx, prec) ? umma->slot_bytes() : sched.work_bytes();
   }
   int launches_per_run(bool cplx, int prec, bool fused) const;
+  // Zero the split-K tile counters and the tcgen05 dependency counters.  A launch
+  // whose bounded wait ran out leaves them part-way (its aborted items never
+  // count in), and the next run would emit tiles too early.
+  void reset_counters(Ctx& c) const;
+  // Failure-path check of the bounded waits: the whole split-precision matvec as
+  // one cooperative launch in which dependency counter `starve` can never reach
+  // its target (the target is raised by one for this launch), every wait limited
+  // to wait_ns.  Leaves the status word set; the caller resets the counters.
+  void run_starved(Ctx& c, bool cplx, const Bases& b, int starve, long long wait_ns) const;
   // whether run() takes the single-launch path for a whole matvec under c's setting
   bool runs_fused(const Ctx& c, bool cplx, int prec) const;
   bool empty() const { return jobs.empty(); }

@@ -109,8 +109,9 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 }
 
 // Bounded wait for the phase with the given parity.  Gives up (false) after
-// kWaitNs, or as soon as *abort is set when abort is non-null.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort) {
+// limit_ns, or as soon as *abort is set when abort is non-null.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort,
+                                          unsigned long long limit_ns = kWaitNs) {
   const unsigned long long t0 = gtime();
   for (long long i = 0; i < kWaitIters; ++i) {
     uint32_t ok;
@@ -123,7 +124,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const v
     if (ok) return true;
     if ((i & 63) == 63) {
       if (abort && *abort) return false;
-      if (gtime() - t0 > kWaitNs) return false;
+      if (gtime() - t0 > limit_ns) return false;
     }
   }
   return false;
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm_raw) + 127) & ~uintptr_t(127));
   const uint32_t sbase = saddr(usm);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned long long wlim = ph.wait_ns > 0 ? (unsigned long long)ph.wait_ns : kWaitNs;
 
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(&tmem_sh)),
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         const unsigned long long t0 = gtime();
         for (long long i = 0; i < kWaitIters; ++i) {
           if (ld_acquire(ub.deps + d) >= target) return true;
-          if ((i & 63) == 63 && (abort_sh || gtime() - t0 > kWaitNs)) return false;
+          if ((i & 63) == 63 && (abort_sh || gtime() - t0 > wlim)) return false;
           __nanosleep(64);
         }
         return false;
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
           }
           const int st = (int)(g % ST);
           const uint32_t n = (uint32_t)(g / ST);
-          if (!mbar_wait(saddr(&empty[st]), (n & 1u) ^ 1u, &abort_sh)) {
+          if (!mbar_wait(saddr(&empty[st]), (n & 1u) ^ 1u, &abort_sh, wlim)) {
             if (!abort_sh) atomicExch(&g_umma_status, 3);
             abort_sh = 1;
             break;
@@ -348,8 +350,15 @@ __global__ void __launch_bounds__(kGThreads, 1)
           ++s;
         }
       }
-      // the copies this thread issued have landed before the CTA can exit
-      if (issued_any && !mbar_wait(last_bar, last_par, nullptr)) atomicExch(&g_umma_status, 4);
+      // every copy this thread issued has landed before the CTA can exit: the last
+      // copy into each stage (bulk copies may complete out of order, and after an
+      // abort the issuer has not consumed them all)
+      (void)last_bar;
+      (void)last_par;
+      if (issued_any)
+        for (long long j = g > ST ? g - ST : 0; j < g; ++j)
+          if (!mbar_wait(saddr(&full[(int)(j % ST)]), (uint32_t)(j / ST) & 1u, nullptr))
+            atomicExch(&g_umma_status, 4);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -363,7 +372,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         const UItem it = items[ii];
         if (ub.mask && !ub.mask[jobs[it.job].tag]) continue;
         const int acc = il & 1;
-        if (!mbar_wait(saddr(&tempty[acc]), (((uint32_t)il >> 1) & 1u) ^ 1u, &abort_sh)) {
+        if (!mbar_wait(saddr(&tempty[acc]), (((uint32_t)il >> 1) & 1u) ^ 1u, &abort_sh, wlim)) {
           if (!abort_sh) atomicExch(&g_umma_status, 5);
           abort_sh = 1;
           break;
@@ -378,7 +387,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
           const int kt = (s == T.nslab - 1) ? T.klast : kPanelK;
           const int st = (int)(g % ST);
           const uint32_t n = (uint32_t)(g / ST);
-          if (!mbar_wait(saddr(&full[st]), n & 1u, &abort_sh)) {
+          if (!mbar_wait(saddr(&full[st]), n & 1u, &abort_sh, wlim)) {
             if (!abort_sh) atomicExch(&g_umma_status, 6);
             abort_sh = 1;
             ok = false;
@@ -427,7 +436,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
       const UJob J = jobs[it.job];
       if (ub.mask && !ub.mask[J.tag]) continue;
       const int acc = il & 1;
-      if (!mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh)) {
+      if (!mbar_wait(saddr(&tfull[acc]), ((uint32_t)il >> 1) & 1u, &abort_sh, wlim)) {
         if (!abort_sh) atomicExch(&g_umma_status, 8);
         abort_sh = 1;
         ep_fail = 1;
@@ -577,11 +586,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
 template <int BN, int ST>
 void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
                    const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(umma_gemm<BN, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG<BN, ST>::SMEM);
-    attr = true;
-  }
+  static unsigned char attr[kMaxDevices] = {0};
+  ensure_smem_attr((const void*)umma_gemm<BN, ST>, (int)UG<BN, ST>::SMEM, attr);
   const int nsm = device_sm_count();
   int grid = nitems > ph.npk_blocks ? nitems : ph.npk_blocks;
   if (grid > nsm) grid = nsm;
@@ -605,16 +611,26 @@ void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, con
 }  // namespace
 
 int device_sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0, v = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
-                                                  cudaSuccess && v > 0)
-      n = v;
-    else
-      return 148;
+  static int n[kMaxDevices] = {0};
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+  if (n[dev] == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) return 148;
+    n[dev] = v;
   }
-  return n;
+  return n[dev];
+}
+
+void ensure_smem_attr(const void* fn, int bytes, unsigned char* done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return;
+  }
+  if (!done[dev]) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    done[dev] = 1;
+  }
 }
 
 void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,

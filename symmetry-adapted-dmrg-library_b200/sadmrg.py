@@ -38,6 +38,7 @@ EXPORTED = [
     "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos", "sadmrg_batch_profile",
     "sadmrg_chain_set_mlanc", "sadmrg_chain_save_ww", "sadmrg_chain_read_ww", "sadmrg_chain_save_enr",
     "sadmrg_chain_read_enr", "sadmrg_chain_ww", "sadmrg_heff_graph_steps", "sadmrg_heff_launches_per_matvec",
+    "sadmrg_heff_wait_fault_test",
 ]
 
 
@@ -92,6 +93,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_graph_bench": ([vp, C.c_int, C.c_int, vp, vp, dp], C.c_int),
         "sadmrg_heff_graph_steps": ([vp, C.c_int, C.c_int, vp, vp, vp, C.c_longlong, dp], C.c_int),
         "sadmrg_heff_launches_per_matvec": ([vp, C.c_int, ip], C.c_int),
+        "sadmrg_heff_wait_fault_test": ([vp, C.c_longlong, ip], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -377,6 +379,13 @@ class Handle:
                                                      out_ptr or None, flush_ptr or None, int(flush_bytes),
                                                      ms.ctypes.data_as(C.POINTER(C.c_double))), "heff_graph_steps")
         return ms
+
+    def heff_wait_fault_test(self, wait_ns: int = 50_000_000) -> int:
+        """One split-precision matvec whose first psi panels never complete (bounded waits of
+        wait_ns): returns the status word it left (nonzero: a wait ran out); the plan is reset."""
+        st = C.c_int()
+        self._check(self.lib.sadmrg_heff_wait_fault_test(self.h, int(wait_ns), C.byref(st)), "heff_wait_fault_test")
+        return st.value
 
     def heff_launches_per_matvec(self, precision: int) -> int:
         n = C.c_int()

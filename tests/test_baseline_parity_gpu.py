@@ -125,7 +125,8 @@ def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
         out = subprocess.run([HARNESS, "-sym", "su2", "-L", str(ns), "-d", str(D), "-sweeps", "1", "-read", ck,
                               "-mlanc", str(MLANC), "-lanc_check", str(CHECK), "-maxangm", str(max(20, maxj + 6)),
                               "-threads", str(os.cpu_count() or 1), "-sweepdir", os.path.join(d, "sw")],
-                             capture_output=True, text=True, timeout=1500)
+                             capture_output=True, text=True, timeout=1500,
+                             env=dict(os.environ, OPENBLAS_NUM_THREADS="1"))
         assert out.returncode == 0, out.stderr[-500:]
     eref, ref_b = None, {}
     for line in out.stdout.splitlines():
