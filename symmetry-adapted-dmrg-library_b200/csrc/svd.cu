@@ -16,6 +16,7 @@
 // one-sided Jacobi on small singular values, which the reference's 1e-10
 // relative cut-off depends on.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -369,15 +370,315 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   if (tid == 0) atomicAdd(rotations, nrot);
 }
 
+// ---------------------------------------------------------------------------
+// Resident visit (b = 8, pairs of 16 columns): the pair's columns of W and V are
+// read into shared memory once, so the visit takes a handful of block barriers
+// instead of several per 128-row chunk.  Same arithmetic as jacobi_pair_visit
+// (Gram matrix on DMMA, one-sided rotations on G with the exact 2 x 2 values,
+// Wp <- Wp Q, Vp <- Vp Q), except that
+//   * the Gram matrix is summed over the rows in a fixed order: every warp a
+//     contiguous slice of rows, then the 16 partial matrices in warp order;
+//   * the rotations of G run in one warp (a round's disjoint pairs at once,
+//     warp barriers only), repeated until a sweep of G rotates nothing (at most
+//     kResInner sweeps), which cuts the outer sweeps.
+constexpr int kResB = 8;
+constexpr int kResNc = 2 * kResB;
+constexpr int kResLd = kResNc + 1;
+constexpr int kResInner = 4;
+
+template <bool CPLX>
+__host__ __device__ constexpr size_t res_fixed_bytes() {
+  // G, Q, the per-warp partial Gram matrices, and the rotation table of one round
+  return (size_t)(2 * kResNc * kResLd + kSvdWarps * kResNc * kResNc) * (CPLX ? 16 : 8) + 16 * 64;
+}
+template <bool CPLX>
+__host__ __device__ constexpr size_t res_bytes(int R, int C) {
+  return res_fixed_bytes<CPLX>() + (size_t)(((R + 7) / 8) * 8 + ((C + 7) / 8) * 8) * kResLd * (CPLX ? 16 : 8);
+}
+
+struct ResRot {        // one rotation of a round (computed by lane k of the rotating warp)
+  int p, q, act;
+  double c, sr, si, a_new, b_new;
+};
+
+template <bool CPLX>
+__device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
+                                      double tol, unsigned char* smem_raw, int* rotations) {
+  using T = typename SvdT<CPLX>::T;
+  constexpr int kNc = kResNc, kLd = kResLd;
+  const int R = J.trans ? J.n : J.m;
+  const int C = J.trans ? J.m : J.n;
+  const int Rp = ((R + 7) / 8) * 8, Cp = ((C + 7) / 8) * 8;
+  __shared__ int cols[kNc];
+  __shared__ int nrot_sh;
+  T* G = reinterpret_cast<T*>(smem_raw);           // kNc x kLd
+  T* Q = G + kNc * kLd;                            // kNc x kLd
+  T* Gp = Q + kNc * kLd;                           // kSvdWarps x kNc x kNc partial Gram matrices
+  ResRot* rot = reinterpret_cast<ResRot*>(Gp + kSvdWarps * kNc * kNc);   // kNc / 2 entries
+  T* Wp = reinterpret_cast<T*>(smem_raw + res_fixed_bytes<CPLX>());       // Rp x kLd
+  T* Vp = Wp + (size_t)Rp * kLd;                   // Cp x kLd
+  T* W = static_cast<T*>(work) + J.woff;
+  T* V = static_cast<T*>(vmat) + J.voff;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n0 = min(kResB, C - P.bi * kResB);
+  const int n1 = P.bj >= 0 ? min(kResB, C - P.bj * kResB) : 0;
+  const int nc = n0 + n1;
+  {
+    const int* pj = perm + J.soff;
+    if (tid < n0) cols[tid] = pj[P.bi * kResB + tid];
+    else if (tid < nc) cols[tid] = pj[P.bj * kResB + (tid - n0)];
+    if (tid == 0) nrot_sh = 0;
+  }
+  __syncthreads();
+  // 1. the pair's columns of W and V -> shared memory (rows past the end and
+  //    columns past nc zero), consecutive threads on consecutive rows of a column
+  for (int e = tid; e < Rp * kNc; e += kSvdThreads) {
+    const int r = e % Rp, c = e / Rp;
+    Wp[r * kLd + c] = (r < R && c < nc) ? W[r + (long long)cols[c] * R] : czero<T>();
+  }
+  for (int e = tid; e < Cp * kNc; e += kSvdThreads) {
+    const int r = e % Cp, c = e / Cp;
+    Vp[r * kLd + c] = (r < C && c < nc) ? V[r + (long long)cols[c] * C] : czero<T>();
+  }
+  __syncthreads();
+  // 2. Gram matrix: warp w sums rows [w rs, (w + 1) rs) into its partial (all
+  //    four 8 x 8 tiles), then the partials are added in warp order
+  {
+    const int fr = lane >> 2, fk = lane & 3;
+    const int rs = ((Rp / 4 + kSvdWarps - 1) / kSvdWarps) * 4;
+    const int r0 = warp * rs, r1 = min(Rp, r0 + rs);
+    double g[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) g[t][0] = g[t][1] = g[t][2] = g[t][3] = 0.0;
+    for (int k0 = r0; k0 < r1; k0 += 4) {
+      const T* row = Wp + (k0 + fk) * kLd;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int pt = t >> 1, qt = t & 1;
+        const T x = row[pt * 8 + fr];   // A(p, r) = conj(W(r, p))
+        const T y = row[qt * 8 + fr];   // B(r, q) = W(r, q)
+        if constexpr (CPLX) {
+          dmma(g[t][0], g[t][1], x.x, y.x);
+          dmma(g[t][0], g[t][1], x.y, y.y);
+          dmma(g[t][2], g[t][3], x.x, y.y);
+          dmma(g[t][2], g[t][3], -x.y, y.x);
+        } else {
+          dmma(g[t][0], g[t][1], x, y);
+        }
+      }
+    }
+    T* mine = Gp + warp * kNc * kNc;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int pt = t >> 1, qt = t & 1;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        T v;
+        if constexpr (CPLX) v = make_double2(g[t][i], g[t][2 + i]);
+        else v = g[t][i];
+        mine[(pt * 8 + fr) * kNc + qt * 8 + 2 * fk + i] = v;
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kNc * kNc; e += kSvdThreads) {
+    const int p = e / kNc, q = e % kNc;
+    // entries on and above the diagonal, mirrored, so that G is exactly Hermitian
+    const int pp = min(p, q), qq = max(p, q);
+    T v = czero<T>();
+    for (int w = 0; w < kSvdWarps; ++w) v = cadd(v, Gp[w * kNc * kNc + pp * kNc + qq]);
+    G[p * kLd + q] = p <= q ? v : cconj(v);
+    Q[p * kLd + q] = czero<T>();
+    if (p == q) reinterpret_cast<double*>(Q + p * kLd + q)[0] = 1.0;
+  }
+  __syncthreads();
+  {
+    int need = 0;
+    for (int e = tid; e < nc * nc; e += kSvdThreads) {
+      const int p = e / nc, q = e % nc;
+      if (p >= q) continue;
+      const double ab = cre(G[p * kLd + p]) * cre(G[q * kLd + q]);
+      const T gpq = G[p * kLd + q];
+      double g2;
+      if constexpr (CPLX) g2 = gpq.x * gpq.x + gpq.y * gpq.y; else g2 = gpq * gpq;
+      if (ab > 0.0 && g2 > tol * tol * ab) need = 1;
+    }
+    if (!__syncthreads_or(need)) return;
+  }
+  // 3. rotations of G in warp 0: every round's disjoint pairs at once
+  if (warp == 0) {
+    const int N = nc + (nc & 1), npair = N / 2;
+    int total = 0;
+    for (int isw = 0; isw < kResInner && N > 1; ++isw) {
+      int swept = 0;
+      for (int rnd = 0; rnd < N - 1; ++rnd) {
+        if (lane < npair) {
+          int p, q;
+          if (lane == 0) { p = N - 1; q = rnd; }
+          else { p = (rnd + lane) % (N - 1); q = (rnd - lane + (N - 1)) % (N - 1); }
+          if (p > q) { const int t = p; p = q; q = t; }
+          ResRot r{p, q, 0, 1.0, 0.0, 0.0, 0.0, 0.0};
+          if (q < nc) {
+            const double a = cre(G[p * kLd + p]), b = cre(G[q * kLd + q]);
+            const T gpq = G[p * kLd + q];
+            double gr, gi = 0.0;
+            if constexpr (CPLX) { gr = gpq.x; gi = gpq.y; } else { gr = gpq; }
+            const double g2 = gr * gr + gi * gi;
+            // rotate when |g| > tol sqrt(ab), compared squared (as jacobi_pair_visit)
+            if (a * b > 0.0 && g2 > tol * tol * (a * b)) {
+              const double gm = CPLX ? sqrt(g2) : fabs(gr);
+              const double ig = 1.0 / gm;
+              const double zeta = 0.5 * (b - a) * ig;
+              const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
+                                                  : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+              if (t != 0.0) {
+                const double c = rsqrt(1.0 + t * t), sv = c * t;
+                const double er = CPLX ? gr * ig : (gr >= 0.0 ? 1.0 : -1.0), ei = CPLX ? gi * ig : 0.0;
+                r.act = 1;
+                r.c = c;
+                r.sr = sv * er;
+                r.si = sv * ei;
+                r.a_new = a - t * gm;
+                r.b_new = b + t * gm;
+              }
+            }
+          }
+          rot[lane] = r;
+        }
+        __syncwarp();
+        // columns p, q of G and Q: [x y] <- [x y] [[c, s e^{i phi}], [-s e^{-i phi}, c]]
+        for (int e = lane; e < 2 * nc * npair; e += 32) {
+          const int k = e % npair, rr = (e / npair) % nc, m = e / (npair * nc);
+          const ResRot& r = rot[k];
+          if (!r.act) continue;
+          T* row = (m == 0 ? G : Q) + rr * kLd;
+          if constexpr (CPLX) {
+            const double2 ep = make_double2(r.sr, r.si), em = make_double2(-r.sr, r.si);
+            const double2 x = row[r.p], y = row[r.q];
+            row[r.p] = cadd(make_double2(r.c * x.x, r.c * x.y), cmul(y, em));
+            row[r.q] = cadd(cmul(x, ep), make_double2(r.c * y.x, r.c * y.y));
+          } else {
+            const double x = row[r.p], y = row[r.q];
+            row[r.p] = r.c * x - r.sr * y;
+            row[r.q] = r.sr * x + r.c * y;
+          }
+        }
+        __syncwarp();
+        // rows p, q of G: G <- J^H G
+        for (int e = lane; e < nc * npair; e += 32) {
+          const int k = e % npair, j = e / npair;
+          const ResRot& r = rot[k];
+          if (!r.act) continue;
+          T* rp = G + r.p * kLd;
+          T* rq = G + r.q * kLd;
+          if constexpr (CPLX) {
+            const double2 mp = make_double2(-r.sr, -r.si), pm = make_double2(r.sr, -r.si);
+            const double2 x = rp[j], y = rq[j];
+            rp[j] = cadd(make_double2(r.c * x.x, r.c * x.y), cmul(mp, y));
+            rq[j] = cadd(cmul(pm, x), make_double2(r.c * y.x, r.c * y.y));
+          } else {
+            const double x = rp[j], y = rq[j];
+            rp[j] = r.c * x - r.sr * y;
+            rq[j] = r.sr * x + r.c * y;
+          }
+        }
+        __syncwarp();
+        // the rotated 2 x 2 blocks to their exact values
+        if (lane < npair && rot[lane].act) {
+          const ResRot& r = rot[lane];
+          G[r.p * kLd + r.p] = czero<T>();
+          reinterpret_cast<double*>(G + r.p * kLd + r.p)[0] = r.a_new;
+          G[r.q * kLd + r.q] = czero<T>();
+          reinterpret_cast<double*>(G + r.q * kLd + r.q)[0] = r.b_new;
+          G[r.p * kLd + r.q] = czero<T>();
+          G[r.q * kLd + r.p] = czero<T>();
+        }
+        swept += __popc(__ballot_sync(0xffffffffu, lane < npair && rot[lane].act));
+        __syncwarp();
+      }
+      total += swept;
+      if (swept == 0) break;
+    }
+    if (lane == 0) nrot_sh = total;
+  }
+  __syncthreads();
+  const int nrot = nrot_sh;
+  if (nrot == 0) return;
+  // 4. Wp <- Wp Q, Vp <- Vp Q: 8-row tiles round-robin over the warps, each
+  //    warp overwriting only its own rows
+  {
+    const int fr = lane >> 2, fk = lane & 3;
+    const int tw = Rp / 8, tv = Cp / 8;
+    for (int t = warp; t < tw + tv; t += kSvdWarps) {
+      T* M = t < tw ? Wp + (size_t)(t * 8) * kLd : Vp + (size_t)((t - tw) * 8) * kLd;
+      double d[2][4];
+#pragma unroll
+      for (int jt = 0; jt < 2; ++jt) {
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+        for (int k0 = 0; k0 < kNc; k0 += 4) {
+          const T x = M[fr * kLd + k0 + fk];
+          const T y = Q[(k0 + fk) * kLd + jt * 8 + fr];
+          if constexpr (CPLX) {
+            dmma(a0, a1, x.x, y.x);
+            dmma(a0, a1, -x.y, y.y);
+            dmma(b0, b1, x.x, y.y);
+            dmma(b0, b1, x.y, y.x);
+          } else {
+            dmma(a0, a1, x, y);
+          }
+        }
+        d[jt][0] = a0; d[jt][1] = a1; d[jt][2] = b0; d[jt][3] = b1;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int jt = 0; jt < 2; ++jt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          T v;
+          if constexpr (CPLX) v = make_double2(d[jt][i], d[jt][2 + i]);
+          else v = d[jt][i];
+          M[fr * kLd + jt * 8 + 2 * fk + i] = v;
+        }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // 5. back to global memory
+  for (int e = tid; e < R * nc; e += kSvdThreads) {
+    const int r = e % R, c = e / R;
+    W[r + (long long)cols[c] * R] = Wp[r * kLd + c];
+  }
+  for (int e = tid; e < C * nc; e += kSvdThreads) {
+    const int r = e % C, c = e / C;
+    V[r + (long long)cols[c] * C] = Vp[r * kLd + c];
+  }
+  if (tid == 0) atomicAdd(rotations, nrot);
+}
+
+// one visit: the resident form when the pair's columns fit the launch's shared memory
+template <bool CPLX, int B>
+__device__ __forceinline__ void visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
+                                      double tol, unsigned char* smem_raw, int* rotations, size_t smem_avail) {
+  if constexpr (B == kResB) {
+    const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
+    if (res_bytes<CPLX>(R, C) <= smem_avail) {
+      jacobi_pair_visit_res<CPLX>(J, P, work, vmat, perm, tol, smem_raw, rotations);
+      return;
+    }
+  }
+  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
+}
+
 template <bool CPLX, int B>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
                                                                   const SvdPair* __restrict__ pairs, void* work,
                                                                   void* vmat, const int* perm, double tol,
-                                                                  int* rotations) {
+                                                                  int* rotations, size_t smem_avail) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SvdPair P = pairs[blockIdx.x];
   const SvdJob J = jobs[P.job];
-  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
+  visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations, smem_avail);
 }
 
 // ---------------------------------------------------------------------------
@@ -437,7 +738,8 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
                                                                   const SvdPair* __restrict__ pairs,
                                                                   const int* __restrict__ roff, int max_rounds,
                                                                   void* work, void* vmat, double* nrm, int* perm,
-                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps) {
+                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps,
+                                                                  size_t smem_avail) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned char done[kSvdMaxJobsCoop];
   __shared__ int all_done;
@@ -495,7 +797,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
         const SvdPair P = pairs[p];
         if (done[P.job]) continue;
         const SvdJob J = jobs[P.job];
-        jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
+        visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job, smem_avail);
       }
       if (!svd_grid_sync(ctl)) return;
     }
@@ -583,6 +885,14 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     max_rounds = std::max(max_rounds, nrounds[j]);
     smem = svd_smem_bytes<CPLX, B>();
   }
+  // resident visits (b = 8) for the sectors whose pair columns fit in shared memory
+  constexpr size_t kSmemCap = 220 * 1024;
+  if (B == kResB)
+    for (int j = 0; j < nj; ++j) {
+      const int R = hjobs[j].trans ? hjobs[j].n : hjobs[j].m, C = hjobs[j].trans ? hjobs[j].m : hjobs[j].n;
+      const size_t need = res_bytes<CPLX>(R, C);
+      if (need <= kSmemCap) smem = std::max(smem, need);
+    }
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
   for (int j = 0; j < nj; ++j) {
@@ -639,6 +949,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     int* pc = dcnt3.as<int>();
     SvdCtl* pctl = dctl.as<SvdCtl>();
     int njv = nj, mr = max_rounds, ms = max_sweeps;
+    size_t avail = smem;
     double tolv = tol;
     void* a_work = work;
     void* a_vmat = vmat;
@@ -646,7 +957,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     int* a_perm = dperm.as<int>();
     void* args[] = {(void*)&pj,     (void*)&njv,    (void*)&pp,   (void*)&pr, (void*)&mr,   (void*)&a_work,
                     (void*)&a_vmat, (void*)&a_nrm, (void*)&a_perm, (void*)&tolv, (void*)&pc, (void*)&pctl,
-                    (void*)&ms};
+                    (void*)&ms,     (void*)&avail};
     SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<CPLX, B>, dim3(grid), dim3(kSvdThreads),
                                             args, smem, s));
     SvdCtl hctl{};
@@ -665,7 +976,8 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
       const int np = roff[r + 1] - roff[r];
       if (np == 0) continue;
       jacobi_pair_kernel<CPLX, B><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
+                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>(),
+                                                                smem);
     }
     SADMRG_CUDA(cudaGetLastError());
     SADMRG_CUDA(cudaMemcpyAsync(&h_rot, dcnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
