@@ -594,6 +594,7 @@ def run_ours(a, wl: dict, ws: int, rank: int, local: int, cores: int):
                      "stage_flops": list(stage_flops),
                      "fp64_frac": value64 / peaks["fp64_tflops"]},
         "peaks_measured": peaks,
+        "tiles": h.heff_tiles(),
         "gpu_launches": a.steps * launches,
         "clocks": clk.summary(),
     } | extra

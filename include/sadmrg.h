@@ -121,6 +121,21 @@ int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadm
  * nvec = 0 removes the penalty.  The per-stage and per-launch profiles and the
  * graph replay time the sector products only. */
 int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, const double* weights);
+/* Autotuning of the split-precision matvec (no counterpart in the reference).
+ * With it on (the default) every new H_eff plan times candidate tcgen05
+ * schedules on itself -- output tile width 64 or 128, split-K chunks of at
+ * least 16 k slabs or none, one cooperative launch or one per stage -- with
+ * CUDA events on the handle's stream, and keeps the fastest; the choice is
+ * cached per block-size histogram of the plan (jobs by log2 of m, n and k) for
+ * the life of the process.  Off: fixed heuristics.  The FP64 path is never
+ * tuned (its rounding does not depend on a timing). */
+int sadmrg_set_autotune(sadmrg_handle* h, int on);
+/* The current plan's tile choice: out[0] tile width, out[1] fewest slabs per
+ * split-K chunk (0: no split), out[2] 1 when a matvec is one cooperative launch,
+ * out[3] 0 heuristic / 1 timed for this plan / 2 from the cache, out[4] the
+ * number of candidates timed, then per candidate (width, chunk, one launch,
+ * ms per matvec).  *n is the number of values; the first min(cap, *n) are written. */
+int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n);
 /* psi elements, algorithmic flops and bytes of one matvec, number of sector products */
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks);
 /* out = H_eff psi with host buffers (copies in and out on the handle's stream) */

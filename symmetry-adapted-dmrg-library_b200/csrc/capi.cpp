@@ -283,6 +283,35 @@ int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, c
   });
 }
 
+int sadmrg_set_autotune(sadmrg_handle* h, int on) {
+  return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
+}
+
+int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.heff && n, SADMRG_ERR_STATE, "heff_tiles: no plan");
+    const GemmPlan& P = S_.heff->plan;
+    const UmmaTune& t = P.tune;
+    std::vector<double> v;
+    const bool fused = P.runs_fused(h->ctx, ScalarInfo<S>::cplx, PREC_TF32X3);
+    v.push_back(P.umma ? P.umma->bn : 0);
+    v.push_back(t.kc_min);
+    v.push_back(fused ? 1 : 0);
+    v.push_back(t.source);
+    v.push_back(t.ncand);
+    for (int i = 0; i < t.ncand; ++i) {
+      v.push_back(t.cand_bn[i]);
+      v.push_back(t.cand_kc[i]);
+      v.push_back(t.cand_fused[i]);
+      v.push_back(t.ms[i]);
+    }
+    *n = (int)v.size();
+    for (int i = 0; i < cap && i < (int)v.size(); ++i) out[i] = v[i];
+  });
+}
+
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;

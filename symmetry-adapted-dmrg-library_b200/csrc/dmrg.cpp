@@ -6,7 +6,10 @@
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 
 namespace sadmrg {
 
@@ -14,6 +17,110 @@ template <class S> static constexpr bool kCx = ScalarInfo<S>::cplx;
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the split-precision matvec.  Candidates: output tile width 64 or
+// 128, split-K chunks of at least 16 k slabs or no split, and, for the fastest of
+// those, one cooperative launch for the whole matvec against one launch per
+// stage.  Each candidate schedule is built on the plan itself and timed with
+// CUDA events on the context's stream (one warm run, then the mean of three);
+// the winner is cached per block-size histogram (GemmPlan::tune_key) for the
+// life of the process, so later plans with the same histogram reuse it untimed.
+// The FP64 path is not tuned: its schedule, and so its rounding, never depends
+// on a timing.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, UmmaTune> g_tune_cache;
+}
+
+template <class S>
+static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
+  GemmPlan& p = H.plan;
+  if (!p.umma || !c.autotune || c.fused_matvec >= 0 || c.prof) return;
+  const std::string key = p.tune_key(kCx<S>);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      const int built_bn = p.umma->bn, built_kc = p.tune.kc_min;
+      p.tune = it->second;
+      p.tune.source = 2;
+      if (p.tune.bn != built_bn || p.tune.kc_min != built_kc) p.rebuild_umma(c, kCx<S>);
+      return;
+    }
+  }
+  const size_t nb = sizeof(S) * std::max<long long>(H.n, 1);
+  DevBuf x(nb, c.stream), y(nb, c.stream);
+  SADMRG_CUDA(cudaMemsetAsync(x.get(), 0, nb, c.stream));
+  Bases b{};
+  b.p[0] = x.get();
+  b.p[1] = y.get();
+  b.p[2] = H.opsbuf->get();
+  b.p[3] = H.scratch->get();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UmmaTune win;
+  float best = 1e30f;
+  auto record = [&](float ms, int bn, int kc, int fused) {
+    if (win.ncand >= 8) return;
+    win.ms[win.ncand] = ms;
+    win.cand_bn[win.ncand] = bn;
+    win.cand_kc[win.ncand] = kc;
+    win.cand_fused[win.ncand] = fused;
+    ++win.ncand;
+  };
+  try {
+    SADMRG_CUDA(cudaEventCreate(&e0));
+    SADMRG_CUDA(cudaEventCreate(&e1));
+    auto time_current = [&]() -> float {
+      p.run(c, kCx<S>, PREC_TF32X3, b);   // warm: first touch of the schedule
+      SADMRG_CUDA(cudaEventRecord(e0, c.stream));
+      for (int r = 0; r < 3; ++r) p.run(c, kCx<S>, PREC_TF32X3, b);
+      SADMRG_CUDA(cudaEventRecord(e1, c.stream));
+      SADMRG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      SADMRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return ms / 3.f;
+    };
+    const int cands[4][2] = {{64, 16}, {128, 16}, {64, 0}, {128, 0}};
+    std::vector<std::tuple<int, size_t, size_t>> seen;   // schedules already timed: (bn, items, reductions)
+    UmmaTune pick;
+    for (const auto& cd : cands) {
+      p.tune = UmmaTune{};
+      p.tune.bn = cd[0];
+      p.tune.kc_min = cd[1];
+      p.tune.fused = 0;
+      if (!p.rebuild_umma(c, kCx<S>)) break;
+      const auto fp = std::make_tuple(p.umma->bn, p.umma->items.size(), p.umma->reds.size());
+      if (std::find(seen.begin(), seen.end(), fp) != seen.end()) continue;   // the same schedule as one timed
+      seen.push_back(fp);
+      const float ms = time_current();
+      record(ms, cd[0], cd[1], 0);
+      if (ms < best) { best = ms; pick = p.tune; }
+    }
+    // the fastest, also as one cooperative launch
+    p.tune = pick;
+    p.rebuild_umma(c, kCx<S>);
+    p.tune.fused = 1;
+    if (p.runs_fused(c, kCx<S>, PREC_TF32X3)) {
+      const float ms = time_current();
+      record(ms, pick.bn, pick.kc_min, 1);
+      if (ms < best) { best = ms; pick.fused = 1; }
+    }
+    win.bn = pick.bn;
+    win.kc_min = pick.kc_min;
+    win.fused = pick.fused;
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  win.source = 1;
+  p.tune = win;   // the schedule built last is win's (the fused run shares it)
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune_cache[key] = win;
 }
 
 // ---------------------------------------------------------------------------
@@ -147,6 +254,7 @@ HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, con
   H.flops = p.flops;
   H.bytes = (2 * H.n + tot) * (long long)sizeof(S);
   H.ntasks = (int)p.flat_terms.size();
+  autotune_heff(c, H);
   return H;
 }
 

@@ -196,7 +196,10 @@ void GemmPlan::finalize(Ctx& c, bool cplx, bool mixed, const Bases* const_bases)
   sched.tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(sched.reds.size(), 1), c.stream);
   SADMRG_CUDA(cudaMemsetAsync(sched.tile_cnt->get(), 0, sched.tile_cnt->bytes(), c.stream));
   umma.reset();
-  if (mixed && const_bases) build_umma(c, *const_bases, cplx);
+  if (mixed && const_bases) {
+    this->const_bases = *const_bases;
+    build_umma(c, *const_bases, cplx);
+  }
   // the host copies must stay alive until the async copies complete
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -211,7 +214,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   long long t128 = 0;
   for (size_t j = 0; j < jobs.size(); ++j)
     t128 += (long long)(((cplx ? 2 : 1) * jobs[j].m + 127) / 128) * ((jobs[j].n + 127) / 128);
-  U->bn = (t128 >= 2LL * nsm * std::max(nstage, 1)) ? 128 : 64;
+  U->bn = tune.bn == 64 || tune.bn == 128 ? tune.bn : (t128 >= 2LL * nsm * std::max(nstage, 1)) ? 128 : 64;
   const int BN = U->bn;
 
   struct Key {
@@ -406,8 +409,8 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
     // slabs per chunk: about one SM's share of the stage and never below 16 --
     // every split item pays for an FP32 partial tile and the fix-up, which at
     // 4 slabs per chunk cost more than the balance won (D=512: 99 -> 60 us)
-    long long kc = std::max<long long>(16, (total + nsm - 1) / nsm);
-    if (ntile >= target / 2) kc = (long long)1 << 40;
+    long long kc = std::max<long long>(std::max(tune.kc_min, 1), (total + nsm - 1) / nsm);
+    if (ntile >= target / 2 || tune.kc_min <= 0) kc = (long long)1 << 40;
     std::vector<std::pair<long long, UItem>> its;
     for (size_t j = 0; j < jobs.size(); ++j) {
       if (job_stage[j] != s) continue;
@@ -502,8 +505,31 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   return true;
 }
 
+bool GemmPlan::rebuild_umma(Ctx& c, bool cplx) {
+  if (!umma) return false;
+  umma.reset();
+  return build_umma(c, const_bases, cplx);
+}
+
+std::string GemmPlan::tune_key(bool cplx) const {
+  auto lg = [](long long v) { int r = 0; while (v > 1) { v >>= 1; ++r; } return r; };
+  std::map<std::tuple<int, int, int, int>, int> hist;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    long long kt = 0;
+    for (auto& t : job_terms[j]) kt += t.k;
+    ++hist[std::make_tuple(job_stage[j], lg(jobs[j].m), lg(jobs[j].n), lg(std::max<long long>(kt, 1)))];
+  }
+  std::string k = std::string(cplx ? "z" : "d") + std::to_string(device_sm_count()) + ":";
+  for (auto& e : hist)
+    k += std::to_string(std::get<0>(e.first)) + "," + std::to_string(std::get<1>(e.first)) + "," +
+         std::to_string(std::get<2>(e.first)) + "," + std::to_string(std::get<3>(e.first)) + "x" +
+         std::to_string(lg(e.second)) + ";";
+  return k;
+}
+
 bool GemmPlan::runs_fused(const Ctx& c, bool cplx, int prec) const {
   if (!uses_umma(cplx, prec) || c.job_mask || (int)umma->vpack.size() > kMaxPackJobs) return false;
+  if (tune.fused >= 0 && c.fused_matvec < 0) return tune.fused > 0;
   // small plans are latency bound and gain from one launch (D=512: 57 -> 46 us);
   // large ones lose to the dependency waits (D=2048: 494 -> 583 us)
   return c.fused_matvec > 0 || (c.fused_matvec < 0 && (double)flops < Ctx::kAutoFuseFlops);

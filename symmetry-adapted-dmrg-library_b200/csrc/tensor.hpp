@@ -11,6 +11,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "cgc.hpp"
@@ -37,6 +38,8 @@ struct Ctx {
   // stage: 1 always, 0 never, -1 (default) for plans below kAutoFuseFlops
   int fused_matvec = -1;
   static constexpr double kAutoFuseFlops = 4e9;
+  // time tile candidates for every new H_eff plan (1) or use the heuristics (0)
+  int autotune = 1;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
@@ -118,6 +121,21 @@ struct UmmaSchedule {
   size_t slot_bytes() const { return slots ? slots->bytes() : 0; }
 };
 
+// Tile choice of a plan's tcgen05 schedule.  Without tuning the heuristics
+// decide (source 0); the autotuner (dmrg.cpp) times candidate schedules on the
+// plan itself and keeps the fastest per block-size histogram (source 1 when it
+// was timed for this plan, 2 when an earlier plan with the same histogram
+// decided it).
+struct UmmaTune {
+  int bn = 0;          // output tile width 64 or 128; 0: 128 when the 128-wide tiles fill the GPU twice
+  int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: never split the reduction
+  int fused = -1;      // 1: a whole matvec in one cooperative launch, 0: one launch per stage, -1: Ctx's setting
+  int source = 0;
+  int ncand = 0;       // candidates timed, with their device time (ms) per matvec
+  float ms[8] = {};
+  int cand_bn[8] = {}, cand_kc[8] = {}, cand_fused[8] = {};
+};
+
 // A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.
 struct GemmPlan {
   std::vector<std::vector<GemmTerm>> job_terms;
@@ -134,6 +152,8 @@ struct GemmPlan {
   GemmJob* d_jobs = nullptr;
   long long flops = 0;            // algorithmic flops of one execution (real multiply-adds * 2)
   int target_items = 148 * 8;     // work items per stage the split-K aims for
+  UmmaTune tune;                  // tcgen05 tile choice (build_umma reads it)
+  Bases const_bases{};            // where the constant panels come from (kept for rebuilds)
 
   int add_job(int stage, int cbuf, long long coff, int m, int n, int ldc, int flags);
   void add_term(int job, int abuf, long long aoff, int lda, int bbuf, long long boff, int ldb, int k, int flags,
@@ -162,6 +182,11 @@ struct GemmPlan {
   // whether run() takes the single-launch path for a whole matvec under c's setting
   bool runs_fused(const Ctx& c, bool cplx, int prec) const;
   bool empty() const { return jobs.empty(); }
+  // the tcgen05 schedule again with the current `tune` (false: the plan has none)
+  bool rebuild_umma(Ctx& c, bool cplx);
+  // block-size histogram of the plan -- jobs bucketed by stage and log2 of m, n
+  // and their total k, bucket counts by log2: the key of the tile-choice cache
+  std::string tune_key(bool cplx) const;
 
  private:
   void build_schedule(GemmSchedule& s, bool cplx);

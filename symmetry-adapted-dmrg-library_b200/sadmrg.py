@@ -38,7 +38,7 @@ EXPORTED = [
     "sadmrg_batch_info", "sadmrg_batch_apply", "sadmrg_batch_lanczos", "sadmrg_batch_profile",
     "sadmrg_chain_set_mlanc", "sadmrg_chain_save_ww", "sadmrg_chain_read_ww", "sadmrg_chain_save_enr",
     "sadmrg_chain_read_enr", "sadmrg_chain_ww", "sadmrg_heff_graph_steps", "sadmrg_heff_launches_per_matvec",
-    "sadmrg_heff_wait_fault_test",
+    "sadmrg_heff_wait_fault_test", "sadmrg_set_autotune", "sadmrg_heff_tiles",
 ]
 
 
@@ -94,6 +94,8 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_graph_steps": ([vp, C.c_int, C.c_int, vp, vp, vp, C.c_longlong, dp], C.c_int),
         "sadmrg_heff_launches_per_matvec": ([vp, C.c_int, ip], C.c_int),
         "sadmrg_heff_wait_fault_test": ([vp, C.c_longlong, ip], C.c_int),
+        "sadmrg_set_autotune": ([vp, C.c_int], C.c_int),
+        "sadmrg_heff_tiles": ([vp, C.c_int, dp, ip], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -386,6 +388,22 @@ class Handle:
         st = C.c_int()
         self._check(self.lib.sadmrg_heff_wait_fault_test(self.h, int(wait_ns), C.byref(st)), "heff_wait_fault_test")
         return st.value
+
+    def set_autotune(self, on: bool):
+        """Time candidate tcgen05 schedules for every new H_eff plan (default on)."""
+        self._check(self.lib.sadmrg_set_autotune(self.h, int(bool(on))), "set_autotune")
+
+    def heff_tiles(self) -> dict:
+        """The current plan's tcgen05 tile choice and the candidates timed for it."""
+        out = np.zeros(64)
+        n = C.c_int()
+        self._check(self.lib.sadmrg_heff_tiles(self.h, 64, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)),
+                    "heff_tiles")
+        v = out[:n.value]
+        cands = [{"bn": int(v[5 + 4 * i]), "kc_min": int(v[6 + 4 * i]), "one_launch": bool(v[7 + 4 * i]),
+                  "ms": float(v[8 + 4 * i])} for i in range(int(v[4]))]
+        return {"bn": int(v[0]), "kc_min": int(v[1]), "one_launch": bool(v[2]),
+                "source": ["heuristic", "timed", "cached"][int(v[3])], "candidates": cands}
 
     def heff_launches_per_matvec(self, precision: int) -> int:
         n = C.c_int()
