@@ -275,7 +275,10 @@ int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, in
 /* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded,
  *          near_ties (truncations whose cut split a pair of singular values equal to 1e-8),
  *          svd_kernel_s (device time of the Jacobi sweeps), svd_sweeps,
- *          plan_s (host time of building H_eff plans, part of lanczos_s)]; the first n are written */
+ *          plan_s (host time of building H_eff plans, part of lanczos_s),
+ *          stop_ties (truncations whose cut gap -- D-th minus (D+1)-th singular value over
+ *          |psi| -- is below 10 sqrt(Lanczos ov_tol): the stop test fixes psi only to about
+ *          that, so two correct runs may cut such a bond differently)]; the first n are written */
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
 /* kind: 0 = uu[site], 1 = hh[site], 2 = opr[site][k] */
 int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t);

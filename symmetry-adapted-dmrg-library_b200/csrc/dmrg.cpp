@@ -670,6 +670,12 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   const int ntot = (int)wsort.size();
   const int dcut = ntot > max_dcut ? max_dcut : ntot;
   if (dcut < ntot && dcut > 0 && std::fabs(wsort[dcut - 1] - wsort[dcut]) <= 1e-8 * wsort[dcut - 1]) out.near_tie = true;
+  // gap at the cut relative to the norm of psi (sum of all squared singular values)
+  if (dcut < ntot && dcut > 0) {
+    double w2 = 0.0;
+    for (double x : wsort) w2 += x * x;
+    out.cut_gap = (wsort[dcut - 1] - wsort[dcut]) / std::sqrt(std::max(w2, 1e-300));
+  }
   std::vector<int> dim(nm1, 0);
   for (int k = 0; k < dcut; ++k) dim[isort[k]]++;
   std::vector<int> amom, bdim;
@@ -1097,6 +1103,9 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   std::copy(w.begin(), w.end(), ww.begin());
   last_discarded = s.discarded_weight;
   if (s.near_tie) ++near_ties;
+  // the stop test fixes the Ritz vector only to about sqrt(ov_tol) (times |E| / gap),
+  // so a cut whose gap is within that of 0 can fall either way in two correct runs
+  if (s.cut_gap < 10.0 * std::sqrt(c.lanczos_ov_tol)) ++stop_ties;
   if (s.jacobi_kernel_ms > 0) timers.svd_kernel += s.jacobi_kernel_ms * 1e-3;
   timers.svd_sweeps += s.sweeps_max > 0 ? s.sweeps_max : 0;
   if (std::getenv("SADMRG_VERBOSE")) {

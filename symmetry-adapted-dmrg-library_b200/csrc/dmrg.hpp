@@ -119,6 +119,7 @@ struct SvdStats {
   double jacobi_kernel_ms = -1.0;
   int max_rows = 0, max_cols = 0;
   bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative)
+  double cut_gap = 1.0;       // (D-th - (D+1)-th singular value) / |psi|; 1 when nothing was cut
 };
 
 // BlockTensor::svd (src/block_tensor_inst.cpp:501-637)
@@ -183,6 +184,7 @@ class Chain {
   std::vector<double> ww;
   double last_discarded = 0.0;
   int near_ties = 0;          // truncations whose cut fell inside a near-degenerate pair
+  int stop_ties = 0;          // truncations whose cut gap is below 10 sqrt(Lanczos ov_tol) |psi|
   // Lanczos settings (reference constants at src/dmrg_inst.cpp:267,1289,1338)
   int mlanc_max = 40;
   int prec = PREC_FP64;

@@ -1,26 +1,35 @@
 """Parity at the benchmark configurations, with the benchmark's Lanczos settings.
 
-Both sides run Lanczos with at most 100 steps and stop once |<v|Hv>|/|Hv| is
-within 1e-10 of 1 (the reference's own constants are 40 and 1e-8,
-src/dmrg_inst.cpp:267,1338; the reference build takes them from the harness's
--mlanc / -lanc_check).
+Both sides run Lanczos with the same length and stop test: at most 100 steps,
+stop once |<v|Hv>|/|Hv| is within 1e-10 of 1 (the benchmark's setting; the
+reference's own constants are 40 and 1e-8, src/dmrg_inst.cpp:267,1338, and its
+build takes them from the harness's -mlanc / -lanc_check).
+
+Two kinds of flagged cut decide how strict a sweep's comparison is, both
+counted by the GPU run (chain_stats):
+  * near_ties: the D-th and (D+1)-th singular values agree to 1e-8 -- for U(1)
+    the sectors q and -q carry equal values in exact arithmetic, and the
+    reference's std::sort has no tie-break, so rounding decides;
+  * stop_ties: the gap at the cut is below 10 sqrt(stop tolerance) of |psi|.  A
+    stop test fixes the Ritz vector only to about that, and two correct runs
+    whose test passes one check apart (the residual of both sides is compared
+    with the same threshold, and rounding can put one just above it) cut such a
+    bond differently.
+Until a flagged cut, every sweep must give the reference's energy to 1e-10
+relative and identical sectors and dimensions on every bond; after one, the
+energy to 1e-8 and the total kept dimension of every bond.
 
 * Configuration 1 (U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps):
   both sides sweep from the reference's own iDMRG checkpoint (its save_mps2
-  files, tests/golden/baseline_u1_L32_D64.npz).  After every sweep the energy
-  agrees to 1e-10 relative and every bond's sectors and dimensions are
-  identical -- unless a truncation cut fell inside a near-degenerate pair of
-  singular values (the U(1) sectors q and -q carry equal singular values in
-  exact arithmetic, and the reference's std::sort has no tie-break), which the
-  GPU run counts (chain_stats()["near_ties"]); then the total kept dimension of
-  every bond must match and the energy agree to 1e-8.  The checkpoint files the
-  reference's sweeps wrote (enr-*.dat after every sweep, ww-*.bin after the
-  last) are compared with the ones written here.
+  files, tests/golden/baseline_u1_L32_D64*.npz) -- with the benchmark's stop
+  test, and with one no run passes (1e-14: every solve takes all 100 steps, so
+  both sides follow the same path and only rounding ties remain).  The
+  checkpoint files the reference's sweeps wrote (enr-*.dat after every sweep,
+  ww-*.bin after the last) are compared with the ones written here.
 * Configuration 2 (SU(2) real Heisenberg chain, open, L = 100, D = 512
   multiplets): the GPU's own iDMRG checkpoint is handed to the reference build
   (read_mps + prepare_sweep), which sweeps once on the host cores; the GPU
-  sweeps once from the same files.  Energy to 1e-10 relative, bonds identical
-  (near ties counted as above).  Needs the reference build (oracle/_ref).
+  sweeps once from the same files.  Needs the reference build (oracle/_ref).
 """
 import os
 import subprocess
@@ -45,23 +54,31 @@ def _total(b):
     return sum(int(x.split("x")[1]) for x in b.split(":")[1].split(",") if x)
 
 
-def _compare_sweep(s, e, eref, got, ref_b, ties):
-    if ties == 0:
+def _flagged(h):
+    st = h.chain_stats()
+    return int(st["near_ties"] + st["stop_ties"])
+
+
+def _compare_sweep(s, e, eref, got, ref_b, flagged):
+    if flagged == 0:
         assert abs(e - eref) <= 1e-10 * abs(eref), (s, e, eref)
         assert got == ref_b, (s, [(a, b) for a, b in zip(got, ref_b) if a != b][:4])
     else:
-        assert abs(e - eref) <= 1e-8 * abs(eref), (s, e, eref, ties)
-        assert [_total(x) for x in got] == [_total(x) for x in ref_b], (s, ties)
+        assert abs(e - eref) <= 1e-8 * abs(eref), (s, e, eref, flagged)
+        assert [_total(x) for x in got] == [_total(x) for x in ref_b], (s, flagged)
 
 
-def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint():
+@pytest.mark.parametrize("fixture", ["baseline_u1_L32_D64.npz", "baseline_u1_L32_D64_converged.npz"])
+def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint(fixture):
     import sadmrg
-    z = np.load(os.path.join(GOLDEN, "baseline_u1_L32_D64.npz"))
+    z = np.load(os.path.join(GOLDEN, fixture))
+    lz = str(z["lanczos"]).split()
+    mlanc, check = int(lz[lz.index("-mlanc") + 1]), float(lz[lz.index("-lanc_check") + 1])
     ns, D = 32, 64
     h = sadmrg.Handle(sym=0, cplx=False)
     h.chain_create(1, ns, D, 1, 0, True, 0.0)
-    h.chain_set_mlanc(MLANC)
-    h.set_lanczos_tol(CHECK)
+    h.chain_set_mlanc(mlanc)
+    h.set_lanczos_tol(check)
     with tempfile.TemporaryDirectory() as d:
         for k in z.files:
             if k.startswith("ck__"):
@@ -72,21 +89,21 @@ def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint():
         for s, eref in enumerate(z["energies"]):
             e = h.chain_sweep()
             h.chain_save_enr(out)
-            ties = h.chain_stats()["near_ties"]
-            _compare_sweep(s, e, float(eref), _bonds(h, ns), [str(x) for x in z["bonds_per_sweep"][s]], ties)
+            _compare_sweep(s, e, float(eref), _bonds(h, ns), [str(x) for x in z["bonds_per_sweep"][s]],
+                           _flagged(h))
         h.chain_save_ww(out)
         # enr-*.dat: one line per sweep, 16 significant digits
         enr_name = f"enr-{ns}-{D}-0-0.dat"
         ours = np.loadtxt(os.path.join(out, enr_name))
         ref = np.array([float(x) for x in bytes(z["sw__" + enr_name]).decode().split()])
         assert ours.shape == ref.shape
-        assert np.all(np.abs(ours - ref) <= 1e-10 * np.abs(ref))
+        assert np.all(np.abs(ours - ref) <= (1e-10 if _flagged(h) == 0 else 1e-8) * np.abs(ref))
         # ww-*.bin: bondd * 2 doubles, the singular values of the last truncations in the reference's layout
         ww_name = f"ww-{ns}-{D}-0-0.bin"
         ours = np.fromfile(os.path.join(out, ww_name))
         ref = np.frombuffer(bytes(z["sw__" + ww_name]), dtype=np.float64)
         assert ours.shape == ref.shape == (2 * D,)
-        if h.chain_stats()["near_ties"] == 0:
+        if _flagged(h) == 0:
             np.testing.assert_allclose(ours, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
         # read_ww / read_enr restore them (DMRG::read_ww, read_enr)
         h2 = sadmrg.Handle(sym=0, cplx=False)
@@ -120,7 +137,7 @@ def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
         g.chain_prepare_sweep()
         e = g.chain_sweep()
         got = _bonds(g, ns)
-        ties = g.chain_stats()["near_ties"]
+        flagged = _flagged(g)
         g.close()
         out = subprocess.run([HARNESS, "-sym", "su2", "-L", str(ns), "-d", str(D), "-sweeps", "1", "-read", ck,
                               "-mlanc", str(MLANC), "-lanc_check", str(CHECK), "-maxangm", str(max(20, maxj + 6)),
@@ -136,4 +153,4 @@ def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
         elif t and t[0] == "BONDS" and t[1] == "0":
             ref_b[int(t[3])] = f"{t[3]}:" + ",".join(x.replace(":", "x") for x in t[4:])
     assert eref is not None
-    _compare_sweep(0, e, eref, got, [ref_b.get(s, f"{s}:") for s in range(ns)], ties)
+    _compare_sweep(0, e, eref, got, [ref_b.get(s, f"{s}:") for s in range(ns)], flagged)
