@@ -125,16 +125,25 @@ int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, c
  * With it on (the default) every new H_eff plan times candidate tcgen05
  * schedules on itself -- output tile width 64 or 128, split-K chunks of at
  * least 16 k slabs or none, one cooperative launch or one per stage -- with
- * CUDA events on the handle's stream, and keeps the fastest; the choice is
+ * CUDA events on the handle's stream (and items capped at 32 k slabs), and keeps the fastest; the choice is
  * cached per block-size histogram of the plan (jobs by log2 of m, n and k) for
  * the life of the process.  Off: fixed heuristics.  The FP64 path is never
  * tuned (its rounding does not depend on a timing). */
 int sadmrg_set_autotune(sadmrg_handle* h, int on);
+/* A fixed tile choice for the H_eff plans made after this call, instead of the
+ * autotuner or the heuristics: width 64 or 128 (0 returns to them), fewest slabs
+ * per split-K chunk when the tiles cannot fill the GPU (0: no such split), most
+ * slabs per item (0: no cap), one cooperative launch per matvec (1), one per
+ * stage (0) or the default rule (-1).  For profiling one schedule. */
+int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int one_launch);
 /* The current plan's tile choice: out[0] tile width, out[1] fewest slabs per
- * split-K chunk (0: no split), out[2] 1 when a matvec is one cooperative launch,
- * out[3] 0 heuristic / 1 timed for this plan / 2 from the cache, out[4] the
- * number of candidates timed, then per candidate (width, chunk, one launch,
- * ms per matvec).  *n is the number of values; the first min(cap, *n) are written. */
+ * split-K chunk when the tiles cannot fill the GPU (0: no such split), out[2]
+ * most slabs per item (0: no cap), out[3] 1 when a matvec is one cooperative
+ * launch, out[4] 0 heuristic / 1 timed for this plan / 2 from the cache / 3 set by
+ * sadmrg_set_tiles, out[5]
+ * the number of candidates timed, then per candidate (width, chunk, cap, one
+ * launch, ms per matvec).  *n is the number of values; the first min(cap, *n)
+ * are written. */
 int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n);
 /* psi elements, algorithmic flops and bytes of one matvec, number of sector products */
 int sadmrg_heff_info(sadmrg_handle* h, long long* n, double* flops, double* bytes, int* ntasks);
@@ -273,7 +282,8 @@ int sadmrg_chain_freeze(sadmrg_handle* h, int il, const char* export_dir);
 /* sectors of bond 2 of site tensor uu[site]: labels and dimensions */
 int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, int* d);
 /* timers: [lanczos_s, env_s, svd_s, prep_s, matvecs, heff_flops, gemm_flops, launches, discarded,
- *          near_ties (truncations whose cut split a pair of singular values equal to 1e-8),
+ *          near_ties (truncations whose cut split a pair of singular values equal to 1e-8, or
+ *          whose per-sector 1e-10 relative cut-off met a value within two decades of it),
  *          svd_kernel_s (device time of the Jacobi sweeps), svd_sweeps,
  *          plan_s (host time of building H_eff plans, part of lanczos_s),
  *          stop_ties (truncations whose cut gap -- D-th minus (D+1)-th singular value over

@@ -287,6 +287,20 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
 }
 
+int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int one_launch) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(bn == 0 || bn == 64 || bn == 128, SADMRG_ERR_ARG, "set_tiles: width must be 0, 64 or 128");
+    SADMRG_REQUIRE(kc_min >= 0 && kc_max >= 0 && one_launch >= -1 && one_launch <= 1, SADMRG_ERR_ARG,
+                   "set_tiles: arguments");
+    UmmaTune t;
+    t.bn = bn;
+    t.kc_min = kc_min;
+    t.kc_max = kc_max;
+    t.fused = one_launch;
+    h->ctx.forced_tune = t;
+  });
+}
+
 int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
@@ -298,12 +312,14 @@ int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
     const bool fused = P.runs_fused(h->ctx, ScalarInfo<S>::cplx, PREC_TF32X3);
     v.push_back(P.umma ? P.umma->bn : 0);
     v.push_back(t.kc_min);
+    v.push_back(t.kc_max);
     v.push_back(fused ? 1 : 0);
     v.push_back(t.source);
     v.push_back(t.ncand);
     for (int i = 0; i < t.ncand; ++i) {
       v.push_back(t.cand_bn[i]);
       v.push_back(t.cand_kc[i]);
+      v.push_back(t.cand_kmax[i]);
       v.push_back(t.cand_fused[i]);
       v.push_back(t.ms[i]);
     }

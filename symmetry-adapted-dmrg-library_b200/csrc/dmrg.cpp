@@ -21,9 +21,12 @@ static double now_s() {
 
 // ---------------------------------------------------------------------------
 // Autotuner of the split-precision matvec.  Candidates: output tile width 64 or
-// 128, split-K chunks of at least 16 k slabs or no split, and, for the fastest of
-// those, one cooperative launch for the whole matvec against one launch per
-// stage.  Each candidate schedule is built on the plan itself and timed with
+// 128, times three ways to cut the reductions -- split-K chunks of at least 16 k
+// slabs when the output tiles cannot fill the GPU, no split, or no item longer
+// than 32 (or, at width 64, 16) slabs: the longest items set the time of a
+// launch -- and, for the
+// fastest of those, one cooperative launch for the whole matvec against one
+// launch per stage.  Each candidate schedule is built on the plan itself and timed with
 // CUDA events on the context's stream (one warm run, then the mean of three);
 // the winner is cached per block-size histogram (GemmPlan::tune_key) for the
 // life of the process, so later plans with the same histogram reuse it untimed.
@@ -37,16 +40,24 @@ std::map<std::string, UmmaTune> g_tune_cache;
 template <class S>
 static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
   GemmPlan& p = H.plan;
+  if (p.umma && c.forced_tune.bn > 0) {
+    p.tune = c.forced_tune;
+    p.tune.source = 3;
+    p.rebuild_umma(c, kCx<S>);
+    return;
+  }
   if (!p.umma || !c.autotune || c.fused_matvec >= 0 || c.prof) return;
   const std::string key = p.tune_key(kCx<S>);
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      const int built_bn = p.umma->bn, built_kc = p.tune.kc_min;
+      const UmmaTune built = p.tune;
+      const int built_bn = p.umma->bn;
       p.tune = it->second;
       p.tune.source = 2;
-      if (p.tune.bn != built_bn || p.tune.kc_min != built_kc) p.rebuild_umma(c, kCx<S>);
+      if (p.tune.bn != built_bn || p.tune.kc_min != built.kc_min || p.tune.kc_max != built.kc_max)
+        p.rebuild_umma(c, kCx<S>);
       return;
     }
   }
@@ -61,11 +72,12 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   UmmaTune win;
   float best = 1e30f;
-  auto record = [&](float ms, int bn, int kc, int fused) {
+  auto record = [&](float ms, const UmmaTune& t, int fused) {
     if (win.ncand >= 8) return;
     win.ms[win.ncand] = ms;
-    win.cand_bn[win.ncand] = bn;
-    win.cand_kc[win.ncand] = kc;
+    win.cand_bn[win.ncand] = t.bn;
+    win.cand_kc[win.ncand] = t.kc_min;
+    win.cand_kmax[win.ncand] = t.kc_max;
     win.cand_fused[win.ncand] = fused;
     ++win.ncand;
   };
@@ -82,20 +94,22 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
       SADMRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       return ms / 3.f;
     };
-    const int cands[4][2] = {{64, 16}, {128, 16}, {64, 0}, {128, 0}};
+    const int cands[7][3] = {{64, 16, 0}, {128, 16, 0}, {64, 0, 0},  {128, 0, 0},
+                             {64, 16, 32}, {128, 16, 32}, {64, 16, 16}};
     std::vector<std::tuple<int, size_t, size_t>> seen;   // schedules already timed: (bn, items, reductions)
     UmmaTune pick;
     for (const auto& cd : cands) {
       p.tune = UmmaTune{};
       p.tune.bn = cd[0];
       p.tune.kc_min = cd[1];
+      p.tune.kc_max = cd[2];
       p.tune.fused = 0;
       if (!p.rebuild_umma(c, kCx<S>)) break;
       const auto fp = std::make_tuple(p.umma->bn, p.umma->items.size(), p.umma->reds.size());
       if (std::find(seen.begin(), seen.end(), fp) != seen.end()) continue;   // the same schedule as one timed
       seen.push_back(fp);
       const float ms = time_current();
-      record(ms, cd[0], cd[1], 0);
+      record(ms, p.tune, 0);
       if (ms < best) { best = ms; pick = p.tune; }
     }
     // the fastest, also as one cooperative launch
@@ -104,11 +118,12 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
     p.tune.fused = 1;
     if (p.runs_fused(c, kCx<S>, PREC_TF32X3)) {
       const float ms = time_current();
-      record(ms, pick.bn, pick.kc_min, 1);
+      record(ms, pick, 1);
       if (ms < best) { best = ms; pick.fused = 1; }
     }
     win.bn = pick.bn;
     win.kc_min = pick.kc_min;
+    win.kc_max = pick.kc_max;
     win.fused = pick.fused;
   } catch (...) {
     if (e0) cudaEventDestroy(e0);
@@ -670,6 +685,22 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   const int ntot = (int)wsort.size();
   const int dcut = ntot > max_dcut ? max_dcut : ntot;
   if (dcut < ntot && dcut > 0 && std::fabs(wsort[dcut - 1] - wsort[dcut]) <= 1e-8 * wsort[dcut - 1]) out.near_tie = true;
+  // the per-sector relative cut-off decided by rounding: a value within two
+  // decades of 1e-10 s_max (such values are rounding noise of an exactly
+  // rank-deficient block) that the global cut would otherwise keep
+  {
+    int sure = 0;
+    bool grey = false;
+    for (size_t j = 0; j < ssort.size(); ++j) {
+      const auto& sv = ssort[j];
+      const double smax = (!sv.empty() && sv[0] > 1e-16) ? sv[0] : 1.0;
+      for (double x : sv) {
+        if (x / smax >= 1e-8) ++sure;
+        else if (x / smax > 1e-12) grey = true;
+      }
+    }
+    if (grey && sure < max_dcut) out.near_tie = true;
+  }
   // gap at the cut relative to the norm of psi (sum of all squared singular values)
   if (dcut < ntot && dcut > 0) {
     double w2 = 0.0;

@@ -118,7 +118,8 @@ struct SvdStats {
   double jacobi_s = 0.0;       // wall time of the Jacobi solve
   double jacobi_kernel_ms = -1.0;
   int max_rows = 0, max_cols = 0;
-  bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative)
+  bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative), or a
+                              // sector's relative 1e-10 cut-off met a value within two decades of it
   double cut_gap = 1.0;       // (D-th - (D+1)-th singular value) / |psi|; 1 when nothing was cut
 };
 

@@ -411,6 +411,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
     // 4 slabs per chunk cost more than the balance won (D=512: 99 -> 60 us)
     long long kc = std::max<long long>(std::max(tune.kc_min, 1), (total + nsm - 1) / nsm);
     if (ntile >= target / 2 || tune.kc_min <= 0) kc = (long long)1 << 40;
+    if (tune.kc_max > 0) kc = std::min<long long>(kc, tune.kc_max);
     std::vector<std::pair<long long, UItem>> its;
     for (size_t j = 0; j < jobs.size(); ++j) {
       if (job_stage[j] != s) continue;

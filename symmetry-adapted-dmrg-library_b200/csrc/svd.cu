@@ -378,28 +378,22 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
 // Wp <- Wp Q, Vp <- Vp Q), except that
 //   * the Gram matrix is summed over the rows in a fixed order: every warp a
 //     contiguous slice of rows, then the 16 partial matrices in warp order;
-//   * the rotations of G run in one warp (a round's disjoint pairs at once,
-//     warp barriers only), repeated until a sweep of G rotates nothing (at most
-//     kResInner sweeps), which cuts the outer sweeps.
+//   * the rotation rounds of G synchronise the 8 rotating warps only (a named
+//     barrier), not the whole block.
 constexpr int kResB = 8;
 constexpr int kResNc = 2 * kResB;
 constexpr int kResLd = kResNc + 1;
-constexpr int kResInner = 4;
+constexpr int kResInner = 1;   // inner sweeps of G per visit (more did not cut the outer sweeps)
 
 template <bool CPLX>
 __host__ __device__ constexpr size_t res_fixed_bytes() {
-  // G, Q, the per-warp partial Gram matrices, and the rotation table of one round
-  return (size_t)(2 * kResNc * kResLd + kSvdWarps * kResNc * kResNc) * (CPLX ? 16 : 8) + 16 * 64;
+  // G, Q and the per-warp partial Gram matrices
+  return (size_t)(2 * kResNc * kResLd + kSvdWarps * kResNc * kResNc) * (CPLX ? 16 : 8);
 }
 template <bool CPLX>
 __host__ __device__ constexpr size_t res_bytes(int R, int C) {
   return res_fixed_bytes<CPLX>() + (size_t)(((R + 7) / 8) * 8 + ((C + 7) / 8) * 8) * kResLd * (CPLX ? 16 : 8);
 }
-
-struct ResRot {        // one rotation of a round (computed by lane k of the rotating warp)
-  int p, q, act;
-  double c, sr, si, a_new, b_new;
-};
 
 template <bool CPLX>
 __device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
@@ -410,11 +404,10 @@ __device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* w
   const int C = J.trans ? J.m : J.n;
   const int Rp = ((R + 7) / 8) * 8, Cp = ((C + 7) / 8) * 8;
   __shared__ int cols[kNc];
-  __shared__ int nrot_sh;
+  __shared__ int nrot_sh, rot_sh;
   T* G = reinterpret_cast<T*>(smem_raw);           // kNc x kLd
   T* Q = G + kNc * kLd;                            // kNc x kLd
   T* Gp = Q + kNc * kLd;                           // kSvdWarps x kNc x kNc partial Gram matrices
-  ResRot* rot = reinterpret_cast<ResRot*>(Gp + kSvdWarps * kNc * kNc);   // kNc / 2 entries
   T* Wp = reinterpret_cast<T*>(smem_raw + res_fixed_bytes<CPLX>());       // Rp x kLd
   T* Vp = Wp + (size_t)Rp * kLd;                   // Cp x kLd
   T* W = static_cast<T*>(work) + J.woff;
@@ -427,7 +420,7 @@ __device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* w
     const int* pj = perm + J.soff;
     if (tid < n0) cols[tid] = pj[P.bi * kResB + tid];
     else if (tid < nc) cols[tid] = pj[P.bj * kResB + (tid - n0)];
-    if (tid == 0) nrot_sh = 0;
+    if (tid == 0) { nrot_sh = 0; rot_sh = 0; }
   }
   __syncthreads();
   // 1. the pair's columns of W and V -> shared memory (rows past the end and
@@ -505,19 +498,22 @@ __device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* w
     }
     if (!__syncthreads_or(need)) return;
   }
-  // 3. rotations of G in warp 0: every round's disjoint pairs at once
-  if (warp == 0) {
+  // 3. rotations of G: warp k < 8 owns pair k of each round (lane = row of G
+  //    and Q); the 256 threads of warps 0-7 meet at a named barrier between the
+  //    column and the row half of a round, the other warps wait below
+  if (warp < kResNc / 2) {
     const int N = nc + (nc & 1), npair = N / 2;
     int total = 0;
     for (int isw = 0; isw < kResInner && N > 1; ++isw) {
       int swept = 0;
       for (int rnd = 0; rnd < N - 1; ++rnd) {
-        if (lane < npair) {
-          int p, q;
-          if (lane == 0) { p = N - 1; q = rnd; }
-          else { p = (rnd + lane) % (N - 1); q = (rnd - lane + (N - 1)) % (N - 1); }
+        bool act = false;
+        int p = 0, q = 0;
+        double c = 1.0, sr = 0.0, si = 0.0, a_new = 0.0, b_new = 0.0;
+        if (warp < npair) {
+          if (warp == 0) { p = N - 1; q = rnd; }
+          else { p = (rnd + warp) % (N - 1); q = (rnd - warp + (N - 1)) % (N - 1); }
           if (p > q) { const int t = p; p = q; q = t; }
-          ResRot r{p, q, 0, 1.0, 0.0, 0.0, 0.0, 0.0};
           if (q < nc) {
             const double a = cre(G[p * kLd + p]), b = cre(G[q * kLd + q]);
             const T gpq = G[p * kLd + q];
@@ -532,74 +528,71 @@ __device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* w
               const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
                                                   : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
               if (t != 0.0) {
-                const double c = rsqrt(1.0 + t * t), sv = c * t;
+                const double cc = rsqrt(1.0 + t * t), sv = cc * t;
                 const double er = CPLX ? gr * ig : (gr >= 0.0 ? 1.0 : -1.0), ei = CPLX ? gi * ig : 0.0;
-                r.act = 1;
-                r.c = c;
-                r.sr = sv * er;
-                r.si = sv * ei;
-                r.a_new = a - t * gm;
-                r.b_new = b + t * gm;
+                act = true;
+                c = cc;
+                sr = sv * er;
+                si = sv * ei;
+                a_new = a - t * gm;
+                b_new = b + t * gm;
               }
             }
           }
-          rot[lane] = r;
         }
-        __syncwarp();
         // columns p, q of G and Q: [x y] <- [x y] [[c, s e^{i phi}], [-s e^{-i phi}, c]]
-        for (int e = lane; e < 2 * nc * npair; e += 32) {
-          const int k = e % npair, rr = (e / npair) % nc, m = e / (npair * nc);
-          const ResRot& r = rot[k];
-          if (!r.act) continue;
-          T* row = (m == 0 ? G : Q) + rr * kLd;
+        if (act && lane < nc) {
+          T* gr_ = G + lane * kLd;
+          T* qr_ = Q + lane * kLd;
           if constexpr (CPLX) {
-            const double2 ep = make_double2(r.sr, r.si), em = make_double2(-r.sr, r.si);
-            const double2 x = row[r.p], y = row[r.q];
-            row[r.p] = cadd(make_double2(r.c * x.x, r.c * x.y), cmul(y, em));
-            row[r.q] = cadd(cmul(x, ep), make_double2(r.c * y.x, r.c * y.y));
+            const double2 ep = make_double2(sr, si), em = make_double2(-sr, si);
+            double2 x = gr_[p], y = gr_[q];
+            gr_[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
+            gr_[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
+            x = qr_[p]; y = qr_[q];
+            qr_[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
+            qr_[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
           } else {
-            const double x = row[r.p], y = row[r.q];
-            row[r.p] = r.c * x - r.sr * y;
-            row[r.q] = r.sr * x + r.c * y;
+            double x = gr_[p], y = gr_[q];
+            gr_[p] = c * x - sr * y;
+            gr_[q] = sr * x + c * y;
+            x = qr_[p]; y = qr_[q];
+            qr_[p] = c * x - sr * y;
+            qr_[q] = sr * x + c * y;
           }
         }
-        __syncwarp();
-        // rows p, q of G: G <- J^H G
-        for (int e = lane; e < nc * npair; e += 32) {
-          const int k = e % npair, j = e / npair;
-          const ResRot& r = rot[k];
-          if (!r.act) continue;
-          T* rp = G + r.p * kLd;
-          T* rq = G + r.q * kLd;
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
+        // rows p, q of G: G <- J^H G; the rotated 2 x 2 block set to its exact values
+        if (act && lane < nc) {
+          T* rp = G + p * kLd;
+          T* rq = G + q * kLd;
           if constexpr (CPLX) {
-            const double2 mp = make_double2(-r.sr, -r.si), pm = make_double2(r.sr, -r.si);
-            const double2 x = rp[j], y = rq[j];
-            rp[j] = cadd(make_double2(r.c * x.x, r.c * x.y), cmul(mp, y));
-            rq[j] = cadd(cmul(pm, x), make_double2(r.c * y.x, r.c * y.y));
+            const double2 mp = make_double2(-sr, -si), pm = make_double2(sr, -si);
+            const double2 x = rp[lane], y = rq[lane];
+            rp[lane] = cadd(make_double2(c * x.x, c * x.y), cmul(mp, y));
+            rq[lane] = cadd(cmul(pm, x), make_double2(c * y.x, c * y.y));
           } else {
-            const double x = rp[j], y = rq[j];
-            rp[j] = r.c * x - r.sr * y;
-            rq[j] = r.sr * x + r.c * y;
+            const double x = rp[lane], y = rq[lane];
+            rp[lane] = c * x - sr * y;
+            rq[lane] = sr * x + c * y;
           }
+          if (lane == p) { rp[p] = czero<T>(); reinterpret_cast<double*>(rp + p)[0] = a_new; }
+          if (lane == q) { rq[q] = czero<T>(); reinterpret_cast<double*>(rq + q)[0] = b_new; }
+          if (lane == q) rp[q] = czero<T>();
+          if (lane == p) rq[p] = czero<T>();
         }
-        __syncwarp();
-        // the rotated 2 x 2 blocks to their exact values
-        if (lane < npair && rot[lane].act) {
-          const ResRot& r = rot[lane];
-          G[r.p * kLd + r.p] = czero<T>();
-          reinterpret_cast<double*>(G + r.p * kLd + r.p)[0] = r.a_new;
-          G[r.q * kLd + r.q] = czero<T>();
-          reinterpret_cast<double*>(G + r.q * kLd + r.q)[0] = r.b_new;
-          G[r.p * kLd + r.q] = czero<T>();
-          G[r.q * kLd + r.p] = czero<T>();
-        }
-        swept += __popc(__ballot_sync(0xffffffffu, lane < npair && rot[lane].act));
-        __syncwarp();
+        // rotations of this round, counted by lane 0 of every warp
+        if (lane == 0 && act) atomicAdd(&rot_sh, 1);
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
+        swept = rot_sh;
       }
-      total += swept;
-      if (swept == 0) break;
+      asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
+      const int sr_ = rot_sh - total;
+      total = rot_sh;
+      if (sr_ == 0) break;
+      (void)swept;
     }
-    if (lane == 0) nrot_sh = total;
+    if (tid == 0) nrot_sh = total;
   }
   __syncthreads();
   const int nrot = nrot_sh;

@@ -40,6 +40,8 @@ struct Ctx {
   static constexpr double kAutoFuseFlops = 4e9;
   // time tile candidates for every new H_eff plan (1) or use the heuristics (0)
   int autotune = 1;
+  // a tile choice every new H_eff plan takes instead (bn > 0), e.g. to profile one
+  UmmaTune forced_tune;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
   long long gemm_flops = 0;      // running counter of algorithmic GEMM flops issued
   long long launches = 0;        // kernels launched by this context
@@ -125,15 +127,16 @@ struct UmmaSchedule {
 // decide (source 0); the autotuner (dmrg.cpp) times candidate schedules on the
 // plan itself and keeps the fastest per block-size histogram (source 1 when it
 // was timed for this plan, 2 when an earlier plan with the same histogram
-// decided it).
+// decided it, 3 when the caller set it).
 struct UmmaTune {
   int bn = 0;          // output tile width 64 or 128; 0: 128 when the 128-wide tiles fill the GPU twice
-  int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: never split the reduction
+  int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: no split for balance (kc_max still applies)
+  int kc_max = 0;      // most k slabs in one item (longer reductions are split); 0: no cap
   int fused = -1;      // 1: a whole matvec in one cooperative launch, 0: one launch per stage, -1: Ctx's setting
   int source = 0;
   int ncand = 0;       // candidates timed, with their device time (ms) per matvec
   float ms[8] = {};
-  int cand_bn[8] = {}, cand_kc[8] = {}, cand_fused[8] = {};
+  int cand_bn[8] = {}, cand_kc[8] = {}, cand_kmax[8] = {}, cand_fused[8] = {};
 };
 
 // A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.

