@@ -21,6 +21,22 @@
 
 namespace sadmrg {
 
+// Tile choice of a plan's tcgen05 schedule.  Without tuning the heuristics
+// decide (source 0); the autotuner (dmrg.cpp) times candidate schedules on the
+// plan itself and keeps the fastest per block-size histogram (source 1 when it
+// was timed for this plan, 2 when an earlier plan with the same histogram
+// decided it, 3 when the caller set it).
+struct UmmaTune {
+  int bn = 0;          // output tile width 64 or 128; 0: 128 when the 128-wide tiles fill the GPU twice
+  int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: no split for balance (kc_max still applies)
+  int kc_max = 0;      // most k slabs in one item (longer reductions are split); 0: no cap
+  int fused = -1;      // 1: a whole matvec in one cooperative launch, 0: one launch per stage, -1: Ctx's setting
+  int source = 0;
+  int ncand = 0;       // candidates timed, with their device time (ms) per matvec
+  float ms[8] = {};
+  int cand_bn[8] = {}, cand_kc[8] = {}, cand_kmax[8] = {}, cand_fused[8] = {};
+};
+
 struct Ctx {
   cudaStream_t stream = nullptr;
   Sym sym = Sym::U1;
@@ -121,22 +137,6 @@ struct UmmaSchedule {
   URed* d_reds = nullptr;
   int nslot = 0;
   size_t slot_bytes() const { return slots ? slots->bytes() : 0; }
-};
-
-// Tile choice of a plan's tcgen05 schedule.  Without tuning the heuristics
-// decide (source 0); the autotuner (dmrg.cpp) times candidate schedules on the
-// plan itself and keeps the fastest per block-size histogram (source 1 when it
-// was timed for this plan, 2 when an earlier plan with the same histogram
-// decided it, 3 when the caller set it).
-struct UmmaTune {
-  int bn = 0;          // output tile width 64 or 128; 0: 128 when the 128-wide tiles fill the GPU twice
-  int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: no split for balance (kc_max still applies)
-  int kc_max = 0;      // most k slabs in one item (longer reductions are split); 0: no cap
-  int fused = -1;      // 1: a whole matvec in one cooperative launch, 0: one launch per stage, -1: Ctx's setting
-  int source = 0;
-  int ncand = 0;       // candidates timed, with their device time (ms) per matvec
-  float ms[8] = {};
-  int cand_bn[8] = {}, cand_kc[8] = {}, cand_kmax[8] = {}, cand_fused[8] = {};
 };
 
 // A task plan: stage-0 jobs write scratch products, stage-1 jobs the outputs.
