@@ -20,6 +20,7 @@
 // Driver: reads a save_mps2 checkpoint (read_mps + prepare_sweep), sets up open
 // boundaries as the harness does, runs N sweeps and prints
 //   SWEEP s E <energy>     BONDS s site i q:d ...     GPU_LANCZOS_CALLS n
+#include <omp.h>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -214,7 +215,7 @@ static void open_lattice(int** hmap, int** fll, int** frr, double* coup, int ns,
 }
 
 struct Opts {
-  int sym = 1, cplx = 0, lx = 1, ly = 12, D = 16, sweeps = 2;
+  int sym = 1, cplx = 0, lx = 1, ly = 12, D = 16, sweeps = 2, threads = 1;
   double J2 = 0.0;
   std::string read;
 };
@@ -222,6 +223,9 @@ struct Opts {
 template <class S, class Sym>
 static int run(const Opts& o) {
   max_dcut = o.D;
+  // the reference sizes its per-thread buffers by psize: OpenMP must use that many threads
+  psize = o.threads;
+  omp_set_num_threads(o.threads);
   std::streambuf* saved = std::cout.rdbuf();
   std::ostringstream sink;
   std::cout.rdbuf(sink.rdbuf());
@@ -278,6 +282,7 @@ int main(int argc, char** argv) {
     else if (a == "-mlanc") ref_lanczos_mlanc = std::stoi(nxt());
     else if (a == "-lanc_check") ref_lanczos_check = std::stod(nxt());
     else if (a == "-prec") g_gpu_prec = std::stoi(nxt());
+    else if (a == "-threads") o.threads = std::stoi(nxt());
     else { std::cerr << "unknown option " << a << "\n"; return 2; }
   }
   if (o.read.empty()) { std::cerr << "-read <checkpoint dir> is required\n"; return 2; }

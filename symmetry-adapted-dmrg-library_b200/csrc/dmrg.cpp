@@ -143,7 +143,7 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
 // and BlockTensor::hamiltonian_vector_multiplication, src/block_tensor_inst.cpp:2170-2318)
 template <class S>
 HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, const BTensor<S>* hhR,
-                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms) {
+                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms, bool tune) {
   HeffPlan<S> H;
   H.psi_st = psi.st;
   H.psi_off = psi.off;
@@ -269,7 +269,7 @@ HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, con
   H.flops = p.flops;
   H.bytes = (2 * H.n + tot) * (long long)sizeof(S);
   H.ntasks = (int)p.flat_terms.size();
-  autotune_heff(c, H);
+  if (tune || c.forced_tune.bn > 0) autotune_heff(c, H);
   return H;
 }
 
@@ -603,7 +603,7 @@ LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int pr
 // block SVD and truncation (BlockTensor::svd, src/block_tensor_inst.cpp:501-637)
 template <class S>
 SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
-                   int max_dcut, std::vector<double>* wout) {
+                   int max_dcut, std::vector<double>* wout, SvdWarm* warm) {
   SvdStats out;
   const Bond bb20 = tu.st.bonds[0], bb21 = tu.st.bonds[1], bb22 = tv.st.bonds[0], bb23 = tv.st.bonds[1];
   const Bond bb0 = Bond::fuse(c.sym, bb20, bb21), bb1 = Bond::fuse(c.sym, bb22, bb23);
@@ -635,8 +635,56 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
     }
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
   const double tj = now_s();
+  // start from the previous truncation's V at this bond when the sectors match:
+  // W = A V0 (or A^H V0) on the FP64 grouped GEMM, V = V0
+  bool preset = false;
+  if (warm && warm->buf && warm->m.size() == jobs.size() && !jobs.empty()) {
+    preset = true;
+    for (size_t k = 0; k < jobs.size() && preset; ++k)
+      preset = warm->m[k] == jobs[k].m && warm->n[k] == jobs[k].n;
+  }
+  if (warm) (preset ? warm->hits : warm->misses) += 1;
+  if (preset) {
+    GemmPlan g;
+    g.nstage = 1;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+      const SvdJob& J = jobs[k];
+      const int R = std::max(J.m, J.n), C = std::min(J.m, J.n);
+      const int job = g.add_job(0, 1, J.woff, R, C, R, 0);
+      g.add_term(job, 0, J.aoff, J.m, 2, warm->voff[k], C, C, J.trans ? (TF_TA | TF_CA) : 0, 1.0, 0.0);
+      SADMRG_CUDA(cudaMemcpyAsync(wv.template as<S>() + J.voff, warm->buf->template as<S>() + warm->voff[k],
+                                  sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    g.finalize(c, kCx<S>);
+    Bases b{};
+    b.p[0] = const_cast<S*>(psi.data());
+    b.p[1] = wv.get();
+    b.p[2] = warm->buf->get();
+    g.run(c, kCx<S>, PREC_FP64, b);
+    out.warm = true;
+  }
   const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
-                                    &out.jacobi_kernel_ms);
+                                    &out.jacobi_kernel_ms, preset);
+  if (warm && sweeps > 0) {
+    // this truncation's V for the next one at the bond
+    long long vt = 0;
+    warm->m.clear();
+    warm->n.clear();
+    warm->voff.clear();
+    for (auto& J : jobs) {
+      warm->m.push_back(J.m);
+      warm->n.push_back(J.n);
+      warm->voff.push_back(vt);
+      vt += (long long)std::min(J.m, J.n) * std::min(J.m, J.n);
+    }
+    auto nb = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(vt, 1), c.stream);
+    for (size_t k = 0; k < jobs.size(); ++k) {
+      const long long C = std::min(jobs[k].m, jobs[k].n);
+      SADMRG_CUDA(cudaMemcpyAsync(nb->template as<S>() + warm->voff[k], wv.template as<S>() + jobs[k].voff,
+                                  sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    warm->buf = nb;
+  }
   out.jacobi_s = now_s() - tj;
   for (auto& J : jobs) {
     out.max_rows = std::max(out.max_rows, std::max(J.m, J.n));
@@ -1055,7 +1103,7 @@ void Chain<S>::prepare_input_vector_initial(int il, int ir, BTensor<S>& vec) {
 
 // operator set of DMRG::hamiltonian_vector_multiplication_idmrg (src/dmrg_inst.cpp:309-351)
 template <class S>
-HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec) {
+HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec, bool tune) {
   std::vector<const BTensor<S>*> opl;
   std::vector<BTensor<S>> sums;
   sums.reserve(ns);
@@ -1086,7 +1134,8 @@ HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec) {
     else { t.op1 = si; t.op2 = fi; }
     terms.push_back(t);
   }
-  return build_heff<S>(c, vec, hh[il].null() ? nullptr : &hh[il], hh[ir].null() ? nullptr : &hh[ir], opl, terms);
+  return build_heff<S>(c, vec, hh[il].null() ? nullptr : &hh[il], hh[ir].null() ? nullptr : &hh[ir], opl, terms,
+                       tune);
 }
 
 // DMRG::lanczos_solve_eigenvector_idmrg (src/dmrg_inst.cpp:264-279)
@@ -1127,7 +1176,8 @@ template <class S>
 void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   const double t0 = now_s();
   std::vector<double> w;
-  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w);
+  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w, &svd_warm[(long long)il * ns + ir]);
+  if (s.warm) ++timers.svd_warm;
   // BlockTensor::svd overwrites the first n values of the chain's ww array and
   // leaves the rest as it was (src/block_tensor_inst.cpp:576-600)
   if (ww.size() < w.size()) ww.resize(w.size(), 0.0);
@@ -1385,7 +1435,7 @@ HeffPlan<S> Chain<S>::freeze(int il, BTensor<S>& psi) {
   prepare_input_vector(il, ir, psi);
   prepare_site_operator_from_left(il, false);
   prepare_site_operator_from_right(ir, false);
-  return heff_plan(il, ir, psi);
+  return heff_plan(il, ir, psi, /*tune=*/true);
 }
 
 template <class S>
@@ -1446,10 +1496,10 @@ template struct HeffPlan<double>;
 template struct HeffPlan<dcmplex>;
 template HeffPlan<double> build_heff<double>(Ctx&, const BTensor<double>&, const BTensor<double>*,
                                              const BTensor<double>*, const std::vector<const BTensor<double>*>&,
-                                             const std::vector<PairTerm>&);
+                                             const std::vector<PairTerm>&, bool);
 template HeffPlan<dcmplex> build_heff<dcmplex>(Ctx&, const BTensor<dcmplex>&, const BTensor<dcmplex>*,
                                                const BTensor<dcmplex>*, const std::vector<const BTensor<dcmplex>*>&,
-                                               const std::vector<PairTerm>&);
+                                               const std::vector<PairTerm>&, bool);
 template LanczosStats lanczos1<double>(Ctx&, const HeffPlan<double>&, double*, int, int, bool, int, bool);
 template LanczosStats lanczos1<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int, bool, int, bool);
 template LanczosStats lanczos2<double>(Ctx&, const HeffPlan<double>&, double*, int);
@@ -1457,9 +1507,9 @@ template LanczosStats lanczos2<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*
 template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
 template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
 template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,
-                                    int, std::vector<double>*);
+                                    int, std::vector<double>*, SvdWarm*);
 template SvdStats block_svd<dcmplex>(Ctx&, const BTensor<dcmplex>&, BTensor<dcmplex>&, double, BTensor<dcmplex>&,
-                                     double, int, std::vector<double>*);
+                                     double, int, std::vector<double>*, SvdWarm*);
 template class Chain<double>;
 template class Chain<dcmplex>;
 

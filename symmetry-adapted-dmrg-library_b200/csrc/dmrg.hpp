@@ -6,6 +6,7 @@
 // the GPU and only sector bookkeeping on the host.
 #pragma once
 #include <array>
+#include <map>
 #include <chrono>
 #include <random>
 #include <string>
@@ -43,8 +44,12 @@ struct PairTerm {
 };
 
 template <class S>
+// tune: time the tcgen05 schedule candidates for this plan (autotuner, dmrg.cpp) when
+// the context allows it -- worth it for a plan applied many times, not for the
+// ~25 matvecs of one sweep step
 HeffPlan<S> build_heff(Ctx& c, const BTensor<S>& psi, const BTensor<S>* hhL, const BTensor<S>* hhR,
-                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms);
+                       const std::vector<const BTensor<S>*>& opl, const std::vector<PairTerm>& terms,
+                       bool tune = true);
 
 struct LanczosStats {
   int matvecs = 0;
@@ -121,12 +126,24 @@ struct SvdStats {
   bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative), or a
                               // sector's relative 1e-10 cut-off met a value within two decades of it
   double cut_gap = 1.0;       // (D-th - (D+1)-th singular value) / |psi|; 1 when nothing was cut
+  bool warm = false;          // the Jacobi started from the previous truncation's V
 };
 
-// BlockTensor::svd (src/block_tensor_inst.cpp:501-637)
+// Right singular vectors of the last truncation at a bond, kept to start the
+// next one there: one-sided Jacobi converges from any unitary start, and from
+// the previous sweep's V (the state changes little between sweeps) in a few
+// sweeps instead of ~12.  Used only when every sector has the same dimensions.
+struct SvdWarm {
+  std::vector<int> m, n;              // per sector block (the Jacobi jobs, in order)
+  std::vector<long long> voff;        // its V (C x C, C = min(m, n)) in buf
+  std::shared_ptr<DevBuf> buf;
+  int hits = 0, misses = 0;
+};
+
+// BlockTensor::svd (src/block_tensor_inst.cpp:501-637); warm: see SvdWarm (may be null)
 template <class S>
 SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
-                   int max_dcut, std::vector<double>* wout);
+                   int max_dcut, std::vector<double>* wout, SvdWarm* warm = nullptr);
 
 struct Timers {
   double lanczos = 0, env = 0, svd = 0, prep = 0;   // host wall time of each phase
@@ -134,6 +151,7 @@ struct Timers {
   double heff_flops = 0;
   double svd_kernel = 0;        // device time of the Jacobi sweep kernels (s)
   long long svd_sweeps = 0;     // Jacobi sweeps, summed over the truncations
+  long long svd_warm = 0;       // truncations whose Jacobi started from the previous V at the bond
   double plan = 0;              // host wall time of building H_eff plans (part of lanczos)
 };
 
@@ -153,7 +171,7 @@ class Chain {
   void prepare_site_operator_from_right(int i, bool real_env);
   void prepare_input_vector(int il, int ir, BTensor<S>& vec);
   void prepare_input_vector_initial(int il, int ir, BTensor<S>& vec);
-  HeffPlan<S> heff_plan(int il, int ir, const BTensor<S>& vec);
+  HeffPlan<S> heff_plan(int il, int ir, const BTensor<S>& vec, bool tune = false);
   void lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec);
   void wavefunc_transformation(int i, int dir);
   // DMRG::read_mps / save_mps2 checkpoint format (src/dmrg_inst.cpp:947-1079)
@@ -190,6 +208,7 @@ class Chain {
   int mlanc_max = 40;
   int prec = PREC_FP64;
   Timers timers;
+  std::map<long long, SvdWarm> svd_warm;   // per two-site bond (il * ns + ir)
   std::mt19937_64 rng{42};  // the reference's generator (src/dense_inst.cpp:23-24)
   std::uniform_real_distribution<double> dist{-1.0, 1.0};
   std::vector<std::string> log;

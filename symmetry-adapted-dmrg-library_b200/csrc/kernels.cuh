@@ -229,7 +229,9 @@ struct SvdJob {
 // Host driver: one launch per round of block pairs, one sync per sweep to test
 // convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
 // kernel_ms (optional): device time of the sweep kernel when it ran as one launch.
+// preset: W and V already hold a starting point (W = A V0, V = V0, V0 unitary)
+// instead of W = A, V = I.
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr);
+                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, bool preset = false);
 
 }  // namespace sadmrg

@@ -16,7 +16,6 @@
 // one-sided Jacobi on small singular values, which the reference's 1e-10
 // relative cut-off depends on.
 #include <cuda_runtime.h>
-#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -370,308 +369,15 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   if (tid == 0) atomicAdd(rotations, nrot);
 }
 
-// ---------------------------------------------------------------------------
-// Resident visit (b = 8, pairs of 16 columns): the pair's columns of W and V are
-// read into shared memory once, so the visit takes a handful of block barriers
-// instead of several per 128-row chunk.  Same arithmetic as jacobi_pair_visit
-// (Gram matrix on DMMA, one-sided rotations on G with the exact 2 x 2 values,
-// Wp <- Wp Q, Vp <- Vp Q), except that
-//   * the Gram matrix is summed over the rows in a fixed order: every warp a
-//     contiguous slice of rows, then the 16 partial matrices in warp order;
-//   * the rotation rounds of G synchronise the 8 rotating warps only (a named
-//     barrier), not the whole block.
-constexpr int kResB = 8;
-constexpr int kResNc = 2 * kResB;
-constexpr int kResLd = kResNc + 1;
-constexpr int kResInner = 1;   // inner sweeps of G per visit (more did not cut the outer sweeps)
-
-template <bool CPLX>
-__host__ __device__ constexpr size_t res_fixed_bytes() {
-  // G, Q and the per-warp partial Gram matrices
-  return (size_t)(2 * kResNc * kResLd + kSvdWarps * kResNc * kResNc) * (CPLX ? 16 : 8);
-}
-template <bool CPLX>
-__host__ __device__ constexpr size_t res_bytes(int R, int C) {
-  return res_fixed_bytes<CPLX>() + (size_t)(((R + 7) / 8) * 8 + ((C + 7) / 8) * 8) * kResLd * (CPLX ? 16 : 8);
-}
-
-template <bool CPLX>
-__device__ void jacobi_pair_visit_res(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
-                                      double tol, unsigned char* smem_raw, int* rotations) {
-  using T = typename SvdT<CPLX>::T;
-  constexpr int kNc = kResNc, kLd = kResLd;
-  const int R = J.trans ? J.n : J.m;
-  const int C = J.trans ? J.m : J.n;
-  const int Rp = ((R + 7) / 8) * 8, Cp = ((C + 7) / 8) * 8;
-  __shared__ int cols[kNc];
-  __shared__ int nrot_sh, rot_sh;
-  T* G = reinterpret_cast<T*>(smem_raw);           // kNc x kLd
-  T* Q = G + kNc * kLd;                            // kNc x kLd
-  T* Gp = Q + kNc * kLd;                           // kSvdWarps x kNc x kNc partial Gram matrices
-  T* Wp = reinterpret_cast<T*>(smem_raw + res_fixed_bytes<CPLX>());       // Rp x kLd
-  T* Vp = Wp + (size_t)Rp * kLd;                   // Cp x kLd
-  T* W = static_cast<T*>(work) + J.woff;
-  T* V = static_cast<T*>(vmat) + J.voff;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int n0 = min(kResB, C - P.bi * kResB);
-  const int n1 = P.bj >= 0 ? min(kResB, C - P.bj * kResB) : 0;
-  const int nc = n0 + n1;
-  {
-    const int* pj = perm + J.soff;
-    if (tid < n0) cols[tid] = pj[P.bi * kResB + tid];
-    else if (tid < nc) cols[tid] = pj[P.bj * kResB + (tid - n0)];
-    if (tid == 0) { nrot_sh = 0; rot_sh = 0; }
-  }
-  __syncthreads();
-  // 1. the pair's columns of W and V -> shared memory (rows past the end and
-  //    columns past nc zero), consecutive threads on consecutive rows of a column
-  for (int e = tid; e < Rp * kNc; e += kSvdThreads) {
-    const int r = e % Rp, c = e / Rp;
-    Wp[r * kLd + c] = (r < R && c < nc) ? W[r + (long long)cols[c] * R] : czero<T>();
-  }
-  for (int e = tid; e < Cp * kNc; e += kSvdThreads) {
-    const int r = e % Cp, c = e / Cp;
-    Vp[r * kLd + c] = (r < C && c < nc) ? V[r + (long long)cols[c] * C] : czero<T>();
-  }
-  __syncthreads();
-  // 2. Gram matrix: warp w sums rows [w rs, (w + 1) rs) into its partial (all
-  //    four 8 x 8 tiles), then the partials are added in warp order
-  {
-    const int fr = lane >> 2, fk = lane & 3;
-    const int rs = ((Rp / 4 + kSvdWarps - 1) / kSvdWarps) * 4;
-    const int r0 = warp * rs, r1 = min(Rp, r0 + rs);
-    double g[4][4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) g[t][0] = g[t][1] = g[t][2] = g[t][3] = 0.0;
-    for (int k0 = r0; k0 < r1; k0 += 4) {
-      const T* row = Wp + (k0 + fk) * kLd;
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int pt = t >> 1, qt = t & 1;
-        const T x = row[pt * 8 + fr];   // A(p, r) = conj(W(r, p))
-        const T y = row[qt * 8 + fr];   // B(r, q) = W(r, q)
-        if constexpr (CPLX) {
-          dmma(g[t][0], g[t][1], x.x, y.x);
-          dmma(g[t][0], g[t][1], x.y, y.y);
-          dmma(g[t][2], g[t][3], x.x, y.y);
-          dmma(g[t][2], g[t][3], -x.y, y.x);
-        } else {
-          dmma(g[t][0], g[t][1], x, y);
-        }
-      }
-    }
-    T* mine = Gp + warp * kNc * kNc;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int pt = t >> 1, qt = t & 1;
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        T v;
-        if constexpr (CPLX) v = make_double2(g[t][i], g[t][2 + i]);
-        else v = g[t][i];
-        mine[(pt * 8 + fr) * kNc + qt * 8 + 2 * fk + i] = v;
-      }
-    }
-  }
-  __syncthreads();
-  for (int e = tid; e < kNc * kNc; e += kSvdThreads) {
-    const int p = e / kNc, q = e % kNc;
-    // entries on and above the diagonal, mirrored, so that G is exactly Hermitian
-    const int pp = min(p, q), qq = max(p, q);
-    T v = czero<T>();
-    for (int w = 0; w < kSvdWarps; ++w) v = cadd(v, Gp[w * kNc * kNc + pp * kNc + qq]);
-    G[p * kLd + q] = p <= q ? v : cconj(v);
-    Q[p * kLd + q] = czero<T>();
-    if (p == q) reinterpret_cast<double*>(Q + p * kLd + q)[0] = 1.0;
-  }
-  __syncthreads();
-  {
-    int need = 0;
-    for (int e = tid; e < nc * nc; e += kSvdThreads) {
-      const int p = e / nc, q = e % nc;
-      if (p >= q) continue;
-      const double ab = cre(G[p * kLd + p]) * cre(G[q * kLd + q]);
-      const T gpq = G[p * kLd + q];
-      double g2;
-      if constexpr (CPLX) g2 = gpq.x * gpq.x + gpq.y * gpq.y; else g2 = gpq * gpq;
-      if (ab > 0.0 && g2 > tol * tol * ab) need = 1;
-    }
-    if (!__syncthreads_or(need)) return;
-  }
-  // 3. rotations of G: warp k < 8 owns pair k of each round (lane = row of G
-  //    and Q); the 256 threads of warps 0-7 meet at a named barrier between the
-  //    column and the row half of a round, the other warps wait below
-  if (warp < kResNc / 2) {
-    const int N = nc + (nc & 1), npair = N / 2;
-    int total = 0;
-    for (int isw = 0; isw < kResInner && N > 1; ++isw) {
-      int swept = 0;
-      for (int rnd = 0; rnd < N - 1; ++rnd) {
-        bool act = false;
-        int p = 0, q = 0;
-        double c = 1.0, sr = 0.0, si = 0.0, a_new = 0.0, b_new = 0.0;
-        if (warp < npair) {
-          if (warp == 0) { p = N - 1; q = rnd; }
-          else { p = (rnd + warp) % (N - 1); q = (rnd - warp + (N - 1)) % (N - 1); }
-          if (p > q) { const int t = p; p = q; q = t; }
-          if (q < nc) {
-            const double a = cre(G[p * kLd + p]), b = cre(G[q * kLd + q]);
-            const T gpq = G[p * kLd + q];
-            double gr, gi = 0.0;
-            if constexpr (CPLX) { gr = gpq.x; gi = gpq.y; } else { gr = gpq; }
-            const double g2 = gr * gr + gi * gi;
-            // rotate when |g| > tol sqrt(ab), compared squared (as jacobi_pair_visit)
-            if (a * b > 0.0 && g2 > tol * tol * (a * b)) {
-              const double gm = CPLX ? sqrt(g2) : fabs(gr);
-              const double ig = 1.0 / gm;
-              const double zeta = 0.5 * (b - a) * ig;
-              const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
-                                                  : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-              if (t != 0.0) {
-                const double cc = rsqrt(1.0 + t * t), sv = cc * t;
-                const double er = CPLX ? gr * ig : (gr >= 0.0 ? 1.0 : -1.0), ei = CPLX ? gi * ig : 0.0;
-                act = true;
-                c = cc;
-                sr = sv * er;
-                si = sv * ei;
-                a_new = a - t * gm;
-                b_new = b + t * gm;
-              }
-            }
-          }
-        }
-        // columns p, q of G and Q: [x y] <- [x y] [[c, s e^{i phi}], [-s e^{-i phi}, c]]
-        if (act && lane < nc) {
-          T* gr_ = G + lane * kLd;
-          T* qr_ = Q + lane * kLd;
-          if constexpr (CPLX) {
-            const double2 ep = make_double2(sr, si), em = make_double2(-sr, si);
-            double2 x = gr_[p], y = gr_[q];
-            gr_[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
-            gr_[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
-            x = qr_[p]; y = qr_[q];
-            qr_[p] = cadd(make_double2(c * x.x, c * x.y), cmul(y, em));
-            qr_[q] = cadd(cmul(x, ep), make_double2(c * y.x, c * y.y));
-          } else {
-            double x = gr_[p], y = gr_[q];
-            gr_[p] = c * x - sr * y;
-            gr_[q] = sr * x + c * y;
-            x = qr_[p]; y = qr_[q];
-            qr_[p] = c * x - sr * y;
-            qr_[q] = sr * x + c * y;
-          }
-        }
-        asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
-        // rows p, q of G: G <- J^H G; the rotated 2 x 2 block set to its exact values
-        if (act && lane < nc) {
-          T* rp = G + p * kLd;
-          T* rq = G + q * kLd;
-          if constexpr (CPLX) {
-            const double2 mp = make_double2(-sr, -si), pm = make_double2(sr, -si);
-            const double2 x = rp[lane], y = rq[lane];
-            rp[lane] = cadd(make_double2(c * x.x, c * x.y), cmul(mp, y));
-            rq[lane] = cadd(cmul(pm, x), make_double2(c * y.x, c * y.y));
-          } else {
-            const double x = rp[lane], y = rq[lane];
-            rp[lane] = c * x - sr * y;
-            rq[lane] = sr * x + c * y;
-          }
-          if (lane == p) { rp[p] = czero<T>(); reinterpret_cast<double*>(rp + p)[0] = a_new; }
-          if (lane == q) { rq[q] = czero<T>(); reinterpret_cast<double*>(rq + q)[0] = b_new; }
-          if (lane == q) rp[q] = czero<T>();
-          if (lane == p) rq[p] = czero<T>();
-        }
-        // rotations of this round, counted by lane 0 of every warp
-        if (lane == 0 && act) atomicAdd(&rot_sh, 1);
-        asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
-        swept = rot_sh;
-      }
-      asm volatile("bar.sync 1, %0;" ::"n"(32 * kResNc / 2) : "memory");
-      const int sr_ = rot_sh - total;
-      total = rot_sh;
-      if (sr_ == 0) break;
-      (void)swept;
-    }
-    if (tid == 0) nrot_sh = total;
-  }
-  __syncthreads();
-  const int nrot = nrot_sh;
-  if (nrot == 0) return;
-  // 4. Wp <- Wp Q, Vp <- Vp Q: 8-row tiles round-robin over the warps, each
-  //    warp overwriting only its own rows
-  {
-    const int fr = lane >> 2, fk = lane & 3;
-    const int tw = Rp / 8, tv = Cp / 8;
-    for (int t = warp; t < tw + tv; t += kSvdWarps) {
-      T* M = t < tw ? Wp + (size_t)(t * 8) * kLd : Vp + (size_t)((t - tw) * 8) * kLd;
-      double d[2][4];
-#pragma unroll
-      for (int jt = 0; jt < 2; ++jt) {
-        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-#pragma unroll
-        for (int k0 = 0; k0 < kNc; k0 += 4) {
-          const T x = M[fr * kLd + k0 + fk];
-          const T y = Q[(k0 + fk) * kLd + jt * 8 + fr];
-          if constexpr (CPLX) {
-            dmma(a0, a1, x.x, y.x);
-            dmma(a0, a1, -x.y, y.y);
-            dmma(b0, b1, x.x, y.y);
-            dmma(b0, b1, x.y, y.x);
-          } else {
-            dmma(a0, a1, x, y);
-          }
-        }
-        d[jt][0] = a0; d[jt][1] = a1; d[jt][2] = b0; d[jt][3] = b1;
-      }
-      __syncwarp();
-#pragma unroll
-      for (int jt = 0; jt < 2; ++jt)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          T v;
-          if constexpr (CPLX) v = make_double2(d[jt][i], d[jt][2 + i]);
-          else v = d[jt][i];
-          M[fr * kLd + jt * 8 + 2 * fk + i] = v;
-        }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  // 5. back to global memory
-  for (int e = tid; e < R * nc; e += kSvdThreads) {
-    const int r = e % R, c = e / R;
-    W[r + (long long)cols[c] * R] = Wp[r * kLd + c];
-  }
-  for (int e = tid; e < C * nc; e += kSvdThreads) {
-    const int r = e % C, c = e / C;
-    V[r + (long long)cols[c] * C] = Vp[r * kLd + c];
-  }
-  if (tid == 0) atomicAdd(rotations, nrot);
-}
-
-// one visit: the resident form when the pair's columns fit the launch's shared memory
-template <bool CPLX, int B>
-__device__ __forceinline__ void visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
-                                      double tol, unsigned char* smem_raw, int* rotations, size_t smem_avail) {
-  if constexpr (B == kResB) {
-    const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
-    if (res_bytes<CPLX>(R, C) <= smem_avail) {
-      jacobi_pair_visit_res<CPLX>(J, P, work, vmat, perm, tol, smem_raw, rotations);
-      return;
-    }
-  }
-  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
-}
-
 template <bool CPLX, int B>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
                                                                   const SvdPair* __restrict__ pairs, void* work,
                                                                   void* vmat, const int* perm, double tol,
-                                                                  int* rotations, size_t smem_avail) {
+                                                                  int* rotations) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SvdPair P = pairs[blockIdx.x];
   const SvdJob J = jobs[P.job];
-  visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations, smem_avail);
+  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
 }
 
 // ---------------------------------------------------------------------------
@@ -731,8 +437,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
                                                                   const SvdPair* __restrict__ pairs,
                                                                   const int* __restrict__ roff, int max_rounds,
                                                                   void* work, void* vmat, double* nrm, int* perm,
-                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps,
-                                                                  size_t smem_avail) {
+                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned char done[kSvdMaxJobsCoop];
   __shared__ int all_done;
@@ -790,7 +495,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
         const SvdPair P = pairs[p];
         if (done[P.job]) continue;
         const SvdJob J = jobs[P.job];
-        visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job, smem_avail);
+        jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
       }
       if (!svd_grid_sync(ctl)) return;
     }
@@ -809,9 +514,10 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
   }
 }
 
-// W = A (m >= n) or A^H (m < n); V = I
+// W = A (m >= n) or A^H (m < n); V = I.  preset: W and V hold the start already
+// (W = A V0, V = V0 for a starting rotation V0); only the column order is set.
 template <bool CPLX>
-__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm) {
+__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm, int preset) {
   using T = typename SvdT<CPLX>::T;
   const SvdJob J = jobs[blockIdx.x];
   const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
@@ -820,6 +526,7 @@ __global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work
   T* V = static_cast<T*>(vmat) + J.voff;
   if (blockIdx.y == 0)
     for (int c = threadIdx.x; c < C; c += blockDim.x) perm[J.soff + c] = c;
+  if (preset) return;
   for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)R * C;
        e += (long long)blockDim.x * gridDim.y) {
     const int r = (int)(e % R), c = (int)(e / R);
@@ -862,7 +569,7 @@ __global__ void jacobi_norms_kernel(const SvdJob* jobs, const void* work, double
 // was reached).
 template <bool CPLX, int B>
 static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                      int max_sweeps, cudaStream_t s, double* kernel_ms) {
+                      int max_sweeps, cudaStream_t s, double* kernel_ms, bool preset) {
   const int nj = (int)hjobs.size();
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
@@ -878,14 +585,6 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     max_rounds = std::max(max_rounds, nrounds[j]);
     smem = svd_smem_bytes<CPLX, B>();
   }
-  // resident visits (b = 8) for the sectors whose pair columns fit in shared memory
-  constexpr size_t kSmemCap = 220 * 1024;
-  if (B == kResB)
-    for (int j = 0; j < nj; ++j) {
-      const int R = hjobs[j].trans ? hjobs[j].n : hjobs[j].m, C = hjobs[j].trans ? hjobs[j].m : hjobs[j].n;
-      const size_t need = res_bytes<CPLX>(R, C);
-      if (need <= kSmemCap) smem = std::max(smem, need);
-    }
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
   for (int j = 0; j < nj; ++j) {
@@ -915,7 +614,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
   SADMRG_CUDA(cudaMemcpyAsync(djobs.get(), hjobs.data(), sizeof(SvdJob) * nj, cudaMemcpyHostToDevice, s));
   SADMRG_CUDA(cudaMemcpyAsync(dpairs.get(), flat.data(), sizeof(SvdPair) * flat.size(), cudaMemcpyHostToDevice, s));
   dim3 ig(nj, 16);
-  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
+  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>(), preset ? 1 : 0);
   SADMRG_CUDA(cudaGetLastError());
   SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<CPLX, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const double tol = std::sqrt((double)std::max(maxR, 1)) * 2.220446049250313e-16;
@@ -942,7 +641,6 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     int* pc = dcnt3.as<int>();
     SvdCtl* pctl = dctl.as<SvdCtl>();
     int njv = nj, mr = max_rounds, ms = max_sweeps;
-    size_t avail = smem;
     double tolv = tol;
     void* a_work = work;
     void* a_vmat = vmat;
@@ -950,7 +648,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     int* a_perm = dperm.as<int>();
     void* args[] = {(void*)&pj,     (void*)&njv,    (void*)&pp,   (void*)&pr, (void*)&mr,   (void*)&a_work,
                     (void*)&a_vmat, (void*)&a_nrm, (void*)&a_perm, (void*)&tolv, (void*)&pc, (void*)&pctl,
-                    (void*)&ms,     (void*)&avail};
+                    (void*)&ms};
     SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<CPLX, B>, dim3(grid), dim3(kSvdThreads),
                                             args, smem, s));
     SvdCtl hctl{};
@@ -969,8 +667,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
       const int np = roff[r + 1] - roff[r];
       if (np == 0) continue;
       jacobi_pair_kernel<CPLX, B><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>(),
-                                                                smem);
+                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
     }
     SADMRG_CUDA(cudaGetLastError());
     SADMRG_CUDA(cudaMemcpyAsync(&h_rot, dcnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -983,7 +680,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
 }
 
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
+                   int max_sweeps, cudaStream_t s, double* kernel_ms, bool preset) {
   if (kernel_ms) *kernel_ms = -1.0;
   if (hjobs.empty()) return 0;
   // column blocks of 16, or of 8 when the widest round of 16-column pairs would
@@ -1002,10 +699,10 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   }
   const bool narrow = 2 * pairs16 < nsm;
   if (cplx)
-    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
-                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
-  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
-                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
+    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset)
+                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset);
+  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset)
+                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset);
 }
 
 }  // namespace sadmrg

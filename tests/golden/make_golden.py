@@ -56,6 +56,12 @@ SWEEP_CASES = {
 # configuration 1 of the benchmark: U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps,
 # with the benchmark's Lanczos settings (<= 100 steps, stop at 1e-10) and with a stop test no
 # run can pass (1e-14: every solve takes all 100 steps, so both sides follow the same path)
+# configuration 2 of the benchmark: SU(2) real Heisenberg chain, open, L = 100, D = 512
+# multiplets, 8 sweeps from the reference's own iDMRG state, Lanczos <= 100 steps with the
+# stop test at 1e-12; energies and bonds only (the checkpoint is ~400 MB: a test rebuilds it
+# with the same reference build)
+CONFIG2 = ("su2_L100_D512", ["-sym", "su2", "-L", "100", "-d", "512", "-sweeps", "8", "-maxangm", "40"],
+           ["-mlanc", "100", "-lanc_check", "1e-12"])
 BASELINE_CASES = {
     "u1_L32_D64": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"], ["-mlanc", "100", "-lanc_check", "1e-10"]),
     "u1_L32_D64_converged": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"],
@@ -91,8 +97,9 @@ def read_tensor(dirpath: str, name: str, cplx: bool) -> dict:
     }
 
 
-def run(args, workdir):
-    out = subprocess.run([HARNESS] + args, cwd=workdir, capture_output=True, text=True, check=True)
+def run(args, workdir, env=None):
+    out = subprocess.run([HARNESS] + args, cwd=workdir, capture_output=True, text=True, check=True,
+                         env=None if env is None else dict(os.environ, **env))
     return out.stdout
 
 
@@ -116,6 +123,21 @@ def parse_sweeps(stdout: str):
 def main():
     if not os.path.exists(HARNESS):
         sys.exit("build the reference harness first: make -C oracle")
+    if "--config2" in sys.argv:
+        name, args, lanczos = CONFIG2
+        with tempfile.TemporaryDirectory() as wd:
+            stdout = run(args + lanczos + ["-threads", str(os.cpu_count() or 1), "-sweepdir", os.path.join(wd, "sw")],
+                         wd, env={"OPENBLAS_NUM_THREADS": "1"})
+        e_idmrg, energies, bonds = parse_sweeps(stdout)
+        per_sweep = [[f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])]
+                     for s_ in sorted(k for k in bonds if k >= 0)]
+        idmrg_bonds = [f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[-1][s]) for s in sorted(bonds[-1])]
+        np.savez_compressed(os.path.join(HERE, f"baseline_{name}.npz"), args=np.array(" ".join(args)),
+                            lanczos=np.array(" ".join(lanczos)), e_idmrg=np.float64(e_idmrg),
+                            energies=np.array(energies), bonds_per_sweep=np.array(per_sweep),
+                            bonds_idmrg=np.array(idmrg_bonds))
+        print("wrote baseline", name, e_idmrg, energies)
+        return
     only_baseline = "--baseline-only" in sys.argv
     for name, args in ({} if only_baseline else CENTRE_CASES).items():
         cplx = args[args.index("-cplx") + 1] == "1"
