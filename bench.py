@@ -29,8 +29,9 @@ Arms
                       (oracle/_ref, built from the reference sources) on the same
                       problem, all host threads; nothing of this library is loaded.
 
-Timing: CUDA events on the library's stream, a 256 MiB write between timed
-steps (the operands are ~100 MB, under the 126 MB L2).  Multi-GPU runs are
+Timing: CUDA events on the library's stream; before every timed step 256 MiB
+are written and another 256 MiB read (the operands are ~100 MB, under the
+126 MB L2; the read puts the written lines back in memory before the step).  Multi-GPU runs are
 independent replicas (the path has no exchange step); time is the max over ranks.
 """
 from __future__ import annotations
@@ -53,7 +54,7 @@ PKG = os.path.join(ROOT, "symmetry-adapted-dmrg-library_b200")
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 sys.path.insert(0, PKG)
 
-FLUSH_BYTES = 256 << 20
+FLUSH_BYTES = 512 << 20   # 256 MiB written, then another 256 MiB read, before every timed step
 # Lanczos settings of the chain workloads: at most 100 steps (BASELINE), stop once
 # |<v|Hv>|/|Hv| is within lanczos_tol of 1
 LANCZOS_MLANC = 100
@@ -376,7 +377,7 @@ def make_ladder_centre(wl: dict, directory: str) -> dict:
             "leg_multiplets": [int(sum(dl)), int(sum(dr))],
             "block_dims": f"log-uniform in [{sp['dmin']}, {sp['dmax']}], seed {sp['seed']}",
             "pair_terms": nterms, "psi_elems": int(psi.size), "flops_per_step": float(flops), "tasks": tasks,
-            "l2": "flushed before every GPU step (256 MiB write); the host runs are untouched"}
+            "l2": "flushed before every GPU step (256 MiB written, then 256 MiB read); the host runs are untouched"}
 
 
 def run_reference_harness(directory: str, sym: int, cplx: bool, calls: int, threads: int) -> float:
@@ -401,7 +402,7 @@ def chain_config(name: str, wl: dict, sweeps: int) -> dict:
             "J2": wl["J2"], "dz": wl.get("dz", 0.0), "symmetry": "SU2" if wl["sym"] else "U1",
             "scalar": "complex" if wl["cplx"] else "real", "sweeps": sweeps, "lanczos_mlanc": LANCZOS_MLANC,
             "lanczos_ov_tol": wl["lanczos_tol"], "frozen_bond": "centre",
-            "l2": "flushed before every GPU step (256 MiB write); the host runs are untouched"}
+            "l2": "flushed before every GPU step (256 MiB written, then 256 MiB read); the host runs are untouched"}
 
 
 # ---------------------------------------------------------------------------
@@ -520,7 +521,8 @@ def run_ours(a, wl: dict, ws: int, rank: int, local: int, cores: int):
     def launch_profile(prec, reps):
         acc, kinds = None, None
         for _ in range(reps):
-            flush.zero_()
+            flush[:FLUSH_BYTES // 2].zero_()        # the same flush as the timed steps: write, then read
+            flush[FLUSH_BYTES // 2:].max()
             torch.cuda.synchronize()
             lp = h.heff_launch_profile(prec, 1, x.data_ptr(), y.data_ptr())
             if acc is None:

@@ -125,7 +125,8 @@ int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, c
  * With it on (the default) every new H_eff plan times candidate tcgen05
  * schedules on itself -- output tile width 64 or 128, split-K chunks of at
  * least 16 k slabs or none, one cooperative launch or one per stage -- with
- * CUDA events on the handle's stream (and items capped at 32 k slabs), and keeps the fastest; the choice is
+ * items capped at 32 k slabs, two CTAs per SM -- with CUDA events on the
+ * handle's stream, and keeps the fastest; the choice is
  * cached per block-size histogram of the plan (jobs by log2 of m, n and k) for
  * the life of the process.  Off: fixed heuristics.  The FP64 path is never
  * tuned (its rounding does not depend on a timing). */
@@ -133,16 +134,16 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on);
 /* A fixed tile choice for the H_eff plans made after this call, instead of the
  * autotuner or the heuristics: width 64 or 128 (0 returns to them), fewest slabs
  * per split-K chunk when the tiles cannot fill the GPU (0: no such split), most
- * slabs per item (0: no cap), one cooperative launch per matvec (1), one per
- * stage (0) or the default rule (-1).  For profiling one schedule. */
-int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int one_launch);
+ * slabs per item (0: no cap), CTAs per SM (1, or 2 at width 64), one cooperative
+ * launch per matvec (1), one per stage (0) or the default rule (-1).  For
+ * profiling one schedule. */
+int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int ctas_per_sm, int one_launch);
 /* The current plan's tile choice: out[0] tile width, out[1] fewest slabs per
  * split-K chunk when the tiles cannot fill the GPU (0: no such split), out[2]
- * most slabs per item (0: no cap), out[3] 1 when a matvec is one cooperative
- * launch, out[4] 0 heuristic / 1 timed for this plan / 2 from the cache / 3 set by
- * sadmrg_set_tiles, out[5]
- * the number of candidates timed, then per candidate (width, chunk, cap, one
- * launch, ms per matvec).  *n is the number of values; the first min(cap, *n)
+ * most slabs per item (0: no cap), out[3] CTAs per SM, out[4] 1 when a matvec is
+ * one cooperative launch, out[5] 0 heuristic / 1 timed for this plan / 2 from the
+ * cache / 3 set by sadmrg_set_tiles, out[6] the number of candidates timed, then
+ * per candidate (width, chunk, cap, CTAs per SM, one launch, ms per matvec).  *n is the number of values; the first min(cap, *n)
  * are written. */
 int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n);
 /* psi elements, algorithmic flops and bytes of one matvec, number of sector products */
@@ -184,9 +185,11 @@ int sadmrg_heff_graph_bench(sadmrg_handle* h, int precision, int reps, const voi
                             double* ms);
 /* Timed steps of the same captured matvec (no counterpart in the reference):
  * the graph of one H_eff*psi on (psi_dev, out_dev) is captured once; then per
- * step, on the handle's stream, flush_bytes of flush_dev are overwritten (to
- * evict the operands from L2; 0 for none) and the graph is launched between two
- * CUDA events.  ms[i] is the device time of step i (steps values). */
+ * step, on the handle's stream, the first half of the flush_bytes at flush_dev
+ * is overwritten and the second half read (each half larger than the L2, so
+ * the operands are evicted and the written lines are back in memory before the
+ * step; 0 for none), and the graph is launched between two CUDA events.  ms[i]
+ * is the device time of step i (steps values). */
 int sadmrg_heff_graph_steps(sadmrg_handle* h, int precision, int steps, const void* psi_dev, void* out_dev,
                             void* flush_dev, long long flush_bytes, double* ms);
 /* kernels one H_eff*psi launches at this precision (the penalty's included) */

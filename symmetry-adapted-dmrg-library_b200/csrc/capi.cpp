@@ -287,15 +287,17 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
 }
 
-int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int one_launch) {
+int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int ctas_per_sm, int one_launch) {
   return guard(h, [&]() {
     SADMRG_REQUIRE(bn == 0 || bn == 64 || bn == 128, SADMRG_ERR_ARG, "set_tiles: width must be 0, 64 or 128");
-    SADMRG_REQUIRE(kc_min >= 0 && kc_max >= 0 && one_launch >= -1 && one_launch <= 1, SADMRG_ERR_ARG,
-                   "set_tiles: arguments");
+    SADMRG_REQUIRE(kc_min >= 0 && kc_max >= 0 && one_launch >= -1 && one_launch <= 1 &&
+                       (ctas_per_sm == 1 || (ctas_per_sm == 2 && bn == 64)),
+                   SADMRG_ERR_ARG, "set_tiles: arguments");
     UmmaTune t;
     t.bn = bn;
     t.kc_min = kc_min;
     t.kc_max = kc_max;
+    t.ctas = ctas_per_sm;
     t.fused = one_launch;
     h->ctx.forced_tune = t;
   });
@@ -313,6 +315,7 @@ int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
     v.push_back(P.umma ? P.umma->bn : 0);
     v.push_back(t.kc_min);
     v.push_back(t.kc_max);
+    v.push_back(P.umma ? P.umma->ctas : 1);
     v.push_back(fused ? 1 : 0);
     v.push_back(t.source);
     v.push_back(t.ncand);
@@ -320,6 +323,7 @@ int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
       v.push_back(t.cand_bn[i]);
       v.push_back(t.cand_kc[i]);
       v.push_back(t.cand_kmax[i]);
+      v.push_back(t.cand_ctas[i]);
       v.push_back(t.cand_fused[i]);
       v.push_back(t.ms[i]);
     }
@@ -549,9 +553,15 @@ int sadmrg_heff_graph_steps(sadmrg_handle* h, int precision, int steps, const vo
     };
     try {
       for (auto& e : ev) SADMRG_CUDA(cudaEventCreate(&e));
+      const long long half = (flush_bytes / 2) & ~15LL;
       for (int r = 0; r < steps; ++r) {
-        // evict the operands from L2 before the step (a write larger than L2), outside the events
-        if (flush_bytes > 0) SADMRG_CUDA(cudaMemsetAsync(flush_dev, r & 0xff, (size_t)flush_bytes, c.stream));
+        // evict the operands from L2 before the step, outside the events: write the
+        // first half of the flush buffer, then read the second half, so that the
+        // written lines are back in memory before the step starts
+        if (half > 0) {
+          SADMRG_CUDA(cudaMemsetAsync(flush_dev, r & 0xff, (size_t)half, c.stream));
+          launch_read(static_cast<unsigned char*>(flush_dev) + half, half, h->ctx.d_counter, c.stream);
+        }
         SADMRG_CUDA(cudaEventRecord(ev[2 * r], c.stream));
         SADMRG_CUDA(cudaGraphLaunch(ge, c.stream));
         SADMRG_CUDA(cudaEventRecord(ev[2 * r + 1], c.stream));

@@ -24,9 +24,9 @@ static double now_s() {
 // 128, times three ways to cut the reductions -- split-K chunks of at least 16 k
 // slabs when the output tiles cannot fill the GPU, no split, or no item longer
 // than 32 (or, at width 64, 16) slabs: the longest items set the time of a
-// launch -- and, for the
-// fastest of those, one cooperative launch for the whole matvec against one
-// launch per stage.  Each candidate schedule is built on the plan itself and timed with
+// launch -- two CTAs per SM at width 64 (a 2-stage ring each, so one CTA's
+// epilogue overlaps the other's MMAs), and, for the fastest of those, one
+// cooperative launch for the whole matvec against one launch per stage.  Each candidate schedule is built on the plan itself and timed with
 // CUDA events on the context's stream (one warm run, then the mean of three);
 // the winner is cached per block-size histogram (GemmPlan::tune_key) for the
 // life of the process, so later plans with the same histogram reuse it untimed.
@@ -56,7 +56,8 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
       const int built_bn = p.umma->bn;
       p.tune = it->second;
       p.tune.source = 2;
-      if (p.tune.bn != built_bn || p.tune.kc_min != built.kc_min || p.tune.kc_max != built.kc_max)
+      if (p.tune.bn != built_bn || p.tune.kc_min != built.kc_min || p.tune.kc_max != built.kc_max ||
+          p.tune.ctas != built.ctas)
         p.rebuild_umma(c, kCx<S>);
       return;
     }
@@ -79,6 +80,7 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
     win.cand_kc[win.ncand] = t.kc_min;
     win.cand_kmax[win.ncand] = t.kc_max;
     win.cand_fused[win.ncand] = fused;
+    win.cand_ctas[win.ncand] = t.ctas;
     ++win.ncand;
   };
   try {
@@ -94,8 +96,9 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
       SADMRG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       return ms / 3.f;
     };
-    const int cands[7][3] = {{64, 16, 0}, {128, 16, 0}, {64, 0, 0},  {128, 0, 0},
-                             {64, 16, 32}, {128, 16, 32}, {64, 16, 16}};
+    // {width, split floor, item cap, CTAs per SM}
+    const int cands[7][4] = {{64, 16, 0, 1},  {128, 16, 0, 1}, {64, 0, 0, 1},  {128, 0, 0, 1},
+                             {64, 16, 32, 1}, {64, 16, 0, 2},  {64, 16, 32, 2}};
     std::vector<std::tuple<int, size_t, size_t>> seen;   // schedules already timed: (bn, items, reductions)
     UmmaTune pick;
     for (const auto& cd : cands) {
@@ -103,9 +106,10 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
       p.tune.bn = cd[0];
       p.tune.kc_min = cd[1];
       p.tune.kc_max = cd[2];
+      p.tune.ctas = cd[3];
       p.tune.fused = 0;
       if (!p.rebuild_umma(c, kCx<S>)) break;
-      const auto fp = std::make_tuple(p.umma->bn, p.umma->items.size(), p.umma->reds.size());
+      const auto fp = std::make_tuple(p.umma->bn * 4 + p.umma->ctas, p.umma->items.size(), p.umma->reds.size());
       if (std::find(seen.begin(), seen.end(), fp) != seen.end()) continue;   // the same schedule as one timed
       seen.push_back(fp);
       const float ms = time_current();
@@ -124,6 +128,7 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
     win.bn = pick.bn;
     win.kc_min = pick.kc_min;
     win.kc_max = pick.kc_max;
+    win.ctas = pick.ctas;
     win.fused = pick.fused;
   } catch (...) {
     if (e0) cudaEventDestroy(e0);
@@ -635,52 +640,58 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
     }
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
   const double tj = now_s();
-  // start from the previous truncation's V at this bond when the sectors match:
-  // W = A V0 (or A^H V0) on the FP64 grouped GEMM, V = V0
-  bool preset = false;
-  if (warm && warm->buf && warm->m.size() == jobs.size() && !jobs.empty()) {
-    preset = true;
-    for (size_t k = 0; k < jobs.size() && preset; ++k)
-      preset = warm->m[k] == jobs[k].m && warm->n[k] == jobs[k].n;
-  }
-  if (warm) (preset ? warm->hits : warm->misses) += 1;
-  if (preset) {
+  // every sector whose block has the same dimensions as at this bond's last
+  // truncation starts from that truncation's V: W = A V0 (or A^H V0) on the FP64
+  // grouped GEMM, V = V0; the others from W = A, V = I
+  std::vector<long long> v0(jobs.size(), -1);
+  if (warm && warm->buf)
+    for (int i = 0; i < nm1; ++i) {
+      if (job_of[i] < 0) continue;
+      auto it = warm->sec.find(bb0.q[i]);
+      const SvdJob& J = jobs[job_of[i]];
+      if (it != warm->sec.end() && it->second.m == J.m && it->second.n == J.n) v0[job_of[i]] = it->second.voff;
+    }
+  {
     GemmPlan g;
     g.nstage = 1;
     for (size_t k = 0; k < jobs.size(); ++k) {
-      const SvdJob& J = jobs[k];
+      if (v0[k] < 0) continue;
+      SvdJob& J = jobs[k];
+      J.preset = 1;
+      ++out.warm;
       const int R = std::max(J.m, J.n), C = std::min(J.m, J.n);
       const int job = g.add_job(0, 1, J.woff, R, C, R, 0);
-      g.add_term(job, 0, J.aoff, J.m, 2, warm->voff[k], C, C, J.trans ? (TF_TA | TF_CA) : 0, 1.0, 0.0);
-      SADMRG_CUDA(cudaMemcpyAsync(wv.template as<S>() + J.voff, warm->buf->template as<S>() + warm->voff[k],
+      g.add_term(job, 0, J.aoff, J.m, 2, v0[k], C, C, J.trans ? (TF_TA | TF_CA) : 0, 1.0, 0.0);
+      SADMRG_CUDA(cudaMemcpyAsync(wv.template as<S>() + J.voff, warm->buf->template as<S>() + v0[k],
                                   sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
     }
-    g.finalize(c, kCx<S>);
-    Bases b{};
-    b.p[0] = const_cast<S*>(psi.data());
-    b.p[1] = wv.get();
-    b.p[2] = warm->buf->get();
-    g.run(c, kCx<S>, PREC_FP64, b);
-    out.warm = true;
+    if (!g.empty()) {
+      g.finalize(c, kCx<S>);
+      Bases b{};
+      b.p[0] = const_cast<S*>(psi.data());
+      b.p[1] = wv.get();
+      b.p[2] = warm->buf->get();
+      g.run(c, kCx<S>, PREC_FP64, b);
+    }
   }
   const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
-                                    &out.jacobi_kernel_ms, preset);
+                                    &out.jacobi_kernel_ms);
   if (warm && sweeps > 0) {
-    // this truncation's V for the next one at the bond
+    // this truncation's V of every sector, for the next one at the bond
     long long vt = 0;
-    warm->m.clear();
-    warm->n.clear();
-    warm->voff.clear();
-    for (auto& J : jobs) {
-      warm->m.push_back(J.m);
-      warm->n.push_back(J.n);
-      warm->voff.push_back(vt);
+    warm->sec.clear();
+    for (int i = 0; i < nm1; ++i) {
+      if (job_of[i] < 0) continue;
+      const SvdJob& J = jobs[job_of[i]];
+      warm->sec[bb0.q[i]] = SvdWarm::Sector{J.m, J.n, vt};
       vt += (long long)std::min(J.m, J.n) * std::min(J.m, J.n);
     }
     auto nb = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(vt, 1), c.stream);
-    for (size_t k = 0; k < jobs.size(); ++k) {
-      const long long C = std::min(jobs[k].m, jobs[k].n);
-      SADMRG_CUDA(cudaMemcpyAsync(nb->template as<S>() + warm->voff[k], wv.template as<S>() + jobs[k].voff,
+    for (int i = 0; i < nm1; ++i) {
+      if (job_of[i] < 0) continue;
+      const SvdJob& J = jobs[job_of[i]];
+      const long long C = std::min(J.m, J.n);
+      SADMRG_CUDA(cudaMemcpyAsync(nb->template as<S>() + warm->sec[bb0.q[i]].voff, wv.template as<S>() + J.voff,
                                   sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
     }
     warm->buf = nb;
@@ -1177,7 +1188,7 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   const double t0 = now_s();
   std::vector<double> w;
   SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w, &svd_warm[(long long)il * ns + ir]);
-  if (s.warm) ++timers.svd_warm;
+  timers.svd_warm += s.warm;
   // BlockTensor::svd overwrites the first n values of the chain's ww array and
   // leaves the rest as it was (src/block_tensor_inst.cpp:576-600)
   if (ww.size() < w.size()) ww.resize(w.size(), 0.0);

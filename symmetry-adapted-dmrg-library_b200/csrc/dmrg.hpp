@@ -126,18 +126,18 @@ struct SvdStats {
   bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative), or a
                               // sector's relative 1e-10 cut-off met a value within two decades of it
   double cut_gap = 1.0;       // (D-th - (D+1)-th singular value) / |psi|; 1 when nothing was cut
-  bool warm = false;          // the Jacobi started from the previous truncation's V
+  int warm = 0;               // sectors whose Jacobi started from the previous truncation's V
 };
 
 // Right singular vectors of the last truncation at a bond, kept to start the
 // next one there: one-sided Jacobi converges from any unitary start, and from
 // the previous sweep's V (the state changes little between sweeps) in a few
-// sweeps instead of ~12.  Used only when every sector has the same dimensions.
+// sweeps instead of ~12.  Used per sector, for the sectors whose block has the
+// same dimensions as last time (the others start from the identity).
 struct SvdWarm {
-  std::vector<int> m, n;              // per sector block (the Jacobi jobs, in order)
-  std::vector<long long> voff;        // its V (C x C, C = min(m, n)) in buf
+  struct Sector { int m, n; long long voff; };   // block dims, its V (C x C, C = min(m, n)) in buf
+  std::map<int, Sector> sec;                     // by sector label
   std::shared_ptr<DevBuf> buf;
-  int hits = 0, misses = 0;
 };
 
 // BlockTensor::svd (src/block_tensor_inst.cpp:501-637); warm: see SvdWarm (may be null)
@@ -151,7 +151,7 @@ struct Timers {
   double heff_flops = 0;
   double svd_kernel = 0;        // device time of the Jacobi sweep kernels (s)
   long long svd_sweeps = 0;     // Jacobi sweeps, summed over the truncations
-  long long svd_warm = 0;       // truncations whose Jacobi started from the previous V at the bond
+  long long svd_warm = 0;       // sector blocks whose Jacobi started from the previous V at the bond
   double plan = 0;              // host wall time of building H_eff plans (part of lanczos)
 };
 

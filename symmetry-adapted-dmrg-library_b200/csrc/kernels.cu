@@ -131,6 +131,22 @@ void launch_scale(bool cplx, void* x, double ar, double ai, long long n, cudaStr
   else scale_kernel<false><<<blocks, 256, 0, s>>>(x, ar, ai, n);
 }
 
+// Reads bytes (a multiple of 16) of x; writes sink only when the xor of all
+// words is a value no data here holds in practice, so the loads cannot be dropped.
+__global__ void read_kernel(const uint4* __restrict__ x, long long n16, unsigned* sink) {
+  unsigned acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (long long)blockDim.x * gridDim.x) {
+    const uint4 v = __ldcg(x + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == 0x9e3779b9u && sink) *sink = acc;
+}
+
+void launch_read(const void* x, long long bytes, unsigned* sink, cudaStream_t s) {
+  if (bytes < 16) return;
+  read_kernel<<<148 * 8, 256, 0, s>>>(static_cast<const uint4*>(x), bytes / 16, sink);
+}
+
 template <bool CPLX>
 __global__ void fill_kernel(void* x, double vr, double vi, long long n) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)blockDim.x * gridDim.x) {

@@ -122,6 +122,7 @@ struct UPhase {               // what one launch does besides its items
   int wait_deps;              // items wait for panels written in this launch (cooperative launch)
   int ndeps;
   long long wait_ns;          // limit of every bounded wait; 0: the default (2 s)
+  int ctas_per_sm;            // 2: two CTAs per SM, each with a 2-stage ring (tile width 64 only); else one
 };
 // one 256-thread block per 256 chunks; blk_job[block] = its job
 void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bases& b, unsigned char* dst,
@@ -178,6 +179,9 @@ void launch_gather(bool cplx, void* dst, const void* src, const double* w, const
                    cudaStream_t s);
 // x *= alpha (host scalar)
 void launch_scale(bool cplx, void* x, double ar, double ai, long long n, cudaStream_t s);
+// read bytes (a multiple of 16) of x and discard them (sink: a device word, written
+// only by an unlikely data pattern)
+void launch_read(const void* x, long long bytes, unsigned* sink, cudaStream_t s);
 // fill with a constant
 void launch_fill(bool cplx, void* x, double vr, double vi, long long n, cudaStream_t s);
 
@@ -225,13 +229,14 @@ struct SvdJob {
   long long voff;             // accumulated rotations: min(m,n) x min(m,n)
   long long soff;             // singular values (double), min(m,n)
   int m, n, trans;            // trans = 1 when m < n (work on A^H)
+  int preset;                 // W and V hold a starting point already (W = A V0 or A^H V0, V = V0)
 };
 // Host driver: one launch per round of block pairs, one sync per sweep to test
 // convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
 // kernel_ms (optional): device time of the sweep kernel when it ran as one launch.
-// preset: W and V already hold a starting point (W = A V0, V = V0, V0 unitary)
-// instead of W = A, V = I.
+// A job with preset = 1 starts from the W and V already in work / vmat (W = A V0,
+// V = V0, V0 unitary) instead of W = A, V = I.
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, bool preset = false);
+                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr);
 
 }  // namespace sadmrg

@@ -215,6 +215,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   for (size_t j = 0; j < jobs.size(); ++j)
     t128 += (long long)(((cplx ? 2 : 1) * jobs[j].m + 127) / 128) * ((jobs[j].n + 127) / 128);
   U->bn = tune.bn == 64 || tune.bn == 128 ? tune.bn : (t128 >= 2LL * nsm * std::max(nstage, 1)) ? 128 : 64;
+  U->ctas = (tune.ctas == 2 && U->bn == 64) ? 2 : 1;
   const int BN = U->bn;
 
   struct Key {
@@ -588,6 +589,7 @@ void GemmPlan::run_starved(Ctx& c, bool cplx, const Bases& b, int starve, long l
   ph.npk_blocks = (int)U.vblk.size();
   ph.wait_deps = 1;
   ph.wait_ns = wait_ns;
+  ph.ctas_per_sm = U.ctas;
   const int ni = U.stage_items[nstage] - U.stage_items[0];
   launch_umma_items(U.bn, U.d_terms, U.d_jobs, U.d_items, U.d_reds, ni, b, ub, ph, c.stream);
   ++c.launches;
@@ -623,6 +625,7 @@ void GemmPlan::run(Ctx& c, bool cplx, int prec, const Bases& b, int stage_lo, in
     ph.pk_blk = U.d_vblk;
     ph.npk_jobs = (int)U.vpack.size();
     ph.ndeps = (int)U.dep_target.size();
+    ph.ctas_per_sm = U.ctas;
     const bool whole = stage_lo == 0 && stage_hi == nstage;
     if (whole && runs_fused(c, cplx, prec)) {
       // the whole matvec in one cooperative launch: psi packing, stage 0, stage 1

@@ -514,10 +514,10 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
   }
 }
 
-// W = A (m >= n) or A^H (m < n); V = I.  preset: W and V hold the start already
-// (W = A V0, V = V0 for a starting rotation V0); only the column order is set.
+// W = A (m >= n) or A^H (m < n); V = I.  A preset job holds its start already
+// (W = A V0, V = V0 for a starting rotation V0); only its column order is set.
 template <bool CPLX>
-__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm, int preset) {
+__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm) {
   using T = typename SvdT<CPLX>::T;
   const SvdJob J = jobs[blockIdx.x];
   const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
@@ -526,7 +526,7 @@ __global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work
   T* V = static_cast<T*>(vmat) + J.voff;
   if (blockIdx.y == 0)
     for (int c = threadIdx.x; c < C; c += blockDim.x) perm[J.soff + c] = c;
-  if (preset) return;
+  if (J.preset) return;
   for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)R * C;
        e += (long long)blockDim.x * gridDim.y) {
     const int r = (int)(e % R), c = (int)(e / R);
@@ -569,7 +569,7 @@ __global__ void jacobi_norms_kernel(const SvdJob* jobs, const void* work, double
 // was reached).
 template <bool CPLX, int B>
 static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                      int max_sweeps, cudaStream_t s, double* kernel_ms, bool preset) {
+                      int max_sweeps, cudaStream_t s, double* kernel_ms) {
   const int nj = (int)hjobs.size();
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
@@ -614,7 +614,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
   SADMRG_CUDA(cudaMemcpyAsync(djobs.get(), hjobs.data(), sizeof(SvdJob) * nj, cudaMemcpyHostToDevice, s));
   SADMRG_CUDA(cudaMemcpyAsync(dpairs.get(), flat.data(), sizeof(SvdPair) * flat.size(), cudaMemcpyHostToDevice, s));
   dim3 ig(nj, 16);
-  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>(), preset ? 1 : 0);
+  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
   SADMRG_CUDA(cudaGetLastError());
   SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<CPLX, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const double tol = std::sqrt((double)std::max(maxR, 1)) * 2.220446049250313e-16;
@@ -680,7 +680,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
 }
 
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms, bool preset) {
+                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
   if (kernel_ms) *kernel_ms = -1.0;
   if (hjobs.empty()) return 0;
   // column blocks of 16, or of 8 when the widest round of 16-column pairs would
@@ -699,10 +699,10 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   }
   const bool narrow = 2 * pairs16 < nsm;
   if (cplx)
-    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset)
-                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset);
-  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset)
-                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, preset);
+    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
+                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
+  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
+                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
 }
 
 }  // namespace sadmrg

@@ -31,10 +31,11 @@ struct UmmaTune {
   int kc_min = 16;     // fewest k slabs in a split-K chunk; 0: no split for balance (kc_max still applies)
   int kc_max = 0;      // most k slabs in one item (longer reductions are split); 0: no cap
   int fused = -1;      // 1: a whole matvec in one cooperative launch, 0: one launch per stage, -1: Ctx's setting
+  int ctas = 1;        // CTAs per SM (2: width 64 only, a 2-stage ring each)
   int source = 0;
   int ncand = 0;       // candidates timed, with their device time (ms) per matvec
   float ms[8] = {};
-  int cand_bn[8] = {}, cand_kc[8] = {}, cand_kmax[8] = {}, cand_fused[8] = {};
+  int cand_bn[8] = {}, cand_kc[8] = {}, cand_kmax[8] = {}, cand_fused[8] = {}, cand_ctas[8] = {};
 };
 
 struct Ctx {
@@ -118,6 +119,7 @@ struct GemmSchedule {
 // terms with coefficient 1).
 struct UmmaSchedule {
   int bn = 64;
+  int ctas = 1;                            // CTAs per SM of its launches
   std::vector<PackJob> cpack, vpack;       // constant panels (packed once), psi panels (every apply)
   long long cchunks = 0, vchunks = 0;      // multiples of 256 (one block per 256 chunks)
   std::vector<int> cblk, vblk;             // block -> pack job

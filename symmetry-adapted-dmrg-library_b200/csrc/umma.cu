@@ -21,8 +21,9 @@
 //                      partial tile and the last item of its tile to finish
 //                      (atomic count per tile) sums all partials in slot order.
 // Two accumulators (2 x BN TMEM columns) let the epilogue of one item overlap
-// the MMAs of the next; the kernel is persistent (one CTA per SM, static
-// round-robin over the longest-first item list).
+// the MMAs of the next; the kernel is persistent (one CTA per SM -- or two,
+// with a 2-stage ring each, at tile width 64 -- static round-robin over the
+// longest-first item list).
 //
 // Every mbarrier wait is bounded (time and iterations) and also gives up when
 // another role has failed.  A wait that runs out sets a device status word
@@ -229,8 +230,8 @@ struct UG {
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-template <int BN, int ST>
-__global__ void __launch_bounds__(kGThreads, 1)
+template <int BN, int ST, int MINB>
+__global__ void __launch_bounds__(kGThreads, MINB)
     umma_gemm(const UTerm* __restrict__ terms, const UJob* __restrict__ jobs, const UItem* __restrict__ items,
               const URed* __restrict__ reds, int nitems, Bases bases, UBufs ub, UPhase ph) {
   using G = UG<BN, ST>;
@@ -583,12 +584,12 @@ __global__ void __launch_bounds__(kGThreads, 1)
   }
 }
 
-template <int BN, int ST>
+template <int BN, int ST, int MINB>
 void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
                    const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
   static unsigned char attr[kMaxDevices] = {0};
-  ensure_smem_attr((const void*)umma_gemm<BN, ST>, (int)UG<BN, ST>::SMEM, attr);
-  const int nsm = device_sm_count();
+  ensure_smem_attr((const void*)umma_gemm<BN, ST, MINB>, (int)UG<BN, ST>::SMEM, attr);
+  const int nsm = device_sm_count() * MINB;   // resident CTAs
   int grid = nitems > ph.npk_blocks ? nitems : ph.npk_blocks;
   if (grid > nsm) grid = nsm;
   if (grid < 1) grid = 1;
@@ -601,10 +602,10 @@ void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, con
     int ni = nitems;
     void* args[] = {(void*)&terms, (void*)&jobs, (void*)&items, (void*)&reds, (void*)&ni, (void*)&bb, (void*)&uu,
                     (void*)&pp};
-    cudaLaunchCooperativeKernel((const void*)umma_gemm<BN, ST>, dim3(grid), dim3(kGThreads), args,
+    cudaLaunchCooperativeKernel((const void*)umma_gemm<BN, ST, MINB>, dim3(grid), dim3(kGThreads), args,
                                 UG<BN, ST>::SMEM, s);
   } else {
-    umma_gemm<BN, ST><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, reds, nitems, b, u, ph);
+    umma_gemm<BN, ST, MINB><<<grid, kGThreads, UG<BN, ST>::SMEM, s>>>(terms, jobs, items, reds, nitems, b, u, ph);
   }
 }
 
@@ -642,8 +643,9 @@ void launch_pack(const PackJob* jobs, const int* blk_job, int nblocks, const Bas
 void launch_umma_items(int bn, const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
                        const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
   if (nitems <= 0 && ph.npk_blocks <= 0) return;
-  if (bn == 128) launch_gemm_t<128, 3>(terms, jobs, items, reds, nitems, b, u, ph, s);
-  else launch_gemm_t<64, 4>(terms, jobs, items, reds, nitems, b, u, ph, s);
+  if (bn == 128) launch_gemm_t<128, 3, 1>(terms, jobs, items, reds, nitems, b, u, ph, s);
+  else if (ph.ctas_per_sm == 2) launch_gemm_t<64, 2, 2>(terms, jobs, items, reds, nitems, b, u, ph, s);
+  else launch_gemm_t<64, 4, 1>(terms, jobs, items, reds, nitems, b, u, ph, s);
 }
 
 int umma_status(bool reset) {

@@ -96,7 +96,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_heff_wait_fault_test": ([vp, C.c_longlong, ip], C.c_int),
         "sadmrg_set_autotune": ([vp, C.c_int], C.c_int),
         "sadmrg_heff_tiles": ([vp, C.c_int, dp, ip], C.c_int),
-        "sadmrg_set_tiles": ([vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "sadmrg_set_tiles": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
@@ -394,10 +394,10 @@ class Handle:
         """Time candidate tcgen05 schedules for every new H_eff plan (default on)."""
         self._check(self.lib.sadmrg_set_autotune(self.h, int(bool(on))), "set_autotune")
 
-    def set_tiles(self, bn: int, kc_min: int = 16, kc_max: int = 0, one_launch: int = -1):
+    def set_tiles(self, bn: int, kc_min: int = 16, kc_max: int = 0, ctas_per_sm: int = 1, one_launch: int = -1):
         """Fix the tcgen05 schedule of the H_eff plans made from now on (bn = 0: autotune again)."""
-        self._check(self.lib.sadmrg_set_tiles(self.h, int(bn), int(kc_min), int(kc_max), int(one_launch)),
-                    "set_tiles")
+        self._check(self.lib.sadmrg_set_tiles(self.h, int(bn), int(kc_min), int(kc_max), int(ctas_per_sm),
+                                              int(one_launch)), "set_tiles")
 
     def heff_tiles(self) -> dict:
         """The current plan's tcgen05 tile choice and the candidates timed for it."""
@@ -406,10 +406,12 @@ class Handle:
         self._check(self.lib.sadmrg_heff_tiles(self.h, 64, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)),
                     "heff_tiles")
         v = out[:n.value]
-        cands = [{"bn": int(v[6 + 5 * i]), "kc_min": int(v[7 + 5 * i]), "kc_max": int(v[8 + 5 * i]),
-                  "one_launch": bool(v[9 + 5 * i]), "ms": float(v[10 + 5 * i])} for i in range(int(v[5]))]
-        return {"bn": int(v[0]), "kc_min": int(v[1]), "kc_max": int(v[2]), "one_launch": bool(v[3]),
-                "source": ["heuristic", "timed", "cached", "set"][int(v[4])], "candidates": cands}
+        cands = [{"bn": int(v[7 + 6 * i]), "kc_min": int(v[8 + 6 * i]), "kc_max": int(v[9 + 6 * i]),
+                  "ctas_per_sm": int(v[10 + 6 * i]), "one_launch": bool(v[11 + 6 * i]), "ms": float(v[12 + 6 * i])}
+                 for i in range(int(v[6]))]
+        return {"bn": int(v[0]), "kc_min": int(v[1]), "kc_max": int(v[2]), "ctas_per_sm": int(v[3]),
+                "one_launch": bool(v[4]), "source": ["heuristic", "timed", "cached", "set"][int(v[5])],
+                "candidates": cands}
 
     def heff_launches_per_matvec(self, precision: int) -> int:
         n = C.c_int()

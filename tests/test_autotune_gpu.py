@@ -31,5 +31,5 @@ def test_autotune_choice_visible_cached_and_repeatable(name):
     h2, _, _, _ = build_problem(path)
     t2 = h2.heff_tiles()
     assert t2["source"] == "cached"
-    assert (t2["bn"], t2["kc_min"], t2["kc_max"], t2["one_launch"]) == (t["bn"], t["kc_min"], t["kc_max"], t["one_launch"])
+    assert {k: t2[k] for k in ("bn", "kc_min", "kc_max", "ctas_per_sm", "one_launch")} == {k: t[k] for k in ("bn", "kc_min", "kc_max", "ctas_per_sm", "one_launch")}
     assert np.array_equal(h2.heff_apply(psi.data, sadmrg.PREC_TF32X3), a)
