@@ -295,6 +295,10 @@ int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, in
  *          svd_warm (truncations whose Jacobi started from the previous V at the same bond)];
  *          the first n are written */
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
+/* Per bond (index il of its two-site pair (il, il + 1)), what its last truncation
+ * flagged: 1 a rounding tie (as near_ties), 2 a stop-test tie (as stop_ties);
+ * flags[i] for i < cap. */
+int sadmrg_chain_bond_flags(sadmrg_handle* h, int cap, int* flags);
 /* kind: 0 = uu[site], 1 = hh[site], 2 = opr[site][k] */
 int sadmrg_chain_set_tensor(sadmrg_handle* h, int kind, int site, int k, const sadmrg_tensor_desc* t);
 int sadmrg_chain_stage_tensor(sadmrg_handle* h, int kind, int site, int k);

@@ -984,6 +984,16 @@ int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, in
   });
 }
 
+int sadmrg_chain_bond_flags(sadmrg_handle* h, int cap, int* flags) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain && flags, SADMRG_ERR_STATE, "chain_bond_flags: no chain");
+    const auto& f = S_.chain->bond_flags;
+    for (int i = 0; i < cap; ++i) flags[i] = i < (int)f.size() ? f[i] : 0;
+  });
+}
+
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;

@@ -112,7 +112,13 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
       const auto fp = std::make_tuple(p.umma->bn * 4 + p.umma->ctas, p.umma->items.size(), p.umma->reds.size());
       if (std::find(seen.begin(), seen.end(), fp) != seen.end()) continue;   // the same schedule as one timed
       seen.push_back(fp);
-      const float ms = time_current();
+      float ms = 0.f;
+      try {
+        ms = time_current();
+      } catch (const Error&) {
+        cudaGetLastError();   // a launch configuration this device refuses: not a candidate
+        continue;
+      }
       record(ms, p.tune, 0);
       if (ms < best) { best = ms; pick = p.tune; }
     }
@@ -121,9 +127,13 @@ static void autotune_heff(Ctx& c, HeffPlan<S>& H) {
     p.rebuild_umma(c, kCx<S>);
     p.tune.fused = 1;
     if (p.runs_fused(c, kCx<S>, PREC_TF32X3)) {
-      const float ms = time_current();
-      record(ms, pick, 1);
-      if (ms < best) { best = ms; pick.fused = 1; }
+      try {
+        const float ms = time_current();
+        record(ms, pick, 1);
+        if (ms < best) { best = ms; pick.fused = 1; }
+      } catch (const Error&) {
+        cudaGetLastError();
+      }
     }
     win.bn = pick.bn;
     win.kc_min = pick.kc_min;
@@ -1195,6 +1205,12 @@ void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   std::copy(w.begin(), w.end(), ww.begin());
   last_discarded = s.discarded_weight;
   if (s.near_tie) ++near_ties;
+  {
+    int f = s.near_tie ? 1 : 0;
+    if (s.cut_gap < 10.0 * std::sqrt(c.lanczos_ov_tol)) f |= 2;
+    if ((int)bond_flags.size() < ns) bond_flags.assign(ns, 0);
+    bond_flags[il] = f;
+  }
   // the stop test fixes the Ritz vector only to about sqrt(ov_tol) (times |E| / gap),
   // so a cut whose gap is within that of 0 can fall either way in two correct runs
   if (s.cut_gap < 10.0 * std::sqrt(c.lanczos_ov_tol)) ++stop_ties;

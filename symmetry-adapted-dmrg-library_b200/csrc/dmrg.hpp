@@ -204,6 +204,8 @@ class Chain {
   double last_discarded = 0.0;
   int near_ties = 0;          // truncations whose cut fell inside a near-degenerate pair
   int stop_ties = 0;          // truncations whose cut gap is below 10 sqrt(Lanczos ov_tol) |psi|
+  std::vector<int> bond_flags;  // per bond (site il of the pair): flags of its last truncation,
+                                // 1 a rounding tie (near_ties), 2 a stop-test tie
   // Lanczos settings (reference constants at src/dmrg_inst.cpp:267,1289,1338)
   int mlanc_max = 40;
   int prec = PREC_FP64;

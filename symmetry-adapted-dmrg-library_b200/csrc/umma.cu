@@ -588,8 +588,19 @@ template <int BN, int ST, int MINB>
 void launch_gemm_t(const UTerm* terms, const UJob* jobs, const UItem* items, const URed* reds, int nitems,
                    const Bases& b, const UBufs& u, const UPhase& ph, cudaStream_t s) {
   static unsigned char attr[kMaxDevices] = {0};
+  static int occ[kMaxDevices] = {0};   // resident CTAs per SM the device grants this kernel
   ensure_smem_attr((const void*)umma_gemm<BN, ST, MINB>, (int)UG<BN, ST>::SMEM, attr);
-  const int nsm = device_sm_count() * MINB;   // resident CTAs
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < kMaxDevices && occ[dev] == 0) {
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, umma_gemm<BN, ST, MINB>, kGThreads, UG<BN, ST>::SMEM) !=
+            cudaSuccess || v < 1)
+      v = 1;
+    occ[dev] = v < MINB ? v : MINB;
+  }
+  const int per_sm = (dev >= 0 && dev < kMaxDevices) ? occ[dev] : 1;
+  const int nsm = device_sm_count() * per_sm;   // CTAs resident at once
   int grid = nitems > ph.npk_blocks ? nitems : ph.npk_blocks;
   if (grid > nsm) grid = nsm;
   if (grid < 1) grid = 1;
@@ -630,6 +641,8 @@ void ensure_smem_attr(const void* fn, int bytes, unsigned char* done) {
   }
   if (!done[dev]) {
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    // the largest shared-memory carve-out, so that as many CTAs as the smem allows are resident
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
     done[dev] = 1;
   }
 }

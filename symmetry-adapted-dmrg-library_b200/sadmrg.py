@@ -39,6 +39,7 @@ EXPORTED = [
     "sadmrg_chain_set_mlanc", "sadmrg_chain_save_ww", "sadmrg_chain_read_ww", "sadmrg_chain_save_enr",
     "sadmrg_chain_read_enr", "sadmrg_chain_ww", "sadmrg_heff_graph_steps", "sadmrg_heff_launches_per_matvec",
     "sadmrg_heff_wait_fault_test", "sadmrg_set_autotune", "sadmrg_heff_tiles", "sadmrg_set_tiles",
+    "sadmrg_chain_bond_flags",
 ]
 
 
@@ -115,6 +116,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_chain_ww": ([vp, C.c_int, ip, dp], C.c_int),
         "sadmrg_chain_freeze": ([vp, C.c_int, C.c_char_p], C.c_int),
         "sadmrg_chain_stats": ([vp, dp, C.c_int], C.c_int),
+        "sadmrg_chain_bond_flags": ([vp, C.c_int, ip], C.c_int),
         "sadmrg_chain_set_tensor": ([vp, C.c_int, C.c_int, C.c_int, td], C.c_int),
         "sadmrg_chain_stage_tensor": ([vp, C.c_int, C.c_int, C.c_int], C.c_int),
         "sadmrg_chain_env_update": ([vp, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -542,6 +544,13 @@ class Handle:
         self._check(self.lib.sadmrg_chain_bond(self.h, int(site), cap, C.byref(n), q.ctypes.data_as(ip),
                                                d.ctypes.data_as(ip)), "chain_bond")
         return [(int(q[i]), int(d[i])) for i in range(n.value)]
+
+    def chain_bond_flags(self, ns: int) -> List[int]:
+        """Per bond il: flags of its last truncation (1 rounding tie, 2 stop-test tie)."""
+        f = np.zeros(ns, np.int32)
+        self._check(self.lib.sadmrg_chain_bond_flags(self.h, int(ns), f.ctypes.data_as(C.POINTER(C.c_int))),
+                    "chain_bond_flags")
+        return [int(x) for x in f]
 
     def chain_stats(self):
         out = np.zeros(15)
