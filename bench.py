@@ -443,7 +443,7 @@ def chain_sweeps(wl: dict, device: int, sweeps: int, export_dir: str | None, kee
             times.append(round(time.perf_counter() - t0, 3))
             s1 = h.chain_stats()
             stats.append({k: round(s1[k] - s0[k], 4) for k in ("lanczos_s", "svd_s", "svd_kernel_s", "env_s",
-                                                                 "prep_s", "matvecs", "svd_sweeps", "svd_warm")})
+                                                                 "prep_s", "matvecs", "svd_sweeps")})
         st1 = h.chain_stats()
         runs[name] = dict(sweep_s=times, sweep_E=es, per_sweep=stats,
                           totals={k: st1[k] - st0[k] for k in st1 if k not in ("discarded", "near_ties")}

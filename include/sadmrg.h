@@ -291,9 +291,7 @@ int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, in
  *          plan_s (host time of building H_eff plans, part of lanczos_s),
  *          stop_ties (truncations whose cut gap -- D-th minus (D+1)-th singular value over
  *          |psi| -- is below 10 sqrt(Lanczos ov_tol): the stop test fixes psi only to about
- *          that, so two correct runs may cut such a bond differently),
- *          svd_warm (truncations whose Jacobi started from the previous V at the same bond)];
- *          the first n are written */
+ *          that, so two correct runs may cut such a bond differently)]; the first n are written */
 int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n);
 /* Per bond (index il of its two-site pair (il, il + 1)), what its last truncation
  * flagged: 1 a rounding tie (as near_ties), 2 a stop-test tie (as stop_ties);

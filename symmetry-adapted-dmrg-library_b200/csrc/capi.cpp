@@ -1000,11 +1000,11 @@ int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     const Timers& t = S_.chain->timers;
-    const double v[15] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
+    const double v[14] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
                           (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded,
                           (double)S_.chain->near_ties, t.svd_kernel, (double)t.svd_sweeps, t.plan,
-                          (double)S_.chain->stop_ties, (double)t.svd_warm};
-    for (int i = 0; i < n && i < 15; ++i) out[i] = v[i];
+                          (double)S_.chain->stop_ties};
+    for (int i = 0; i < n && i < 14; ++i) out[i] = v[i];
   });
 }
 

@@ -618,7 +618,7 @@ LanczosStats lanczos_solve(Ctx& c, const HeffPlan<S>& H, S* v, int mlanc, int pr
 // block SVD and truncation (BlockTensor::svd, src/block_tensor_inst.cpp:501-637)
 template <class S>
 SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
-                   int max_dcut, std::vector<double>* wout, SvdWarm* warm) {
+                   int max_dcut, std::vector<double>* wout) {
   SvdStats out;
   const Bond bb20 = tu.st.bonds[0], bb21 = tu.st.bonds[1], bb22 = tv.st.bonds[0], bb23 = tv.st.bonds[1];
   const Bond bb0 = Bond::fuse(c.sym, bb20, bb21), bb1 = Bond::fuse(c.sym, bb22, bb23);
@@ -650,62 +650,8 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
     }
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
   const double tj = now_s();
-  // every sector whose block has the same dimensions as at this bond's last
-  // truncation starts from that truncation's V: W = A V0 (or A^H V0) on the FP64
-  // grouped GEMM, V = V0; the others from W = A, V = I
-  std::vector<long long> v0(jobs.size(), -1);
-  if (warm && warm->buf)
-    for (int i = 0; i < nm1; ++i) {
-      if (job_of[i] < 0) continue;
-      auto it = warm->sec.find(bb0.q[i]);
-      const SvdJob& J = jobs[job_of[i]];
-      if (it != warm->sec.end() && it->second.m == J.m && it->second.n == J.n) v0[job_of[i]] = it->second.voff;
-    }
-  {
-    GemmPlan g;
-    g.nstage = 1;
-    for (size_t k = 0; k < jobs.size(); ++k) {
-      if (v0[k] < 0) continue;
-      SvdJob& J = jobs[k];
-      J.preset = 1;
-      ++out.warm;
-      const int R = std::max(J.m, J.n), C = std::min(J.m, J.n);
-      const int job = g.add_job(0, 1, J.woff, R, C, R, 0);
-      g.add_term(job, 0, J.aoff, J.m, 2, v0[k], C, C, J.trans ? (TF_TA | TF_CA) : 0, 1.0, 0.0);
-      SADMRG_CUDA(cudaMemcpyAsync(wv.template as<S>() + J.voff, warm->buf->template as<S>() + v0[k],
-                                  sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
-    }
-    if (!g.empty()) {
-      g.finalize(c, kCx<S>);
-      Bases b{};
-      b.p[0] = const_cast<S*>(psi.data());
-      b.p[1] = wv.get();
-      b.p[2] = warm->buf->get();
-      g.run(c, kCx<S>, PREC_FP64, b);
-    }
-  }
   const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
                                     &out.jacobi_kernel_ms);
-  if (warm && sweeps > 0) {
-    // this truncation's V of every sector, for the next one at the bond
-    long long vt = 0;
-    warm->sec.clear();
-    for (int i = 0; i < nm1; ++i) {
-      if (job_of[i] < 0) continue;
-      const SvdJob& J = jobs[job_of[i]];
-      warm->sec[bb0.q[i]] = SvdWarm::Sector{J.m, J.n, vt};
-      vt += (long long)std::min(J.m, J.n) * std::min(J.m, J.n);
-    }
-    auto nb = std::make_shared<DevBuf>(sizeof(S) * std::max<long long>(vt, 1), c.stream);
-    for (int i = 0; i < nm1; ++i) {
-      if (job_of[i] < 0) continue;
-      const SvdJob& J = jobs[job_of[i]];
-      const long long C = std::min(J.m, J.n);
-      SADMRG_CUDA(cudaMemcpyAsync(nb->template as<S>() + warm->sec[bb0.q[i]].voff, wv.template as<S>() + J.voff,
-                                  sizeof(S) * C * C, cudaMemcpyDeviceToDevice, c.stream));
-    }
-    warm->buf = nb;
-  }
   out.jacobi_s = now_s() - tj;
   for (auto& J : jobs) {
     out.max_rows = std::max(out.max_rows, std::max(J.m, J.n));
@@ -1197,8 +1143,7 @@ template <class S>
 void Chain<S>::svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2) {
   const double t0 = now_s();
   std::vector<double> w;
-  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w, &svd_warm[(long long)il * ns + ir]);
-  timers.svd_warm += s.warm;
+  SvdStats s = block_svd<S>(c, vec, uu[il], p1, uu[ir], p2, max_dcut, &w);
   // BlockTensor::svd overwrites the first n values of the chain's ww array and
   // leaves the rest as it was (src/block_tensor_inst.cpp:576-600)
   if (ww.size() < w.size()) ww.resize(w.size(), 0.0);
@@ -1534,9 +1479,9 @@ template LanczosStats lanczos2<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*
 template LanczosStats lanczos_solve<double>(Ctx&, const HeffPlan<double>&, double*, int, int);
 template LanczosStats lanczos_solve<dcmplex>(Ctx&, const HeffPlan<dcmplex>&, dcmplex*, int, int);
 template SvdStats block_svd<double>(Ctx&, const BTensor<double>&, BTensor<double>&, double, BTensor<double>&, double,
-                                    int, std::vector<double>*, SvdWarm*);
+                                    int, std::vector<double>*);
 template SvdStats block_svd<dcmplex>(Ctx&, const BTensor<dcmplex>&, BTensor<dcmplex>&, double, BTensor<dcmplex>&,
-                                     double, int, std::vector<double>*, SvdWarm*);
+                                     double, int, std::vector<double>*);
 template class Chain<double>;
 template class Chain<dcmplex>;
 

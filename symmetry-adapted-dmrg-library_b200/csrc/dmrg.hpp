@@ -126,24 +126,12 @@ struct SvdStats {
   bool near_tie = false;      // the D-th and (D+1)-th singular values agree to 1e-8 (relative), or a
                               // sector's relative 1e-10 cut-off met a value within two decades of it
   double cut_gap = 1.0;       // (D-th - (D+1)-th singular value) / |psi|; 1 when nothing was cut
-  int warm = 0;               // sectors whose Jacobi started from the previous truncation's V
 };
 
-// Right singular vectors of the last truncation at a bond, kept to start the
-// next one there: one-sided Jacobi converges from any unitary start, and from
-// the previous sweep's V (the state changes little between sweeps) in a few
-// sweeps instead of ~12.  Used per sector, for the sectors whose block has the
-// same dimensions as last time (the others start from the identity).
-struct SvdWarm {
-  struct Sector { int m, n; long long voff; };   // block dims, its V (C x C, C = min(m, n)) in buf
-  std::map<int, Sector> sec;                     // by sector label
-  std::shared_ptr<DevBuf> buf;
-};
-
-// BlockTensor::svd (src/block_tensor_inst.cpp:501-637); warm: see SvdWarm (may be null)
+// BlockTensor::svd (src/block_tensor_inst.cpp:501-637)
 template <class S>
 SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTensor<S>& tv, double p2,
-                   int max_dcut, std::vector<double>* wout, SvdWarm* warm = nullptr);
+                   int max_dcut, std::vector<double>* wout);
 
 struct Timers {
   double lanczos = 0, env = 0, svd = 0, prep = 0;   // host wall time of each phase
@@ -151,7 +139,6 @@ struct Timers {
   double heff_flops = 0;
   double svd_kernel = 0;        // device time of the Jacobi sweep kernels (s)
   long long svd_sweeps = 0;     // Jacobi sweeps, summed over the truncations
-  long long svd_warm = 0;       // sector blocks whose Jacobi started from the previous V at the bond
   double plan = 0;              // host wall time of building H_eff plans (part of lanczos)
 };
 
@@ -210,7 +197,6 @@ class Chain {
   int mlanc_max = 40;
   int prec = PREC_FP64;
   Timers timers;
-  std::map<long long, SvdWarm> svd_warm;   // per two-site bond (il * ns + ir)
   std::mt19937_64 rng{42};  // the reference's generator (src/dense_inst.cpp:23-24)
   std::uniform_real_distribution<double> dist{-1.0, 1.0};
   std::vector<std::string> log;

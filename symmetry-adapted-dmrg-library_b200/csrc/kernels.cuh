@@ -229,13 +229,10 @@ struct SvdJob {
   long long voff;             // accumulated rotations: min(m,n) x min(m,n)
   long long soff;             // singular values (double), min(m,n)
   int m, n, trans;            // trans = 1 when m < n (work on A^H)
-  int preset;                 // W and V hold a starting point already (W = A V0 or A^H V0, V = V0)
 };
 // Host driver: one launch per round of block pairs, one sync per sweep to test
 // convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
 // kernel_ms (optional): device time of the sweep kernel when it ran as one launch.
-// A job with preset = 1 starts from the W and V already in work / vmat (W = A V0,
-// V = V0, V0 unitary) instead of W = A, V = I.
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
                    int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr);
 

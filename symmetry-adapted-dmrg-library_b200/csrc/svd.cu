@@ -514,8 +514,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
   }
 }
 
-// W = A (m >= n) or A^H (m < n); V = I.  A preset job holds its start already
-// (W = A V0, V = V0 for a starting rotation V0); only its column order is set.
+// W = A (m >= n) or A^H (m < n); V = I
 template <bool CPLX>
 __global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm) {
   using T = typename SvdT<CPLX>::T;
@@ -526,7 +525,6 @@ __global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work
   T* V = static_cast<T*>(vmat) + J.voff;
   if (blockIdx.y == 0)
     for (int c = threadIdx.x; c < C; c += blockDim.x) perm[J.soff + c] = c;
-  if (J.preset) return;
   for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)R * C;
        e += (long long)blockDim.x * gridDim.y) {
     const int r = (int)(e % R), c = (int)(e / R);

@@ -553,10 +553,10 @@ class Handle:
         return [int(x) for x in f]
 
     def chain_stats(self):
-        out = np.zeros(15)
-        self._check(self.lib.sadmrg_chain_stats(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), 15), "chain_stats")
+        out = np.zeros(14)
+        self._check(self.lib.sadmrg_chain_stats(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), 14), "chain_stats")
         keys = ["lanczos_s", "env_s", "svd_s", "prep_s", "matvecs", "heff_flops", "gemm_flops", "launches",
-                "discarded", "near_ties", "svd_kernel_s", "svd_sweeps", "plan_s", "stop_ties", "svd_warm"]
+                "discarded", "near_ties", "svd_kernel_s", "svd_sweeps", "plan_s", "stop_ties"]
         return dict(zip(keys, out.tolist()))
 
     def chain_set_tensor(self, kind: int, site: int, k: int, t: Optional[BlockTensorData]):
