@@ -14,9 +14,10 @@ product in one grouped launch per stage, replayed from a captured CUDA graph),
 with the L2 flushed before each step.  Next to it: the FP64 matvec, the matvec
 end to end through the C ABI with pinned host buffers, the roofline of the
 dominant launch, the reference CPU build on the same files (cpu_baseline), and
-(unless --no-sweeps) the SU(2) Heisenberg chain L = 100, D = 512: GPU iDMRG,
+(unless --no-sweeps) the SU(2) Heisenberg chain L = 100 at D = 512 (GPU iDMRG,
 then 8 FP64 and 8 mixed-precision sweeps from the same checkpoint, with the
-energy difference after every sweep.
+energy difference after every sweep) and at D = 2048 multiplets (2 sweeps in
+each precision from one iDMRG checkpoint, and its centre matvec timed in both).
 
 Other workloads (--workload): chain configurations (iDMRG on the GPU, sweeps in
 FP64 and mixed precision from one checkpoint, then the centre problem frozen and
@@ -84,6 +85,8 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "su2_ladder_2x32_D2048"
 SWEEPS_EXTRA = "su2_heisenberg_L100_D512"   # the sweeps a default run adds
+TARGET_EXTRA = "su2_heisenberg_L100_D2048"   # and the D = 2048 sweeps with their centre matvec
+TARGET_SWEEPS = 2
 
 
 def parse(argv=None):
@@ -624,6 +627,26 @@ def run_ours(a, wl: dict, ws: int, rank: int, local: int, cores: int):
         wl2 = WORKLOADS[SWEEPS_EXTRA]
         _, _, meta = chain_sweeps(wl2, local, wl2["sweeps"], None, keep=False)
         line["sweeps_" + SWEEPS_EXTRA] = {"config": chain_config(SWEEPS_EXTRA, wl2, wl2["sweeps"])} | meta
+        # the target: SU(2) Heisenberg L = 100 at D = 2048 multiplets, FP64 and mixed sweeps from one
+        # iDMRG checkpoint, then the centre matvec in both precisions (L2 flushed before each)
+        wl3 = WORKLOADS[TARGET_EXTRA]
+        h3, psi3, meta3 = chain_sweeps(wl3, local, TARGET_SWEEPS, None, keep=True)
+        x3 = torch.from_numpy(np.ascontiguousarray(psi3.data)).to("cuda")
+        y3 = torch.empty_like(x3)
+        for prec in (sadmrg.PREC_FP64, sadmrg.PREC_TF32X3):
+            h3.heff_graph_steps(prec, 3, x3.data_ptr(), y3.data_ptr(), flush.data_ptr(), FLUSH_BYTES)
+        m3 = h3.heff_graph_steps(sadmrg.PREC_TF32X3, 10, x3.data_ptr(), y3.data_ptr(), flush.data_ptr(), FLUSH_BYTES)
+        f3 = h3.heff_graph_steps(sadmrg.PREC_FP64, 10, x3.data_ptr(), y3.data_ptr(), flush.data_ptr(), FLUSH_BYTES)
+        i3 = h3.heff_info()
+        line["target_" + TARGET_EXTRA] = {
+            "config": chain_config(TARGET_EXTRA, wl3, TARGET_SWEEPS),
+            "centre_matvec": {"psi_elems": i3["n"], "flops": i3["flops"], "tasks": i3["ntasks"],
+                              "mixed_ms": float(m3.mean()), "fp64_ms": float(f3.mean()),
+                              "mixed_tflops": i3["flops"] / (float(m3.mean()) * 1e-3) / 1e12,
+                              "fp64_tflops": i3["flops"] / (float(f3.mean()) * 1e-3) / 1e12,
+                              "speedup_mixed_over_fp64": float(f3.mean() / m3.mean()), "tiles": h3.heff_tiles()},
+        } | meta3
+        h3.close()
     if not a.export:
         shutil.rmtree(export_dir, ignore_errors=True)
     if rank == 0:
