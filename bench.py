@@ -101,6 +101,9 @@ def parse(argv=None):
     ap.add_argument("--no-sweeps", action="store_true", help="frozen workload: skip the chain sweeps it adds")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--export", default=None, help="also write the frozen problem to this directory")
+    ap.add_argument("--tiles", default=None,
+                    help="frozen workload: impose the tcgen05 schedule bn,kc_min,kc_max,ctas_per_sm,one_launch "
+                         "instead of timing candidates (a fixed schedule for profiling)")
     return ap.parse_args(argv)
 
 
@@ -478,6 +481,8 @@ def run_ours(a, wl: dict, ws: int, rank: int, local: int, cores: int):
     if wl["kind"] == "frozen":
         config = make_ladder_centre(wl, export_dir)
         h = sadmrg.Handle(sym=wl["sym"], cplx=wl["cplx"], device=local)
+        if a.tiles:
+            h.set_tiles(*(int(t) for t in a.tiles.split(",")))
         psi = sadmrg.load_exported_problem(h, export_dir)
         info = h.heff_info()
         if int(info["ntasks"]) != config["tasks"] or abs(info["flops"] - config["flops_per_step"]) > 0.5:
