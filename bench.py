@@ -551,7 +551,9 @@ def run_ours(a, wl: dict, ws: int, rank: int, local: int, cores: int):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f).get(a.workload, {})
-        if tj.get("psi_elems") == n and tj.get("flops_per_step") == flops:
+        tl = h.heff_tiles()
+        same_schedule = all(tl.get(k) == v for k, v in tj.get("tiles", {}).items())
+        if tj.get("psi_elems") == n and tj.get("flops_per_step") == flops and same_schedule:
             traffic = tj.get("umma_gemm_matvec" if stage is None else f"umma_gemm_stage{stage}")
     except Exception:
         pass
