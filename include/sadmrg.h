@@ -131,6 +131,16 @@ int sadmrg_heff_set_penalty(sadmrg_handle* h, int nvec, const void* vecs_host, c
  * the life of the process.  Off: fixed heuristics.  The FP64 path is never
  * tuned (its rounding does not depend on a timing). */
 int sadmrg_set_autotune(sadmrg_handle* h, int on);
+/* QR preconditioning of the block SVD (no counterpart in the reference, whose
+ * LAPACK gesvd needs none).  With it the one-sided Jacobi runs on R1^H, where
+ * Q R is a Householder QR of a sector block's columns ordered by decreasing
+ * norm and Q1 R1 one of R^H (Drmac & Veselic 2008), which cuts its sweeps by
+ * about 40%; without it the Jacobi runs on the block itself.  on = 1 (the
+ * default): for calls whose widest block has at least 32 columns (below that
+ * the QRs cost about what they save); 2: always; 0: never.  The truncation
+ * means the same either way: the same singular values and vectors to
+ * rounding. */
+int sadmrg_set_svd_precondition(sadmrg_handle* h, int on);
 /* A fixed tile choice for the H_eff plans made after this call, instead of the
  * autotuner or the heuristics: width 64 or 128 (0 returns to them), fewest slabs
  * per split-K chunk when the tiles cannot fill the GPU (0: no such split), most

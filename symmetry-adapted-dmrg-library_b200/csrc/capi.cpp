@@ -287,6 +287,13 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
 }
 
+int sadmrg_set_svd_precondition(sadmrg_handle* h, int on) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(on >= 0 && on <= 2, SADMRG_ERR_ARG, "set_svd_precondition: 0, 1 or 2");
+    h->ctx.svd_qr = on;
+  });
+}
+
 int sadmrg_set_tiles(sadmrg_handle* h, int bn, int kc_min, int kc_max, int ctas_per_sm, int one_launch) {
   return guard(h, [&]() {
     SADMRG_REQUIRE(bn == 0 || bn == 64 || bn == 128, SADMRG_ERR_ARG, "set_tiles: width must be 0, 64 or 128");

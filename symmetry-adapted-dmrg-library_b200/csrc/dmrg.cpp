@@ -655,7 +655,7 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
   const double tj = now_s();
   const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
-                                    &out.jacobi_kernel_ms);
+                                    &out.jacobi_kernel_ms, c.svd_qr);
   out.jacobi_s = now_s() - tj;
   for (auto& J : jobs) {
     out.max_rows = std::max(out.max_rows, std::max(J.m, J.n));
@@ -667,6 +667,13 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   std::vector<double> hs(stot);
   if (stot > 0) SADMRG_CUDA(cudaMemcpyAsync(hs.data(), sv.get(), sizeof(double) * stot, cudaMemcpyDeviceToHost, c.stream));
   SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  // SADMRG_VERBOSE=2: every block's singular values (in the Jacobi's column order)
+  if (const char* v = std::getenv("SADMRG_VERBOSE"); v && v[0] == '2')
+    for (const SvdJob& J : jobs) {
+      std::fprintf(stderr, "  block %dx%d:", J.m, J.n);
+      for (int k = 0; k < std::min(J.m, J.n); ++k) std::fprintf(stderr, " %.17g", hs[J.soff + k]);
+      std::fprintf(stderr, "\n");
+    }
   // per sector: descending order, relative cut-off 1e-10, cap max_dcut (Dense::svd, src/dense_inst.cpp:497-506)
   std::vector<std::vector<int>> order(jobs.size());
   std::vector<std::vector<double>> ssort(jobs.size());

@@ -232,8 +232,12 @@ struct SvdJob {
 };
 // Host driver: one launch per round of block pairs, one sync per sweep to test
 // convergence.  Returns the sweeps taken, or -1 if max_sweeps was reached.
-// kernel_ms (optional): device time of the sweep kernel when it ran as one launch.
+// kernel_ms (optional): device time of the sweep kernel when it ran as one launch
+// (with the QR preconditioning: plus the QR and the Q application).
+// precondition: Jacobi on R1^H after Householder QRs of the norm-ordered columns
+// and of R^H (fewer sweeps): 0 never, 1 when the widest block has at least 32
+// columns, 2 always; the outputs have the same meaning either way.
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr);
+                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, int precondition = 1);
 
 }  // namespace sadmrg

@@ -16,6 +16,7 @@
 // one-sided Jacobi on small singular values, which the reference's 1e-10
 // relative cut-off depends on.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -514,9 +515,10 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
   }
 }
 
-// W = A (m >= n) or A^H (m < n); V = I
+// W = A (m >= n) or A^H (m < n); V = I (copy = 0: only the column order, when the
+// caller has set W and V itself)
 template <bool CPLX>
-__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm) {
+__global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work, void* vmat, int* perm, int copy) {
   using T = typename SvdT<CPLX>::T;
   const SvdJob J = jobs[blockIdx.x];
   const int R = J.trans ? J.n : J.m, C = J.trans ? J.m : J.n;
@@ -525,6 +527,7 @@ __global__ void jacobi_init_kernel(const SvdJob* jobs, const void* a, void* work
   T* V = static_cast<T*>(vmat) + J.voff;
   if (blockIdx.y == 0)
     for (int c = threadIdx.x; c < C; c += blockDim.x) perm[J.soff + c] = c;
+  if (!copy) return;
   for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)R * C;
        e += (long long)blockDim.x * gridDim.y) {
     const int r = (int)(e % R), c = (int)(e / R);
@@ -561,13 +564,393 @@ __global__ void jacobi_norms_kernel(const SvdJob* jobs, const void* work, double
   }
 }
 
+// ---------------------------------------------------------------------------
+// QR preconditioning (Drmac & Veselic, "New fast and accurate Jacobi SVD
+// algorithm I", SIAM J. Matrix Anal. Appl. 29, 2008): with the columns of
+// W0 = op(A) ordered by decreasing norm (P), W0 = Q R and R^H = Q1 R1 by
+// Householder reflections, and the one-sided Jacobi runs on R1^H (C x C) instead
+// of W0:
+//   R1^H V2 = U2 S  =>  op(A) = (Q U2) S (P Q1 V2)^H,
+// so the outputs keep the meaning they have without preconditioning -- W =
+// Q [R1^H V2; 0] = Q U2 S, the left factor times S, and V = P Q1 V2 -- with no
+// division by S.  The graded rows of R make the Jacobi converge in well under
+// the sweeps it takes on W0 itself.  Each QR is
+// blocked (panels of NB columns, compact WY form H_1 ... H_NB = I - Y T Y^H as in
+// LAPACK's larft): one CTA factors a job's panel in shared memory, then every
+// CTA updates one NB-column tile of a trailing matrix; Q (V1 S) applies the same
+// block reflectors in reverse.  All panels run in one cooperative launch with
+// bounded grid barriers.
+template <bool CPLX> struct QrGeom {
+  static constexpr int NB = CPLX ? 8 : 16;     // panel width
+  static constexpr int RC = 256;               // rows per chunk of a tile update
+  static constexpr int LD = RC + 1;            // shared row stride of a chunk (odd: no bank conflicts)
+  static constexpr int NT = NB * NB;
+  static constexpr int G = kSvdThreads / NT;   // row groups of the Y = V^H X sums
+};
+constexpr size_t kQrSmemMax = 200 * 1024;       // largest panel kept in shared memory
+// Calls whose widest block has fewer columns run the Jacobi directly: it needs a
+// few rounds per sweep there, so the QRs would cost about what they save.  (It
+// also keeps the first steps of an iDMRG warm-up -- blocks of a few columns,
+// some of pure rounding noise, whose kept count the 1e-16 floor of the
+// per-sector cut-off then decides -- on the path of the plain Jacobi.)
+constexpr int kQrMinCols = 32;
+
+struct QrJob {
+  long long aoff;             // input block (m x n, lda m)
+  long long qoff;             // the matrix factored (R x C, ld R), then R above and the reflectors below the diagonal
+  long long toff;             // T factors of the panels, NB x NB each (column-major)
+  long long jwoff, jvoff;     // the Jacobi's W = R1^H and V (C x C each)
+  long long woff, voff, soff; // outputs as in SvdJob; for a Q application: the matrix it multiplies (ld R)
+  int m, n, trans, R, C;
+  int x_in_q;                 // Q application: the matrix is in the QR buffer (1) or in the output W (0)
+};
+struct QrTile {
+  int job, c1;                // a tile of NB columns starting at column c1
+};
+
+__device__ __forceinline__ double cabs2(double a) { return a * a; }
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double cim(double) { return 0.0; }
+__device__ __forceinline__ double cim(double2 a) { return a.y; }
+__device__ __forceinline__ double csub(double a, double b) { return a - b; }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+template <class T> __device__ __forceinline__ T cmake(double re, double im);
+template <> __device__ __forceinline__ double cmake<double>(double re, double) { return re; }
+template <> __device__ __forceinline__ double2 cmake<double2>(double re, double im) { return make_double2(re, im); }
+__device__ __forceinline__ double wsum_t(double v) { return wsum(v); }
+__device__ __forceinline__ double2 wsum_t(double2 v) { return make_double2(wsum(v.x), wsum(v.y)); }
+__device__ __forceinline__ double cscale(double a, double s) { return a * s; }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// column c of op(A) at row r: A(r, c), or conj(A(c, r)) when the job works on A^H
+template <class T>
+__device__ __forceinline__ T op_a(const T* A, int m, int trans, int r, int c) {
+  return trans ? cconj(A[c + (long long)r * m]) : A[r + (long long)c * m];
+}
+
+// Column norms of op(A) and their order (decreasing, ties by index): P.
+template <bool CPLX>
+__global__ void qr_order_kernel(const QrJob* jobs, const void* a, double* nrm, int* perm) {
+  using T = typename SvdT<CPLX>::T;
+  const QrJob J = jobs[blockIdx.x];
+  const T* A = static_cast<const T*>(a) + J.aoff;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* nj = nrm + J.soff;
+  for (int c = warp; c < J.C; c += nw) {
+    double s = 0.0;
+    for (int r = lane; r < J.R; r += 32) s += cabs2(op_a(A, J.m, J.trans, r, c));
+    s = wsum(s);
+    if (lane == 0) nj[c] = s;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < J.C; c += blockDim.x) {
+    const double v = nj[c];
+    int rank = 0;
+    for (int k = 0; k < J.C; ++k) {
+      const double u = nj[k];
+      rank += (u > v || (u == v && k < c)) ? 1 : 0;
+    }
+    perm[J.soff + rank] = c;
+  }
+}
+
+// W0 = op(A) P
+template <bool CPLX>
+__global__ void qr_gather_kernel(const QrJob* jobs, const void* a, void* qbuf, const int* perm) {
+  using T = typename SvdT<CPLX>::T;
+  const QrJob J = jobs[blockIdx.x];
+  const T* A = static_cast<const T*>(a) + J.aoff;
+  T* W = static_cast<T*>(qbuf) + J.qoff;
+  const int* p = perm + J.soff;
+  for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)J.R * J.C;
+       e += (long long)blockDim.x * gridDim.y) {
+    const int r = (int)(e % J.R), i = (int)(e / J.R);
+    W[e] = op_a(A, J.m, J.trans, r, p[i]);
+  }
+}
+
+// Panel k of job J: Householder reflections of its NB columns (rows k NB .. R-1)
+// in shared memory (LAPACK larfg: beta = -sign(Re alpha) |x|, tau = (beta -
+// alpha) / beta, v = x / (alpha - beta) below the unit diagonal; no reflection
+// when the column below the diagonal is zero and alpha is real), each applied as
+// H^H to the panel's later columns; then T of the compact WY form (forward,
+// columnwise).  Writes R's panel rows, the reflectors and T back.
+template <bool CPLX>
+__device__ void qr_panel(const QrJob& J, int k, void* qbuf, unsigned char* smem) {
+  using T = typename SvdT<CPLX>::T;
+  constexpr int NB = QrGeom<CPLX>::NB;
+  const int r0 = k * NB, nr = J.R - r0, w = min(NB, J.C - r0);
+  T* A = static_cast<T*>(qbuf) + J.qoff;
+  T* P = reinterpret_cast<T*>(smem);   // nr x w, column-major, ld nr
+  __shared__ T tau_sh[NB];
+  __shared__ T S_sh[NB * NB];          // S(k, j) = v_k^H v_j, k < j
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < nr * w; e += blockDim.x) {
+    const int i = e % nr, l = e / nr;
+    P[e] = A[(r0 + i) + (long long)(r0 + l) * J.R];
+  }
+  __syncthreads();
+  for (int j = 0; j < w; ++j) {
+    T* x = P + (long long)j * nr;
+    if (warp == 0) {
+      double s2 = 0.0;
+      for (int i = j + 1 + lane; i < nr; i += 32) s2 += cabs2(x[i]);
+      s2 = wsum(s2);
+      const T alpha = x[j];
+      T tau = czero<T>();
+      const bool refl = s2 > 0.0 || cim(alpha) != 0.0;
+      double beta = 0.0;
+      if (refl) {
+        beta = -copysign(sqrt(cabs2(alpha) + s2), cre(alpha));
+        tau = cmake<T>((beta - cre(alpha)) / beta, -cim(alpha) / beta);
+        // 1 / (alpha - beta)
+        T scale;
+        if constexpr (CPLX) {
+          const double dr = alpha.x - beta, di = alpha.y, dd = 1.0 / (dr * dr + di * di);
+          scale = make_double2(dr * dd, -di * dd);
+        } else {
+          scale = 1.0 / (alpha - beta);
+        }
+        for (int i = j + 1 + lane; i < nr; i += 32) x[i] = cmul(x[i], scale);
+      }
+      __syncwarp();
+      if (lane == 0) {
+        tau_sh[j] = tau;
+        if (refl) x[j] = cmake<T>(beta, 0.0);
+      }
+    }
+    __syncthreads();
+    const T tau = tau_sh[j];
+    if (warp < w - 1 - j && cabs2(tau) != 0.0) {
+      T* y = P + (long long)(j + 1 + warp) * nr;
+      T d = lane == 0 ? y[j] : czero<T>();   // v_j = 1
+      for (int i = j + 1 + lane; i < nr; i += 32) d = cadd(d, cj_mul(x[i], y[i]));
+      d = wsum_t(d);
+      const T f = cmul(cconj(tau), d);
+      if (lane == 0) y[j] = csub(y[j], f);
+      for (int i = j + 1 + lane; i < nr; i += 32) y[i] = csub(y[i], cmul(x[i], f));
+    }
+    __syncthreads();
+  }
+  // S(q, j) = v_q^H v_j for q < j (rows j .. nr-1; v_j(j) = 1, v_q(j) = P(j, q))
+  for (int pr = warp; pr < w * w; pr += kSvdWarps) {
+    const int q = pr / w, j = pr % w;
+    if (q >= j) continue;
+    const T* vq = P + (long long)q * nr;
+    const T* vj = P + (long long)j * nr;
+    T d = lane == 0 ? cconj(vq[j]) : czero<T>();
+    for (int i = j + 1 + lane; i < nr; i += 32) d = cadd(d, cj_mul(vq[i], vj[i]));
+    d = wsum_t(d);
+    if (lane == 0) S_sh[q + j * NB] = d;
+  }
+  __syncthreads();
+  // T: T(j, j) = tau_j, T(0:j, j) = -tau_j T(0:j, 0:j) S(0:j, j)
+  T* Tm = static_cast<T*>(qbuf) + J.toff + (long long)k * NB * NB;
+  if (warp == 0) {
+    __shared__ T T_sh[NB * NB];
+    for (int e = lane; e < NB * NB; e += 32) T_sh[e] = czero<T>();
+    __syncwarp();
+    for (int j = 0; j < w; ++j) {
+      const T tj = tau_sh[j];
+      T v = czero<T>();
+      if (lane < j) {
+        for (int q = lane; q < j; ++q) v = cadd(v, cmul(T_sh[lane + q * NB], S_sh[q + j * NB]));
+        v = cmul(cscale(tj, -1.0), v);
+      }
+      __syncwarp();
+      if (lane < j) T_sh[lane + j * NB] = v;
+      if (lane == j) T_sh[j + j * NB] = tj;
+      __syncwarp();
+    }
+    for (int e = lane; e < NB * NB; e += 32) Tm[e] = T_sh[e];
+  }
+  for (int e = tid; e < nr * w; e += blockDim.x) {
+    const int i = e % nr, l = e / nr;
+    A[(r0 + i) + (long long)(r0 + l) * J.R] = P[e];
+  }
+  __syncthreads();   // P, tau_sh and S_sh are reused by the next panel this CTA takes
+}
+
+// X(r0:R, c1:c1+tw) <- H X with H = I - Y T Y^H (adj = 0) or H^H = I - Y T^H Y^H
+// (adj = 1), Y = the unit lower trapezoidal reflectors of panel k.  Two passes
+// over row chunks: Z = T' (Y^H X), then X -= Y Z (a single chunk stays in shared
+// memory between the passes).
+template <bool CPLX>
+__device__ void qr_apply_tile(const QrJob& J, int k, int c1, int ncols, int adj, const void* qbuf, void* xbase,
+                              long long xoff, unsigned char* smem) {
+  using T = typename SvdT<CPLX>::T;
+  using Gm = QrGeom<CPLX>;
+  constexpr int NB = Gm::NB, RC = Gm::RC, LD = Gm::LD, NT = Gm::NT, G = Gm::G;
+  const int r0 = k * NB, nr = J.R - r0, w = min(NB, J.C - r0), tw = min(NB, ncols - c1);
+  const T* A = static_cast<const T*>(qbuf) + J.qoff;
+  const T* Tm = static_cast<const T*>(qbuf) + J.toff + (long long)k * NB * NB;
+  T* X = static_cast<T*>(xbase) + xoff;
+  T* Vs = reinterpret_cast<T*>(smem);      // RC x NB (ld LD)
+  T* Xs = Vs + LD * NB;                    // RC x NB (ld LD)
+  T* Yp = Xs + LD * NB;                    // G partial sums of Y (NB x NB each)
+  T* Zs = Yp + G * NT;                     // Z (NB x NB)
+  const int tid = threadIdx.x;
+  const int g = tid / NT, l = (tid % NT) / NB, t = tid % NB;
+  const int nch = (nr + RC - 1) / RC;
+  auto load = [&](int rr0, int rows) {
+    for (int e = tid; e < RC * NB; e += kSvdThreads) {
+      const int i = e % RC, c = e / RC, gi = rr0 + i;
+      T v = czero<T>(), x = czero<T>();
+      if (i < rows) {
+        if (c < w) v = gi < c ? czero<T>() : (gi == c ? cmake<T>(1.0, 0.0) : A[(r0 + gi) + (long long)(r0 + c) * J.R]);
+        if (c < tw) x = X[(r0 + gi) + (long long)(c1 + c) * J.R];
+      }
+      Vs[i + c * LD] = v;
+      Xs[i + c * LD] = x;
+    }
+  };
+  T acc = czero<T>();
+  for (int ch = 0; ch < nch; ++ch) {
+    const int rr0 = ch * RC, rows = min(RC, nr - rr0);
+    load(rr0, rows);
+    __syncthreads();
+    for (int i = g; i < rows; i += G) acc = cadd(acc, cj_mul(Vs[i + l * LD], Xs[i + t * LD]));
+    __syncthreads();
+  }
+  Yp[g * NT + l * NB + t] = acc;
+  __syncthreads();
+  if (tid < NT) {
+    T y = czero<T>();
+    for (int q = 0; q < G; ++q) y = cadd(y, Yp[q * NT + l * NB + t]);
+    Zs[l * NB + t] = y;   // Y(l, t), row-major
+  }
+  __syncthreads();
+  T z = czero<T>();
+  if (tid < NT) {
+    // Z(l, t) = sum_q T'(l, q) Y(q, t), T' = T (upper) or T^H (lower)
+    for (int q = 0; q < w; ++q) {
+      const T tq = adj ? cconj(Tm[q + l * NB]) : Tm[l + q * NB];
+      z = cadd(z, cmul(tq, Zs[q * NB + t]));
+    }
+  }
+  __syncthreads();
+  if (tid < NT) Zs[l * NB + t] = z;
+  __syncthreads();
+  for (int ch = 0; ch < nch; ++ch) {
+    const int rr0 = ch * RC, rows = min(RC, nr - rr0);
+    if (nch > 1) {
+      load(rr0, rows);
+      __syncthreads();
+    }
+    for (int e = tid; e < RC * NB; e += kSvdThreads) {
+      const int i = e % RC, c = e / RC;
+      if (i >= rows || c >= tw) continue;
+      T x = Xs[i + c * LD];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) x = csub(x, cmul(Vs[i + q * LD], Zs[q * NB + c]));
+      X[(r0 + rr0 + i) + (long long)(c1 + c) * J.R] = x;
+    }
+    __syncthreads();
+  }
+}
+
+template <bool CPLX>
+constexpr size_t qr_tile_smem() {
+  using Gm = QrGeom<CPLX>;
+  return (size_t)(2 * Gm::LD * Gm::NB + Gm::G * Gm::NT + Gm::NT) * (CPLX ? 16 : 8);
+}
+
+// The blocked QR of every job: step k factors panel k of every job that has one,
+// then updates every NB-column tile right of it; a bounded grid barrier after
+// each phase.
+template <bool CPLX>
+__global__ void __launch_bounds__(kSvdThreads) qr_coop_kernel(const QrJob* __restrict__ jobs,
+                                                              const int* __restrict__ panels, const int* __restrict__ poff,
+                                                              const QrTile* __restrict__ tiles, const int* __restrict__ toff,
+                                                              int steps, void* qbuf, SvdCtl* ctl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->t0 = svd_gtime();
+  for (int k = 0; k < steps; ++k) {
+    for (int p = poff[k] + blockIdx.x; p < poff[k + 1]; p += gridDim.x) qr_panel<CPLX>(jobs[panels[p]], k, qbuf, smem_raw);
+    if (!svd_grid_sync(ctl)) return;
+    for (int t = toff[k] + blockIdx.x; t < toff[k + 1]; t += gridDim.x) {
+      const QrTile tl = tiles[t];
+      const QrJob& J = jobs[tl.job];
+      qr_apply_tile<CPLX>(J, k, tl.c1, J.C, 1, qbuf, qbuf, J.qoff, smem_raw);
+    }
+    if (!svd_grid_sync(ctl)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->t1 = svd_gtime();
+}
+
+// X <- Q X for every job: its block reflectors applied from the last panel to
+// the first to X (R x C at woff, in the output W or in the QR buffer).
+template <bool CPLX>
+__global__ void __launch_bounds__(kSvdThreads) qr_unmq_kernel(const QrJob* __restrict__ jobs,
+                                                              const QrTile* __restrict__ tiles, const int* __restrict__ toff,
+                                                              int steps, void* qbuf, void* out, SvdCtl* ctl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->t0 = svd_gtime();
+  for (int k = steps - 1; k >= 0; --k) {
+    for (int t = toff[k] + blockIdx.x; t < toff[k + 1]; t += gridDim.x) {
+      const QrTile tl = tiles[t];
+      const QrJob& J = jobs[tl.job];
+      qr_apply_tile<CPLX>(J, k, tl.c1, J.C, 0, qbuf, J.x_in_q ? qbuf : out, J.woff, smem_raw);
+    }
+    if (k > 0 && !svd_grid_sync(ctl)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->t1 = svd_gtime();
+}
+
+// R^H (lower triangular, C x C) of src's factor into dst's matrix to factor
+// (to_jacobi = 0), or into dst's Jacobi W with V = I (to_jacobi = 1).
+template <bool CPLX>
+__global__ void qr_rh_kernel(const QrJob* src, const QrJob* dst, void* qbuf, int to_jacobi) {
+  using T = typename SvdT<CPLX>::T;
+  const QrJob S = src[blockIdx.x], D = dst[blockIdx.x];
+  const T* A = static_cast<const T*>(qbuf) + S.qoff;
+  T* W = static_cast<T*>(qbuf) + (to_jacobi ? D.jwoff : D.qoff);
+  T* V = static_cast<T*>(qbuf) + D.jvoff;
+  const int C = S.C;
+  for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)C * C;
+       e += (long long)blockDim.x * gridDim.y) {
+    const int r = (int)(e % C), c = (int)(e / C);
+    W[e] = r >= c ? cconj(A[c + (long long)r * S.R]) : czero<T>();
+    if (to_jacobi) V[e] = cmake<T>(r == c ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// Before the Q applications: the output W = [R1^H V2; 0] (R x C).
+template <bool CPLX>
+__global__ void qr_wout_kernel(const QrJob* jobs, const void* qbuf, void* work) {
+  using T = typename SvdT<CPLX>::T;
+  const QrJob J = jobs[blockIdx.x];
+  const T* Wj = static_cast<const T*>(qbuf) + J.jwoff;
+  T* W = static_cast<T*>(work) + J.woff;
+  for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)J.R * J.C;
+       e += (long long)blockDim.x * gridDim.y) {
+    const int r = (int)(e % J.R), c = (int)(e / J.R);
+    W[e] = r < J.C ? Wj[r + (long long)c * J.C] : czero<T>();
+  }
+}
+
+// After them: the output V = P (Q1 V2), rows put back in the order of op(A)'s columns.
+template <bool CPLX>
+__global__ void qr_vout_kernel(const QrJob* jobs, const void* qbuf, void* vmat, const int* perm) {
+  using T = typename SvdT<CPLX>::T;
+  const QrJob J = jobs[blockIdx.x];
+  const T* Vj = static_cast<const T*>(qbuf) + J.jvoff;
+  T* V = static_cast<T*>(vmat) + J.voff;
+  const int* p = perm + J.soff;
+  for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < (long long)J.C * J.C;
+       e += (long long)blockDim.x * gridDim.y) {
+    const int i = (int)(e % J.C), c = (int)(e / J.C);
+    V[p[i] + (long long)c * J.C] = Vj[e];
+  }
+}
+
 // Host driver.  Runs all sweeps in one cooperative launch when the device allows
 // it, otherwise one launch per round and one host synchronisation per sweep to
 // test convergence.  Returns the number of sweeps taken (or -1 when max_sweeps
 // was reached).
 template <bool CPLX, int B>
 static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                      int max_sweeps, cudaStream_t s, double* kernel_ms) {
+                      int max_sweeps, cudaStream_t s, double* kernel_ms, int copy = 1) {
   const int nj = (int)hjobs.size();
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
@@ -612,7 +995,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
   SADMRG_CUDA(cudaMemcpyAsync(djobs.get(), hjobs.data(), sizeof(SvdJob) * nj, cudaMemcpyHostToDevice, s));
   SADMRG_CUDA(cudaMemcpyAsync(dpairs.get(), flat.data(), sizeof(SvdPair) * flat.size(), cudaMemcpyHostToDevice, s));
   dim3 ig(nj, 16);
-  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>());
+  jacobi_init_kernel<CPLX><<<ig, 256, 0, s>>>(djobs.as<SvdJob>(), a, work, vmat, dperm.as<int>(), copy);
   SADMRG_CUDA(cudaGetLastError());
   SADMRG_CUDA(cudaFuncSetAttribute(jacobi_pair_kernel<CPLX, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const double tol = std::sqrt((double)std::max(maxR, 1)) * 2.220446049250313e-16;
@@ -677,15 +1060,9 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
   return sweeps;
 }
 
-int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms) {
-  if (kernel_ms) *kernel_ms = -1.0;
-  if (hjobs.empty()) return 0;
-  // column blocks of 16, or of 8 when the widest round of 16-column pairs would
-  // keep fewer than half the SMs busy: narrower pairs double the CTAs per round
-  // and cut each visit's work to a quarter, which wins while SMs are idle (D=512:
-  // 1.87 -> 1.65 s of SVD per sweep) and loses once they are not (complex D=2048:
-  // 4.8 -> 5.5 s per iDMRG)
+// Column blocks of the Jacobi for these jobs: 8 when the widest round of
+// 16-column pairs would keep fewer than half the SMs busy, else 16.
+static bool narrow_blocks(const std::vector<SvdJob>& hjobs) {
   int dev = 0, nsm = 0;
   SADMRG_CUDA(cudaGetDevice(&dev));
   SADMRG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -695,7 +1072,214 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     const int nb = (C + 15) / 16;
     pairs16 += nb <= 1 ? 1 : nb / 2;
   }
-  const bool narrow = 2 * pairs16 < nsm;
+  return 2 * pairs16 < nsm;
+}
+
+// Launches a cooperative kernel on the largest grid the device keeps resident,
+// capped at `want` CTAs.  Returns false (nothing launched) when it cannot.
+static bool coop_launch(const void* fn, int want, size_t smem, void** args, cudaStream_t s) {
+  int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+  SADMRG_CUDA(cudaGetDevice(&dev));
+  SADMRG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  SADMRG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  SADMRG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SADMRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSvdThreads, smem));
+  if (!coop || per_sm <= 0) return false;
+  const int grid = std::max(1, std::min(want, per_sm * nsm));
+  SADMRG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSvdThreads), args, smem, s));
+  return true;
+}
+
+// Per-step work lists of a set of QrJobs: the panels and trailing tiles of the
+// QR (qr_coop_kernel), or the tiles of a Q application (qr_unmq_kernel).
+struct QrLists {
+  std::vector<int> panels, poff, toff;
+  std::vector<QrTile> tiles;
+  int steps = 0, want = 1;
+};
+template <int NB>
+static QrLists qr_lists(const std::vector<QrJob>& jobs, bool unmq) {
+  QrLists L;
+  for (const QrJob& J : jobs) L.steps = std::max(L.steps, (J.C + NB - 1) / NB);
+  L.poff.assign(L.steps + 1, 0);
+  L.toff.assign(L.steps + 1, 0);
+  for (int k = 0; k < L.steps; ++k) {
+    L.poff[k] = (int)L.panels.size();
+    L.toff[k] = (int)L.tiles.size();
+    for (int j = 0; j < (int)jobs.size(); ++j) {
+      if (jobs[j].C <= k * NB) continue;
+      if (!unmq) L.panels.push_back(j);
+      for (int c1 = unmq ? 0 : (k + 1) * NB; c1 < jobs[j].C; c1 += NB) L.tiles.push_back({j, c1});
+    }
+    L.want = std::max({L.want, (int)L.panels.size() - L.poff[k], (int)L.tiles.size() - L.toff[k]});
+  }
+  L.poff[L.steps] = (int)L.panels.size();
+  L.toff[L.steps] = (int)L.tiles.size();
+  return L;
+}
+
+// Device copies of a job array and its lists, and the cooperative launch of the
+// QR (unmq = false) or of the Q application (unmq = true).  Returns false when
+// the device cannot run it cooperatively.
+template <bool CPLX>
+struct QrLaunch {
+  DevBuf dj, dpan, dpoff, dtl, dtoff;
+  QrLists L;
+  bool run(const std::vector<QrJob>& jobs, bool unmq, void* qbuf, void* out, SvdCtl* ctl, cudaStream_t s) {
+    constexpr int NB = QrGeom<CPLX>::NB;
+    L = qr_lists<NB>(jobs, unmq);
+    int maxR = 0;
+    for (const QrJob& J : jobs) maxR = std::max(maxR, J.R);
+    dj.alloc(sizeof(QrJob) * jobs.size(), s);
+    dpan.alloc(sizeof(int) * std::max<size_t>(L.panels.size(), 1), s);
+    dpoff.alloc(sizeof(int) * (L.steps + 1), s);
+    dtl.alloc(sizeof(QrTile) * std::max<size_t>(L.tiles.size(), 1), s);
+    dtoff.alloc(sizeof(int) * (L.steps + 1), s);
+    SADMRG_CUDA(cudaMemcpyAsync(dj.get(), jobs.data(), sizeof(QrJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    if (!L.panels.empty())
+      SADMRG_CUDA(cudaMemcpyAsync(dpan.get(), L.panels.data(), sizeof(int) * L.panels.size(), cudaMemcpyHostToDevice, s));
+    if (!L.tiles.empty())
+      SADMRG_CUDA(cudaMemcpyAsync(dtl.get(), L.tiles.data(), sizeof(QrTile) * L.tiles.size(), cudaMemcpyHostToDevice, s));
+    SADMRG_CUDA(cudaMemcpyAsync(dpoff.get(), L.poff.data(), sizeof(int) * (L.steps + 1), cudaMemcpyHostToDevice, s));
+    SADMRG_CUDA(cudaMemcpyAsync(dtoff.get(), L.toff.data(), sizeof(int) * (L.steps + 1), cudaMemcpyHostToDevice, s));
+    const QrJob* pj = dj.as<QrJob>();
+    const int* pp = dpan.as<int>();
+    const int* ppo = dpoff.as<int>();
+    const QrTile* pt = dtl.as<QrTile>();
+    const int* pto = dtoff.as<int>();
+    int st = L.steps;
+    void* qb = qbuf;
+    void* o = out;
+    SvdCtl* pc = ctl;
+    if (unmq) {
+      void* args[] = {(void*)&pj, (void*)&pt, (void*)&pto, (void*)&st, (void*)&qb, (void*)&o, (void*)&pc};
+      return coop_launch((const void*)qr_unmq_kernel<CPLX>, L.want, qr_tile_smem<CPLX>(), args, s);
+    }
+    const size_t smem = std::max((size_t)maxR * NB * sizeof(typename SvdT<CPLX>::T), qr_tile_smem<CPLX>());
+    void* args[] = {(void*)&pj, (void*)&pp, (void*)&ppo, (void*)&pt, (void*)&pto, (void*)&st, (void*)&qb, (void*)&pc};
+    return coop_launch((const void*)qr_coop_kernel<CPLX>, L.want, smem, args, s);
+  }
+};
+
+// The QR-preconditioned SVD (see the QR preconditioning notes above).  Returns
+// the Jacobi sweeps (as jacobi_run), or 0 with *fallback set when the device
+// cannot run the cooperative kernels (the call then runs without
+// preconditioning).
+template <bool CPLX>
+static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
+                         int max_sweeps, cudaStream_t s, double* kernel_ms, bool* fallback) {
+  using T = typename SvdT<CPLX>::T;
+  constexpr int NB = QrGeom<CPLX>::NB;
+  *fallback = false;
+  const int nj = (int)hjobs.size();
+  // q1: op(A) P = Q R (R x C); q2: R^H = Q1 R1 (C x C), whose Jacobi W = R1^H and V
+  // live at jwoff / jvoff; the second Q application multiplies that V
+  std::vector<QrJob> q1(nj), q2(nj);
+  long long tot = 0, nsv = 1;
+  for (int j = 0; j < nj; ++j) {
+    const SvdJob& J = hjobs[j];
+    const int R = std::max(J.m, J.n), C = std::min(J.m, J.n), np = (C + NB - 1) / NB;
+    QrJob& A = q1[j];
+    QrJob& B = q2[j];
+    A = QrJob{};
+    A.aoff = J.aoff; A.woff = J.woff; A.voff = J.voff; A.soff = J.soff;
+    A.m = J.m; A.n = J.n; A.trans = J.trans; A.R = R; A.C = C; A.x_in_q = 0;
+    A.qoff = tot;  tot += (long long)R * C;
+    A.toff = tot;  tot += (long long)np * NB * NB;
+    B = A;
+    B.m = B.n = B.R = C; B.trans = 0;
+    B.qoff = tot;  tot += (long long)C * C;
+    B.toff = tot;  tot += (long long)np * NB * NB;
+    A.jwoff = B.jwoff = tot; tot += (long long)C * C;
+    A.jvoff = B.jvoff = tot; tot += (long long)C * C;
+    B.woff = B.jvoff;   // the second Q application multiplies the Jacobi's V
+    B.x_in_q = 1;
+    nsv = std::max<long long>(nsv, J.soff + C);
+  }
+  DevBuf qbuf(sizeof(T) * std::max<long long>(tot, 1), s), dperm(sizeof(int) * nsv, s), dctl(3 * sizeof(SvdCtl), s);
+  SADMRG_CUDA(cudaMemsetAsync(dctl.get(), 0, 3 * sizeof(SvdCtl), s));
+  SvdCtl* ctl = dctl.as<SvdCtl>();
+  QrLaunch<CPLX> L1, L2, LU;
+  // P and W0 = op(A) P need the job array on the device: the first QR's copy
+  L1.dj.alloc(sizeof(QrJob) * nj, s);
+  SADMRG_CUDA(cudaMemcpyAsync(L1.dj.get(), q1.data(), sizeof(QrJob) * nj, cudaMemcpyHostToDevice, s));
+  qr_order_kernel<CPLX><<<nj, kSvdThreads, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), a, sv, dperm.as<int>());
+  qr_gather_kernel<CPLX><<<dim3(nj, 32), 256, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), a, qbuf.get(), dperm.as<int>());
+  SADMRG_CUDA(cudaGetLastError());
+  if (!L1.run(q1, false, qbuf.get(), work, ctl, s)) {
+    *fallback = true;
+    return 0;
+  }
+  L2.dj.alloc(sizeof(QrJob) * nj, s);
+  SADMRG_CUDA(cudaMemcpyAsync(L2.dj.get(), q2.data(), sizeof(QrJob) * nj, cudaMemcpyHostToDevice, s));
+  qr_rh_kernel<CPLX><<<dim3(nj, 16), 256, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), static_cast<const QrJob*>(L2.dj.get()), qbuf.get(), 0);
+  SADMRG_CUDA(cudaGetLastError());
+  SADMRG_REQUIRE(L2.run(q2, false, qbuf.get(), work, ctl + 1, s), SADMRG_ERR_CUDA,
+                 "svd: the second cooperative QR cannot be launched");
+  qr_rh_kernel<CPLX><<<dim3(nj, 16), 256, 0, s>>>(static_cast<const QrJob*>(L2.dj.get()), static_cast<const QrJob*>(L2.dj.get()), qbuf.get(), 1);
+  SADMRG_CUDA(cudaGetLastError());
+  // the Jacobi on R1^H (C x C, W and V in qbuf)
+  std::vector<SvdJob> jj(nj);
+  for (int j = 0; j < nj; ++j) {
+    SvdJob& J = jj[j];
+    J.aoff = 0;
+    J.woff = q2[j].jwoff;
+    J.voff = q2[j].jvoff;
+    J.soff = q2[j].soff;
+    J.m = J.n = q2[j].C;
+    J.trans = 0;
+  }
+  double jms = -1.0;
+  const int sweeps = narrow_blocks(jj)
+                         ? jacobi_run<CPLX, 8>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0)
+                         : jacobi_run<CPLX, 16>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0);
+  if (sweeps <= 0) return sweeps;
+  // W = Q [R1^H V2; 0] and Q1 V2, both Q applications in one launch, then V = P (Q1 V2)
+  qr_wout_kernel<CPLX><<<dim3(nj, 16), 256, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), qbuf.get(), work);
+  SADMRG_CUDA(cudaGetLastError());
+  std::vector<QrJob> qu(q1);
+  qu.insert(qu.end(), q2.begin(), q2.end());
+  SADMRG_REQUIRE(LU.run(qu, true, qbuf.get(), work, ctl + 2, s), SADMRG_ERR_CUDA,
+                 "svd: the cooperative Q application cannot be launched");
+  qr_vout_kernel<CPLX><<<dim3(nj, 16), 256, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), qbuf.get(), vmat, dperm.as<int>());
+  SADMRG_CUDA(cudaGetLastError());
+  SvdCtl hctl[3];
+  SADMRG_CUDA(cudaMemcpyAsync(hctl, dctl.get(), 3 * sizeof(SvdCtl), cudaMemcpyDeviceToHost, s));
+  SADMRG_CUDA(cudaStreamSynchronize(s));
+  SADMRG_REQUIRE(hctl[0].status == 0 && hctl[1].status == 0 && hctl[2].status == 0, SADMRG_ERR_CUDA,
+                 "svd: a grid barrier of the QR preconditioning ran out of time");
+  if (kernel_ms && jms >= 0.0) {
+    *kernel_ms = jms;
+    for (const SvdCtl& c : hctl) *kernel_ms += (double)(c.t1 - c.t0) * 1e-6;
+  }
+  return sweeps;
+}
+
+int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
+                   int max_sweeps, cudaStream_t s, double* kernel_ms, int precondition) {
+  if (kernel_ms) *kernel_ms = -1.0;
+  if (hjobs.empty()) return 0;
+  if (precondition) {
+    // the panel of the tallest block must fit in shared memory
+    int maxR = 0, maxC = 0;
+    for (const SvdJob& J : hjobs) {
+      maxR = std::max(maxR, std::max(J.m, J.n));
+      maxC = std::max(maxC, std::min(J.m, J.n));
+    }
+    const size_t panel = (size_t)maxR * (cplx ? QrGeom<true>::NB * 16 : QrGeom<false>::NB * 8);
+    if (panel <= kQrSmemMax && (maxC >= kQrMinCols || precondition == 2)) {
+      bool fallback = false;
+      const int sw = cplx ? qr_jacobi_run<true>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback)
+                          : qr_jacobi_run<false>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback);
+      if (!fallback) return sw;
+    }
+  }
+  // column blocks of 16, or of 8 when the widest round of 16-column pairs would
+  // keep fewer than half the SMs busy: narrower pairs double the CTAs per round
+  // and cut each visit's work to a quarter, which wins while SMs are idle (D=512:
+  // 1.87 -> 1.65 s of SVD per sweep) and loses once they are not (complex D=2048:
+  // 4.8 -> 5.5 s per iDMRG)
+  const bool narrow = narrow_blocks(hjobs);
   if (cplx)
     return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
                   : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);

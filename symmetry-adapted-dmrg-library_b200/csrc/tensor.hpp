@@ -57,6 +57,9 @@ struct Ctx {
   static constexpr double kAutoFuseFlops = 4e9;
   // time tile candidates for every new H_eff plan (1) or use the heuristics (0)
   int autotune = 1;
+  // block SVD: Householder QRs before the Jacobi: 0 never, 1 for calls whose widest
+  // block has at least 32 columns, 2 always
+  int svd_qr = 1;
   // a tile choice every new H_eff plan takes instead (bn > 0), e.g. to profile one
   UmmaTune forced_tune;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
