@@ -70,6 +70,34 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// 2^-k for a normal double m = 2^k (1 + f): m times it lies in [1, 2) (built from the
+// exponent bits, exact)
+__device__ __forceinline__ double pow2_scale_of(double m) {
+  const int e = (__double2hiint(m) >> 20) & 0x7ff;
+  return __hiloint2double((2046 - e) << 20, 0);
+}
+// The one-sided rotation of a pair with squared norms a, b and |<w_p, w_q>| = g > 0,
+// as on the columns themselves: t = tan(theta) = 2 g sgn(d) / (|d| + r) with d = b - a,
+// r = sqrt(d^2 + 4 g^2).  With u = |d| + r and q = 1 / sqrt(2 r u) (since
+// 1 + t^2 = 2 r / u): c = cos(theta) = u q, s = sin(theta) = 2 g q sgn(d) and
+// t = 4 g r q^2 sgn(d) -- two inverse square roots and no division on the chain
+// that sets the time of an inner round.  d and g are first scaled by a power of two
+// (the larger of |d| and 2 g into [1, 2)), so that the squares neither overflow nor
+// underflow; c, s and t do not depend on the scale.  Returns c, s and t g.
+__device__ __forceinline__ void jacobi_rotation(double a, double b, double g, double& c, double& s, double& tg) {
+  const double d = b - a;
+  const double sc = pow2_scale_of(fmax(fabs(d), 2.0 * g));
+  const double dn = d * sc, gn = g * sc;
+  const double x = fma(dn, dn, 4.0 * gn * gn);
+  const double r = x * rsqrt(x);
+  const double u = fabs(dn) + r;
+  const double q = rsqrt(2.0 * r * u);
+  const double sg = d >= 0.0 ? 1.0 : -1.0;
+  c = u * q;
+  s = sg * (2.0 * gn * q);
+  tg = sg * (4.0 * gn * r * q * q) * g;
+}
+
 constexpr int kChunk = 128;            // rows per streamed chunk of W or V
 constexpr int kInnerMax = 1;           // inner sweeps of one visit (more cut outer sweeps by less than they cost)
 
@@ -85,6 +113,14 @@ template <bool CPLX, int B>
 constexpr size_t svd_smem_bytes() {
   return (size_t)(2 * SvdGeom<B>::Nc + kChunk) * SvdGeom<B>::Ld * (CPLX ? 16 : 8);
 }
+// shared memory of a resident visit (all rows of the pair's W and V columns) of a
+// block with R + C rows in total; launches whose largest pair needs more stream
+// row chunks instead
+template <bool CPLX, int B>
+constexpr size_t svd_res_smem_bytes(long long rows) {
+  return (size_t)(2 * SvdGeom<B>::Nc + rows) * SvdGeom<B>::Ld * (CPLX ? 16 : 8) + (size_t)kSvdWarps * 32 * 4 * 8;
+}
+constexpr size_t kSvdResMax = 160 * 1024;
 
 // One visit of a column-block pair (Hestenes one-sided Jacobi in Gram form):
 //   1. G = Wp^H Wp for the pair's nc <= 2B columns Wp, streamed from W in row chunks;
@@ -94,7 +130,10 @@ constexpr size_t svd_smem_bytes() {
 //      kInnerMax sweeps, stopping after a sweep that rotates nothing;
 //   3. Wp <- Wp Q and Vp <- Vp Q, streamed in row chunks.
 // Only G, Q and one row chunk live in shared memory, so the visit width does not
-// depend on the height of the block.  The rotations rotate the Gram entries of
+// depend on the height of the block -- or, when the launch's largest pair fits
+// (res), all rows of the pair's columns of W and V: one load, the Gram tiles with
+// their rows split over all warps (partials summed in a fixed order), and Q applied
+// in place by warps that own whole 8-row tiles.  The rotations rotate the Gram entries of
 // the columns exactly as the column updates would (a rotation that mixes a small
 // column with a large one has |s| <= sqrt(a_small / a_large)), so the entries
 // keep the columnwise relative accuracy of the direct method; W itself changes
@@ -102,7 +141,7 @@ constexpr size_t svd_smem_bytes() {
 // thread of the block calls it; 16 warps, warp k owns pair k of each round.
 template <bool CPLX, int B>
 __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work, void* vmat, const int* perm,
-                                  double tol, unsigned char* smem_raw, int* rotations) {
+                                  double tol, unsigned char* smem_raw, int* rotations, bool res) {
   using T = typename SvdT<CPLX>::T;
   constexpr int kNc = SvdGeom<B>::Nc, kTD = SvdGeom<B>::TD, kLdG = SvdGeom<B>::Ld;
   constexpr int kChunkPer = SvdGeom<B>::ChunkPer;
@@ -110,10 +149,13 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   const int R = J.trans ? J.n : J.m;
   const int C = J.trans ? J.m : J.n;
   __shared__ int cols[kNc];
-  __shared__ int nrot_sh, sweep_rot_sh;
   T* G = reinterpret_cast<T*>(smem_raw);   // kNc x kLdG, row-major
   T* Q = G + kNc * kLdG;
   T* Ck = Q + kNc * kLdG;                  // kChunk x kLdG: rows of W or V, row-major
+  // resident visit: all R rows of the pair's W columns, then all C rows of its V columns
+  T* Ws = Ck;
+  T* Vs = Ws + R * kLdG;
+  double* Gp = reinterpret_cast<double*>(Vs + C * kLdG);   // Gram partials, 4 per lane per warp
   T* W = static_cast<T*>(work) + J.woff;
   T* V = static_cast<T*>(vmat) + J.voff;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -126,7 +168,6 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     const int* pj = perm + J.soff;
     if (tid < n0) cols[tid] = pj[P.bi * P.b + tid];
     else if (tid < nc) cols[tid] = pj[P.bj * P.b + (tid - n0)];
-    if (tid == 0) nrot_sh = 0;
   }
   __syncthreads();
 
@@ -134,8 +175,8 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   //    (w / kTD, w % kTD) of G = Wp^H Wp; k runs over the rows of the chunk
   //    (zero-filled past the block)
   static_assert(kNc % 8 == 0 && kTD * kTD <= kSvdWarps, "one warp per Gram tile");
-  const bool gram_warp = warp < kTD * kTD;
-  const int pt = warp / kTD, qt = warp % kTD;
+  constexpr int kTiles = kTD * kTD, kSplit = kSvdWarps / kTiles;
+  const bool gram_warp = warp < kTiles;
   const int fr = lane >> 2, fk = lane & 3;
   double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;   // Re (and Im) of D(fr, 2 fk + i)
   // Row chunks of a column set (W or V), read into registers one chunk ahead of
@@ -155,6 +196,63 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
       Ck[r * kLdG + c] = pre[u];
     }
   };
+  if (res) {
+    // one load of everything the visit touches (columns past nc zero-filled), then
+    // the Gram tiles with their rows split over all warps: warp w computes tile
+    // w % kTiles over the w / kTiles-th part of the rows; the parts are summed in
+    // part order
+    // one thread per row of W then V, its columns read into registers together so
+    // that all of a thread's loads are in flight at once (coalesced along rows)
+    constexpr int kU = CPLX ? 8 : 16;
+    for (int r0 = 0; r0 < R + C; r0 += kSvdThreads) {
+      const int rr = r0 + tid;
+      if (rr < R + C) {
+        const bool isw = rr < R;
+        const int r = isw ? rr : rr - R, ld = isw ? R : C;
+        const T* M = isw ? W : V;
+        T* D = (isw ? Ws : Vs) + r * kLdG;
+#pragma unroll
+        for (int c0 = 0; c0 < kNc; c0 += kU) {
+          T v[kU];
+#pragma unroll
+          for (int u = 0; u < kU; ++u) v[u] = c0 + u < nc ? M[r + (long long)cols[c0 + u] * ld] : czero<T>();
+#pragma unroll
+          for (int u = 0; u < kU; ++u) D[c0 + u] = v[u];
+        }
+      }
+    }
+    __syncthreads();
+    const int tile = warp % kTiles, part = warp / kTiles;
+    const int pt = tile / kTD, qt = tile % kTD;
+    const int rs = (((R + kSplit - 1) / kSplit) + 3) & ~3;
+    const int k0s = part * rs, k1s = min(R, k0s + rs);
+    for (int k0 = k0s; k0 < k1s; k0 += 4) {
+      const int k = k0 + fk;
+      const T x = k < k1s ? Ws[k * kLdG + pt * 8 + fr] : czero<T>();   // A(p, r) = conj(W(r, p))
+      const T y = k < k1s ? Ws[k * kLdG + qt * 8 + fr] : czero<T>();   // B(r, q) = W(r, q)
+      if constexpr (CPLX) {
+        dmma(g0, g1, x.x, y.x);
+        dmma(g0, g1, x.y, y.y);
+        dmma(h0, h1, x.x, y.y);
+        dmma(h0, h1, -x.y, y.x);
+      } else {
+        dmma(g0, g1, x, y);
+      }
+    }
+    if constexpr (kSplit > 1) {
+      if (part > 0) {
+        double* o = Gp + (warp * 32 + lane) * 4;
+        o[0] = g0; o[1] = g1; o[2] = h0; o[3] = h1;
+      }
+      __syncthreads();
+      if (part == 0)
+        for (int pp = 1; pp < kSplit; ++pp) {
+          const double* o = Gp + ((tile + pp * kTiles) * 32 + lane) * 4;
+          g0 += o[0]; g1 += o[1]; h0 += o[2]; h1 += o[3];
+        }
+    }
+  } else {
+  const int pt = warp / kTD, qt = warp % kTD;
   fetch(W, R, 0, min(kChunk, R));
   for (int r0 = 0; r0 < R; r0 += kChunk) {
     stage();
@@ -175,7 +273,9 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
     }
     __syncthreads();
   }
+  }
   // stored from the tiles on and above the diagonal, mirrored, so that G is exactly Hermitian
+  const int pt = warp / kTD, qt = warp % kTD;
   for (int i = 0; i < 2 && gram_warp; ++i) {
     const int p = pt * 8 + fr, q = qt * 8 + 2 * fk + i;
     if (p > q) continue;
@@ -210,16 +310,21 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
 
   // 2. inner sweeps on G
   const int N = nc + (nc & 1);
+  int nrot = 0;
   for (int isw = 0; isw < kInnerMax && N > 1; ++isw) {
-    if (tid == 0) sweep_rot_sh = 0;
-    __syncthreads();
+    int sr = 0;   // rotations of this inner sweep (the same count in every thread)
     for (int rnd = 0; rnd < N - 1; ++rnd) {
       bool act = false;
       int p = 0, q = 0;
       double c = 1.0, s = 0.0, er = 1.0, ei = 0.0, tg = 0.0, a = 0.0, b = 0.0;
       if (warp < N / 2) {
         if (warp == 0) { p = N - 1; q = rnd; }
-        else { p = (rnd + warp) % (N - 1); q = (rnd - warp + (N - 1)) % (N - 1); }
+        else {
+          p = rnd + warp;
+          if (p >= N - 1) p -= N - 1;
+          q = rnd - warp;
+          if (q < 0) q += N - 1;
+        }
         if (p > q) { const int t = p; p = q; q = t; }
         if (q < nc) {
           a = cre(G[p * kLdG + p]);
@@ -231,20 +336,18 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
           // rotate when |g| > tol sqrt(ab), compared squared; the parameters keep the
           // dependent chain of square roots and divisions short (it sets the round time)
           if (a * b > 0.0 && g2 > tol * tol * (a * b)) {
-            const double g = CPLX ? sqrt(g2) : fabs(gr);
-            const double ig = 1.0 / g;
-            // same rotation as on the columns; for |zeta| > 1e150 zeta^2 would overflow
-            const double zeta = 0.5 * (b - a) * ig;
-            const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
-                                                : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-            if (t != 0.0) {
-              act = true;
-              c = rsqrt(1.0 + t * t);
-              s = c * t;
-              er = CPLX ? gr * ig : (gr >= 0.0 ? 1.0 : -1.0);
-              ei = CPLX ? gi * ig : 0.0;
-              tg = t * g;
+            double g;
+            if constexpr (CPLX) {
+              g = sqrt(g2);
+              const double ig = 1.0 / g;
+              er = gr * ig;
+              ei = gi * ig;
+            } else {
+              g = fabs(gr);
+              er = gr >= 0.0 ? 1.0 : -1.0;
             }
+            jacobi_rotation(a, b, g, c, s, tg);
+            act = true;
           }
         }
       }
@@ -291,17 +394,70 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
         if (lane == q) { rq[q] = czero<T>(); reinterpret_cast<double*>(rq + q)[0] = b + tg; }
         if (lane == q) rp[q] = czero<T>();
         if (lane == p) rq[p] = czero<T>();
-        if (lane == 0) atomicAdd(&sweep_rot_sh, 1);
       }
-      __syncthreads();
+      sr += __syncthreads_count(act && lane == 0);
     }
-    const int sr = sweep_rot_sh;
-    if (tid == 0) nrot_sh += sr;
-    __syncthreads();
+    nrot += sr;
     if (sr == 0) break;
   }
-  const int nrot = nrot_sh;
   if (nrot == 0) return;        // nothing moved: W and V stay as they are
+
+  if (res) {
+    // 3. Ws <- Ws Q and Vs <- Vs Q in place: warp w owns the 8-row tiles w, w + 16, ...
+    //    of the rows of Ws then Vs and computes all their output columns before it
+    //    writes them back; then every thread stores the new columns
+    const int ntw = (R + 7) / 8, ntv = (C + 7) / 8;
+    for (int t = warp; t < ntw + ntv; t += kSvdWarps) {
+      T* M = t < ntw ? Ws : Vs;
+      const int rows = t < ntw ? R : C, r = (t < ntw ? t : t - ntw) * 8 + fr;
+      double acc[kTD][4];
+#pragma unroll
+      for (int jt = 0; jt < kTD; ++jt) acc[jt][0] = acc[jt][1] = acc[jt][2] = acc[jt][3] = 0.0;
+#pragma unroll
+      for (int k0 = 0; k0 < kNc; k0 += 4) {
+        const T x = r < rows ? M[r * kLdG + k0 + fk] : czero<T>();
+#pragma unroll
+        for (int jt = 0; jt < kTD; ++jt) {
+          const T y = Q[(k0 + fk) * kLdG + jt * 8 + fr];
+          if constexpr (CPLX) {
+            dmma(acc[jt][0], acc[jt][1], x.x, y.x);
+            dmma(acc[jt][0], acc[jt][1], -x.y, y.y);
+            dmma(acc[jt][2], acc[jt][3], x.x, y.y);
+            dmma(acc[jt][2], acc[jt][3], x.y, y.x);
+          } else {
+            dmma(acc[jt][0], acc[jt][1], x, y);
+          }
+        }
+      }
+      __syncwarp();
+      if (r < rows) {
+#pragma unroll
+        for (int jt = 0; jt < kTD; ++jt)
+          for (int i = 0; i < 2; ++i) {
+            T v;
+            if constexpr (CPLX) v = make_double2(acc[jt][i], acc[jt][2 + i]);
+            else v = acc[jt][i];
+            M[r * kLdG + jt * 8 + 2 * fk + i] = v;
+          }
+      }
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < R + C; r0 += kSvdThreads) {
+      const int rr = r0 + tid;
+      if (rr < R + C) {
+        const bool isw = rr < R;
+        const int r = isw ? rr : rr - R, ld = isw ? R : C;
+        T* M = isw ? W : V;
+        const T* S = (isw ? Ws : Vs) + r * kLdG;
+#pragma unroll
+        for (int c = 0; c < kNc; ++c)
+          if (c < nc) M[r + (long long)cols[c] * ld] = S[c];
+      }
+    }
+    __syncthreads();   // the next visit of this CTA reloads the shared arrays
+    if (tid == 0) atomicAdd(rotations, nrot);
+    return;
+  }
 
   // 3. W_pair <- W_pair Q and V_pair <- V_pair Q, in row chunks (W's, then V's): each
   //    chunk (128 x 32, zero-filled) times Q on the FP64 tensor cores (warp w: output
@@ -374,11 +530,11 @@ template <bool CPLX, int B>
 __global__ void __launch_bounds__(kSvdThreads) jacobi_pair_kernel(const SvdJob* __restrict__ jobs,
                                                                   const SvdPair* __restrict__ pairs, void* work,
                                                                   void* vmat, const int* perm, double tol,
-                                                                  int* rotations) {
+                                                                  int* rotations, int res) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SvdPair P = pairs[blockIdx.x];
   const SvdJob J = jobs[P.job];
-  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations);
+  jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, rotations, res != 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -438,7 +594,8 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
                                                                   const SvdPair* __restrict__ pairs,
                                                                   const int* __restrict__ roff, int max_rounds,
                                                                   void* work, void* vmat, double* nrm, int* perm,
-                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps) {
+                                                                  double tol, int* cnt, SvdCtl* ctl, int max_sweeps,
+                                                                  int res) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned char done[kSvdMaxJobsCoop];
   __shared__ int all_done;
@@ -496,7 +653,7 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_coop_kernel(const SvdJob* 
         const SvdPair P = pairs[p];
         if (done[P.job]) continue;
         const SvdJob J = jobs[P.job];
-        jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job);
+        jacobi_pair_visit<CPLX, B>(J, P, work, vmat, perm, tol, smem_raw, cur + P.job, res != 0);
       }
       if (!svd_grid_sync(ctl)) return;
     }
@@ -954,11 +1111,13 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
   const int nj = (int)hjobs.size();
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
+  long long maxRC = 0;
   size_t smem = 0;
   for (int j = 0; j < nj; ++j) {
     const int R = hjobs[j].trans ? hjobs[j].n : hjobs[j].m;
     const int C = hjobs[j].trans ? hjobs[j].m : hjobs[j].n;
     maxR = std::max(maxR, R);
+    maxRC = std::max<long long>(maxRC, (long long)R + C);
     bsz[j] = B;
     nblk[j] = (C + bsz[j] - 1) / bsz[j];
     const int N = nblk[j] + (nblk[j] & 1);
@@ -966,6 +1125,9 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     max_rounds = std::max(max_rounds, nrounds[j]);
     smem = svd_smem_bytes<CPLX, B>();
   }
+  // visits hold the pair's columns of W and V in shared memory when the largest fits
+  const int res = svd_res_smem_bytes<CPLX, B>(maxRC) <= kSvdResMax ? 1 : 0;
+  if (res) smem = std::max(smem, svd_res_smem_bytes<CPLX, B>(maxRC));
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
   for (int j = 0; j < nj; ++j) {
@@ -1023,13 +1185,14 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     SvdCtl* pctl = dctl.as<SvdCtl>();
     int njv = nj, mr = max_rounds, ms = max_sweeps;
     double tolv = tol;
+    int resv = res;
     void* a_work = work;
     void* a_vmat = vmat;
     double* a_nrm = sv;   // column norms of each sweep; the final singular values overwrite them
     int* a_perm = dperm.as<int>();
     void* args[] = {(void*)&pj,     (void*)&njv,    (void*)&pp,   (void*)&pr, (void*)&mr,   (void*)&a_work,
                     (void*)&a_vmat, (void*)&a_nrm, (void*)&a_perm, (void*)&tolv, (void*)&pc, (void*)&pctl,
-                    (void*)&ms};
+                    (void*)&ms, (void*)&resv};
     SADMRG_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_coop_kernel<CPLX, B>, dim3(grid), dim3(kSvdThreads),
                                             args, smem, s));
     SvdCtl hctl{};
@@ -1048,7 +1211,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
       const int np = roff[r + 1] - roff[r];
       if (np == 0) continue;
       jacobi_pair_kernel<CPLX, B><<<np, kSvdThreads, smem, s>>>(djobs.as<SvdJob>(), dpairs.as<SvdPair>() + roff[r],
-                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>());
+                                                                work, vmat, dperm.as<int>(), tol, dcnt.as<int>(), res);
     }
     SADMRG_CUDA(cudaGetLastError());
     SADMRG_CUDA(cudaMemcpyAsync(&h_rot, dcnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));

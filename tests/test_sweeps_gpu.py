@@ -5,7 +5,11 @@ written by its save_mps2 and read here by sadmrg_chain_read_mps (the
 reference's checkpoint format).  Tolerances:
   * SU(2): energy after every sweep to 1e-9 relative (the Lanczos stopping rule
     |<v|Hv>|/|Hv| within 1e-8 of 1 bounds the agreement of two FP64 runs), kept
-    sectors and dimensions of every bond identical.
+    sectors and dimensions of every bond identical until the GPU run reports a
+    near-tie cut (the D-th and (D+1)-th singular values equal to 1e-8: multiplets
+    of different spin degenerate to rounding, whose order the reference's
+    std::sort leaves to rounding too); from then on the energy still to 1e-9 and
+    the total kept dimension of every bond.
   * U(1): the singular values of sectors q and -q are equal in exact arithmetic,
     so a cut that falls between such a pair is decided by rounding (the
     reference's std::sort has no tie-break).  When the GPU run reports no
@@ -72,11 +76,12 @@ def test_sweeps_from_reference_checkpoint(path):
         got = _bonds(h, ns)
         ties = h.chain_stats()["near_ties"]
         ref_b = [str(x) for x in z["bonds_per_sweep"][s]]
-        if a["sym"] == 1 or ties == 0:
+        if ties == 0:
             assert abs(e - eref) <= 1e-9 * abs(eref), (s, e, eref, ties)
             assert got == ref_b, (s, ties)
         else:
-            assert abs(e - eref) <= 1e-7 * abs(eref), (s, e, eref, ties)
+            tol = 1e-9 if a["sym"] == 1 else 1e-7
+            assert abs(e - eref) <= tol * abs(eref), (s, e, eref, ties)
             assert [_total(x) for x in got] == [_total(x) for x in ref_b], (s, ties)
 
 
