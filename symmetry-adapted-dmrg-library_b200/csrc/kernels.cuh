@@ -78,6 +78,8 @@ struct PackJob {              // FP64 matrix -> panels
   int cmode;                  // 0 real; complex source (src, ld in complex elements, rows / K of the real
                               // form): 1 Ah (rows 2m, K 2k), 2 Bh read as rows n x K 2k
   int conj;                   // complex: conjugate the source elements first
+  int sparse;                 // 1: chunks of the real rows and k only (the padding of the
+                              // panels is zero already and never written), 0: whole panels
 };
 struct UTerm {                // a term's operands as panel sets: A (T = 128), B (T = BN)
   long long a, b;             // byte offsets of panel (0, 0)

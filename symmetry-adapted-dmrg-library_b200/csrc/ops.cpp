@@ -298,7 +298,11 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
     P.T = p.k.T;
     P.cmode = p.k.cm >> 1;
     P.conj = p.k.cm & 1;
-    const long long nch = (long long)((P.rows + P.T - 1) / P.T) * P.T * nslab_of(P.K) * 8;
+    // psi (packed every matvec): only its real rows and k groups; the padding of its
+    // panels is zeroed once below and never written
+    P.sparse = p.cls == 1 ? 1 : 0;
+    const long long nch = P.sparse ? (long long)P.rows * ((P.K + 3) / 4)
+                                   : (long long)((P.rows + P.T - 1) / P.T) * P.T * nslab_of(P.K) * 8;
     long long& cc = p.cls == 0 ? U->cchunks : U->vchunks;
     auto& blk = p.cls == 0 ? U->cblk : U->vblk;
     auto& list = p.cls == 0 ? U->cpack : U->vpack;
@@ -493,6 +497,7 @@ bool GemmPlan::build_umma(Ctx& c, const Bases& cb, bool cplx) {
   U->d_dep_target = reinterpret_cast<int*>(base + o8);
   U->pconst = std::make_shared<DevBuf>((size_t)std::max<long long>(cbytes, 256), c.stream);
   U->pvar = std::make_shared<DevBuf>((size_t)std::max<long long>(vbytes, 256), c.stream);
+  SADMRG_CUDA(cudaMemsetAsync(U->pvar->get(), 0, U->pvar->bytes(), c.stream));   // the padding of the psi panels
   U->slots = std::make_shared<DevBuf>((size_t)std::max(nslot, 1) * kUmmaTileM * BN * sizeof(float), c.stream);
   U->tile_cnt = std::make_shared<DevBuf>(sizeof(int) * std::max<size_t>(U->reds.size(), 1), c.stream);
   SADMRG_CUDA(cudaMemsetAsync(U->tile_cnt->get(), 0, U->tile_cnt->bytes(), c.stream));

@@ -151,7 +151,9 @@ __device__ __forceinline__ void st_global_v4(void* p, uint32_t x, uint32_t y, ui
 
 // ---------------------------------------------------------------------------
 // FP64 matrices -> TF32 hi/lo panels.  One thread per 16-byte chunk (4 k of one
-// row); consecutive threads take consecutive rows of one (slab, kg) column, so
+// row) -- of every row and k group of the padded panels, or (sparse jobs: psi,
+// packed every matvec into panels zeroed when the plan was built) of the real rows
+// and k only; consecutive threads take consecutive rows of one (slab, kg) column, so
 // the stores are contiguous and the loads coalesce along rows (trans 0) or read
 // one 32-byte sector per thread (trans 1).  Every job starts on a multiple of
 // 256 chunks, so a block works for one job, looked up in blk_job.
@@ -159,9 +161,18 @@ __device__ __forceinline__ void pack_chunk(const PackJob& P, unsigned local, con
                                            unsigned char* __restrict__ dst) {
   const unsigned T = (unsigned)P.T;
   const unsigned nslab = ((unsigned)P.K + kPanelK - 1) / kPanelK;
-  const unsigned Rp = (((unsigned)P.rows + T - 1) / T) * T;
-  if (local >= Rp * nslab * 8u) return;
-  const unsigned r = local % Rp, kgs = local / Rp;
+  unsigned r, kgs;
+  if (P.sparse) {
+    const unsigned rows = (unsigned)P.rows;
+    if (local >= rows * (((unsigned)P.K + 3u) / 4u)) return;
+    r = local % rows;
+    kgs = local / rows;
+  } else {
+    const unsigned Rp = (((unsigned)P.rows + T - 1) / T) * T;
+    if (local >= Rp * nslab * 8u) return;
+    r = local % Rp;
+    kgs = local / Rp;
+  }
   const unsigned s = kgs >> 3, kg = kgs & 7u;
   const unsigned p = r / T, rr = r - p * T;
   uint32_t h[4], l[4];
