@@ -141,6 +141,11 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on);
  * means the same either way: the same singular values and vectors to
  * rounding. */
 int sadmrg_set_svd_precondition(sadmrg_handle* h, int on);
+/* Block SVD visits (no counterpart in the reference): 0 (the default) keeps a
+ * Jacobi visit's columns of W and V in shared memory where the launch's largest
+ * pair fits, 1 always streams them in row chunks as for blocks too tall to fit.
+ * The same results either way; for tests and profiling. */
+int sadmrg_set_svd_stream(sadmrg_handle* h, int on);
 /* A fixed tile choice for the H_eff plans made after this call, instead of the
  * autotuner or the heuristics: width 64 or 128 (0 returns to them), fewest slabs
  * per split-K chunk when the tiles cannot fill the GPU (0: no such split), most

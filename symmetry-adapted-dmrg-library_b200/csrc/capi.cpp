@@ -287,6 +287,10 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
 }
 
+int sadmrg_set_svd_stream(sadmrg_handle* h, int on) {
+  return guard(h, [&]() { h->ctx.svd_stream = on ? 1 : 0; });
+}
+
 int sadmrg_set_svd_precondition(sadmrg_handle* h, int on) {
   return guard(h, [&]() {
     SADMRG_REQUIRE(on >= 0 && on <= 2, SADMRG_ERR_ARG, "set_svd_precondition: 0, 1 or 2");

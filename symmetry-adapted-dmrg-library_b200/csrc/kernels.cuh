@@ -239,7 +239,10 @@ struct SvdJob {
 // precondition: Jacobi on R1^H after Householder QRs of the norm-ordered columns
 // and of R^H (fewer sweeps): 0 never, 1 when the widest block has at least 32
 // columns, 2 always; the outputs have the same meaning either way.
+// stream: 1 streams every visit's rows in chunks even where the pair's columns
+// would fit in shared memory (same results; covers that path on small problems).
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, int precondition = 1);
+                   int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, int precondition = 1,
+                   int stream = 0);
 
 }  // namespace sadmrg

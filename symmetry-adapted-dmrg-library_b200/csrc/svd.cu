@@ -98,6 +98,21 @@ __device__ __forceinline__ void jacobi_rotation(double a, double b, double g, do
   tg = sg * (4.0 * gn * r * q * q) * g;
 }
 
+// One element (8 or 16 bytes) copied global -> shared without passing through
+// registers (cp.async, Ampere and later); zero-filled instead when !ok (src must
+// still be a valid address).
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src, bool ok) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 16 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all but the most recently committed group of this thread's copies have landed
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 constexpr int kChunk = 128;            // rows per streamed chunk of W or V
 constexpr int kInnerMax = 1;           // inner sweeps of one visit (more cut outer sweeps by less than they cost)
 
@@ -110,8 +125,8 @@ struct SvdGeom {
 };
 
 template <bool CPLX, int B>
-constexpr size_t svd_smem_bytes() {
-  return (size_t)(2 * SvdGeom<B>::Nc + kChunk) * SvdGeom<B>::Ld * (CPLX ? 16 : 8);
+constexpr size_t svd_smem_bytes() {   // G, Q and two row-chunk buffers
+  return (size_t)(2 * SvdGeom<B>::Nc + 2 * kChunk) * SvdGeom<B>::Ld * (CPLX ? 16 : 8);
 }
 // shared memory of a resident visit (all rows of the pair's W and V columns) of a
 // block with R + C rows in total; launches whose largest pair needs more stream
@@ -179,22 +194,19 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   const bool gram_warp = warp < kTiles;
   const int fr = lane >> 2, fk = lane & 3;
   double g0 = 0.0, g1 = 0.0, h0 = 0.0, h1 = 0.0;   // Re (and Im) of D(fr, 2 fk + i)
-  // Row chunks of a column set (W or V), read into registers one chunk ahead of
-  // the one in shared memory so that the global loads overlap the products.
-  T pre[kChunkPer];
-  auto fetch = [&](const T* M, int ld, int r0, int rows) {
+  // Streamed visits: row chunks of a column set (W or V) copied asynchronously
+  // into two shared buffers, the next chunk in flight while one is multiplied
+  // (rows past the block and columns past nc zero-filled); one group per chunk.
+  T* const Cb0 = Ck;
+  T* const Cb1 = Ck + kChunk * kLdG;
+  auto issue = [&](const T* M, int ld, int r0, int rows, T* dst) {
 #pragma unroll
     for (int u = 0; u < kChunkPer; ++u) {
       const int e = tid + u * kSvdThreads, r = e % kChunk, c = e / kChunk;
-      pre[u] = (r < rows && c < nc) ? M[(r0 + r) + (long long)cols[c] * ld] : czero<T>();
+      const bool ok = r < rows && c < nc;
+      cp_async_elem(dst + r * kLdG + c, ok ? M + (r0 + r) + (long long)cols[c] * ld : M, ok);
     }
-  };
-  auto stage = [&]() {
-#pragma unroll
-    for (int u = 0; u < kChunkPer; ++u) {
-      const int e = tid + u * kSvdThreads, r = e % kChunk, c = e / kChunk;
-      Ck[r * kLdG + c] = pre[u];
-    }
+    cp_async_commit();
   };
   if (res) {
     // one load of everything the visit touches (columns past nc zero-filled), then
@@ -252,27 +264,43 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
         }
     }
   } else {
-  const int pt = warp / kTD, qt = warp % kTD;
-  fetch(W, R, 0, min(kChunk, R));
-  for (int r0 = 0; r0 < R; r0 += kChunk) {
-    stage();
-    __syncthreads();
-    if (r0 + kChunk < R) fetch(W, R, r0 + kChunk, min(kChunk, R - r0 - kChunk));
+    const int pt = warp / kTD, qt = warp % kTD;
+    const int nch = (R + kChunk - 1) / kChunk;
+    issue(W, R, 0, min(kChunk, R), Cb0);
+    if (nch > 1) issue(W, R, kChunk, min(kChunk, R - kChunk), Cb1);
+    else cp_async_commit();
+    double e0 = 0.0, e1 = 0.0, f0 = 0.0, f1 = 0.0;   // a second chain over the odd k steps
+    for (int ch = 0; ch < nch; ++ch) {
+      cp_async_wait1();
+      __syncthreads();
+      const T* Cc = (ch & 1) ? Cb1 : Cb0;
+      if (gram_warp) {
 #pragma unroll 4
-    for (int k0 = 0; k0 < kChunk && gram_warp; k0 += 4) {
-      const T x = Ck[(k0 + fk) * kLdG + pt * 8 + fr];   // A(p, r) = conj(W(r, p))
-      const T y = Ck[(k0 + fk) * kLdG + qt * 8 + fr];   // B(r, q) = W(r, q)
-      if constexpr (CPLX) {
-        dmma(g0, g1, x.x, y.x);
-        dmma(g0, g1, x.y, y.y);
-        dmma(h0, h1, x.x, y.y);
-        dmma(h0, h1, -x.y, y.x);
-      } else {
-        dmma(g0, g1, x, y);
+        for (int k0 = 0; k0 < kChunk; k0 += 8) {
+          const T x = Cc[(k0 + fk) * kLdG + pt * 8 + fr];       // A(p, r) = conj(W(r, p))
+          const T y = Cc[(k0 + fk) * kLdG + qt * 8 + fr];       // B(r, q) = W(r, q)
+          const T x2 = Cc[(k0 + 4 + fk) * kLdG + pt * 8 + fr];
+          const T y2 = Cc[(k0 + 4 + fk) * kLdG + qt * 8 + fr];
+          if constexpr (CPLX) {
+            dmma(g0, g1, x.x, y.x);
+            dmma(g0, g1, x.y, y.y);
+            dmma(h0, h1, x.x, y.y);
+            dmma(h0, h1, -x.y, y.x);
+            dmma(e0, e1, x2.x, y2.x);
+            dmma(e0, e1, x2.y, y2.y);
+            dmma(f0, f1, x2.x, y2.y);
+            dmma(f0, f1, -x2.y, y2.x);
+          } else {
+            dmma(g0, g1, x, y);
+            dmma(e0, e1, x2, y2);
+          }
+        }
       }
+      __syncthreads();
+      if (ch + 2 < nch) issue(W, R, (ch + 2) * kChunk, min(kChunk, R - (ch + 2) * kChunk), (ch & 1) ? Cb1 : Cb0);
+      else cp_async_commit();
     }
-    __syncthreads();
-  }
+    g0 += e0; g1 += e1; h0 += f0; h1 += f1;
   }
   // stored from the tiles on and above the diagonal, mirrored, so that G is exactly Hermitian
   const int pt = warp / kTD, qt = warp % kTD;
@@ -460,39 +488,39 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
   }
 
   // 3. W_pair <- W_pair Q and V_pair <- V_pair Q, in row chunks (W's, then V's): each
-  //    chunk (128 x 32, zero-filled) times Q on the FP64 tensor cores (warp w: output
-  //    tiles w, w + 16, ... of the 16 x 4 tile grid), the product written back over the
-  //    chunk and stored coalesced; the next chunk is read while this one is multiplied
+  //    chunk (128 x 2B, zero-filled) times Q on the FP64 tensor cores (warp w: output
+  //    tiles w, w + 16, ... of the chunk's 8 x 8 tile grid), the products stored
+  //    from registers; the chunk after next is copied in while one is multiplied
   const int nw_chunks = (R + kChunk - 1) / kChunk, nv_chunks = (C + kChunk - 1) / kChunk;
+  const int nall = nw_chunks + nv_chunks;
   auto chunk_of = [&](int k, T*& M, int& ld, int& r0, int& rows) {
     if (k < nw_chunks) { M = W; ld = R; r0 = k * kChunk; }
     else { M = V; ld = C; r0 = (k - nw_chunks) * kChunk; }
     rows = min(kChunk, ld - r0);
   };
-  {
-    T* M; int ld, r0, rows;
-    chunk_of(0, M, ld, r0, rows);
-    fetch(M, ld, r0, rows);
+  for (int k = 0; k < 2; ++k) {
+    if (k < nall) {
+      T* M; int ld, r0, rows;
+      chunk_of(k, M, ld, r0, rows);
+      issue(M, ld, r0, rows, k ? Cb1 : Cb0);
+    } else {
+      cp_async_commit();
+    }
   }
-  for (int k = 0; k < nw_chunks + nv_chunks; ++k) {
+  for (int k = 0; k < nall; ++k) {
     T* M; int ld, r0, rows;
     chunk_of(k, M, ld, r0, rows);
-    stage();
+    cp_async_wait1();
     __syncthreads();
-    if (k + 1 < nw_chunks + nv_chunks) {
-      T* M2; int ld2, r2, rows2;
-      chunk_of(k + 1, M2, ld2, r2, rows2);
-      fetch(M2, ld2, r2, rows2);
-    }
+    const T* Cc = (k & 1) ? Cb1 : Cb0;
     constexpr int kTiles = (kChunk / 8) * (kNc / 8) / kSvdWarps;   // output tiles per warp
-    double d[kTiles][4];
 #pragma unroll
     for (int u = 0; u < kTiles; ++u) {
       const int t = warp + kSvdWarps * u, rt = t / kTD, jt = t % kTD;
       double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
 #pragma unroll
       for (int k0 = 0; k0 < kNc; k0 += 4) {
-        const T x = Ck[(rt * 8 + fr) * kLdG + k0 + fk];
+        const T x = Cc[(rt * 8 + fr) * kLdG + k0 + fk];
         const T y = Q[(k0 + fk) * kLdG + jt * 8 + fr];
         if constexpr (CPLX) {
           dmma(a0, a1, x.x, y.x);
@@ -503,25 +531,27 @@ __device__ void jacobi_pair_visit(const SvdJob& J, const SvdPair& P, void* work,
           dmma(a0, a1, x, y);
         }
       }
-      d[u][0] = a0; d[u][1] = a1; d[u][2] = b0; d[u][3] = b1;
-    }
-    __syncthreads();
+      const int r = rt * 8 + fr;
+      if (r < rows) {
 #pragma unroll
-    for (int u = 0; u < kTiles; ++u) {
-      const int t = warp + kSvdWarps * u, rt = t / kTD, jt = t % kTD;
-      for (int i = 0; i < 2; ++i) {
-        T v;
-        if constexpr (CPLX) v = make_double2(d[u][i], d[u][2 + i]);
-        else v = d[u][i];
-        Ck[(rt * 8 + fr) * kLdG + jt * 8 + 2 * fk + i] = v;
+        for (int i = 0; i < 2; ++i) {
+          const int j = jt * 8 + 2 * fk + i;
+          if (j >= nc) continue;
+          T v;
+          if constexpr (CPLX) v = make_double2(i ? a1 : a0, i ? b1 : b0);
+          else v = i ? a1 : a0;
+          M[(r0 + r) + (long long)cols[j] * ld] = v;
+        }
       }
     }
-    __syncthreads();
-    for (int e = tid; e < kChunk * kNc; e += kSvdThreads) {
-      const int r = e % kChunk, j = e / kChunk;
-      if (r < rows && j < nc) M[(r0 + r) + (long long)cols[j] * ld] = Ck[r * kLdG + j];
+    __syncthreads();   // every warp is done with this buffer
+    if (k + 2 < nall) {
+      T* M2; int ld2, r2, rows2;
+      chunk_of(k + 2, M2, ld2, r2, rows2);
+      issue(M2, ld2, r2, rows2, (k & 1) ? Cb1 : Cb0);
+    } else {
+      cp_async_commit();
     }
-    __syncthreads();
   }
   if (tid == 0) atomicAdd(rotations, nrot);
 }
@@ -1107,7 +1137,7 @@ __global__ void qr_vout_kernel(const QrJob* jobs, const void* qbuf, void* vmat, 
 // was reached).
 template <bool CPLX, int B>
 static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                      int max_sweeps, cudaStream_t s, double* kernel_ms, int copy = 1) {
+                      int max_sweeps, cudaStream_t s, double* kernel_ms, int copy = 1, int stream = 0) {
   const int nj = (int)hjobs.size();
   std::vector<int> bsz(nj), nblk(nj), nrounds(nj);
   int max_rounds = 0, maxR = 0;
@@ -1126,7 +1156,7 @@ static int jacobi_run(const void* a, void* work, void* vmat, double* sv, const s
     smem = svd_smem_bytes<CPLX, B>();
   }
   // visits hold the pair's columns of W and V in shared memory when the largest fits
-  const int res = svd_res_smem_bytes<CPLX, B>(maxRC) <= kSvdResMax ? 1 : 0;
+  const int res = !stream && svd_res_smem_bytes<CPLX, B>(maxRC) <= kSvdResMax ? 1 : 0;
   if (res) smem = std::max(smem, svd_res_smem_bytes<CPLX, B>(maxRC));
   // pair lists per round
   std::vector<std::vector<SvdPair>> rounds(max_rounds);
@@ -1330,7 +1360,7 @@ struct QrLaunch {
 // preconditioning).
 template <bool CPLX>
 static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                         int max_sweeps, cudaStream_t s, double* kernel_ms, bool* fallback) {
+                         int max_sweeps, cudaStream_t s, double* kernel_ms, bool* fallback, int stream) {
   using T = typename SvdT<CPLX>::T;
   constexpr int NB = QrGeom<CPLX>::NB;
   *fallback = false;
@@ -1394,8 +1424,8 @@ static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, cons
   }
   double jms = -1.0;
   const int sweeps = narrow_blocks(jj)
-                         ? jacobi_run<CPLX, 8>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0)
-                         : jacobi_run<CPLX, 16>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0);
+                         ? jacobi_run<CPLX, 8>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0, stream)
+                         : jacobi_run<CPLX, 16>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0, stream);
   if (sweeps <= 0) return sweeps;
   // W = Q [R1^H V2; 0] and Q1 V2, both Q applications in one launch, then V = P (Q1 V2)
   qr_wout_kernel<CPLX><<<dim3(nj, 16), 256, 0, s>>>(static_cast<const QrJob*>(L1.dj.get()), qbuf.get(), work);
@@ -1419,7 +1449,7 @@ static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, cons
 }
 
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms, int precondition) {
+                   int max_sweeps, cudaStream_t s, double* kernel_ms, int precondition, int stream) {
   if (kernel_ms) *kernel_ms = -1.0;
   if (hjobs.empty()) return 0;
   if (precondition) {
@@ -1432,8 +1462,8 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     const size_t panel = (size_t)maxR * (cplx ? QrGeom<true>::NB * 16 : QrGeom<false>::NB * 8);
     if (panel <= kQrSmemMax && (maxC >= kQrMinCols || precondition == 2)) {
       bool fallback = false;
-      const int sw = cplx ? qr_jacobi_run<true>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback)
-                          : qr_jacobi_run<false>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback);
+      const int sw = cplx ? qr_jacobi_run<true>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream)
+                          : qr_jacobi_run<false>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream);
       if (!fallback) return sw;
     }
   }
@@ -1444,10 +1474,10 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   // 4.8 -> 5.5 s per iDMRG)
   const bool narrow = narrow_blocks(hjobs);
   if (cplx)
-    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
-                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
-  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms)
-                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms);
+    return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream)
+                  : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream);
+  return narrow ? jacobi_run<false, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream)
+                : jacobi_run<false, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream);
 }
 
 }  // namespace sadmrg

@@ -60,6 +60,9 @@ struct Ctx {
   // block SVD: Householder QRs before the Jacobi: 0 never, 1 for calls whose widest
   // block has at least 32 columns, 2 always
   int svd_qr = 1;
+  // block SVD: stream every Jacobi visit's rows in chunks (1) or keep the pair's
+  // columns in shared memory where they fit (0)
+  int svd_stream = 0;
   // a tile choice every new H_eff plan takes instead (bn > 0), e.g. to profile one
   UmmaTune forced_tune;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0
