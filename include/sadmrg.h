@@ -260,13 +260,24 @@ int sadmrg_chain_create(sadmrg_handle* h, int lx, int ly, int bondd, int physpn,
  * counterpart in the reference (one real coupling per pair, coup[] in
  * src/dmrg_inst.cpp:146-160); SADMRG_ERR_ARG for SU(2) or real scalars. */
 int sadmrg_chain_set_dm(sadmrg_handle* h, double dz);
+/* The chain targets excited state exci (the max_exci argument of the reference's
+ * DMRG constructor, src/dmrg_inst.cpp:64-112).  Call before sadmrg_chain_read_mps,
+ * which then reads this state's files (index exci) and, as DMRG::read_mps(read1,
+ * read2) (:1081-1140), the lower states 0 .. exci-1 and the last energy of each
+ * (enr-<ns>-<D>-<2S>-<idx>.dat); the sweeps keep their overlap environments
+ * (:440-583, 862-868), project them on every two-site basis (:412-437) and add
+ * the penalty -E_j <o_j|psi> o_j to H_eff*psi (:352-363).  U(1) chains only
+ * (SADMRG_ERR_ARG for SU(2)); an excited state starts from read_mps, not iDMRG.
+ * Checkpoint, ww and enr files carry the state's index. */
+int sadmrg_chain_set_excited(sadmrg_handle* h, int exci);
 int sadmrg_chain_set_precision(sadmrg_handle* h, int precision);
 int sadmrg_chain_idmrg(sadmrg_handle* h, double* energy);
 int sadmrg_chain_prepare_sweep(sadmrg_handle* h);
 int sadmrg_chain_sweep(sadmrg_handle* h, double* energy);
 /* DMRG::read_mps(bond_read) / save_mps2 checkpoint files (src/dmrg_inst.cpp:947-1079):
- * uu-<ns>-<D>-<2S>-0-<site>.dat (bond structure, text) and .bin (block data, then
- * SU(2) CGC blocks) in directory dir.  read_mps is followed by prepare_sweep. */
+ * uu-<ns>-<D>-<2S>-<exci>-<site>.dat (bond structure, text) and .bin (block data,
+ * then SU(2) CGC blocks) in directory dir, exci = 0 but for an excited-state chain
+ * (sadmrg_chain_set_excited).  read_mps is followed by prepare_sweep. */
 int sadmrg_chain_read_mps(sadmrg_handle* h, const char* dir, int bond_read);
 int sadmrg_chain_save_mps(sadmrg_handle* h, const char* dir);
 /* DMRG::save_ww / read_ww (src/dmrg_inst.cpp:1145-1165): the singular values of

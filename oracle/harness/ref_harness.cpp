@@ -74,6 +74,8 @@ struct Opts {
   int mlanc = 40;           // Lanczos length (reference: 40)
   double lanc_check = 1e-8; // Lanczos stop test (reference: 1e-8)
   std::string sweepdir = "/tmp";
+  int exci = 0;             // excited state: DMRG(..., max_exci = exci); with -read, read_mps(D, D)
+                            // loads this state's files (index exci) and the lower states' (0..exci-1)
 };
 
 template <class S, class Sym>
@@ -162,7 +164,7 @@ static int run(const Opts& o) {
   auto unmute = [&]() { std::cout.rdbuf(saved); sink.str(""); };
 
   mute();
-  DMRG<S, Sym> chain(o.lx, o.ly, o.D, 1, o.sec, 0);
+  DMRG<S, Sym> chain(o.lx, o.ly, o.D, 1, o.sec, o.exci);
   if constexpr (Sym::has_cgc) {
     if (o.maxangm > 20) {
       delete g_cgc_tables;
@@ -174,8 +176,10 @@ static int run(const Opts& o) {
   patch_geometry(chain, o);
   // room for every singular value BlockTensor::svd may write
   int wlen = 64 * o.D + 4096;
-  delete[] chain.ww[0];
-  chain.ww[0] = new double[wlen]();
+  for (int e = 0; e <= o.exci; ++e) {
+    delete[] chain.ww[e];
+    chain.ww[e] = new double[wlen]();
+  }
 
   auto t0 = std::chrono::steady_clock::now();
   char cwd[4096];
@@ -184,7 +188,9 @@ static int run(const Opts& o) {
     // DMRG::read_mps + prepare_sweep (src/dmrg_inst.cpp:1031-1079, 808-854)
     if (chdir(o.read.c_str()) != 0) { std::cerr << "cannot enter " << o.read << "\n"; return 3; }
     mute();
-    bool ok = chain.read_mps(o.D);
+    // an excited state: DMRG::read_mps(read1, read2) (src/dmrg_inst.cpp:1081-1140) also
+    // loads the lower states into orth and their energies (read_enr)
+    bool ok = o.exci > 0 ? chain.read_mps(o.D, o.D) : chain.read_mps(o.D);
     if (ok) chain.prepare_sweep();
     unmute();
     if (chdir(cwd) != 0) return 3;
@@ -496,6 +502,7 @@ int main(int argc, char** argv) {
     else if (a == "-mlanc") o.mlanc = std::stoi(nxt());
     else if (a == "-lanc_check") o.lanc_check = std::stod(nxt());
     else if (a == "-sweepdir") o.sweepdir = nxt();
+    else if (a == "-exci") o.exci = std::stoi(nxt());
     else { std::cerr << "unknown option " << a << "\n"; return 2; }
   }
   ref_lanczos_mlanc = o.mlanc;

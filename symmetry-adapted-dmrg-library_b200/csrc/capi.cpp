@@ -849,6 +849,15 @@ int sadmrg_chain_set_dm(sadmrg_handle* h, double dz) {
   });
 }
 
+int sadmrg_chain_set_excited(sadmrg_handle* h, int exci) {
+  return dispatch(h, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    auto& S_ = st_of<S>(h);
+    SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    S_.chain->set_excited(exci);
+  });
+}
+
 int sadmrg_chain_set_precision(sadmrg_handle* h, int precision) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;

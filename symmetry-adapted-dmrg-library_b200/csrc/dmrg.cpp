@@ -966,6 +966,21 @@ void Chain<S>::set_dm(double d) {
 }
 
 template <class S>
+void Chain<S>::set_excited(int k) {
+  SADMRG_REQUIRE(k >= 0 && k <= 16, SADMRG_ERR_ARG, "chain: excited state index 0..16");
+  SADMRG_REQUIRE(k == 0 || c.sym == Sym::U1, SADMRG_ERR_ARG,
+                 "chain: excited states are built for U(1) chains (the SU(2) projections move CGC blocks)");
+  for (int i = 0; i < ns; ++i)
+    SADMRG_REQUIRE(uu[i].null() && hh[i].null(), SADMRG_ERR_STATE,
+                   "chain: set the excited state before iDMRG or loading a checkpoint");
+  exci = k;
+  orth.assign(k, std::vector<BTensor<S>>(ns));
+  ovlp.assign(k, std::vector<BTensor<S>>(ns));
+  low_enr.assign(k, 0.0);
+  overlapvec.assign(k, BTensor<S>());
+}
+
+template <class S>
 void Chain<S>::random_init(BTensor<S>& t) {
   std::vector<S> h(t.nelem);
   for (long long i = 0; i < t.nelem; ++i) {
@@ -979,17 +994,36 @@ void Chain<S>::random_init(BTensor<S>& t) {
 
 // DMRG::prepare_site_operator_from_left (src/dmrg_inst.cpp:440-511 and 587-639)
 template <class S>
-void Chain<S>::prepare_site_operator_from_left(int i, bool real_env) {
+void Chain<S>::prepare_site_operator_from_left(int i, bool real_env, int flag) {
   const double t0 = now_s();
   BTensor<S> u1;
   if (!real_env) u1 = ops::fuse<S>(c, uu[i].st.bonds[0], uu[i].st.bonds[1]);
   const BTensor<S>& U = real_env ? uu[i] : u1;
   if (real_env && i == 0) {
     opr[0][0] = ops::operator_initial<S>(c, U, U, sigma[0], 0);
+    for (int j = 0; j < exci; ++j) ovlp[j][0] = ops::overlap_initial<S>(c, orth[j][0], uu[0], 0);
     hh[0] = BTensor<S>();
     timers.env += now_s() - t0;
     return;
   }
+  // the lower states' overlap environments (src/dmrg_inst.cpp:495-501); with flag,
+  // the lower state's sites i+1 and i+2 in the current bases: the left
+  // environment contracted into orth[i+1], orth[i+2] into the right one.  The
+  // latter contracts orth's middle leg: BlockTensor::contract lists the remaining
+  // bonds cyclically after the contracted one (src/block_tensor_inst.cpp:1067-1071),
+  // (orth.2, orth.0, env.1), which the contraction here gives after rotating orth
+  // to (orth.2, orth.0, orth.1); BlockTensor::shift(1, 0) then rotates the result
+  // to (orth.0, env.1, orth.2), the leg order of the right-side site tensors.
+  if (real_env)
+    for (int j = 0; j < exci; ++j) {
+      ovlp[j][i] = ops::overlap_transformation<S>(c, orth[j][i], uu[i], ovlp[j][i - 1], 0);
+      if (flag == 1) {
+        ovlp[j][i + 1] = ops::contract<S>(c, ovlp[j][i], 0, orth[j][i + 1], 0);
+        static const int cyc[3] = {2, 0, 1}, rot[3] = {1, 2, 0};
+        BTensor<S> t = ops::permute3<S>(c, orth[j][i + 2], cyc);
+        ovlp[j][i + 2] = ops::permute3<S>(c, ops::contract<S>(c, t, 2, ovlp[j][i + 3], 0), rot);
+      }
+    }
   BTensor<S> hnew;
   if (!hh[i - 1].null()) hnew = ops::overlap_transformation<S>(c, U, U, hh[i - 1], 0);
   std::vector<BTensor<S>> newopr(i);
@@ -1011,17 +1045,29 @@ void Chain<S>::prepare_site_operator_from_left(int i, bool real_env) {
 
 // DMRG::prepare_site_operator_from_right (src/dmrg_inst.cpp:515-583 and 643-695)
 template <class S>
-void Chain<S>::prepare_site_operator_from_right(int i, bool real_env) {
+void Chain<S>::prepare_site_operator_from_right(int i, bool real_env, int flag) {
   const double t0 = now_s();
   BTensor<S> u1;
   if (!real_env) u1 = ops::fuse<S>(c, uu[i].st.bonds[0], uu[i].st.bonds[1]);
   const BTensor<S>& U = real_env ? uu[i] : u1;
   if (real_env && i == ns - 1) {
     opr[i][i] = ops::operator_initial<S>(c, U, U, sigma[1], 1);
+    for (int j = 0; j < exci; ++j) ovlp[j][i] = ops::overlap_initial<S>(c, orth[j][i], uu[i], 1);
     hh[i] = BTensor<S>();
     timers.env += now_s() - t0;
     return;
   }
+  // the mirror image of the left update (src/dmrg_inst.cpp:567-573)
+  if (real_env)
+    for (int j = 0; j < exci; ++j) {
+      ovlp[j][i] = ops::overlap_transformation<S>(c, orth[j][i], uu[i], ovlp[j][i + 1], 1);
+      if (flag == 1) {
+        ovlp[j][i - 2] = ops::contract<S>(c, ovlp[j][i - 3], 0, orth[j][i - 2], 0);
+        static const int cyc[3] = {2, 0, 1}, rot[3] = {1, 2, 0};
+        BTensor<S> t = ops::permute3<S>(c, orth[j][i - 1], cyc);
+        ovlp[j][i - 1] = ops::permute3<S>(c, ops::contract<S>(c, t, 2, ovlp[j][i], 0), rot);
+      }
+    }
   BTensor<S> hnew;
   if (!hh[i + 1].null()) hnew = ops::overlap_transformation<S>(c, U, U, hh[i + 1], 1);
   std::vector<BTensor<S>> newopr(ns);
@@ -1058,6 +1104,14 @@ void Chain<S>::prepare_input_vector(int il, int ir, BTensor<S>& vec) {
   if (c.sym == Sym::SU2) ops::take_conjugate(left, 0);
   vec = ops::contract<S>(c, left, 0, rght, 0);
   ops::makeup_input_vector<S>(c, vec);
+  // the lower states in the same two-site basis (src/dmrg_inst.cpp:429-436)
+  if (il + 1 == ir)
+    for (int j = 0; j < exci; ++j) {
+      BTensor<S> lj = ops::overlap_initial<S>(c, ovlp[j][il], t1, 0);
+      BTensor<S> rj = ops::overlap_initial<S>(c, ovlp[j][ir], t2, 1);
+      overlapvec[j] = ops::contract<S>(c, lj, 0, rj, 0);
+      ops::makeup_input_vector<S>(c, overlapvec[j]);
+    }
   timers.prep += now_s() - t0;
 }
 
@@ -1117,6 +1171,36 @@ HeffPlan<S> Chain<S>::heff_plan(int il, int ir, const BTensor<S>& vec, bool tune
 }
 
 // DMRG::lanczos_solve_eigenvector_idmrg (src/dmrg_inst.cpp:264-279)
+// The excited-state penalty of DMRG::hamiltonian_vector_multiplication_idmrg
+// (src/dmrg_inst.cpp:352-363): out -= sum_j gs_enr[j] <overlapvec[j]|psi> overlapvec[j]
+// over the lower states j, their projections taken into psi's block layout (both
+// are built on the same fused bonds, so a block present in one is at the same
+// index in the other).
+template <class S>
+void Chain<S>::set_penalty(HeffPlan<S>& H, const BTensor<S>& vec) {
+  const size_t bytes = sizeof(S) * (size_t)H.n * exci;
+  H.pen_o = std::make_shared<DevBuf>(bytes, c.stream);
+  H.pen_wo = std::make_shared<DevBuf>(bytes, c.stream);
+  H.pen_dot = std::make_shared<DevBuf>(sizeof(S) * (exci + 1), c.stream);
+  SADMRG_CUDA(cudaMemsetAsync(H.pen_o->get(), 0, bytes, c.stream));
+  int q[8], d[8];
+  for (int j = 0; j < exci; ++j) {
+    const BTensor<S>& o = overlapvec[j];
+    SADMRG_REQUIRE(!o.null() && o.nten() == vec.nten(), SADMRG_ERR_STATE,
+                   "excited state: the lower state's projection does not match the two-site basis");
+    S* dst = static_cast<S*>(H.pen_o->get()) + (size_t)j * H.n;
+    for (long b = 0; b < vec.nten(); ++b) {
+      if (!vec.present(b) || !o.present(b) || !vec.st.block(b, q, d)) continue;
+      SADMRG_CUDA(cudaMemcpyAsync(dst + vec.off[b], o.data() + o.off[b], sizeof(S) * vec.st.block_elems(b),
+                                  cudaMemcpyDeviceToDevice, c.stream));
+    }
+  }
+  SADMRG_CUDA(cudaMemcpyAsync(H.pen_wo->get(), H.pen_o->get(), bytes, cudaMemcpyDeviceToDevice, c.stream));
+  for (int j = 0; j < exci; ++j)
+    launch_scale(kCx<S>, static_cast<S*>(H.pen_wo->get()) + (size_t)j * H.n, low_enr[j], 0.0, H.n, c.stream);
+  H.npen = exci;
+}
+
 template <class S>
 void Chain<S>::lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec) {
   const double t0 = now_s();
@@ -1132,6 +1216,7 @@ void Chain<S>::lanczos_solve_eigenvector(int il, int ir, BTensor<S>& vec) {
   const double tp = now_s();
   HeffPlan<S> H = heff_plan(il, ir, vec);
   timers.plan += now_s() - tp;
+  if (exci > 0 && il + 1 == ir) set_penalty(H, vec);
   LanczosStats st = lanczos_solve<S>(c, H, vec.data(), mlanc, prec);
   gs_enr = st.energy;
   if (std::getenv("SADMRG_VERBOSE"))
@@ -1147,6 +1232,10 @@ void Chain<S>::wavefunc_transformation(int i, int dir) {
   const double t0 = now_s();
   if (dir == 0) ops::right2left_vectran<S>(c, uu[i]);
   else ops::left2right_vectran<S>(c, uu[i]);
+  for (int j = 0; j < exci; ++j) {   // src/dmrg_inst.cpp:862-868
+    if (dir == 0) ops::right2left_vectran<S>(c, orth[j][i]);
+    else ops::left2right_vectran<S>(c, orth[j][i]);
+  }
   timers.prep += now_s() - t0;
 }
 
@@ -1207,6 +1296,7 @@ static void edge_tensors(Chain<S>& ch, Bond& bphys_l, Bond& bphys_r) {
 // DMRG::do_idmrg (src/dmrg_inst.cpp:699-804)
 template <class S>
 void Chain<S>::do_idmrg() {
+  SADMRG_REQUIRE(exci == 0, SADMRG_ERR_STATE, "chain: an excited state starts from read_mps, not iDMRG");
   Bond bl, br;
   edge_tensors(*this, bl, br);
   BTensor<S> vec;
@@ -1236,8 +1326,8 @@ void Chain<S>::prepare_sweep() {
   Bond bl, br;
   edge_tensors(*this, bl, br);
   for (int i = 0; i < ns / 2 - 1; ++i) {
-    prepare_site_operator_from_left(i, true);
-    prepare_site_operator_from_right(ns - 1 - i, true);
+    prepare_site_operator_from_left(i, true, 0);
+    prepare_site_operator_from_right(ns - 1 - i, true, i < ns / 2 - 2 ? 0 : 1);
   }
 }
 
@@ -1247,7 +1337,7 @@ void Chain<S>::sweep() {
   BTensor<S> vec;
   for (int i = ns / 2; i >= nfree + 2; --i) {
     wavefunc_transformation(i - 1, 1);
-    prepare_site_operator_from_right(i, true);
+    prepare_site_operator_from_right(i, true, 1);
     prepare_input_vector(i - 2, i - 1, vec);
     prepare_site_operator_from_left(i - 2, false);
     prepare_site_operator_from_right(i - 1, false);
@@ -1257,7 +1347,7 @@ void Chain<S>::sweep() {
   }
   for (int i = nfree; i < ns - nfree - 2; ++i) {
     wavefunc_transformation(i + 1, 0);
-    prepare_site_operator_from_left(i, true);
+    prepare_site_operator_from_left(i, true, 1);
     prepare_input_vector(i + 1, i + 2, vec);
     prepare_site_operator_from_left(i + 1, false);
     prepare_site_operator_from_right(i + 2, false);
@@ -1267,7 +1357,7 @@ void Chain<S>::sweep() {
   }
   for (int i = ns - nfree - 1; i >= ns / 2 + 1; --i) {
     wavefunc_transformation(i - 1, 1);
-    prepare_site_operator_from_right(i, true);
+    prepare_site_operator_from_right(i, true, 1);
     prepare_input_vector(i - 2, i - 1, vec);
     prepare_site_operator_from_left(i - 2, false);
     prepare_site_operator_from_right(i - 1, false);
@@ -1277,11 +1367,35 @@ void Chain<S>::sweep() {
   }
 }
 
+// DMRG::read_mps (src/dmrg_inst.cpp:1031-1079): this state's site tensors,
+// uu-<ns>-<D>-<2S>-<exci>-<i>; for an excited state also, as
+// DMRG::read_mps(read1, read2) (:1081-1140), the lower states idx < exci into orth
+// and their last energies from enr-<ns>-<D>-<2S>-<idx>.dat
 template <class S>
 bool Chain<S>::read_mps(const std::string& dir, int bond_read) {
+  if (!read_state(dir, bond_read, exci, uu)) return false;
+  for (int idx = 0; idx < exci; ++idx) {
+    SADMRG_REQUIRE(read_state(dir, bond_read, idx, orth[idx]), SADMRG_ERR_ARG,
+                   "read_mps: lower state " + std::to_string(idx) + " not found in " + dir);
+    const std::string name = dir + "/enr-" + std::to_string(ns) + "-" + std::to_string(bond_read) + "-" +
+                             std::to_string(totspin) + "-" + std::to_string(idx) + ".dat";
+    FILE* f = std::fopen(name.c_str(), "r");
+    SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "read_mps: no energy of lower state " + std::to_string(idx) + " (" + name + ")");
+    double e;
+    bool any = false;
+    while (std::fscanf(f, "%lf", &e) == 1) { low_enr[idx] = e; any = true; }
+    std::fclose(f);
+    SADMRG_REQUIRE(any, SADMRG_ERR_ARG, "read_mps: empty " + name);
+  }
+  return true;
+}
+
+template <class S>
+bool Chain<S>::read_state(const std::string& dir, int bond_read, int idx, std::vector<BTensor<S>>& out) {
+  out.resize(ns);
   for (int i = 0; i < ns; ++i) {
     const std::string base = dir + "/uu-" + std::to_string(ns) + "-" + std::to_string(bond_read) + "-" +
-                             std::to_string(totspin) + "-0-" + std::to_string(i);
+                             std::to_string(totspin) + "-" + std::to_string(idx) + "-" + std::to_string(i);
     FILE* f = std::fopen((base + ".dat").c_str(), "r");
     if (!f) return false;
     int nb = 0, lc = 0;
@@ -1309,7 +1423,7 @@ bool Chain<S>::read_mps(const std::string& dir, int bond_read) {
     const size_t got = std::fread(data.data(), sizeof(S), ndata, fb);
     std::fclose(fb);
     SADMRG_REQUIRE((long long)got == ndata, SADMRG_ERR_ARG, "read_mps: short " + base + ".bin");
-    uu[i] = ops::from_host<S>(c, st, pres, data.data());
+    out[i] = ops::from_host<S>(c, st, pres, data.data());
   }
   return true;
 }
@@ -1319,7 +1433,7 @@ void Chain<S>::save_mps(const std::string& dir) const {
   for (int i = 0; i < ns; ++i) {
     const BTensor<S>& t = uu[i];
     const std::string base = dir + "/uu-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
-                             std::to_string(totspin) + "-0-" + std::to_string(i);
+                             std::to_string(totspin) + "-" + std::to_string(exci) + "-" + std::to_string(i);
     FILE* f = std::fopen((base + ".dat").c_str(), "w");
     SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "save_mps: cannot write " + base + ".dat");
     std::fprintf(f, "%d\t%d\n", t.st.nbond(), t.st.locspin);
@@ -1354,12 +1468,12 @@ void Chain<S>::save_mps(const std::string& dir) const {
 }
 
 // DMRG::save_ww (src/dmrg_inst.cpp:1145-1153): bondd * phdim doubles of the ww
-// array, ww-<ns>-<bondd>-<2S>-0.bin (the array is kept at least that long here,
+// array, ww-<ns>-<bondd>-<2S>-<exci>.bin (the array is kept at least that long here,
 // zero beyond what the truncations wrote)
 template <class S>
 void Chain<S>::save_ww(const std::string& dir) const {
   const std::string name = dir + "/ww-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
-                           std::to_string(totspin) + "-0.bin";
+                           std::to_string(totspin) + "-" + std::to_string(exci) + ".bin";
   std::vector<double> w((size_t)bondd * (physpn + 1), 0.0);
   std::copy(ww.begin(), ww.begin() + std::min(ww.size(), w.size()), w.begin());
   FILE* f = std::fopen(name.c_str(), "wb");
@@ -1370,11 +1484,11 @@ void Chain<S>::save_ww(const std::string& dir) const {
 }
 
 // DMRG::read_ww (src/dmrg_inst.cpp:1156-1165): the first read1 doubles of
-// ww-<ns>-<read1>-<2S>-0.bin, or read1 ones when the file is absent
+// ww-<ns>-<read1>-<2S>-<exci>.bin, or read1 ones when the file is absent
 template <class S>
 void Chain<S>::read_ww(const std::string& dir, int read1) {
   const std::string name = dir + "/ww-" + std::to_string(ns) + "-" + std::to_string(read1) + "-" +
-                           std::to_string(totspin) + "-0.bin";
+                           std::to_string(totspin) + "-" + std::to_string(exci) + ".bin";
   if (ww.size() < (size_t)read1) ww.resize(read1, 0.0);
   FILE* f = std::fopen(name.c_str(), "rb");
   if (!f) {
@@ -1391,7 +1505,7 @@ void Chain<S>::read_ww(const std::string& dir, int read1) {
 template <class S>
 void Chain<S>::save_enr(const std::string& dir) const {
   const std::string name = dir + "/enr-" + std::to_string(ns) + "-" + std::to_string(bondd) + "-" +
-                           std::to_string(totspin) + "-0.dat";
+                           std::to_string(totspin) + "-" + std::to_string(exci) + ".dat";
   FILE* f = std::fopen(name.c_str(), "a");
   SADMRG_REQUIRE(f, SADMRG_ERR_ARG, "save_enr: cannot write " + name);
   std::fprintf(f, "%.16g\n", gs_enr);
@@ -1399,11 +1513,11 @@ void Chain<S>::save_enr(const std::string& dir) const {
 }
 
 // DMRG::read_enr (src/dmrg_inst.cpp:1008-1016): gs_enr = the last value of
-// enr-<ns>-<read1>-<2S>-0.dat; unchanged when the file is absent
+// enr-<ns>-<read1>-<2S>-<exci>.dat; unchanged when the file is absent
 template <class S>
 void Chain<S>::read_enr(const std::string& dir, int read1) {
   const std::string name = dir + "/enr-" + std::to_string(ns) + "-" + std::to_string(read1) + "-" +
-                           std::to_string(totspin) + "-0.dat";
+                           std::to_string(totspin) + "-" + std::to_string(exci) + ".dat";
   FILE* f = std::fopen(name.c_str(), "r");
   if (!f) return;
   double e;

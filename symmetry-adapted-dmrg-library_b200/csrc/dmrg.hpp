@@ -152,10 +152,17 @@ class Chain {
   double energy() const { return gs_enr; }
   // Dz (S_a x S_b)_z on every J1 bond a < b (U(1), complex only; before iDMRG)
   void set_dm(double d);
+  // the k-th excited state (the constructor's max_exci, src/dmrg_inst.cpp:64-112):
+  // read_mps then loads this state's files (index k) and the lower states' (0 .. k-1,
+  // into orth) with their energies, and the sweeps add the overlap environments and
+  // the penalty (U(1) chains; before read_mps)
+  void set_excited(int k);
 
   // building blocks (public for the frozen-problem API and tests)
-  void prepare_site_operator_from_left(int i, bool real_env);
-  void prepare_site_operator_from_right(int i, bool real_env);
+  // flag (real environments of an excited-state chain): also the lower states
+  // projected on sites i+1, i+2 (from the left) or i-2, i-1 (from the right)
+  void prepare_site_operator_from_left(int i, bool real_env, int flag = 0);
+  void prepare_site_operator_from_right(int i, bool real_env, int flag = 0);
   void prepare_input_vector(int il, int ir, BTensor<S>& vec);
   void prepare_input_vector_initial(int il, int ir, BTensor<S>& vec);
   HeffPlan<S> heff_plan(int il, int ir, const BTensor<S>& vec, bool tune = false);
@@ -163,6 +170,7 @@ class Chain {
   void wavefunc_transformation(int i, int dir);
   // DMRG::read_mps / save_mps2 checkpoint format (src/dmrg_inst.cpp:947-1079)
   bool read_mps(const std::string& dir, int bond_read);
+  bool read_state(const std::string& dir, int bond_read, int idx, std::vector<BTensor<S>>& out);
   void save_mps(const std::string& dir) const;
   // DMRG::save_ww / read_ww / save_enr / read_enr (src/dmrg_inst.cpp:993-1030, 1145-1177)
   void save_ww(const std::string& dir) const;
@@ -185,6 +193,14 @@ class Chain {
   std::vector<std::vector<BTensor<S>>> opr;
   std::array<BTensor<S>, 2> sigma;
   double gs_enr = 0.0;
+  // excited states (set_excited): exci lower states orth[j][i], their overlap
+  // environments with uu ovlp[j][i] (site tensors of the lower state projected on
+  // the current basis at the two sites of a step), their energies and their
+  // projections on the current two-site basis (the penalty vectors)
+  int exci = 0;
+  std::vector<std::vector<BTensor<S>>> orth, ovlp;
+  std::vector<double> low_enr;
+  std::vector<BTensor<S>> overlapvec;
   // singular values of the truncations, laid out as the reference's ww array:
   // each truncation overwrites its first n values (kept, then discarded)
   std::vector<double> ww;
@@ -205,6 +221,7 @@ class Chain {
   void random_init(BTensor<S>& t);
   void init_local_operators();
   void svd_step(BTensor<S>& vec, int il, int ir, double p1, double p2);
+  void set_penalty(HeffPlan<S>& H, const BTensor<S>& vec);
   void add_coupled(BTensor<S>& op, const BTensor<S>& src, int a, int b);
 };
 

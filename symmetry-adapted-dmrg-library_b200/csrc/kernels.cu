@@ -65,6 +65,27 @@ void launch_block_transpose(bool cplx, void* dst, const void* src, const Transp*
   else block_transpose_kernel<double><<<grid, 256, 0, s>>>((double*)dst, (const double*)src, t);
 }
 
+// leg permutation of 3-leg blocks: one block of threads per tensor block, every
+// destination element gathered from its source position (the tensors this serves,
+// projected lower states of an excited-state sweep, are small)
+template <class T>
+__global__ void permute3_kernel(T* dst, const T* src, const Perm3* jobs) {
+  const Perm3 J = jobs[blockIdx.x];
+  const long long nd0 = J.d[J.p[0]], nd1 = J.d[J.p[1]], n = (long long)J.d[0] * J.d[1] * J.d[2];
+  const long long st[3] = {1, J.d[0], (long long)J.d[0] * J.d[1]};   // source strides
+  for (long long e = threadIdx.x + (long long)blockIdx.y * blockDim.x; e < n; e += (long long)blockDim.x * gridDim.y) {
+    const long long i0 = e % nd0, i1 = (e / nd0) % nd1, i2 = e / (nd0 * nd1);
+    dst[J.doff + e] = src[J.soff + i0 * st[J.p[0]] + i1 * st[J.p[1]] + i2 * st[J.p[2]]];
+  }
+}
+
+void launch_permute3(bool cplx, void* dst, const void* src, const Perm3* t, int nt, cudaStream_t s) {
+  if (nt <= 0) return;
+  dim3 grid(nt, 8);
+  if (cplx) permute3_kernel<double2><<<grid, 256, 0, s>>>((double2*)dst, (const double2*)src, t);
+  else permute3_kernel<double><<<grid, 256, 0, s>>>((double*)dst, (const double*)src, t);
+}
+
 template <bool CPLX>
 __global__ void fuse_fill_kernel(void* data, const FuseFill* f) {
   const FuseFill ff = f[blockIdx.x];

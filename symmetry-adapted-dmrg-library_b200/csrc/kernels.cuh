@@ -164,6 +164,12 @@ struct Transp {               // dst (cols x rows) = src (rows x cols)^T
 };
 void launch_block_transpose(bool cplx, void* dst, const void* src, const Transp* t, int nt, cudaStream_t s);
 
+struct Perm3 {                // dst block = src block (d0 x d1 x d2, column-major) with its legs
+  long long soff, doff;       // permuted: leg k of dst is leg p[k] of src
+  int d[3], p[3];
+};
+void launch_permute3(bool cplx, void* dst, const void* src, const Perm3* t, int nt, cudaStream_t s);
+
 struct FuseFill {             // identity embedding of a fuse block (d0,d1,d2): 1 at (a,b,pos+b*d0+a)
   long long off;
   int d0, d1, d2, pos;

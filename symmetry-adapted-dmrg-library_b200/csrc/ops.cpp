@@ -1245,6 +1245,49 @@ static void vectran(Ctx& c, BTensor<S>& t, int ishift, int s0, int s1) {
 template <class S> void left2right_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 2, 1, 0); }
 template <class S> void right2left_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 1, 2, 0); }
 
+// leg permutation of a 3-leg U(1) tensor (BlockTensor::shift / exchangeindex,
+// src/block_tensor_inst.cpp:913-990): the bonds move with their directions, a
+// block keeps its presence under its permuted labels and its data is permuted
+// on the device.  SU(2) tensors are refused: their CGC blocks would move along,
+// which the reduced-element representation here does not express.
+template <class S>
+BTensor<S> permute3(Ctx& c, const BTensor<S>& t, const int p[3]) {
+  SADMRG_REQUIRE(c.sym == Sym::U1, SADMRG_ERR_ARG, "permute3: U(1) tensors only");
+  SADMRG_REQUIRE(t.st.nbond() == 3, SADMRG_ERR_ARG, "permute3: a 3-leg tensor");
+  std::vector<Bond> nb(3);
+  for (int k = 0; k < 3; ++k) nb[k] = t.st.bonds[p[k]];
+  Struct nst(c.sym, t.st.locspin, nb);
+  std::vector<char> pres(nst.nten(), 0);
+  std::vector<std::pair<long, long>> map;
+  int q[8], d[8];
+  for (long i = 0; i < t.nten(); ++i) {
+    if (!t.present(i) || !t.st.block(i, q, d)) continue;
+    const int nq[3] = {q[p[0]], q[p[1]], q[p[2]]};
+    const long j = nst.index(nq);
+    SADMRG_REQUIRE(j >= 0 && nst.allowed_labels(nq), SADMRG_ERR_STATE, "permute3: a block without a place");
+    pres[j] = 1;
+    map.push_back({i, j});
+  }
+  BTensor<S> n = alloc_tensor<S>(c, nst, pres);
+  std::vector<Perm3> jobs;
+  for (auto& ij : map) {
+    t.st.block(ij.first, q, d);
+    Perm3 J{};
+    J.soff = t.off[ij.first];
+    J.doff = n.off[ij.second];
+    for (int k = 0; k < 3; ++k) { J.d[k] = d[k]; J.p[k] = p[k]; }
+    jobs.push_back(J);
+  }
+  if (!jobs.empty()) {
+    DevBuf dj(sizeof(Perm3) * jobs.size(), c.stream);
+    SADMRG_CUDA(cudaMemcpyAsync(dj.get(), jobs.data(), sizeof(Perm3) * jobs.size(), cudaMemcpyHostToDevice, c.stream));
+    launch_permute3(kC<S>, n.data(), t.data(), dj.as<Perm3>(), (int)jobs.size(), c.stream);
+    ++c.launches;
+    SADMRG_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return n;
+}
+
 template <class S>
 BTensor<S> from_host(Ctx& c, const Struct& st, const std::vector<char>& present, const S* data) {
   BTensor<S> t = alloc_tensor<S>(c, st, present);
@@ -1282,6 +1325,7 @@ std::vector<S> to_host(Ctx& c, const BTensor<S>& t) {
   template void makeup_input_vector<S>(Ctx&, BTensor<S>&);                                                       \
   template void left2right_vectran<S>(Ctx&, BTensor<S>&);                                                        \
   template void right2left_vectran<S>(Ctx&, BTensor<S>&);                                                        \
+  template BTensor<S> permute3<S>(Ctx&, const BTensor<S>&, const int*);                                          \
   template BTensor<S> from_host<S>(Ctx&, const Struct&, const std::vector<char>&, const S*);                     \
   template std::vector<S> to_host<S>(Ctx&, const BTensor<S>&);
 

@@ -30,7 +30,7 @@ EXPORTED = [
     "sadmrg_version", "sadmrg_create", "sadmrg_destroy", "sadmrg_last_error",
     "sadmrg_set_lanczos_tol", "sadmrg_heff_plan", "sadmrg_heff_info", "sadmrg_heff_apply", "sadmrg_heff_apply_device", "sadmrg_heff_apply_noalloc",
     "sadmrg_heff_profile", "sadmrg_heff_lanczos", "sadmrg_heff_lanczos2", "sadmrg_svd_truncate",
-    "sadmrg_chain_create", "sadmrg_chain_set_dm", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
+    "sadmrg_chain_create", "sadmrg_chain_set_dm", "sadmrg_chain_set_excited", "sadmrg_chain_set_precision", "sadmrg_chain_idmrg", "sadmrg_chain_prepare_sweep",
     "sadmrg_chain_sweep", "sadmrg_chain_read_mps", "sadmrg_chain_save_mps", "sadmrg_chain_freeze", "sadmrg_chain_bond", "sadmrg_chain_stats", "sadmrg_chain_set_tensor",
     "sadmrg_chain_stage_tensor", "sadmrg_chain_env_update", "sadmrg_staged_info", "sadmrg_staged_read",
     "sadmrg_device_status", "sadmrg_heff_launch_profile", "sadmrg_set_matvec_fusion", "sadmrg_heff_graph_bench",
@@ -105,6 +105,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_chain_create": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
         "sadmrg_chain_set_precision": ([vp, C.c_int], C.c_int),
         "sadmrg_chain_set_dm": ([vp, C.c_double], C.c_int),
+        "sadmrg_chain_set_excited": ([vp, C.c_int], C.c_int),
         "sadmrg_chain_idmrg": ([vp, dp], C.c_int),
         "sadmrg_chain_prepare_sweep": ([vp], C.c_int),
         "sadmrg_chain_sweep": ([vp, dp], C.c_int),
@@ -494,6 +495,11 @@ class Handle:
     def chain_set_dm(self, dz: float):
         """Dz (S_a x S_b)_z on every J1 bond (U(1) complex chains, before iDMRG)."""
         self._check(self.lib.sadmrg_chain_set_dm(self.h, float(dz)), "chain_set_dm")
+
+    def chain_set_excited(self, exci: int):
+        """Target excited state exci (U(1) chains, before chain_read_mps): the lower
+        states 0 .. exci-1 and their energies are read with the chain's own files."""
+        self._check(self.lib.sadmrg_chain_set_excited(self.h, int(exci)), "chain_set_excited")
 
     def chain_set_precision(self, prec: int):
         self._check(self.lib.sadmrg_chain_set_precision(self.h, int(prec)), "chain_set_precision")

@@ -9,13 +9,20 @@ Run in a container that has the reference sources (the harness is built by
   energy and the SVD factors / singular values that follow.
 * ``sweeps_<case>.npz``   -- energies after iDMRG and after every sweep, and the
   sector dimensions of every bond after every sweep.
+* ``excited_<case>.npz``  -- the first excited state: the reference's ground-state
+  sweeps and the checkpoint and energy files they wrote (save_mps2(0), save_enr),
+  then its excited-state sweeps (DMRG(..., max_exci = 1), read_mps(D, D) with the
+  ground state also as the starting state): energies and bonds after every
+  sweep, and the exact eigenvalues of the chain's Sz = 0 sector.
 * ``baseline_<case>.npz`` -- the same for the benchmark configurations, run with
   the benchmark's Lanczos settings (at most 100 steps, stop at |<v|Hv>|/|Hv|
   within 1e-10 of 1; the reference's constants are 40 and 1e-8), with the
   reference's iDMRG checkpoint (both sides sweep from it) and the checkpoint
   files of singular values and energies its sweeps wrote (ww-*.bin, enr-*.dat).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             # all but configuration 2
+    python tests/golden/make_golden.py --config2   # configuration 2 only
+    python tests/golden/make_golden.py --excited   # the excited-state cases only
 """
 from __future__ import annotations
 
@@ -62,6 +69,15 @@ SWEEP_CASES = {
 # with the same reference build)
 CONFIG2 = ("su2_L100_D512", ["-sym", "su2", "-L", "100", "-d", "512", "-sweeps", "8", "-maxangm", "40"],
            ["-mlanc", "100", "-lanc_check", "1e-12"])
+# excited states (U(1) chains): ground state by iDMRG + 3 sweeps, then 4 sweeps of the
+# first excited state started from it, both with a Lanczos stop test no solve passes
+# (all 100 steps), so that both sides follow the same path through the unconverged
+# first sweeps
+EXCITED_LANCZOS = ["-mlanc", "100", "-lanc_check", "1e-14"]
+EXCITED_CASES = {
+    "u1_L12_D16": ["-sym", "u1", "-L", "12", "-d", "16"],
+    "u1c_j2_L12_D16": ["-sym", "u1", "-cplx", "1", "-L", "12", "-d", "16", "-J2", "0.5"],
+}
 BASELINE_CASES = {
     "u1_L32_D64": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"], ["-mlanc", "100", "-lanc_check", "1e-10"]),
     "u1_L32_D64_converged": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"],
@@ -137,6 +153,35 @@ def main():
                             energies=np.array(energies), bonds_per_sweep=np.array(per_sweep),
                             bonds_idmrg=np.array(idmrg_bonds))
         print("wrote baseline", name, e_idmrg, energies)
+        return
+    if "--excited" in sys.argv:
+        sys.path.insert(0, ROOT)
+        from oracle.ed import chain_bonds, hamiltonian
+        for name, args in EXCITED_CASES.items():
+            arrays = {}
+            with tempfile.TemporaryDirectory() as wd:
+                gsd, exd = os.path.join(wd, "gs"), os.path.join(wd, "ex")
+                out_gs = run(args + EXCITED_LANCZOS + ["-sweeps", "3", "-sweepdir", gsd], wd)
+                for fn in sorted(os.listdir(gsd)):
+                    if fn.startswith(("uu-", "enr-")):
+                        arrays["gs__" + fn] = np.frombuffer(open(os.path.join(gsd, fn), "rb").read(), dtype=np.uint8)
+                        if fn.startswith("uu-"):   # the excited run starts from the ground state
+                            parts = fn.split("-")
+                            parts[4] = "1"
+                            shutil.copy(os.path.join(gsd, fn), os.path.join(gsd, "-".join(parts)))
+                out_ex = run(args + EXCITED_LANCZOS + ["-sweeps", "4", "-exci", "1", "-read", gsd, "-sweepdir", exd], wd)
+            _, e_gs, _ = parse_sweeps(out_gs)
+            _, energies, bonds = parse_sweeps(out_ex)
+            per_sweep = [[f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])]
+                         for s_ in sorted(k for k in bonds if k >= 0)]
+            L = int(args[args.index("-L") + 1])
+            J2 = float(args[args.index("-J2") + 1]) if "-J2" in args else 0.0
+            ed = np.linalg.eigvalsh(hamiltonian(L, chain_bonds(L, False, J2), two_sz=0))[:3]
+            np.savez_compressed(os.path.join(HERE, f"excited_{name}.npz"), args=np.array(" ".join(args)),
+                                lanczos=np.array(" ".join(EXCITED_LANCZOS)),
+                                energies_gs=np.array(e_gs), energies=np.array(energies),
+                                bonds_per_sweep=np.array(per_sweep), ed=ed, **arrays)
+            print("wrote excited", name, e_gs[-1], energies, ed)
         return
     only_baseline = "--baseline-only" in sys.argv
     for name, args in ({} if only_baseline else CENTRE_CASES).items():
