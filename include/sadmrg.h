@@ -266,8 +266,8 @@ int sadmrg_chain_set_dm(sadmrg_handle* h, double dz);
  * read2) (:1081-1140), the lower states 0 .. exci-1 and the last energy of each
  * (enr-<ns>-<D>-<2S>-<idx>.dat); the sweeps keep their overlap environments
  * (:440-583, 862-868), project them on every two-site basis (:412-437) and add
- * the penalty -E_j <o_j|psi> o_j to H_eff*psi (:352-363).  U(1) chains only
- * (SADMRG_ERR_ARG for SU(2)); an excited state starts from read_mps, not iDMRG.
+ * the penalty -E_j <o_j|psi> o_j to H_eff*psi (:352-363).  U(1) and SU(2);
+ * an excited state starts from read_mps, not iDMRG.
  * Checkpoint, ww and enr files carry the state's index. */
 int sadmrg_chain_set_excited(sadmrg_handle* h, int exci);
 int sadmrg_chain_set_precision(sadmrg_handle* h, int precision);

@@ -968,8 +968,6 @@ void Chain<S>::set_dm(double d) {
 template <class S>
 void Chain<S>::set_excited(int k) {
   SADMRG_REQUIRE(k >= 0 && k <= 16, SADMRG_ERR_ARG, "chain: excited state index 0..16");
-  SADMRG_REQUIRE(k == 0 || c.sym == Sym::U1, SADMRG_ERR_ARG,
-                 "chain: excited states are built for U(1) chains (the SU(2) projections move CGC blocks)");
   for (int i = 0; i < ns; ++i)
     SADMRG_REQUIRE(uu[i].null() && hh[i].null(), SADMRG_ERR_STATE,
                    "chain: set the excited state before iDMRG or loading a checkpoint");
@@ -1109,6 +1107,7 @@ void Chain<S>::prepare_input_vector(int il, int ir, BTensor<S>& vec) {
     for (int j = 0; j < exci; ++j) {
       BTensor<S> lj = ops::overlap_initial<S>(c, ovlp[j][il], t1, 0);
       BTensor<S> rj = ops::overlap_initial<S>(c, ovlp[j][ir], t2, 1);
+      if (c.sym == Sym::SU2) ops::take_conjugate(lj, 0);
       overlapvec[j] = ops::contract<S>(c, lj, 0, rj, 0);
       ops::makeup_input_vector<S>(c, overlapvec[j]);
     }

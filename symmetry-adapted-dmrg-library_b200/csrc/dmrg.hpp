@@ -155,7 +155,7 @@ class Chain {
   // the k-th excited state (the constructor's max_exci, src/dmrg_inst.cpp:64-112):
   // read_mps then loads this state's files (index k) and the lower states' (0 .. k-1,
   // into orth) with their energies, and the sweeps add the overlap environments and
-  // the penalty (U(1) chains; before read_mps)
+  // the penalty (before read_mps; U(1) and SU(2))
   void set_excited(int k);
 
   // building blocks (public for the frozen-problem API and tests)

@@ -1245,14 +1245,13 @@ static void vectran(Ctx& c, BTensor<S>& t, int ishift, int s0, int s1) {
 template <class S> void left2right_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 2, 1, 0); }
 template <class S> void right2left_vectran(Ctx& c, BTensor<S>& t) { vectran(c, t, 1, 2, 0); }
 
-// leg permutation of a 3-leg U(1) tensor (BlockTensor::shift / exchangeindex,
-// src/block_tensor_inst.cpp:913-990): the bonds move with their directions, a
-// block keeps its presence under its permuted labels and its data is permuted
-// on the device.  SU(2) tensors are refused: their CGC blocks would move along,
-// which the reduced-element representation here does not express.
+// leg permutation of a 3-leg tensor (BlockTensor::shift / exchangeindex,
+// src/block_tensor_inst.cpp:913-990, SU2Struct::shift src/symmetry/su2.cpp:509-518):
+// the bonds move with their directions, a block keeps its presence under its
+// permuted labels and its data is permuted on the device; for SU(2) the
+// reference moves the CGC blocks along, which here the permuted bonds imply.
 template <class S>
 BTensor<S> permute3(Ctx& c, const BTensor<S>& t, const int p[3]) {
-  SADMRG_REQUIRE(c.sym == Sym::U1, SADMRG_ERR_ARG, "permute3: U(1) tensors only");
   SADMRG_REQUIRE(t.st.nbond() == 3, SADMRG_ERR_ARG, "permute3: a 3-leg tensor");
   std::vector<Bond> nb(3);
   for (int k = 0; k < 3; ++k) nb[k] = t.st.bonds[p[k]];

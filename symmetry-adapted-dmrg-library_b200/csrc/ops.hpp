@@ -24,9 +24,10 @@ template <class S>
 BTensor<S> operator_pairup(Ctx& c, const BTensor<S>& uu, const BTensor<S>& vv, const BTensor<S>& op1,
                            const BTensor<S>& op2, int flag);
 template <class S> BTensor<S> contract(Ctx& c, const BTensor<S>& t1, int i1, const BTensor<S>& t2, int i2);
-// leg permutation of a 3-leg U(1) tensor: leg k of the result is leg p[k] of t
-// (BlockTensor::shift / exchangeindex, src/block_tensor_inst.cpp:913-990, for U(1),
-// where no CGC block moves along)
+// leg permutation of a 3-leg tensor: leg k of the result is leg p[k] of t, the
+// bonds moving with their directions (BlockTensor::shift / exchangeindex,
+// src/block_tensor_inst.cpp:913-990; for SU(2) the CGC blocks the reference moves
+// along are implied by the permuted bonds)
 template <class S> BTensor<S> permute3(Ctx& c, const BTensor<S>& t, const int p[3]);
 
 // dst = dst (+) alpha * src with the reference's operator+= presence rules

@@ -497,7 +497,7 @@ class Handle:
         self._check(self.lib.sadmrg_chain_set_dm(self.h, float(dz)), "chain_set_dm")
 
     def chain_set_excited(self, exci: int):
-        """Target excited state exci (U(1) chains, before chain_read_mps): the lower
+        """Target excited state exci (before chain_read_mps): the lower
         states 0 .. exci-1 and their energies are read with the chain's own files."""
         self._check(self.lib.sadmrg_chain_set_excited(self.h, int(exci)), "chain_set_excited")
 

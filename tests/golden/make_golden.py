@@ -13,7 +13,8 @@ Run in a container that has the reference sources (the harness is built by
   sweeps and the checkpoint and energy files they wrote (save_mps2(0), save_enr),
   then its excited-state sweeps (DMRG(..., max_exci = 1), read_mps(D, D) with the
   ground state also as the starting state): energies and bonds after every
-  sweep, and the exact eigenvalues of the chain's Sz = 0 sector.
+  sweep, and the exact eigenvalues of the chain's Sz = 0 sector (of its singlets
+  for an SU(2) chain).
 * ``baseline_<case>.npz`` -- the same for the benchmark configurations, run with
   the benchmark's Lanczos settings (at most 100 steps, stop at |<v|Hv>|/|Hv|
   within 1e-10 of 1; the reference's constants are 40 and 1e-8), with the
@@ -77,6 +78,7 @@ EXCITED_LANCZOS = ["-mlanc", "100", "-lanc_check", "1e-14"]
 EXCITED_CASES = {
     "u1_L12_D16": ["-sym", "u1", "-L", "12", "-d", "16"],
     "u1c_j2_L12_D16": ["-sym", "u1", "-cplx", "1", "-L", "12", "-d", "16", "-J2", "0.5"],
+    "su2_L12_D16": ["-sym", "su2", "-L", "12", "-d", "16"],
 }
 BASELINE_CASES = {
     "u1_L32_D64": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"], ["-mlanc", "100", "-lanc_check", "1e-10"]),
@@ -176,7 +178,13 @@ def main():
                          for s_ in sorted(k for k in bonds if k >= 0)]
             L = int(args[args.index("-L") + 1])
             J2 = float(args[args.index("-J2") + 1]) if "-J2" in args else 0.0
-            ed = np.linalg.eigvalsh(hamiltonian(L, chain_bonds(L, False, J2), two_sz=0))[:3]
+            w, v = np.linalg.eigh(hamiltonian(L, chain_bonds(L, False, J2), two_sz=0))
+            if "su2" in args:
+                # the SU(2) chain targets total spin 0: the lowest singlets, by <S^2> (S_i.S_j over all pairs)
+                s2 = hamiltonian(L, [(a, b, 1.0, True) for a in range(L) for b in range(a + 1, L)], two_sz=0)
+                s2 = 0.75 * L * np.eye(len(w)) + 2.0 * s2
+                w = w[np.abs(np.einsum("ik,ij,jk->k", v, s2, v)) < 1e-6]
+            ed = w[:3]
             np.savez_compressed(os.path.join(HERE, f"excited_{name}.npz"), args=np.array(" ".join(args)),
                                 lanczos=np.array(" ".join(EXCITED_LANCZOS)),
                                 energies_gs=np.array(e_gs), energies=np.array(energies),

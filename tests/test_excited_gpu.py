@@ -1,4 +1,4 @@
-"""The first excited state of U(1) chains on the GPU against the reference's own
+"""The first excited state of U(1) and SU(2) chains on the GPU against the reference's own
 excited-state sweeps (tests/golden/excited_*.npz, made by make_golden.py --excited).
 
 Both sides run the Lanczos with a stop test no solve passes (all 100 steps, as the
@@ -34,7 +34,8 @@ CASES = sorted(glob.glob(os.path.join(GOLDEN, "excited_*.npz")))
 def _parse(args):
     t = args.split()
     o = {t[i][1:]: t[i + 1] for i in range(0, len(t), 2)}
-    return dict(cplx=o.get("cplx", "0") == "1", L=int(o["L"]), D=int(o["d"]), J2=float(o.get("J2", "0")))
+    return dict(sym=1 if o.get("sym") == "su2" else 0, cplx=o.get("cplx", "0") == "1", L=int(o["L"]), D=int(o["d"]),
+                J2=float(o.get("J2", "0")))
 
 
 @pytest.mark.parametrize("path", CASES, ids=lambda p: os.path.basename(p))
@@ -44,7 +45,7 @@ def test_excited_state_sweeps_match_reference(path):
     z = np.load(path)
     a = _parse(str(z["args"]))
     L, D = a["L"], a["D"]
-    h = sadmrg.Handle(sym=sadmrg.SYM_U1, cplx=a["cplx"])
+    h = sadmrg.Handle(sym=a["sym"], cplx=a["cplx"])
     h.chain_create(1, L, D, 1, 0, True, a["J2"])
     lz = str(z["lanczos"]).split()   # the reference run's Lanczos length and stop test
     h.chain_set_mlanc(int(lz[lz.index("-mlanc") + 1]))
@@ -79,11 +80,3 @@ def test_excited_state_sweeps_match_reference(path):
         names = os.listdir(out)
         assert f"uu-{L}-{D}-0-1-0.dat" in names and f"enr-{L}-{D}-0-1.dat" in names, sorted(names)[:4]
     assert h.device_status() == 0
-
-
-def test_excited_state_refused_for_su2():
-    import sadmrg
-    h = sadmrg.Handle(sym=sadmrg.SYM_SU2, cplx=False)
-    h.chain_create(1, 12, 16, 1, 0, True, 0.0)
-    with pytest.raises(sadmrg.SadmrgError, match="U\\(1\\)"):
-        h.chain_set_excited(1)
