@@ -79,6 +79,7 @@ EXCITED_CASES = {
     "u1_L12_D16": ["-sym", "u1", "-L", "12", "-d", "16"],
     "u1c_j2_L12_D16": ["-sym", "u1", "-cplx", "1", "-L", "12", "-d", "16", "-J2", "0.5"],
     "su2_L12_D16": ["-sym", "su2", "-L", "12", "-d", "16"],
+    "su2c_L12_D16": ["-sym", "su2", "-cplx", "1", "-L", "12", "-d", "16"],
 }
 BASELINE_CASES = {
     "u1_L32_D64": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"], ["-mlanc", "100", "-lanc_check", "1e-10"]),
