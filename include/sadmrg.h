@@ -146,6 +146,11 @@ int sadmrg_set_svd_precondition(sadmrg_handle* h, int on);
  * pair fits, 1 always streams them in row chunks as for blocks too tall to fit.
  * The same results either way; for tests and profiling. */
 int sadmrg_set_svd_stream(sadmrg_handle* h, int on);
+/* Block SVD Jacobi column blocks (no counterpart in the reference): 8 or 16
+ * columns per block, or 0 (the default) for 8 when the widest round of 16-column
+ * pairs would keep fewer than half the SMs busy and 16 otherwise.  The same
+ * results either way; for tests and profiling. */
+int sadmrg_set_svd_block(sadmrg_handle* h, int b);
 /* A fixed tile choice for the H_eff plans made after this call, instead of the
  * autotuner or the heuristics: width 64 or 128 (0 returns to them), fewest slabs
  * per split-K chunk when the tiles cannot fill the GPU (0: no such split), most

@@ -287,6 +287,13 @@ int sadmrg_set_autotune(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.autotune = on ? 1 : 0; });
 }
 
+int sadmrg_set_svd_block(sadmrg_handle* h, int b) {
+  return guard(h, [&]() {
+    SADMRG_REQUIRE(b == 0 || b == 8 || b == 16, SADMRG_ERR_ARG, "set_svd_block: 0, 8 or 16");
+    h->ctx.svd_block = b;
+  });
+}
+
 int sadmrg_set_svd_stream(sadmrg_handle* h, int on) {
   return guard(h, [&]() { h->ctx.svd_stream = on ? 1 : 0; });
 }

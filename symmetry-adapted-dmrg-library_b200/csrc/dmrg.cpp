@@ -655,7 +655,7 @@ SvdStats block_svd(Ctx& c, const BTensor<S>& psi, BTensor<S>& tu, double p1, BTe
   DevBuf wv(sizeof(S) * std::max<long long>(wtot, 1), c.stream), sv(sizeof(double) * std::max<long long>(stot, 1), c.stream);
   const double tj = now_s();
   const int sweeps = run_jacobi_svd(kCx<S>, psi.data(), wv.get(), wv.get(), sv.as<double>(), jobs, 60, c.stream,
-                                    &out.jacobi_kernel_ms, c.svd_qr, c.svd_stream);
+                                    &out.jacobi_kernel_ms, c.svd_qr, c.svd_stream, c.svd_block);
   out.jacobi_s = now_s() - tj;
   for (auto& J : jobs) {
     out.max_rows = std::max(out.max_rows, std::max(J.m, J.n));

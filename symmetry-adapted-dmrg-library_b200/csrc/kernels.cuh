@@ -247,8 +247,10 @@ struct SvdJob {
 // columns, 2 always; the outputs have the same meaning either way.
 // stream: 1 streams every visit's rows in chunks even where the pair's columns
 // would fit in shared memory (same results; covers that path on small problems).
+// block: Jacobi column blocks of 8 or 16, 0 for the rule (8 when the widest round
+// of 16-column pairs would keep fewer than half the SMs busy).
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& jobs,
                    int max_sweeps, cudaStream_t s, double* kernel_ms = nullptr, int precondition = 1,
-                   int stream = 0);
+                   int stream = 0, int block = 0);
 
 }  // namespace sadmrg

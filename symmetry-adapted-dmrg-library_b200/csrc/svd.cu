@@ -1360,7 +1360,7 @@ struct QrLaunch {
 // preconditioning).
 template <bool CPLX>
 static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                         int max_sweeps, cudaStream_t s, double* kernel_ms, bool* fallback, int stream) {
+                         int max_sweeps, cudaStream_t s, double* kernel_ms, bool* fallback, int stream, int block) {
   using T = typename SvdT<CPLX>::T;
   constexpr int NB = QrGeom<CPLX>::NB;
   *fallback = false;
@@ -1423,7 +1423,8 @@ static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, cons
     J.trans = 0;
   }
   double jms = -1.0;
-  const int sweeps = narrow_blocks(jj)
+  const bool narrow = block == 8 || (block == 0 && narrow_blocks(jj));
+  const int sweeps = narrow
                          ? jacobi_run<CPLX, 8>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0, stream)
                          : jacobi_run<CPLX, 16>(nullptr, qbuf.get(), qbuf.get(), sv, jj, max_sweeps, s, &jms, 0, stream);
   if (sweeps <= 0) return sweeps;
@@ -1449,7 +1450,7 @@ static int qr_jacobi_run(const void* a, void* work, void* vmat, double* sv, cons
 }
 
 int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv, const std::vector<SvdJob>& hjobs,
-                   int max_sweeps, cudaStream_t s, double* kernel_ms, int precondition, int stream) {
+                   int max_sweeps, cudaStream_t s, double* kernel_ms, int precondition, int stream, int block) {
   if (kernel_ms) *kernel_ms = -1.0;
   if (hjobs.empty()) return 0;
   if (precondition) {
@@ -1462,8 +1463,8 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
     const size_t panel = (size_t)maxR * (cplx ? QrGeom<true>::NB * 16 : QrGeom<false>::NB * 8);
     if (panel <= kQrSmemMax && (maxC >= kQrMinCols || precondition == 2)) {
       bool fallback = false;
-      const int sw = cplx ? qr_jacobi_run<true>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream)
-                          : qr_jacobi_run<false>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream);
+      const int sw = cplx ? qr_jacobi_run<true>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream, block)
+                          : qr_jacobi_run<false>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, &fallback, stream, block);
       if (!fallback) return sw;
     }
   }
@@ -1472,7 +1473,7 @@ int run_jacobi_svd(bool cplx, const void* a, void* work, void* vmat, double* sv,
   // and cut each visit's work to a quarter, which wins while SMs are idle (D=512:
   // 1.87 -> 1.65 s of SVD per sweep) and loses once they are not (complex D=2048:
   // 4.8 -> 5.5 s per iDMRG)
-  const bool narrow = narrow_blocks(hjobs);
+  const bool narrow = block == 8 || (block == 0 && narrow_blocks(hjobs));
   if (cplx)
     return narrow ? jacobi_run<true, 8>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream)
                   : jacobi_run<true, 16>(a, work, vmat, sv, hjobs, max_sweeps, s, kernel_ms, 1, stream);

@@ -63,6 +63,8 @@ struct Ctx {
   // block SVD: stream every Jacobi visit's rows in chunks (1) or keep the pair's
   // columns in shared memory where they fit (0)
   int svd_stream = 0;
+  // block SVD: Jacobi column blocks of 8 or 16, or 0 for the rule in run_jacobi_svd
+  int svd_block = 0;
   // a tile choice every new H_eff plan takes instead (bn > 0), e.g. to profile one
   UmmaTune forced_tune;
   const int* job_mask = nullptr; // device flags per job tag; GemmPlan::run skips jobs whose flag is 0

@@ -39,7 +39,7 @@ EXPORTED = [
     "sadmrg_chain_set_mlanc", "sadmrg_chain_save_ww", "sadmrg_chain_read_ww", "sadmrg_chain_save_enr",
     "sadmrg_chain_read_enr", "sadmrg_chain_ww", "sadmrg_heff_graph_steps", "sadmrg_heff_launches_per_matvec",
     "sadmrg_heff_wait_fault_test", "sadmrg_set_autotune", "sadmrg_heff_tiles", "sadmrg_set_tiles",
-    "sadmrg_set_svd_precondition", "sadmrg_set_svd_stream",
+    "sadmrg_set_svd_precondition", "sadmrg_set_svd_stream", "sadmrg_set_svd_block",
     "sadmrg_chain_bond_flags",
 ]
 
@@ -99,6 +99,7 @@ def load(path: str = LIB_PATH):
         "sadmrg_set_autotune": ([vp, C.c_int], C.c_int),
         "sadmrg_set_svd_precondition": ([vp, C.c_int], C.c_int),
         "sadmrg_set_svd_stream": ([vp, C.c_int], C.c_int),
+        "sadmrg_set_svd_block": ([vp, C.c_int], C.c_int),
         "sadmrg_heff_tiles": ([vp, C.c_int, dp, ip], C.c_int),
         "sadmrg_set_tiles": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "sadmrg_svd_truncate": ([vp, td, td, td, C.c_double, C.c_double, C.c_int, ip, dp], C.c_int),
@@ -404,6 +405,10 @@ class Handle:
         """Householder QRs before the block SVD's Jacobi: 0 never, 1 for calls whose
         widest block has at least 32 columns (the default), 2 always."""
         self._check(self.lib.sadmrg_set_svd_precondition(self.h, int(on)), "set_svd_precondition")
+
+    def set_svd_block(self, b: int):
+        """Jacobi column blocks of the block SVD: 8, 16, or 0 for the default rule."""
+        self._check(self.lib.sadmrg_set_svd_block(self.h, int(b)), "set_svd_block")
 
     def set_svd_stream(self, on: bool):
         """Stream every Jacobi visit's rows in chunks (default off: resident where they fit)."""

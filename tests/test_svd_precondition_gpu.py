@@ -11,7 +11,8 @@ on the reference's truncations), through sadmrg_svd_truncate:
     noise);
   * each with the Jacobi visits holding their columns in shared memory (the
     default where they fit) and streaming them in row chunks (the path of blocks
-    too tall to fit, sadmrg_set_svd_stream);
+    too tall to fit, sadmrg_set_svd_stream), with column blocks of 8 and of 16
+    (sadmrg_set_svd_block);
   * full sweeps from the reference's checkpoint with the preconditioning on and
     off: the same energies (1e-10) and bonds until either run reports a near-tie
     cut (the D-th and (D+1)-th singular values equal to 1e-8, decided by
@@ -41,12 +42,13 @@ def _block_slices(t):
         off += n
 
 
+@pytest.mark.parametrize("block", [8, 16], ids=["b8", "b16"])
 @pytest.mark.parametrize("stream", [0, 1], ids=["resident", "streamed"])
 @pytest.mark.parametrize("sym,cplx,L,D,mode", [
     (0, False, 16, 48, "random"), (1, False, 24, 40, "random"), (0, True, 16, 32, "random"),
     (1, False, 24, 40, "zero_block"), (0, True, 16, 32, "zero_block"), (0, False, 16, 48, "rank1_blocks"),
 ])
-def test_preconditioned_svd_matches_plain_and_oracle(sym, cplx, L, D, mode, stream):
+def test_preconditioned_svd_matches_plain_and_oracle(sym, cplx, L, D, mode, stream, block):
     import sadmrg
     h = sadmrg.Handle(sym=sym, cplx=cplx)
     h.chain_create(1, L, D, 1, 0, True, 0.0)
@@ -68,6 +70,7 @@ def test_preconditioned_svd_matches_plain_and_oracle(sym, cplx, L, D, mode, stre
             x[off:off + dims[0] * dims[1]] = np.outer(a, b).ravel(order="F")
     psi.data = x
     h.set_svd_stream(stream)
+    h.set_svd_block(block)
     res = {}
     for on in (True, False):
         h.set_svd_precondition(2 if on else 0)   # 2: also for blocks narrower than 32 columns
