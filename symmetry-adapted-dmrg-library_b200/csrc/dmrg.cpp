@@ -1182,14 +1182,18 @@ void Chain<S>::set_penalty(HeffPlan<S>& H, const BTensor<S>& vec) {
   H.pen_wo = std::make_shared<DevBuf>(bytes, c.stream);
   H.pen_dot = std::make_shared<DevBuf>(sizeof(S) * (exci + 1), c.stream);
   SADMRG_CUDA(cudaMemsetAsync(H.pen_o->get(), 0, bytes, c.stream));
-  int q[8], d[8];
+  int q[8], d[8], qo[8], dn[8];
   for (int j = 0; j < exci; ++j) {
     const BTensor<S>& o = overlapvec[j];
-    SADMRG_REQUIRE(!o.null() && o.nten() == vec.nten(), SADMRG_ERR_STATE,
+    SADMRG_REQUIRE(!o.null() && o.nten() == vec.nten() && o.st.nbond() == vec.st.nbond(), SADMRG_ERR_STATE,
                    "excited state: the lower state's projection does not match the two-site basis");
     S* dst = static_cast<S*>(H.pen_o->get()) + (size_t)j * H.n;
     for (long b = 0; b < vec.nten(); ++b) {
       if (!vec.present(b) || !o.present(b) || !vec.st.block(b, q, d)) continue;
+      o.st.block(b, qo, dn);
+      for (int k = 0; k < vec.st.nbond(); ++k)
+        SADMRG_REQUIRE(qo[k] == q[k] && dn[k] == d[k], SADMRG_ERR_STATE,
+                       "excited state: a block of the lower state's projection has other sectors or dims");
       SADMRG_CUDA(cudaMemcpyAsync(dst + vec.off[b], o.data() + o.off[b], sizeof(S) * vec.st.block_elems(b),
                                   cudaMemcpyDeviceToDevice, c.stream));
     }
