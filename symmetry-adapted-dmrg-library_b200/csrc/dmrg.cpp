@@ -1406,10 +1406,10 @@ bool Chain<S>::read_state(const std::string& dir, int bond_read, int idx, std::v
     bool ok = std::fscanf(f, "%d %d", &nb, &lc) == 2 && nb >= 1 && nb <= 4;
     for (int b = 0; ok && b < nb; ++b) {
       int dir_ = 0, nc = 0;
-      ok = std::fscanf(f, "%d %d", &dir_, &nc) == 2 && nc >= 1;
-      std::vector<int> q(nc), d(nc);
+      ok = std::fscanf(f, "%d %d", &dir_, &nc) == 2 && nc >= 1 && nc <= (1 << 16);
+      std::vector<int> q(ok ? nc : 0), d(ok ? nc : 0);
       for (int k = 0; ok && k < nc; ++k) ok = std::fscanf(f, "%d", &q[k]) == 1;
-      for (int k = 0; ok && k < nc; ++k) ok = std::fscanf(f, "%d", &d[k]) == 1;
+      for (int k = 0; ok && k < nc; ++k) ok = std::fscanf(f, "%d", &d[k]) == 1 && d[k] >= 1 && d[k] <= (1 << 20);
       if (ok) bonds.push_back(Bond(dir_, q, d));
     }
     std::fclose(f);
