@@ -325,7 +325,8 @@ int sadmrg_heff_tiles(sadmrg_handle* h, int cap, double* out, int* n) {
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     auto& S_ = st_of<S>(h);
-    SADMRG_REQUIRE(S_.heff && n, SADMRG_ERR_STATE, "heff_tiles: no plan");
+    SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_tiles: no plan");
+    SADMRG_REQUIRE(n && (cap <= 0 || out), SADMRG_ERR_ARG, "heff_tiles: null count or buffer");
     const GemmPlan& P = S_.heff->plan;
     const UmmaTune& t = P.tune;
     std::vector<double> v;
@@ -974,7 +975,7 @@ int sadmrg_chain_ww(sadmrg_handle* h, int cap, int* n, double* out) {
     using S = std::remove_pointer_t<decltype(tag)>;
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
-    SADMRG_REQUIRE(n, SADMRG_ERR_ARG, "chain_ww: null count");
+    SADMRG_REQUIRE(n && (cap <= 0 || out), SADMRG_ERR_ARG, "chain_ww: null count or buffer");
     const auto& w = S_.chain->ww;
     *n = (int)w.size();
     for (int i = 0; i < cap && i < (int)w.size(); ++i) out[i] = w[i];
@@ -1002,6 +1003,7 @@ int sadmrg_chain_bond(sadmrg_handle* h, int site, int cap, int* nsec, int* q, in
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
     SADMRG_REQUIRE(site >= 0 && site < S_.chain->ns, SADMRG_ERR_ARG, "chain_bond: site");
+    SADMRG_REQUIRE(nsec && (cap <= 0 || (q && d)), SADMRG_ERR_ARG, "chain_bond: null count or buffers");
     const auto& u = S_.chain->uu[site];
     if (u.st.nbond() < 3) { *nsec = 0; return; }
     const Bond& b = u.st.bonds[2];

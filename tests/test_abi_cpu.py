@@ -1,4 +1,5 @@
-"""The C ABI library: builds, loads and exports every function include/sadmrg.h declares."""
+"""The C ABI library: builds, loads, exports every function include/sadmrg.h declares and
+rejects null handles and null out-pointers without a device."""
 import ctypes
 import os
 import re
@@ -52,3 +53,43 @@ def test_python_binding_signatures_match_header():
         assert len(f.argtypes) == n, (name, len(f.argtypes), n)
         checked += 1
     assert checked >= len(counts) - 2
+
+
+_NULL_HANDLE_SCRIPT = r"""
+import ctypes as C, re, sys
+sys.path.insert(0, sys.argv[1])
+import sadmrg
+lib = sadmrg.load()
+src = open(sys.argv[2]).read()
+ok = 0
+for m in re.finditer(r"^\s*(int|const char\*)\s+(sadmrg_\w+)\s*\(([^;]*?)\)\s*;", src, re.M | re.S):
+    name, params = m.group(2), " ".join(m.group(3).split())
+    if not re.match(r"(const )?sadmrg_handle\*", params):
+        continue
+    f = getattr(lib, name)
+    args = [0 if t in (C.c_int, C.c_double, C.c_longlong, C.c_long) else None for t in f.argtypes]
+    r = f(*args)
+    if name == "sadmrg_destroy":
+        assert r == 0, name
+    elif name == "sadmrg_last_error":
+        assert r == b"null handle", r
+    else:
+        assert r == 1, (name, r)   # SADMRG_ERR_ARG
+    ok += 1
+assert lib.sadmrg_create(0, 0, 0, None) == 1
+assert lib.sadmrg_create(2, 0, 0, C.byref(C.c_void_p())) == 1
+print(ok)
+"""
+
+
+def test_null_handle_and_null_out_are_errors_not_crashes():
+    """every entry point that takes a handle returns SADMRG_ERR_ARG for a null handle
+    (null and zero for its other arguments) before touching the device; destroy
+    accepts it; create rejects a null out-pointer and a bad symmetry.  Run in a
+    child process so that a crash shows as a failure."""
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, "-c", _NULL_HANDLE_SCRIPT, PKG, os.path.join(ROOT, "include", "sadmrg.h")],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert int(r.stdout.split()[-1]) >= 50
