@@ -218,7 +218,7 @@ int sadmrg_heff_plan(sadmrg_handle* h, const sadmrg_tensor_desc* psi, const sadm
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     Ctx& c = h->ctx;
-    SADMRG_REQUIRE(psi && nops >= 0 && nterms >= 0, SADMRG_ERR_ARG, "heff_plan: bad arguments");
+    SADMRG_REQUIRE(psi && nops >= 0 && nterms >= 0 && (nops == 0 || opsd), SADMRG_ERR_ARG, "heff_plan: bad arguments");
     BTensor<S> p = from_desc<S>(c, psi);
     BTensor<S> hl, hr;
     if (hhl) hl = from_desc<S>(c, hhl);
@@ -371,6 +371,7 @@ int sadmrg_heff_apply(sadmrg_handle* h, const void* psi_host, void* out_host, in
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply: no plan");
     SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_apply: precision");
     const long long n = S_.heff->n;
+    SADMRG_REQUIRE(n == 0 || (psi_host && out_host), SADMRG_ERR_ARG, "heff_apply: null buffer");
     S* din = S_.io.template as<S>();
     S* dout = din + n;
     SADMRG_CUDA(cudaMemcpyAsync(din, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
@@ -431,7 +432,7 @@ int sadmrg_heff_profile(sadmrg_handle* h, int precision, int reps, const void* p
     auto& S_ = st_of<S>(h);
     Ctx& c = h->ctx;
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_profile: no plan");
-    SADMRG_REQUIRE(reps >= 1, SADMRG_ERR_ARG, "heff_profile: reps");
+    SADMRG_REQUIRE(reps >= 1 && ms && flops, SADMRG_ERR_ARG, "heff_profile: reps or null outputs");
     const HeffPlan<S>& H = *S_.heff;
     const S* in = psi_dev ? static_cast<const S*>(psi_dev) : S_.io.template as<S>();
     S* out = out_dev ? static_cast<S*>(out_dev) : S_.io.template as<S>() + H.n;
@@ -676,7 +677,9 @@ int sadmrg_heff_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precisi
     Ctx& c = h->ctx;
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_lanczos: no plan");
     SADMRG_REQUIRE(mlanc >= 2, SADMRG_ERR_ARG, "heff_lanczos: mlanc < 2");
+    SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_lanczos: precision");
     const long long n = S_.heff->n;
+    SADMRG_REQUIRE(n == 0 || psi_host, SADMRG_ERR_ARG, "heff_lanczos: null vector");
     S* dv = S_.io.template as<S>();
     SADMRG_CUDA(cudaMemcpyAsync(dv, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
     LanczosStats st = lanczos_solve<S>(c, *S_.heff, dv, mlanc, precision);
@@ -696,6 +699,7 @@ int sadmrg_heff_lanczos2(sadmrg_handle* h, void* psi_host, int mlanc, double* en
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_lanczos2: no plan");
     SADMRG_REQUIRE(mlanc >= 2, SADMRG_ERR_ARG, "heff_lanczos2: mlanc < 2");
     const long long n = S_.heff->n;
+    SADMRG_REQUIRE(n == 0 || psi_host, SADMRG_ERR_ARG, "heff_lanczos2: null vector");
     S* dv = S_.io.template as<S>();
     SADMRG_CUDA(cudaMemcpyAsync(dv, psi_host, sizeof(S) * n, cudaMemcpyHostToDevice, c.stream));
     LanczosStats st = lanczos2<S>(c, *S_.heff, dv, mlanc);
@@ -760,6 +764,7 @@ int sadmrg_batch_apply(sadmrg_handle* h, const void* psi_host, void* out_host, i
     SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_apply: not finalized");
     SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "batch_apply: precision");
     const HeffPlan<S>& H = S_.batch->merged;
+    SADMRG_REQUIRE(H.n == 0 || (psi_host && out_host), SADMRG_ERR_ARG, "batch_apply: null buffer");
     DevBuf io(sizeof(S) * 2 * std::max<long long>(H.n, 1), c.stream);
     S* din = io.as<S>();
     S* dout = din + H.n;
@@ -808,7 +813,9 @@ int sadmrg_batch_lanczos(sadmrg_handle* h, void* psi_host, int mlanc, int precis
     Ctx& c = h->ctx;
     SADMRG_REQUIRE(S_.batch && S_.batch->ready, SADMRG_ERR_STATE, "batch_lanczos: not finalized");
     SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "batch_lanczos: precision");
+    SADMRG_REQUIRE(mlanc >= 2, SADMRG_ERR_ARG, "batch_lanczos: mlanc < 2");
     const HeffBatch<S>& B = *S_.batch;
+    SADMRG_REQUIRE(B.merged.n == 0 || psi_host, SADMRG_ERR_ARG, "batch_lanczos: null vector");
     DevBuf io(sizeof(S) * std::max<long long>(B.merged.n, 1), c.stream);
     SADMRG_CUDA(cudaMemcpyAsync(io.get(), psi_host, sizeof(S) * B.merged.n, cudaMemcpyHostToDevice, c.stream));
     BatchStats st = batch_lanczos_solve<S>(c, B, io.as<S>(), mlanc, precision);
@@ -1028,6 +1035,7 @@ int sadmrg_chain_stats(sadmrg_handle* h, double* out, int n) {
     using S = std::remove_pointer_t<decltype(tag)>;
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.chain, SADMRG_ERR_STATE, "no chain");
+    SADMRG_REQUIRE(n <= 0 || out, SADMRG_ERR_ARG, "chain_stats: null buffer");
     const Timers& t = S_.chain->timers;
     const double v[14] = {t.lanczos, t.env, t.svd, t.prep, (double)t.matvecs, t.heff_flops,
                           (double)h->ctx.gemm_flops, (double)h->ctx.launches, S_.chain->last_discarded,
@@ -1086,6 +1094,7 @@ int sadmrg_staged_info(sadmrg_handle* h, int which, int* nbond, int* locspin, in
   return dispatch(h, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     SADMRG_REQUIRE(which == 0 || which == 1, SADMRG_ERR_ARG, "staged: which");
+    SADMRG_REQUIRE(nbond && locspin && nsectors && nblocks && nelem, SADMRG_ERR_ARG, "staged_info: null output");
     const BTensor<S>& t = st_of<S>(h).staged[which];
     *nbond = t.st.nbond();
     *locspin = t.st.locspin;
@@ -1104,6 +1113,9 @@ int sadmrg_staged_read(sadmrg_handle* h, int which, int* dir, int* nmom, int* q,
     using S = std::remove_pointer_t<decltype(tag)>;
     SADMRG_REQUIRE(which == 0 || which == 1, SADMRG_ERR_ARG, "staged: which");
     const BTensor<S>& t = st_of<S>(h).staged[which];
+    SADMRG_REQUIRE(t.st.nbond() == 0 || (dir && nmom && q && d), SADMRG_ERR_ARG, "staged_read: null bond buffers");
+    SADMRG_REQUIRE(t.nten() == 0 || block_index, SADMRG_ERR_ARG, "staged_read: null block_index");
+    SADMRG_REQUIRE(t.nelem == 0 || data, SADMRG_ERR_ARG, "staged_read: null data");
     int o = 0;
     for (int b = 0; b < t.st.nbond(); ++b) {
       dir[b] = t.st.bonds[b].dir;
