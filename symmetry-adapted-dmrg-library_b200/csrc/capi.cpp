@@ -388,6 +388,7 @@ int sadmrg_heff_apply_device(sadmrg_handle* h, const void* psi_dev, void* out_de
     auto& S_ = st_of<S>(h);
     SADMRG_REQUIRE(S_.heff, SADMRG_ERR_STATE, "heff_apply_device: no plan");
     SADMRG_REQUIRE(precision == PREC_FP64 || precision == PREC_TF32X3, SADMRG_ERR_ARG, "heff_apply: precision");
+    SADMRG_REQUIRE(S_.heff->n == 0 || (psi_dev && out_dev), SADMRG_ERR_ARG, "heff_apply_device: null buffer");
     S_.heff->apply(h->ctx, static_cast<const S*>(psi_dev), static_cast<S*>(out_dev), precision);
   });
 }
