@@ -1,5 +1,5 @@
-"""The C ABI library: builds, loads, exports every function include/sadmrg.h declares and
-rejects null handles and null out-pointers without a device."""
+"""The C ABI library: builds, loads, exports every function include/sadmrg.h declares,
+rejects null handles and null out-pointers without a device, and its header is plain C."""
 import ctypes
 import os
 import re
@@ -93,3 +93,31 @@ def test_null_handle_and_null_out_are_errors_not_crashes():
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[-2000:]
     assert int(r.stdout.split()[-1]) >= 50
+
+
+_C_CLIENT = r"""
+#include <stdio.h>
+#include "sadmrg.h"
+int main(void) {
+  sadmrg_handle* h = 0;
+  int st = 0;
+  printf("%d %d %d %s\n", sadmrg_version(), sadmrg_create(0, 0, 0, 0), sadmrg_device_status(h, &st),
+         sadmrg_last_error(h));
+  return 0;
+}
+"""
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/sadmrg.h compiles as strict C99 (no C++ in the declarations) and a C
+    client links against the shared library and calls it without a device"""
+    import subprocess
+    src = tmp_path / "client.c"
+    src.write_text(_C_CLIENT)
+    exe = tmp_path / "client"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                        os.path.join(ROOT, "include"), str(src), "-L", PKG, "-l:libsadmrg_b200.so",
+                        "-Wl,-rpath," + PKG, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.split() == ["10000", "1", "1", "null", "handle"], r.stdout + r.stderr
