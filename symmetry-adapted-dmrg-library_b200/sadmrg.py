@@ -140,6 +140,11 @@ class SadmrgError(RuntimeError):
     pass
 
 
+# status codes of include/sadmrg.h
+STATUS_NAMES = {1: "SADMRG_ERR_ARG", 2: "SADMRG_ERR_CUDA", 3: "SADMRG_ERR_NOMEM", 4: "SADMRG_ERR_STATE",
+                5: "SADMRG_ERR_NUMERIC", 6: "SADMRG_ERR_LIMIT", 7: "SADMRG_ERR_DEVICE_FLAG"}
+
+
 @dataclass
 class BlockTensorData:
     """Host image of a BlockTensor: bonds, present blocks, concatenated data."""
@@ -216,7 +221,8 @@ class Handle:
         h = C.c_void_p()
         rc = self.lib.sadmrg_create(int(sym), int(bool(cplx)), int(device), C.byref(h))
         if rc != 0:
-            raise SadmrgError(f"sadmrg_create failed with status {rc}")
+            why = " (no usable CUDA device)" if rc == 2 else ""
+            raise SadmrgError(f"sadmrg_create failed with status {rc} {STATUS_NAMES.get(rc, '')}{why}")
         self.h = h
         # Handles still open at interpreter exit are destroyed by an exit hook that
         # is registered after the first handle (and so after the CUDA runtime's own
@@ -242,7 +248,7 @@ class Handle:
     def _check(self, rc: int, what: str):
         if rc != 0:
             msg = self.lib.sadmrg_last_error(self.h)
-            raise SadmrgError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
+            raise SadmrgError(f"{what}: status {rc} {STATUS_NAMES.get(rc, '')}: {msg.decode() if msg else ''}")
 
     def set_matvec_fusion(self, fused: Optional[bool]):
         """True: the split-precision matvec as one cooperative launch; False: pack + one

@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from conftest import ROOT, PKG
 
 
@@ -121,3 +123,14 @@ def test_header_is_plain_c_and_links(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.split() == ["10000", "1", "1", "null", "handle"], r.stdout + r.stderr
+
+
+def test_no_device_fails_loudly():
+    """without a GPU the library refuses to create a handle (SADMRG_ERR_CUDA): there is
+    no CPU fallback behind the C ABI"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import sadmrg
+    with pytest.raises(sadmrg.SadmrgError, match="SADMRG_ERR_CUDA"):
+        sadmrg.Handle(sym=sadmrg.SYM_SU2)
