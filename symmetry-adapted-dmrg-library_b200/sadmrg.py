@@ -161,6 +161,8 @@ class BlockTensorData:
         return len(self.dirs)
 
     def block_labels(self, idx: int):
+        """Per-bond sector positions of block `idx` (mixed radix, bond 0 fastest): the
+        sector label of bond b is qs[b][pos[b]], its dimension ds[b][pos[b]]."""
         out = []
         for b in range(self.nbond):
             n = len(self.qs[b])
