@@ -9,10 +9,12 @@
 //     vs U1Bond::fuse / SU2Bond::fuse (src/symmetry/u1.cpp, su2.cpp);
 //   every block index of a 2-4 bond structure: allowed or not, labels and dims
 //     vs U1Struct / SU2Struct::get_tensor_argument, and the block index found
-//     back from the labels vs get_tensor_index.
+//     back from the labels vs get_tensor_index;
+//   the cyclic move of a bond (Struct::shifted vs the reference's shift, every
+//     (i0, i1) pair of the structure): each bond's direction, labels and dims.
 //
 // usage: sym_check <cases> <seed>
-// prints one line per symmetry (cases, blocks, allowed blocks, mismatches);
+// prints one line per symmetry (cases, blocks, allowed blocks, mismatches, shifts);
 // exits 1 on any mismatch.
 #include <cstdio>
 #include <cstdlib>
@@ -49,7 +51,7 @@ bool same_bond(const RB& r, const sadmrg::Bond& b) {
 
 struct Tally {
   const char* name;
-  long cases = 0, blocks = 0, allowed = 0, bad = 0;
+  long cases = 0, blocks = 0, allowed = 0, shifts = 0, bad = 0;
 };
 
 template <class RB, class RS>
@@ -87,6 +89,21 @@ void run(Tally& t, sadmrg::Sym sym, int cases) {
     rs.set_struct(nb, locspin, rb.data());
     const sadmrg::Struct ls(sym, locspin, lb);
     if (rs.get_nten() != ls.nten()) { ++t.bad; continue; }
+    for (int i0 = 0; i0 < nb; ++i0)
+      for (int i1 = 0; i1 < nb; ++i1) {
+        ++t.shifts;
+        RS r2;
+        r2.set_struct(nb, locspin, rb.data());
+        r2.shift(i0, i1);
+        const sadmrg::Struct l2 = ls.shifted(i0, i1);
+        bool ok = r2.get_nbond() == l2.nbond();
+        for (int k = 0; ok && k < nb; ++k) {
+          RB got;
+          r2.get_bond(k, got);
+          ok = same_bond(got, l2.bonds[k]);
+        }
+        if (!ok) ++t.bad;
+      }
     for (long i = 0; i < ls.nten(); ++i) {
       ++t.blocks;
       int rq[8], rd[8], q[8], d[8];
@@ -116,7 +133,7 @@ int main(int argc, char** argv) {
   run<U1Bond, U1Struct>(u, sadmrg::Sym::U1, cases);
   run<SU2Bond, SU2Struct>(s, sadmrg::Sym::SU2, cases);
   for (const Tally* t : {&u, &s})
-    std::printf("%s cases %ld blocks %ld allowed %ld mismatches %ld\n", t->name, t->cases, t->blocks, t->allowed,
-                t->bad);
+    std::printf("%s cases %ld blocks %ld allowed %ld mismatches %ld shifts %ld\n", t->name, t->cases, t->blocks,
+                t->allowed, t->bad, t->shifts);
   return (u.bad || s.bad) ? 1 : 0;
 }

@@ -5,7 +5,8 @@ oracle/harness/sym_check.cpp draws seeded random bonds and compares the fusion o
 two bonds (direction, sector labels in order, dims) with U1Bond/SU2Bond::fuse,
 and every block of random 2-4 bond structures (allowed or not, labels, dims, the
 index found back from the labels) with U1Struct/SU2Struct::get_tensor_argument
-and get_tensor_index (src/symmetry/u1.cpp, src/symmetry/su2.cpp).  The block
+and get_tensor_index, and the cyclic move of a bond (Struct::shifted) with the
+reference's shift (src/symmetry/u1.cpp, src/symmetry/su2.cpp).  The block
 order of every tensor, task list and checkpoint file rests on these rules.
 """
 import os
@@ -36,6 +37,6 @@ def test_fusion_and_block_enumeration_equal_reference(seed):
     assert [ln.split()[0] for ln in lines] == ["u1", "su2"], lines
     for ln in lines:
         t = ln.split()
-        cases, blocks, allowed, mism = int(t[2]), int(t[4]), int(t[6]), int(t[8])
-        assert cases == 1000 and mism == 0, ln
+        cases, blocks, allowed, mism, shifts = int(t[2]), int(t[4]), int(t[6]), int(t[8]), int(t[10])
+        assert cases == 1000 and mism == 0 and shifts >= 4 * cases, ln
         assert blocks > 10000 and 1000 < allowed < blocks, ln
