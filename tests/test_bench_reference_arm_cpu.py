@@ -54,3 +54,14 @@ def test_reference_arm_two_ranks_rank0_prints_once():
     lines = _json_lines(p.stdout)
     assert len(lines) == 1, p.stdout
     _check_line(lines[0], 2)
+
+
+def test_library_arm_without_gpu_fails_loudly():
+    """the library's own arm has no CPU fallback: without a GPU it exits non-zero
+    and prints no result line"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = subprocess.run([sys.executable, "bench.py", "--steps", "1", "--warmup", "0"], cwd=ROOT, capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode != 0 and not _json_lines(p.stdout), p.stdout[-2000:]
