@@ -1115,7 +1115,9 @@ int sadmrg_staged_read(sadmrg_handle* h, int which, int* dir, int* nmom, int* q,
     SADMRG_REQUIRE(which == 0 || which == 1, SADMRG_ERR_ARG, "staged: which");
     const BTensor<S>& t = st_of<S>(h).staged[which];
     SADMRG_REQUIRE(t.st.nbond() == 0 || (dir && nmom && q && d), SADMRG_ERR_ARG, "staged_read: null bond buffers");
-    SADMRG_REQUIRE(t.nten() == 0 || block_index, SADMRG_ERR_ARG, "staged_read: null block_index");
+    long npresent = 0;
+    for (long i = 0; i < t.nten(); ++i) npresent += t.present(i) ? 1 : 0;
+    SADMRG_REQUIRE(npresent == 0 || block_index, SADMRG_ERR_ARG, "staged_read: null block_index");
     SADMRG_REQUIRE(t.nelem == 0 || data, SADMRG_ERR_ARG, "staged_read: null data");
     int o = 0;
     for (int b = 0; b < t.st.nbond(); ++b) {
