@@ -56,7 +56,7 @@ HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 sys.path.insert(0, PKG)
 
 FLUSH_BYTES = 512 << 20   # 256 MiB written, then another 256 MiB read, before every timed step
-# Lanczos settings of the chain workloads: at most 100 steps (BASELINE), stop once
+# Lanczos settings of the chain workloads: at most 100 steps (the benchmark's Krylov length), stop once
 # |<v|Hv>|/|Hv| is within lanczos_tol of 1
 LANCZOS_MLANC = 100
 
