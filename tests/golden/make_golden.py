@@ -15,15 +15,16 @@ Run in a container that has the reference sources (the harness is built by
   ground state also as the starting state): energies and bonds after every
   sweep, and the exact eigenvalues of the chain's Sz = 0 sector (of its singlets
   for an SU(2) chain).
-* ``baseline_<case>.npz`` -- the same for the benchmark configurations, run with
+* ``bench_<case>.npz`` -- the same for the benchmark chains, run with
   the benchmark's Lanczos settings (at most 100 steps, stop at |<v|Hv>|/|Hv|
   within 1e-10 of 1; the reference's constants are 40 and 1e-8), with the
   reference's iDMRG checkpoint (both sides sweep from it) and the checkpoint
   files of singular values and energies its sweeps wrote (ww-*.bin, enr-*.dat).
 
-    python tests/golden/make_golden.py             # all but configuration 2
-    python tests/golden/make_golden.py --config2   # configuration 2 only
-    python tests/golden/make_golden.py --excited   # the excited-state cases only
+    python tests/golden/make_golden.py                  # all but the SU(2) L=100 chain
+    python tests/golden/make_golden.py --su2-L100-D512   # the SU(2) L=100 D=512 chain only
+    python tests/golden/make_golden.py --excited        # the excited-state cases only
+    python tests/golden/make_golden.py --bench-only     # the U(1) L=32 benchmark chain only
 """
 from __future__ import annotations
 
@@ -61,14 +62,14 @@ SWEEP_CASES = {
     "u1_L32_D64": ["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "2"],
 }
 
-# configuration 1 of the benchmark: U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps,
+# the benchmark's U(1) chain: real Heisenberg chain, open, L = 32, D = 64, 6 sweeps,
 # with the benchmark's Lanczos settings (<= 100 steps, stop at 1e-10) and with a stop test no
 # run can pass (1e-14: every solve takes all 100 steps, so both sides follow the same path)
-# configuration 2 of the benchmark: SU(2) real Heisenberg chain, open, L = 100, D = 512
+# the benchmark's SU(2) chain: real Heisenberg chain, open, L = 100, D = 512
 # multiplets, 8 sweeps from the reference's own iDMRG state, Lanczos <= 100 steps with the
 # stop test at 1e-12; energies and bonds only (the checkpoint is ~400 MB: a test rebuilds it
 # with the same reference build)
-CONFIG2 = ("su2_L100_D512", ["-sym", "su2", "-L", "100", "-d", "512", "-sweeps", "8", "-maxangm", "40"],
+SU2_L100_D512 = ("su2_L100_D512", ["-sym", "su2", "-L", "100", "-d", "512", "-sweeps", "8", "-maxangm", "40"],
            ["-mlanc", "100", "-lanc_check", "1e-12"])
 # excited states (U(1) chains): ground state by iDMRG + 3 sweeps, then 4 sweeps of the
 # first excited state started from it, both with a Lanczos stop test no solve passes
@@ -81,7 +82,7 @@ EXCITED_CASES = {
     "su2_L12_D16": ["-sym", "su2", "-L", "12", "-d", "16"],
     "su2c_L12_D16": ["-sym", "su2", "-cplx", "1", "-L", "12", "-d", "16"],
 }
-BASELINE_CASES = {
+BENCH_CASES = {
     "u1_L32_D64": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"], ["-mlanc", "100", "-lanc_check", "1e-10"]),
     "u1_L32_D64_converged": (["-sym", "u1", "-L", "32", "-d", "64", "-sweeps", "6"],
                              ["-mlanc", "100", "-lanc_check", "1e-14"]),
@@ -142,8 +143,8 @@ def parse_sweeps(stdout: str):
 def main():
     if not os.path.exists(HARNESS):
         sys.exit("build the reference harness first: make -C oracle")
-    if "--config2" in sys.argv:
-        name, args, lanczos = CONFIG2
+    if "--su2-L100-D512" in sys.argv:
+        name, args, lanczos = SU2_L100_D512
         with tempfile.TemporaryDirectory() as wd:
             stdout = run(args + lanczos + ["-threads", str(os.cpu_count() or 1), "-sweepdir", os.path.join(wd, "sw")],
                          wd, env={"OPENBLAS_NUM_THREADS": "1"})
@@ -151,11 +152,11 @@ def main():
         per_sweep = [[f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])]
                      for s_ in sorted(k for k in bonds if k >= 0)]
         idmrg_bonds = [f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[-1][s]) for s in sorted(bonds[-1])]
-        np.savez_compressed(os.path.join(HERE, f"baseline_{name}.npz"), args=np.array(" ".join(args)),
+        np.savez_compressed(os.path.join(HERE, f"bench_{name}.npz"), args=np.array(" ".join(args)),
                             lanczos=np.array(" ".join(lanczos)), e_idmrg=np.float64(e_idmrg),
                             energies=np.array(energies), bonds_per_sweep=np.array(per_sweep),
                             bonds_idmrg=np.array(idmrg_bonds))
-        print("wrote baseline", name, e_idmrg, energies)
+        print("wrote bench", name, e_idmrg, energies)
         return
     if "--excited" in sys.argv:
         sys.path.insert(0, ROOT)
@@ -192,8 +193,8 @@ def main():
                                 bonds_per_sweep=np.array(per_sweep), ed=ed, **arrays)
             print("wrote excited", name, e_gs[-1], energies, ed)
         return
-    only_baseline = "--baseline-only" in sys.argv
-    for name, args in ({} if only_baseline else CENTRE_CASES).items():
+    only_bench = "--bench-only" in sys.argv
+    for name, args in ({} if only_bench else CENTRE_CASES).items():
         cplx = args[args.index("-cplx") + 1] == "1"
         with tempfile.TemporaryDirectory() as wd:
             dd = os.path.join(wd, "dump")
@@ -210,7 +211,7 @@ def main():
             arrays["sweep_energies"] = np.array(energies)
             np.savez_compressed(os.path.join(HERE, f"centre_{name}.npz"), **arrays)
             print("wrote", name, len(arrays))
-    for name, args in ({} if only_baseline else SWEEP_CASES).items():
+    for name, args in ({} if only_bench else SWEEP_CASES).items():
         ck = {}
         with tempfile.TemporaryDirectory() as wd:
             # the MPS after the reference's iDMRG, in its save_mps2 format: both sides sweep from it
@@ -230,7 +231,7 @@ def main():
                             bonds=np.array(per_sweep[-1]), bonds_per_sweep=np.array(per_sweep), **ck)
         print("wrote", name, e_idmrg, energies, len(ck))
 
-    for name, (args, lanczos) in BASELINE_CASES.items():
+    for name, (args, lanczos) in BENCH_CASES.items():
         arrays = {}
         with tempfile.TemporaryDirectory() as wd:
             ckd, swd = os.path.join(wd, "ck"), os.path.join(wd, "sw")
@@ -244,10 +245,10 @@ def main():
         per_sweep = []
         for s_ in sorted(k for k in bonds if k >= 0):
             per_sweep.append([f"{s}:" + ",".join(f"{q}x{d}" for q, d in bonds[s_][s]) for s in sorted(bonds[s_])])
-        np.savez_compressed(os.path.join(HERE, f"baseline_{name}.npz"), args=np.array(" ".join(args)),
+        np.savez_compressed(os.path.join(HERE, f"bench_{name}.npz"), args=np.array(" ".join(args)),
                             lanczos=np.array(" ".join(lanczos)), e_idmrg=np.float64(e_idmrg),
                             energies=np.array(energies), bonds_per_sweep=np.array(per_sweep), **arrays)
-        print("wrote baseline", name, e_idmrg, energies)
+        print("wrote bench", name, e_idmrg, energies)
 
 
 if __name__ == "__main__":

@@ -22,18 +22,18 @@ Until a flagged cut, every sweep must give the reference's energy to 1e-10
 relative and identical sectors and dimensions on every bond; after one, the
 energy to 1e-8 and the total kept dimension of every bond to 1% (at least 2).
 
-* Configuration 1 (U(1) real Heisenberg chain, open, L = 32, D = 64, 6 sweeps):
+* The U(1) chain (real Heisenberg chain, open, L = 32, D = 64, 6 sweeps):
   both sides sweep from the reference's own iDMRG checkpoint (its save_mps2
-  files, tests/golden/baseline_u1_L32_D64*.npz) -- with the benchmark's stop
+  files, tests/golden/bench_u1_L32_D64*.npz) -- with the benchmark's stop
   test, and with one no run passes (1e-14: every solve takes all 100 steps, so
   both sides follow the same path and only rounding ties remain).  The
   checkpoint files the reference's sweeps wrote (enr-*.dat after every sweep,
   ww-*.bin after the last) are compared with the ones written here.
-* Configuration 2 (SU(2) real Heisenberg chain, open, L = 100, D = 512
+* The SU(2) chain (real Heisenberg chain, open, L = 100, D = 512
   multiplets, 8 sweeps, stop test 1e-12): the reference build runs its own
   iDMRG on the host cores (the checkpoint is ~400 MB, too large to store) and
   the GPU sweeps 8 times from it; the reference's 8 sweeps from the same start
-  are the fixture tests/golden/baseline_su2_L100_D512.npz.  When the host
+  are the fixture tests/golden/bench_su2_L100_D512.npz.  When the host
   reproduces the fixture's iDMRG energy (same build and thread count, so the
   same start), every sweep is compared as above.  It need not: iDMRG is
   chaotic under rounding (its early truncations cut a dense spectrum, so a
@@ -83,8 +83,8 @@ def _compare_sweep(s, e, eref, got, ref_b, flagged):
         assert all(abs(a - b) <= max(2, b // 100) for a, b in zip(tg, tr)), (s, flagged)
 
 
-@pytest.mark.parametrize("fixture", ["baseline_u1_L32_D64.npz", "baseline_u1_L32_D64_converged.npz"])
-def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint(fixture):
+@pytest.mark.parametrize("fixture", ["bench_u1_L32_D64.npz", "bench_u1_L32_D64_converged.npz"])
+def test_u1_L32_D64_six_sweeps_from_reference_checkpoint(fixture):
     import sadmrg
     z = np.load(os.path.join(GOLDEN, fixture))
     lz = str(z["lanczos"]).split()
@@ -129,12 +129,12 @@ def test_config1_u1_L32_D64_six_sweeps_from_reference_checkpoint(fixture):
         h2.close()
 
 
-C2 = os.path.join(GOLDEN, "baseline_su2_L100_D512.npz")
+C2 = os.path.join(GOLDEN, "bench_su2_L100_D512.npz")
 
 
 @pytest.mark.skipif(not os.path.exists(HARNESS) or not os.path.exists(C2),
-                    reason="reference build (oracle/_ref) or the configuration-2 fixture not present")
-def test_config2_su2_L100_D512_eight_sweeps_from_reference_idmrg():
+                    reason="reference build (oracle/_ref) or the SU(2) L=100 D=512 fixture not present")
+def test_su2_L100_D512_eight_sweeps_from_reference_idmrg():
     import sadmrg
     z = np.load(C2)
     args = str(z["args"]).split()
